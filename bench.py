@@ -1,0 +1,515 @@
+"""Benchmark of the filtered hash group-by on B200.
+
+Workload (the 100M-row configuration): 100,000,000 rows; keys k1 = Int32
+Zipf(s=1.1) over 1,000,000 values and k2 = UInt32 codes of a 64-value
+dictionary; v Float64 ~ Normal(0, 1e3) with 5% random nulls; filter on a
+second Int32 column p uniform in [0, 100) < 50; aggregations sum, mean, min,
+max, count, var of v; groups in first-appearance order (maintain_order=True).
+Synthetic and seeded (seed 2 + rank).
+
+One step = one whole query (scan + finish, result columns on the device) over
+inputs already resident in HBM; `value` = rows all ranks processed per second,
+timed with CUDA events on the query's stream, max over ranks.  Inputs are
+2.01 GB per rank (> 126 MB L2), so no L2 flush is needed between steps.
+`e2e` = the same query through the C ABI with host buffers: every step
+registers the inputs from pinned host memory (host->device copies), runs the
+query and copies every result column back (device->host), timed by CUDA
+events on the library's stream.
+
+`--impl reference` times the CPU restatement of the reference's parallel
+aggregate table (oracle/, all host threads) on a bounded sample of the same
+workload; rank 0 only.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+ROWS = 100_000_000
+DISTINCT = 1_000_000
+ZIPF_S = 1.1
+CODES = 64
+BYTES_PER_ROW = 4 + 4 + 8 + 4 + 1 / 8  # k1, k2, v, p, v's validity bit
+METRIC = "group-by rows/s"
+WORKLOAD = (
+    "100M-row filtered group-by: keys (Int32 Zipf s=1.1 over 1M, UInt32 codes of 64), "
+    "v Float64 N(0,1e3) 5% nulls, filter p<50 (p Int32 uniform [0,100)), "
+    "aggs sum/mean/min/max/count/var, maintain_order=True"
+)
+FALLBACK_HBM_GBS = 6650.0
+
+
+def measured_hbm_gbs() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def generate(rows: int, seed: int, device: str):
+    """Seeded synthetic columns of the workload, generated on `device`."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    ranks = torch.arange(1, DISTINCT + 1, dtype=torch.float64, device=device)
+    cdf = torch.cumsum(ranks.pow(-ZIPF_S), 0)
+    cdf /= cdf[-1].clone()
+    perm = torch.randperm(DISTINCT, generator=g, device=device).to(torch.int32)
+    out = {}
+    chunk = 1 << 24
+    k1 = torch.empty(rows, dtype=torch.int32, device=device)
+    for s in range(0, rows, chunk):
+        e = min(rows, s + chunk)
+        u = torch.rand(e - s, generator=g, dtype=torch.float64, device=device)
+        r = torch.searchsorted(cdf, u, right=True).clamp_(max=DISTINCT - 1)
+        k1[s:e] = perm[r]
+    out["k1"] = k1
+    out["k2"] = torch.randint(0, CODES, (rows,), generator=g, device=device, dtype=torch.int64).to(torch.int32)
+    out["v"] = torch.randn(rows, generator=g, dtype=torch.float64, device=device) * 1e3
+    out["v_valid"] = torch.rand(rows, generator=g, device=device) >= 0.05
+    out["p"] = torch.randint(0, 100, (rows,), generator=g, device=device, dtype=torch.int64).to(torch.int32)
+    return out
+
+
+def pack_bits_torch(valid):
+    """LSB-first packed validity bytes of a bool tensor (on its device)."""
+    import torch
+
+    n = valid.numel()
+    pad = (-n) % 8
+    v = torch.cat([valid, torch.zeros(pad, dtype=torch.bool, device=valid.device)]) if pad else valid
+    w = (v.view(-1, 8).to(torch.uint8) << torch.arange(8, device=valid.device, dtype=torch.uint8)).sum(1, dtype=torch.uint8)
+    return w
+
+
+def plan_for(frame_like):
+    from dataframe_mojo_b200.frame import col
+
+    return (
+        frame_like.lazy()
+        .filter(col("p") < 50)
+        .group_by(["k1", "k2"], maintain_order=True)
+        .agg(
+            [
+                col("v").sum().alias("sum"),
+                col("v").mean().alias("mean"),
+                col("v").min().alias("min"),
+                col("v").max().alias("max"),
+                col("v").count().alias("count"),
+                col("v").var().alias("var"),
+            ]
+        )
+    )
+
+
+class Clocks:
+    """nvidia-smi clock and throttle samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+        self.proc = None
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                [
+                    "nvidia-smi",
+                    f"--id={index}",
+                    "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                    "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                    "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                    "--format=csv,noheader,nounits",
+                    "-lms",
+                    "100",
+                ],
+                stdout=self.f,
+                stderr=subprocess.DEVNULL,
+            )
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {
+            "sm_mhz": float(np.median(sm)) if sm else None,
+            "sm_max_mhz": float(max(mx)) if mx else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def traffic_per_launch() -> float | None:
+    """DRAM bytes of one scan launch from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "scan_kernel_traffic.json"
+    try:
+        d = json.loads(p.read_text())
+        return float(d["dram_bytes_per_full_launch"])
+    except Exception:
+        return None
+
+
+def cpu_baseline(frame_np, sample_rows: int, threads: int) -> dict:
+    """The oracle's parallel restatement of the reference CPU aggregate table
+    on the first `sample_rows` rows, all host threads."""
+    from dataframe_mojo_b200.frame import DataFrame, Series
+    from oracle import binding
+
+    sub = DataFrame(
+        [
+            Series("k1", frame_np["k1"][:sample_rows]),
+            Series("k2", frame_np["k2"][:sample_rows]),
+            Series("v", frame_np["v"][:sample_rows], frame_np["v_valid"][:sample_rows]),
+            Series("p", frame_np["p"][:sample_rows]),
+        ]
+    )
+    plan = plan_for(sub)
+    binding.run(plan, threads=threads)  # warm caches
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        binding.run(plan, threads=threads)
+        times.append(time.perf_counter() - t0)
+    t = float(np.median(times))
+    return {
+        "value": sample_rows / t,
+        "unit": "rows/s",
+        "cores": threads,
+        "kind": "port",
+        "sample": f"first {sample_rows:,} rows of the workload, median of 3 runs, {t:.3f} s each",
+    }
+
+
+def host_numpy(cols):
+    return {
+        "k1": cols["k1"].cpu().numpy(),
+        "k2": cols["k2"].cpu().numpy().view(np.uint32),
+        "v": cols["v"].cpu().numpy(),
+        "v_valid": cols["v_valid"].cpu().numpy(),
+        "p": cols["p"].cpu().numpy(),
+    }
+
+
+def run_reference(args, rank: int, world: int) -> int:
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    rows = args.sample_rows
+    import torch
+
+    cols = generate(rows, 2, "cpu")
+    frame_np = {
+        "k1": cols["k1"].numpy(),
+        "k2": cols["k2"].numpy().view(np.uint32),
+        "v": cols["v"].numpy(),
+        "v_valid": cols["v_valid"].numpy(),
+        "p": cols["p"].numpy(),
+    }
+    from dataframe_mojo_b200.frame import DataFrame, Series
+    from oracle import binding
+
+    sub = DataFrame(
+        [Series("k1", frame_np["k1"]), Series("k2", frame_np["k2"]), Series("v", frame_np["v"], frame_np["v_valid"]),
+         Series("p", frame_np["p"])]
+    )
+    plan = plan_for(sub)
+    for _ in range(args.warmup):
+        binding.run(plan, threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        binding.run(plan, threads=threads)
+    dt = time.perf_counter() - t0
+    value = rows * args.steps / dt
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "rows/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded generator, seed 2)",
+        "config": {"workload": WORKLOAD, "rows_per_step": rows, "full_rows": ROWS},
+        "cpu_baseline": {
+            "value": value,
+            "unit": "rows/s",
+            "cores": threads,
+            "kind": "port",
+            "sample": f"{rows:,} rows of the workload per step (the full 100M-row query does not fit a few-minute run)",
+        },
+        "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="dfcuda")
+    ap.add_argument("--rows", type=int, default=ROWS)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--sample-rows", type=int, default=10_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("at least 3 warm-up steps")
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device(f"cuda:{local}"))
+
+    from dataframe_mojo_b200 import provider
+    from dataframe_mojo_b200.frame import Bound, bind
+
+    device = local
+    rows = args.rows
+    cols = generate(rows, 2 + rank, f"cuda:{local}")
+    vbits = pack_bits_torch(cols["v_valid"])
+    torch.cuda.synchronize()
+
+    # Device-resident inputs (registered as borrowed device columns; the
+    # validity bitmap is normalised into the library's own buffer).
+    lib = provider.N.lib()
+    import ctypes as C
+
+    handles = {}
+    for name in ("k1", "k2", "v", "p"):
+        h = C.c_void_p()
+        t = cols[name]
+        dt = {"k1": provider.N.INT32, "k2": provider.N.UINT32, "v": provider.N.FLOAT64, "p": provider.N.INT32}[name]
+        validity = vbits.data_ptr() if name == "v" else None
+        st = lib.dfc_column_register(device, dt, rows, t.data_ptr(), validity, 0, provider.N.COLUMN_DEVICE, C.byref(h))
+        provider._check(st)
+        handles[name] = h
+
+    class _Shape:
+        """Plan builder over the workload's schema (values never read)."""
+
+        def lazy(self):
+            from dataframe_mojo_b200.frame import DataFrame, LazyFrame, Series
+
+            df = DataFrame(
+                [
+                    Series("k1", np.zeros(1, np.int32)),
+                    Series("k2", np.zeros(1, np.uint32)),
+                    Series("v", np.zeros(1, np.float64)),
+                    Series("p", np.zeros(1, np.int32)),
+                ]
+            )
+            return df.lazy()
+
+    bound = bind(plan_for(_Shape()).plan)
+    stream = torch.cuda.Stream()
+    col_list = [type("H", (), {"handle": handles[n]})() for n in bound.names]
+
+    def step():
+        res = provider.run_bound(bound, col_list, stream=stream.cuda_stream)
+        return res
+
+    for _ in range(args.warmup):
+        r = step()
+        groups = r.rows
+        r.free()
+    torch.cuda.synchronize()
+
+    clocks = Clocks(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    scan_ns = []
+    launches = 0
+    results = []
+    start.record(stream)
+    for _ in range(args.steps):
+        r = step()
+        t = provider.last_timings()
+        scan_ns.append(t["scan_ns"])
+        launches += t["launches"]
+        results.append(r)
+    end.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = start.elapsed_time(end) / args.steps
+    for r in results:
+        r.free()
+    ms_t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = rows * world / (ms_max * 1e-3)
+
+    # Roofline of the scan kernel: algorithmic bytes / its event-timed duration.
+    peak, peak_kind = measured_hbm_gbs()
+    scan_s = float(np.mean(scan_ns)) * 1e-9
+    algo_bytes = rows * BYTES_PER_ROW
+    achieved = algo_bytes / scan_s / 1e9
+    roofline = {
+        "bound": "hbm",
+        "kernel": "scan_kernel",
+        "achieved": achieved,
+        "peak": peak,
+        "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+        "unit": "GB/s",
+        "frac": achieved / peak,
+        "traffic": traffic_per_launch(),
+        "algorithmic_bytes": algo_bytes,
+        "scan_ms": scan_s * 1e3,
+    }
+
+    # End to end through the C ABI with host buffers (pinned).
+    host = {n: cols[n].cpu().pin_memory() for n in ("k1", "k2", "v", "p")}
+    host_bits = vbits.cpu().pin_memory()
+    torch.cuda.synchronize()
+    e2e_stream = torch.cuda.Stream()
+    provider.set_thread_stream(device, e2e_stream.cuda_stream)
+    dtypes = {"k1": np.int32, "k2": np.uint32, "v": np.float64, "p": np.int32}
+    h2d = sum(host[n].numel() * host[n].element_size() for n in host) + host_bits.numel()
+
+    def e2e_step():
+        dcols = {}
+        for n in ("k1", "k2", "v", "p"):
+            dcols[n] = provider.DeviceColumn.from_host_pointer(
+                n, dtypes[n], rows, host[n].data_ptr(), host_bits.data_ptr() if n == "v" else None, 0, device
+            )
+        res = provider.run_bound(bound, [dcols[n] for n in bound.names])
+        frame = res.to_frame()
+        out_bytes = sum(frame.column(c).values.nbytes + (len(frame.column(c)) + 7) // 8 for c in frame.columns)
+        res.free()
+        for c in dcols.values():
+            c.release()
+        return out_bytes
+
+    for _ in range(1):
+        e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(e2e_stream)
+    d2h = 0
+    for _ in range(args.e2e_steps):
+        d2h = e2e_step()
+    e1.record(e2e_stream)
+    torch.cuda.synchronize()
+    provider.set_thread_stream(device, None)
+    e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+    et = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+    e2e = {
+        "value": rows * world / (float(et.item()) * 1e-3),
+        "unit": "rows/s",
+        "h2d_bytes_per_step": int(h2d),
+        "d2h_bytes_per_step": int(d2h),
+        "steps": args.e2e_steps,
+        "ms_per_step": float(et.item()),
+    }
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        sample = min(args.sample_rows, rows)
+        frame_np = {
+            "k1": cols["k1"][:sample].cpu().numpy(),
+            "k2": cols["k2"][:sample].cpu().numpy().view(np.uint32),
+            "v": cols["v"][:sample].cpu().numpy(),
+            "v_valid": cols["v_valid"][:sample].cpu().numpy(),
+            "p": cols["p"][:sample].cpu().numpy(),
+        }
+        cpu = cpu_baseline(frame_np, sample, os.cpu_count() or 1)
+
+    for h in handles.values():
+        lib.dfc_column_release(h)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "rows/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_max,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded torch generator, seed 2 + rank)",
+            "config": {
+                "workload": WORKLOAD,
+                "rows_per_gpu": rows,
+                "groups": int(groups),
+                "parallelism": f"replicas x{world} (independent row partitions, no collective)",
+                "l2": "inputs 2.01 GB per GPU > 126 MB L2 (no flush needed)",
+            },
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,167 @@
+"""ctypes binding of libdfcuda.so (include/dfcuda.h).
+
+The library is loaded from this package directory only; when it is missing the
+import of any provider entry point that needs it raises.  There is no CPU
+fallback anywhere in the provider.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libdfcuda.so"
+
+ABI_VERSION = 1
+
+# dfc_status
+OK, UNSUPPORTED, INVALID, DATA_OVERFLOW, DATA_FAULT, CAPACITY, OOM, TIMEOUT, DEVICE, NO_DEVICE = range(10)
+
+# dfc_dtype
+INT8, INT16, INT32, INT64, UINT8, UINT16, UINT32, UINT64, FLOAT32, FLOAT64 = range(1, 11)
+
+# predicate kinds / comparisons
+PRED_CMP, PRED_IS_NULL, PRED_IS_NOT_NULL, PRED_AND, PRED_OR, PRED_NOT, PRED_TRUE = range(1, 8)
+LT, LE, GT, GE, EQ, NE = range(1, 7)
+
+# aggregations
+AGG_COUNT, AGG_SUM, AGG_MEAN, AGG_MIN, AGG_MAX, AGG_VAR, AGG_STD, AGG_LEN, AGG_NULL_COUNT = range(1, 10)
+
+# query flags
+Q_MAINTAIN_ORDER = 1
+Q_FORCE_GLOBAL = 2
+Q_FORCE_SHARED = 4
+Q_FLOAT32_FP64 = 8
+
+COLUMN_HOST = 0
+COLUMN_DEVICE = 1
+
+
+class Lit(C.Union):
+    _fields_ = [("i", C.c_int64), ("u", C.c_uint64), ("f", C.c_double)]
+
+
+class PredOp(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("column", C.c_int32),
+        ("cmp", C.c_int32),
+        ("reserved", C.c_int32),
+        ("lit", Lit),
+    ]
+
+
+class Agg(C.Structure):
+    _fields_ = [("op", C.c_int32), ("column", C.c_int32), ("ddof", C.c_int32), ("min_count", C.c_int32)]
+
+
+class Query(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_uint32),
+        ("flags", C.c_uint32),
+        ("n_inputs", C.c_int32),
+        ("n_keys", C.c_int32),
+        ("inputs", C.POINTER(C.c_void_p)),
+        ("keys", C.POINTER(C.c_int32)),
+        ("n_pred", C.c_int32),
+        ("n_aggs", C.c_int32),
+        ("pred", C.POINTER(PredOp)),
+        ("aggs", C.POINTER(Agg)),
+        ("stream", C.c_void_p),
+    ]
+
+
+class DeviceInfo(C.Structure):
+    _fields_ = [
+        ("ordinal", C.c_int32),
+        ("sm_count", C.c_int32),
+        ("cc_major", C.c_int32),
+        ("cc_minor", C.c_int32),
+        ("total_bytes", C.c_uint64),
+        ("budget_bytes", C.c_int64),
+        ("name", C.c_char * 96),
+    ]
+
+
+class Timings(C.Structure):
+    _fields_ = [
+        ("scan_ns", C.c_double),
+        ("finish_ns", C.c_double),
+        ("total_ns", C.c_double),
+        ("groups", C.c_uint64),
+        ("table_slots", C.c_uint64),
+        ("regime", C.c_int32),
+        ("retries", C.c_int32),
+        ("launches", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+# (name, restype, argtypes) of every entry point include/dfcuda.h declares.
+SIGNATURES = [
+    ("dfc_version", C.c_uint32, []),
+    ("dfc_installed", C.c_int32, []),
+    ("dfc_device_count", C.c_int32, []),
+    ("dfc_device_info_get", C.c_int, [C.c_int32, C.POINTER(DeviceInfo)]),
+    (
+        "dfc_column_register",
+        C.c_int,
+        [C.c_int32, C.c_int, C.c_uint64, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.POINTER(C.c_void_p)],
+    ),
+    ("dfc_column_release", C.c_int, [C.c_void_p]),
+    ("dfc_column_rows", C.c_uint64, [C.c_void_p]),
+    ("dfc_column_null_count", C.c_int32, [C.c_void_p]),
+    ("dfc_groupby", C.c_int, [C.POINTER(Query), C.POINTER(C.c_void_p)]),
+    ("dfc_result_rows", C.c_uint64, [C.c_void_p]),
+    ("dfc_result_columns", C.c_int32, [C.c_void_p]),
+    (
+        "dfc_result_column",
+        C.c_int,
+        [C.c_void_p, C.c_int32, C.POINTER(C.c_int), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)],
+    ),
+    ("dfc_result_copy_to_host", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    ("dfc_result_free", None, [C.c_void_p]),
+    ("dfc_result_residence", C.c_void_p, [C.c_void_p, C.c_int32]),
+    ("dfc_residence_to_host", C.c_int32, [C.c_void_p, C.c_void_p, C.c_int64]),
+    ("dfc_residence_release", None, [C.c_void_p]),
+    ("dfc_last_timings", C.c_int, [C.POINTER(Timings)]),
+    ("dfc_set_thread_stream", C.c_int, [C.c_int32, C.c_void_p]),
+    ("dfc_last_error", C.c_char_p, []),
+    ("dfc_status_name", C.c_char_p, [C.c_int]),
+]
+
+_lock = threading.Lock()
+_lib = None
+
+
+def library_present() -> bool:
+    return LIB_PATH.exists()
+
+
+def lib() -> C.CDLL:
+    """The loaded library; raises when it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not LIB_PATH.exists():
+                raise RuntimeError(
+                    f"{LIB_PATH} is missing: build it with `python -m dataframe_mojo_b200.build` "
+                    "(the provider has no CPU fallback)"
+                )
+            handle = C.CDLL(str(LIB_PATH), mode=os.RTLD_NOW | os.RTLD_LOCAL)
+            for name, res, args in SIGNATURES:
+                fn = getattr(handle, name)
+                fn.restype = res
+                fn.argtypes = args
+            if handle.dfc_version() != ABI_VERSION:
+                raise RuntimeError("libdfcuda.so ABI version mismatch")
+            _lib = handle
+    return _lib
+
+
+def last_error() -> str:
+    msg = lib().dfc_last_error()
+    return msg.decode() if msg else ""

@@ -1,0 +1,28 @@
+// kernels.h — kernel entry points and launch constants.
+#pragma once
+
+#include "dfc_internal.h"
+
+namespace dfc {
+
+constexpr int kScanConsumerWarps = 8;
+constexpr int kScanConsumerThreads = kScanConsumerWarps * 32;
+constexpr int kScanThreads = kScanConsumerThreads + 32;  // + one producer warp
+constexpr int kFinishThreads = 256;
+constexpr int kFinishChunk = 4096;  // bitmap words per prefix-scan block
+
+__global__ void scan_kernel(const __grid_constant__ ScanParams p);
+__global__ void finish_mark(const __grid_constant__ FinishParams f);
+__global__ void finish_chunk_sums(const __grid_constant__ FinishParams f);
+__global__ void finish_scan_chunks(const __grid_constant__ FinishParams f, uint32_t chunks);
+__global__ void finish_word_prefix(const __grid_constant__ FinishParams f);
+__global__ void finish_rank(const __grid_constant__ FinishParams f);
+__global__ void finish_output(const __grid_constant__ FinishParams f);
+
+}  // namespace dfc
+
+namespace dfc {
+__global__ void normalize_validity(const uint8_t* src, uint64_t nbytes, uint64_t off, uint64_t rows, uint32_t* dst,
+                                   unsigned long long* valid_rows);
+__global__ void column_minmax(DevColumn c, uint64_t rows, unsigned long long* out);
+}  // namespace dfc

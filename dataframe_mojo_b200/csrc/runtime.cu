@@ -1,0 +1,1043 @@
+// runtime.cu — host side of libdfcuda.so: the C ABI of include/dfcuda.h, the
+// resident-column registry, the query planner (key packing, group-record
+// layout, shared-memory stage layout, table capacity), launches, bounded
+// waits, capacity regrowth and results.
+//
+// Behaviour mirrors the reference provider contract
+// (docs/design/accelerator-contract.md): unsupported work is rejected before
+// anything is submitted; errors after submission propagate; checked sums
+// report the CPU's exact overflow text; nothing is retried on the CPU.
+#include <cuda_runtime.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/dfcuda.h"
+#include "dfc_internal.h"
+#include "kernels.h"
+
+using namespace dfc;
+
+struct dfc_column {
+  int32_t device = 0;
+  dfc_dtype dtype = DFC_INT64;
+  uint64_t rows = 0;
+  void* values = nullptr;        // device
+  bool owns_values = false;
+  uint32_t* validity = nullptr;  // device, normalised; nullptr when no row is null
+  uint64_t null_count = 0;
+  uint64_t min_enc = ~0ull, max_enc = 0;  // order-encoded value range (integers)
+  bool have_range = false;
+};
+
+struct ResultCol {
+  dfc_dtype dtype;
+  void* values = nullptr;
+  uint32_t* validity = nullptr;
+  bool has_nulls = false;
+};
+
+struct dfc_result {
+  int32_t device = 0;
+  uint64_t rows = 0;
+  std::vector<ResultCol> cols;
+  std::atomic<int> refs{1};
+};
+
+namespace {
+
+thread_local std::string t_error;
+thread_local dfc_timings t_timings{};
+
+dfc_status fail(dfc_status st, const std::string& msg) {
+  t_error = msg;
+  return st;
+}
+
+dfc_status cuda_fail(cudaError_t e, const char* what) {
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    return fail(DFC_OOM, std::string("device memory exhausted: ") + what);
+  }
+  return fail(DFC_DEVICE, std::string("CUDA error ") + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ") in " +
+                              what);
+}
+
+#define CK(call, what)                                   \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what);   \
+  } while (0)
+
+int dtype_size(int dt) {
+  switch (dt) {
+    case DFC_INT8: case DFC_UINT8: return 1;
+    case DFC_INT16: case DFC_UINT16: return 2;
+    case DFC_INT32: case DFC_UINT32: case DFC_FLOAT32: return 4;
+    case DFC_INT64: case DFC_UINT64: case DFC_FLOAT64: return 8;
+  }
+  return 0;
+}
+bool is_float(int dt) { return dt == DFC_FLOAT32 || dt == DFC_FLOAT64; }
+bool is_unsigned(int dt) { return dt == DFC_UINT8 || dt == DFC_UINT16 || dt == DFC_UINT32 || dt == DFC_UINT64; }
+const char* dtype_name(int dt) {
+  switch (dt) {
+    case DFC_INT8: return "int8";
+    case DFC_INT16: return "int16";
+    case DFC_INT32: return "int32";
+    case DFC_INT64: return "int64";
+    case DFC_UINT8: return "uint8";
+    case DFC_UINT16: return "uint16";
+    case DFC_UINT32: return "uint32";
+    case DFC_UINT64: return "uint64";
+    case DFC_FLOAT32: return "float32";
+    case DFC_FLOAT64: return "float64";
+  }
+  return "?";
+}
+
+// Result type of a sum (dataframe/dtype.mojo:838-849).
+int sum_dtype(int dt) {
+  if (dt == DFC_INT8 || dt == DFC_INT16 || dt == DFC_UINT8 || dt == DFC_UINT16) return DFC_INT64;
+  return dt;
+}
+
+// Overflow text of the CPU provider (function.mojo:2798 for Int64 inputs,
+// :2914 / reducer.mojo:3412 for the others).
+std::string overflow_message(int input_dtype) {
+  if (input_dtype == DFC_INT64) return "Int64 expression sum overflow";
+  return std::string(dtype_name(sum_dtype(input_dtype))) + " expression sum overflow";
+}
+
+struct DeviceState {
+  bool ready = false;
+  int sms = 0;
+  size_t smem_optin = 0;
+  int scan_occupancy = 1;
+};
+std::mutex g_dev_mu;
+std::map<int, DeviceState> g_dev;
+
+// Group counts seen per key-column set: the next query on the same keys sizes
+// its table from them (the reference sizes from column statistics,
+// dataframe/aggregation/hash_table.mojo:699-714).
+std::mutex g_learn_mu;
+std::map<std::vector<const void*>, uint64_t> g_learned;
+
+dfc_status device_ready(int dev, DeviceState** out) {
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  DeviceState& d = g_dev[dev];
+  if (!d.ready) {
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
+    if (prop.major < 10) return fail(DFC_NO_DEVICE, "device is not sm_100 class");
+    CK(cudaSetDevice(dev), "cudaSetDevice");
+    d.sms = prop.multiProcessorCount;
+    d.smem_optin = prop.sharedMemPerBlockOptin;
+    // Keep freed pool memory cached: queries reuse it without returning to the OS.
+    cudaMemPool_t pool;
+    CK(cudaDeviceGetDefaultMemPool(&pool, dev), "cudaDeviceGetDefaultMemPool");
+    uint64_t threshold = UINT64_MAX;
+    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold), "cudaMemPoolSetAttribute");
+    CK(cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin - 1024),
+       "cudaFuncSetAttribute");
+    d.ready = true;
+  }
+  *out = &d;
+  return DFC_OK;
+}
+
+// One non-blocking stream per thread and device, for calls without a stream
+// (or the stream the thread chose with dfc_set_thread_stream).
+thread_local std::map<int, cudaStream_t> t_streams;
+thread_local std::map<int, cudaStream_t> t_chosen;
+
+cudaStream_t thread_stream(int dev) {
+  auto c = t_chosen.find(dev);
+  if (c != t_chosen.end()) return c->second;
+  auto it = t_streams.find(dev);
+  if (it != t_streams.end()) return it->second;
+  cudaStream_t s = nullptr;
+  cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  t_streams[dev] = s;
+  return s;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+double wait_limit_seconds() {
+  const char* s = getenv("DFC_WAIT_TIMEOUT_S");
+  if (s) {
+    double v = atof(s);
+    if (v > 0) return v;
+  }
+  return 300.0;
+}
+
+// Host-side bounded wait on the stream's work (cudaEventQuery polling).
+dfc_status wait_bounded(cudaStream_t stream) {
+  cudaEvent_t ev;
+  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+  cudaError_t e = cudaEventRecord(ev, stream);
+  if (e != cudaSuccess) {
+    cudaEventDestroy(ev);
+    return cuda_fail(e, "cudaEventRecord");
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  const double limit = wait_limit_seconds();
+  int spins = 0;
+  while (true) {
+    e = cudaEventQuery(ev);
+    if (e == cudaSuccess) break;
+    if (e != cudaErrorNotReady) {
+      cudaEventDestroy(ev);
+      return cuda_fail(e, "query execution");
+    }
+    if (++spins > 64) std::this_thread::sleep_for(std::chrono::microseconds(20));
+    if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > limit) {
+      cudaEventDestroy(ev);
+      return fail(DFC_TIMEOUT, "device work did not finish within the wait limit");
+    }
+  }
+  cudaEventDestroy(ev);
+  return DFC_OK;
+}
+
+uint64_t next_pow2(uint64_t x) {
+  uint64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+// Host decoding of the order encoding (kernels' order_encode) for integer ranges.
+__int128 order_value(uint64_t e, int dt) {
+  if (is_unsigned(dt)) return (__int128)e;
+  return (__int128)(int64_t)(e ^ 0x8000000000000000ull);
+}
+
+// ---------------------------------------------------------------------------
+// Planning.
+// ---------------------------------------------------------------------------
+struct Plan {
+  ScanParams sp{};
+  FinishParams fp{};
+  int n_out = 0;
+  int out_dtype[kMaxOut];
+  int out_agg_input_dtype[kMaxOut];  // for overflow messages, by aggregation index
+  int tile_rows = 1024;
+  size_t smem = 0;
+  int device = 0;
+  uint64_t rows = 0;
+  uint64_t est_groups = 0;
+  std::vector<const void*> key_sig;
+};
+
+dfc_status plan_query(const dfc_query* q, Plan& P) {
+  if (!q) return fail(DFC_INVALID, "null query");
+  if (q->abi_version != DFC_ABI_VERSION) return fail(DFC_INVALID, "ABI version mismatch");
+  if (q->n_inputs < 1 || q->n_inputs > kMaxInputs || !q->inputs)
+    return fail(DFC_UNSUPPORTED, "between 1 and 16 input columns are supported");
+  if (q->n_keys < 1 || q->n_keys > kMaxKeys || !q->keys) return fail(DFC_UNSUPPORTED, "between 1 and 4 keys are supported");
+  if (q->n_aggs < 0 || q->n_aggs > kMaxAggs || (q->n_aggs > 0 && !q->aggs))
+    return fail(DFC_UNSUPPORTED, "at most 32 aggregations are supported");
+  if (q->n_pred < 0 || q->n_pred > kMaxPred || (q->n_pred > 0 && !q->pred))
+    return fail(DFC_UNSUPPORTED, "filter programs of at most 32 operations are supported");
+  for (int i = 0; i < q->n_inputs; ++i)
+    if (!q->inputs[i]) return fail(DFC_INVALID, "null input column");
+  const dfc_column* c0 = q->inputs[0];
+  P.device = c0->device;
+  P.rows = c0->rows;
+  for (int i = 1; i < q->n_inputs; ++i) {
+    if (q->inputs[i]->rows != P.rows) return fail(DFC_INVALID, "input columns differ in length");
+    if (q->inputs[i]->device != P.device) return fail(DFC_UNSUPPORTED, "input columns live on different devices");
+  }
+  if (P.rows >= 0xFFFFFFFFull) return fail(DFC_UNSUPPORTED, "at most 2^32-2 rows per query");
+
+  ScanParams& sp = P.sp;
+  // Slots: the columns the query touches, staged per tile.
+  int slot_of[kMaxInputs];
+  for (int i = 0; i < kMaxInputs; ++i) slot_of[i] = -1;
+  int n_slots = 0;
+  auto use = [&](int input) -> int {
+    if (slot_of[input] < 0) {
+      slot_of[input] = n_slots;
+      const dfc_column* c = q->inputs[input];
+      DevColumn& dc = sp.cols[n_slots];
+      dc.values = c->values;
+      dc.validity = c->validity;
+      dc.dtype = c->dtype;
+      dc.size = dtype_size(c->dtype);
+      ++n_slots;
+    }
+    return slot_of[input];
+  };
+
+  // Keys.
+  int total_bits = 0;
+  sp.n_keys = q->n_keys;
+  for (int k = 0; k < q->n_keys; ++k) {
+    int in = q->keys[k];
+    if (in < 0 || in >= q->n_inputs) return fail(DFC_INVALID, "key index out of range");
+    for (int j = 0; j < k; ++j)
+      if (q->keys[j] == in) return fail(DFC_INVALID, "duplicate key column");
+    const dfc_column* c = q->inputs[in];
+    KeyField& f = sp.keys[k];
+    f.input = use(in);
+    f.dtype = c->dtype;
+    f.bits = 8 * dtype_size(c->dtype);
+    total_bits += f.bits + (c->validity ? 1 : 0);
+    P.key_sig.push_back(c);
+  }
+  if (total_bits <= 64) {
+    sp.key_mode = KEY_PACKED;
+    int at = 0;
+    for (int k = 0; k < q->n_keys; ++k) {
+      KeyField& f = sp.keys[k];
+      f.shift = at;
+      at += f.bits;
+      f.null_bit = -1;
+      if (q->inputs[q->keys[k]]->validity) f.null_bit = at++;
+    }
+  } else {
+    sp.key_mode = KEY_TICKET;
+    for (int k = 0; k < q->n_keys; ++k) {
+      sp.keys[k].shift = 0;
+      sp.keys[k].null_bit = -1;
+    }
+  }
+
+  // Filter program (stack discipline checked here, before submission).
+  sp.n_pred = q->n_pred;
+  int depth = 0;
+  for (int i = 0; i < q->n_pred; ++i) {
+    const dfc_pred_op& op = q->pred[i];
+    PredOp& d = sp.pred[i];
+    d.kind = op.kind;
+    d.cmp = op.cmp;
+    d.lit.u = op.lit.u;
+    d.input = 0;
+    switch (op.kind) {
+      case DFC_PRED_CMP:
+        if (op.cmp < DFC_LT || op.cmp > DFC_NE) return fail(DFC_INVALID, "bad comparison operator");
+        /* fallthrough */
+      case DFC_PRED_IS_NULL:
+      case DFC_PRED_IS_NOT_NULL:
+        if (op.column < 0 || op.column >= q->n_inputs) return fail(DFC_INVALID, "filter column out of range");
+        d.input = use(op.column);
+        ++depth;
+        break;
+      case DFC_PRED_TRUE:
+        ++depth;
+        break;
+      case DFC_PRED_NOT:
+        if (depth < 1) return fail(DFC_INVALID, "malformed filter program");
+        break;
+      case DFC_PRED_AND:
+      case DFC_PRED_OR:
+        if (depth < 2) return fail(DFC_INVALID, "malformed filter program");
+        --depth;
+        break;
+      default:
+        return fail(DFC_UNSUPPORTED, "unsupported filter operation");
+    }
+    if (depth > 32) return fail(DFC_UNSUPPORTED, "filter program too deep");
+  }
+  if (q->n_pred > 0 && depth != 1) return fail(DFC_INVALID, "malformed filter program");
+
+  // Value states: one ValField per distinct aggregated column.
+  struct Need {
+    int input;
+    bool sum = false, mn = false, mx = false, m2 = false;
+  };
+  std::vector<Need> needs;
+  int val_of_agg[kMaxAggs];
+  bool track_len = false;
+  for (int a = 0; a < q->n_aggs; ++a) {
+    const dfc_agg& ag = q->aggs[a];
+    if (ag.column < 0 || ag.column >= q->n_inputs) return fail(DFC_INVALID, "aggregation column out of range");
+    if (ag.op < DFC_AGG_COUNT || ag.op > DFC_AGG_NULL_COUNT) return fail(DFC_UNSUPPORTED, "unsupported aggregation");
+    if ((ag.op == DFC_AGG_VAR || ag.op == DFC_AGG_STD) && ag.ddof < 0) return fail(DFC_INVALID, "negative ddof");
+    int v = -1;
+    for (size_t j = 0; j < needs.size(); ++j)
+      if (needs[j].input == ag.column) v = (int)j;
+    if (v < 0) {
+      if (needs.size() >= (size_t)kMaxVals) return fail(DFC_UNSUPPORTED, "at most 8 aggregated columns");
+      v = (int)needs.size();
+      needs.push_back(Need{ag.column});
+    }
+    val_of_agg[a] = v;
+    Need& n = needs[v];
+    switch (ag.op) {
+      case DFC_AGG_SUM: case DFC_AGG_MEAN: n.sum = true; break;
+      case DFC_AGG_MIN: n.mn = true; break;
+      case DFC_AGG_MAX: n.mx = true; break;
+      case DFC_AGG_VAR: case DFC_AGG_STD: n.m2 = true; n.sum = true; break;
+      case DFC_AGG_LEN: case DFC_AGG_NULL_COUNT: track_len = true; break;
+      default: break;
+    }
+  }
+  sp.n_vals = (int)needs.size();
+  int off = kRecHeader;
+  for (int j = 0; j < sp.n_vals; ++j) {  // counts first (u32 each)
+    ValField& f = sp.vals[j];
+    f.input = use(needs[j].input);
+    f.dtype = q->inputs[needs[j].input]->dtype;
+    f.off_count = off;
+    off += 4;
+  }
+  off = (off + 7) & ~7;
+  for (int j = 0; j < sp.n_vals; ++j) {
+    ValField& f = sp.vals[j];
+    const Need& n = needs[j];
+    const int sz = dtype_size(f.dtype);
+    f.nan_bit = j;
+    f.sum_kind = SUM_NONE;
+    f.off_sum = f.off_min = f.off_max = f.off_zero = f.off_m2 = f.off_shift = -1;
+    if (n.sum) {
+      if (is_float(f.dtype)) f.sum_kind = SUM_F64;
+      else if (sz <= 2 || (sz == 4 && P.rows < (1ull << 31))) f.sum_kind = SUM_I64;
+      else f.sum_kind = SUM_I128;
+      off = (f.sum_kind == SUM_I128) ? ((off + 15) & ~15) : off;
+      f.off_sum = off;
+      off += f.sum_kind == SUM_I128 ? 16 : 8;
+    }
+    if (n.mn) { f.off_min = off; off += 8; }
+    if (n.mx) { f.off_max = off; off += 8; }
+    if ((n.mn || n.mx) && is_float(f.dtype)) { f.off_zero = off; off += 8; }
+    if (n.m2) {
+      f.off_m2 = off; off += 8;
+      f.off_shift = off; off += 8;
+    }
+  }
+  sp.rec_stride = (off + 15) & ~15;
+  if (sp.rec_stride > kMaxRecWords * 8) return fail(DFC_UNSUPPORTED, "group record too wide");
+  sp.rec_words = sp.rec_stride / 8;
+  sp.track_first = 1;  // groups are always emitted in first-row order
+  sp.track_len = track_len ? 1 : 0;
+  // Identity record.
+  std::vector<uint8_t> tpl(sp.rec_stride, 0);
+  auto put64 = [&](int o, uint64_t v) { memcpy(tpl.data() + o, &v, 8); };
+  auto put32 = [&](int o, uint32_t v) { memcpy(tpl.data() + o, &v, 4); };
+  put32(kRecFirst, kNoRow);
+  for (int j = 0; j < sp.n_vals; ++j) {
+    const ValField& f = sp.vals[j];
+    if (f.off_min >= 0) put64(f.off_min, ~0ull);
+    if (f.off_max >= 0) put64(f.off_max, 0ull);
+    if (f.off_zero >= 0) put64(f.off_zero, ~0ull);
+    if (f.off_shift >= 0) put64(f.off_shift, kShiftUnset);
+  }
+  memcpy(sp.rec_template, tpl.data(), sp.rec_stride);
+
+  // Output columns: keys, then one per aggregation.
+  FinishParams& fp = P.fp;
+  int n_out = 0;
+  for (int k = 0; k < q->n_keys; ++k) {
+    OutCol& oc = fp.out[n_out];
+    oc.kind = OUT_KEY;
+    oc.index = k;
+    oc.dtype = q->inputs[q->keys[k]]->dtype;
+    P.out_dtype[n_out++] = oc.dtype;
+  }
+  for (int a = 0; a < q->n_aggs; ++a) {
+    const dfc_agg& ag = q->aggs[a];
+    const int idt = q->inputs[ag.column]->dtype;
+    OutCol& oc = fp.out[n_out];
+    oc.kind = OUT_AGG;
+    oc.index = a;
+    oc.val = val_of_agg[a];
+    oc.op = ag.op;
+    oc.ddof = ag.ddof;
+    oc.min_count = ag.min_count;
+    switch (ag.op) {
+      case DFC_AGG_COUNT: case DFC_AGG_LEN: case DFC_AGG_NULL_COUNT: oc.dtype = DFC_INT64; break;
+      case DFC_AGG_SUM: oc.dtype = sum_dtype(idt); break;
+      case DFC_AGG_MIN: case DFC_AGG_MAX: oc.dtype = idt; break;
+      default: oc.dtype = DFC_FLOAT64; break;
+    }
+    P.out_agg_input_dtype[a] = idt;
+    P.out_dtype[n_out++] = oc.dtype;
+  }
+  fp.n_out = n_out;
+  P.n_out = n_out;
+
+  // Stage layout: the largest tile whose ring of >= 3 stages fits.
+  sp.n_stage = n_slots;
+  sp.n_cols = n_slots;
+  sp.rows = P.rows;
+  bool aligned = true;
+  for (int c = 0; c < n_slots; ++c)
+    if (((uintptr_t)sp.cols[c].values & 15u) != 0) aligned = false;
+  int tile = 1024;
+  size_t stage_bytes = 0, stage_tx = 0;
+  for (; tile >= 128; tile >>= 1) {
+    // tile >= 128: every values block (tile * size) and validity block
+    // (tile / 8) is a multiple of 16 bytes, as bulk copies require.
+    size_t b = 0;
+    for (int c = 0; c < n_slots; ++c) {
+      sp.stage_off[c] = (int)b;
+      b += (size_t)tile * sp.cols[c].size;
+      if (sp.cols[c].validity) {
+        sp.stage_voff[c] = (int)b;
+        b += (size_t)tile / 8;
+      } else {
+        sp.stage_voff[c] = -1;
+      }
+    }
+    stage_tx = b;
+    b = (b + 127) & ~(size_t)127;
+    stage_bytes = b;
+    if (b * 4 <= 96 * 1024) break;
+  }
+  if (tile < 128) return fail(DFC_UNSUPPORTED, "too many input columns for the stage ring");
+  sp.tile_rows = tile;
+  sp.stage_bytes = (int)stage_bytes;
+  sp.stage_tx = (int)stage_tx;
+  sp.stages = 4;
+  sp.use_tma = aligned ? 1 : 0;
+  sp.tiles = (P.rows + tile - 1) / tile;
+  sp.full_tiles = P.rows / tile;
+  P.tile_rows = tile;
+  P.smem = (size_t)sp.stages * stage_bytes + 2 * sp.stages * sizeof(uint64_t);
+  return DFC_OK;
+}
+
+// Estimated number of groups: what the last query on these keys found, else
+// the product of the key columns' value ranges, capped by the row count.
+uint64_t estimate_groups(const dfc_query* q, const Plan& P) {
+  {
+    std::lock_guard<std::mutex> lk(g_learn_mu);
+    auto it = g_learned.find(P.key_sig);
+    if (it != g_learned.end()) return it->second;
+  }
+  double prod = 1.0;
+  for (int k = 0; k < q->n_keys; ++k) {
+    const dfc_column* c = q->inputs[q->keys[k]];
+    double d = (double)c->rows;
+    if (c->have_range && !is_float(c->dtype)) {
+      __int128 span = order_value(c->max_enc, c->dtype) - order_value(c->min_enc, c->dtype) + 1;
+      if (span > 0 && (double)span < d) d = (double)span;
+    }
+    if (c->validity) d += 1;
+    prod *= d;
+  }
+  double est = std::min(prod, (double)P.rows);
+  return (uint64_t)std::max(1.0, est);
+}
+
+void learn_groups(const Plan& P, uint64_t groups) {
+  std::lock_guard<std::mutex> lk(g_learn_mu);
+  g_learned[P.key_sig] = groups;
+}
+
+struct Scratch {
+  cudaStream_t stream = nullptr;
+  std::vector<void*> ptrs;
+  dfc_status alloc(void** p, size_t bytes, const char* what) {
+    cudaError_t e = cudaMallocAsync(p, std::max<size_t>(bytes, 256), stream);
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    ptrs.push_back(*p);
+    return DFC_OK;
+  }
+  void release() {
+    for (void* p : ptrs) cudaFreeAsync(p, stream);
+    ptrs.clear();
+  }
+};
+
+// Control block copied back after every attempt.
+struct Control {
+  uint32_t status[4];
+  uint32_t groups;
+  uint32_t overflow_agg;
+  uint32_t alloc;
+  uint32_t pad;
+  uint32_t has_nulls[kMaxOut];
+};
+
+dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_t stream, uint64_t slots,
+                       dfc_result** out, bool* grow, Control* host_ctl) {
+  *grow = false;
+  ScanParams& sp = P.sp;
+  FinishParams& fp = P.fp;
+  Scratch S;
+  S.stream = stream;
+
+  int occ = 1;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_kernel, kScanThreads, P.smem), "occupancy");
+  occ = std::max(1, occ);
+  uint64_t ncta = (uint64_t)ds->sms * (uint64_t)occ;
+  ncta = std::max<uint64_t>(1, std::min<uint64_t>(ncta, std::max<uint64_t>(1, sp.tiles)));
+  // Records: the groups the table may hold (load factor <= 1/2) plus every
+  // CTA's partly used last chunk.
+  const uint64_t groups_cap = std::min<uint64_t>(P.rows, slots / 2);
+  uint64_t chunk = 64;
+  while (chunk < 1024 && chunk * ncta * 8 < groups_cap) chunk <<= 1;
+  const uint64_t recs = groups_cap + chunk * ncta;
+  if (recs >= 0xFFFFFFFFull) return fail(DFC_CAPACITY, "group capacity exceeds 2^32 records");
+
+  void *table, *records, *ctl, *bits, *prefix, *bsums, *perm;
+  const uint64_t words = (P.rows + 31) / 32;
+  const uint64_t chunks = std::max<uint64_t>(1, (words + kFinishChunk - 1) / kFinishChunk);
+  dfc_status st;
+  if ((st = S.alloc(&table, (slots + 1) * sizeof(KeyEntry), "key table"))) return S.release(), st;
+  if ((st = S.alloc(&records, recs * sp.rec_stride, "group records"))) return S.release(), st;
+  if ((st = S.alloc(&ctl, sizeof(Control), "control block"))) return S.release(), st;
+  if ((st = S.alloc(&bits, words * 4 + 16, "order bitmap"))) return S.release(), st;
+  if ((st = S.alloc(&prefix, words * 4 + 16, "order prefix"))) return S.release(), st;
+  if ((st = S.alloc(&bsums, chunks * 4, "prefix chunks"))) return S.release(), st;
+  if ((st = S.alloc(&perm, recs * 4, "group permutation"))) return S.release(), st;
+  // Output columns sized for the group capacity (the group count is known
+  // only on the device; the host reads it once, at the end).
+  const uint64_t out_rows = std::min<uint64_t>(P.rows, recs);
+  std::vector<ResultCol> rc(P.n_out);
+  for (int c = 0; c < P.n_out; ++c) {
+    rc[c].dtype = (dfc_dtype)P.out_dtype[c];
+    cudaError_t e = cudaMallocAsync(&rc[c].values, std::max<uint64_t>(256, out_rows * dtype_size(P.out_dtype[c])), stream);
+    if (e == cudaSuccess)
+      e = cudaMallocAsync((void**)&rc[c].validity, std::max<uint64_t>(256, ((out_rows + 31) / 32) * 4), stream);
+    if (e != cudaSuccess) {
+      for (auto& r : rc) {
+        if (r.values) cudaFreeAsync(r.values, stream);
+        if (r.validity) cudaFreeAsync(r.validity, stream);
+      }
+      S.release();
+      return cuda_fail(e, "output columns");
+    }
+  }
+  auto free_outputs = [&]() {
+    for (auto& r : rc) {
+      if (r.values) cudaFreeAsync(r.values, stream);
+      if (r.validity) cudaFreeAsync(r.validity, stream);
+    }
+  };
+
+  Control* dctl = static_cast<Control*>(ctl);
+  cudaError_t e = cudaMemsetAsync(table, 0xFF, (slots + 1) * sizeof(KeyEntry), stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ctl, 0, sizeof(Control), stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(&dctl->overflow_agg, 0xFF, 4, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(bits, 0, words * 4 + 16, stream);
+  if (e != cudaSuccess) {
+    free_outputs();
+    S.release();
+    return cuda_fail(e, "scratch initialisation");
+  }
+
+  sp.table = static_cast<KeyEntry*>(table);
+  sp.table_mask = slots - 1;
+  sp.records = static_cast<unsigned char*>(records);
+  sp.recs_total = (uint32_t)recs;
+  sp.chunk = (uint32_t)chunk;
+  sp.alloc = &dctl->alloc;
+  sp.status = dctl->status;
+
+  cudaEvent_t ev[3];
+  for (auto& x : ev) cudaEventCreate(&x);
+  cudaEventRecord(ev[0], stream);
+  if (P.rows > 0) {
+    scan_kernel<<<(unsigned)ncta, kScanThreads, P.smem, stream>>>(sp);
+    t_timings.launches += 1;
+  }
+  cudaEventRecord(ev[1], stream);
+
+  fp.scan = sp;
+  fp.order_bits = static_cast<uint32_t*>(bits);
+  fp.word_prefix = static_cast<uint32_t*>(prefix);
+  fp.block_sums = static_cast<uint32_t*>(bsums);
+  fp.perm = static_cast<uint32_t*>(perm);
+  fp.groups = &dctl->groups;
+  fp.has_nulls = dctl->has_nulls;
+  fp.overflow_agg = &dctl->overflow_agg;
+  fp.words = words;
+  for (int c = 0; c < P.n_out; ++c) {
+    fp.out[c].values = rc[c].values;
+    fp.out[c].validity = rc[c].validity;
+  }
+  const unsigned rec_blocks = (unsigned)std::min<uint64_t>((recs + kFinishThreads - 1) / kFinishThreads, (uint64_t)ds->sms * 16);
+  finish_mark<<<std::max(1u, rec_blocks), kFinishThreads, 0, stream>>>(fp);
+  finish_chunk_sums<<<(unsigned)chunks, kFinishThreads, 0, stream>>>(fp);
+  finish_scan_chunks<<<1, 1024, 0, stream>>>(fp, (uint32_t)chunks);
+  finish_word_prefix<<<(unsigned)chunks, 1024, 0, stream>>>(fp);
+  finish_rank<<<std::max(1u, rec_blocks), kFinishThreads, 0, stream>>>(fp);
+  const unsigned out_blocks = (unsigned)std::min<uint64_t>((out_rows + kFinishThreads - 1) / kFinishThreads, (uint64_t)ds->sms * 16);
+  finish_output<<<std::max(1u, out_blocks), kFinishThreads, 0, stream>>>(fp);
+  t_timings.launches += 6;
+  cudaEventRecord(ev[2], stream);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host_ctl, ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream);
+  S.release();
+  if (e != cudaSuccess) {
+    free_outputs();
+    for (auto& x : ev) cudaEventDestroy(x);
+    return cuda_fail(e, "kernel launch");
+  }
+  st = wait_bounded(stream);
+  if (st) {
+    for (auto& x : ev) cudaEventDestroy(x);
+    free_outputs();
+    return st;
+  }
+  float ms_scan = 0, ms_finish = 0;
+  cudaEventElapsedTime(&ms_scan, ev[0], ev[1]);
+  cudaEventElapsedTime(&ms_finish, ev[1], ev[2]);
+  for (auto& x : ev) cudaEventDestroy(x);
+  t_timings.scan_ns += ms_scan * 1e6;
+  t_timings.finish_ns += ms_finish * 1e6;
+  t_timings.table_slots = slots;
+
+  const uint32_t status = host_ctl->status[0];
+  if (status & ST_TIMEOUT) {
+    free_outputs();
+    return fail(DFC_TIMEOUT, "a bounded device wait gave up");
+  }
+  if (status & ST_CAPACITY) {
+    free_outputs();
+    *grow = true;
+    return DFC_CAPACITY;
+  }
+  if (status & ST_OVERFLOW) {
+    free_outputs();
+    const uint32_t a = host_ctl->overflow_agg;
+    const int idt = (a < (uint32_t)q->n_aggs) ? P.out_agg_input_dtype[a] : DFC_INT64;
+    return fail(DFC_DATA_OVERFLOW, overflow_message(idt));
+  }
+  if (status & ST_FAULT) {
+    free_outputs();
+    return fail(DFC_DATA_FAULT,
+                "Mojo GPU data fault: variance of a group whose mean is far from its spread; the CPU adjudicates");
+  }
+  auto* r = new dfc_result();
+  r->device = P.device;
+  r->rows = host_ctl->groups;
+  for (int c = 0; c < P.n_out; ++c) rc[c].has_nulls = host_ctl->has_nulls[c] != 0;
+  r->cols = std::move(rc);
+  *out = r;
+  return DFC_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI.
+// ---------------------------------------------------------------------------
+extern "C" {
+
+DFC_API uint32_t dfc_version(void) { return DFC_ABI_VERSION; }
+
+DFC_API int32_t dfc_installed(void) {
+  // No driver call: the library exists (it was loaded) and a device node is present.
+  return access("/dev/nvidiactl", F_OK) == 0 ? 1 : 0;
+}
+
+DFC_API int32_t dfc_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  int usable = 0;
+  for (int i = 0; i < n; ++i) {
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, i);
+    if (major >= 10) ++usable;
+  }
+  return usable;
+}
+
+DFC_API dfc_status dfc_device_info_get(int32_t ordinal, dfc_device_info* out) {
+  if (!out) return fail(DFC_INVALID, "null output");
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || ordinal < 0 || ordinal >= n) {
+    cudaGetLastError();
+    return fail(DFC_NO_DEVICE, "no such device");
+  }
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, ordinal), "cudaGetDeviceProperties");
+  memset(out, 0, sizeof(*out));
+  out->ordinal = ordinal;
+  out->sm_count = prop.multiProcessorCount;
+  out->cc_major = prop.major;
+  out->cc_minor = prop.minor;
+  out->total_bytes = prop.totalGlobalMem;
+  out->budget_bytes = -1;
+  const char* lim = getenv("DATAFRAME_ACCEL_MEMORY_LIMIT");
+  if (lim && *lim) {
+    char* end = nullptr;
+    long long v = strtoll(lim, &end, 10);
+    if (end && *end == 0 && v > 0) out->budget_bytes = v;
+  }
+  snprintf(out->name, sizeof(out->name), "%s", prop.name);
+  return DFC_OK;
+}
+
+DFC_API dfc_status dfc_column_register(int32_t device, dfc_dtype dtype, uint64_t rows, const void* values,
+                                       const uint8_t* validity, uint64_t validity_bit_offset, uint32_t flags,
+                                       dfc_column** out) {
+  if (!out) return fail(DFC_INVALID, "null output");
+  *out = nullptr;
+  const int sz = dtype_size(dtype);
+  if (sz == 0) return fail(DFC_UNSUPPORTED, "unsupported column type");
+  if (rows > 0 && !values) return fail(DFC_INVALID, "null values");
+  if (flags != DFC_COLUMN_HOST && flags != DFC_COLUMN_DEVICE) return fail(DFC_INVALID, "bad column flags");
+  DeviceState* ds;
+  dfc_status st = device_ready(device, &ds);
+  if (st) return st;
+  DeviceGuard guard(device);
+  cudaStream_t stream = thread_stream(device);
+  auto* c = new dfc_column();
+  c->device = device;
+  c->dtype = dtype;
+  c->rows = rows;
+  const size_t bytes = (size_t)rows * sz;
+  auto bail = [&](dfc_status s) {
+    if (c->owns_values && c->values) cudaFreeAsync(c->values, stream);
+    if (c->validity) cudaFreeAsync(c->validity, stream);
+    cudaStreamSynchronize(stream);
+    delete c;
+    return s;
+  };
+  if (flags == DFC_COLUMN_HOST) {
+    cudaError_t e = cudaMallocAsync(&c->values, std::max<size_t>(256, (bytes + 255) & ~(size_t)255), stream);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "column values"));
+    c->owns_values = true;
+    if (bytes) {
+      e = cudaMemcpyAsync(c->values, values, bytes, cudaMemcpyHostToDevice, stream);
+      if (e != cudaSuccess) return bail(cuda_fail(e, "column upload"));
+    }
+  } else {
+    c->values = const_cast<void*>(values);
+  }
+  if (validity && rows > 0) {
+    const uint64_t nbytes = (validity_bit_offset + rows + 7) / 8;
+    const uint64_t words = (rows + 31) / 32;
+    cudaError_t e = cudaMallocAsync((void**)&c->validity, ((words * 4 + 255) & ~(uint64_t)255), stream);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "validity bitmap"));
+    const uint8_t* src = validity;
+    void* staging = nullptr;
+    unsigned long long* d_count = nullptr;
+    e = cudaMallocAsync((void**)&d_count, 8, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_count, 0, 8, stream);
+    if (e == cudaSuccess && flags == DFC_COLUMN_HOST) {
+      e = cudaMallocAsync(&staging, nbytes, stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(staging, validity, nbytes, cudaMemcpyHostToDevice, stream);
+      src = static_cast<const uint8_t*>(staging);
+    }
+    if (e == cudaSuccess) {
+      unsigned blocks = (unsigned)std::min<uint64_t>((words + 255) / 256, (uint64_t)ds->sms * 8);
+      normalize_validity<<<std::max(1u, blocks), 256, 0, stream>>>(src, nbytes, validity_bit_offset, rows, c->validity,
+                                                                  d_count);
+      e = cudaGetLastError();
+    }
+    unsigned long long valid_rows = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&valid_rows, d_count, 8, cudaMemcpyDeviceToHost, stream);
+    if (staging) cudaFreeAsync(staging, stream);
+    if (d_count) cudaFreeAsync(d_count, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "validity normalisation"));
+    c->null_count = rows - valid_rows;
+    if (c->null_count == 0) {
+      cudaFreeAsync(c->validity, stream);
+      c->validity = nullptr;
+    }
+  }
+  // Value range of integer columns (bounds a key's domain for table sizing).
+  if (!is_float(dtype) && rows > 0) {
+    unsigned long long* d_mm = nullptr;
+    unsigned long long h_mm[2] = {~0ull, 0ull};
+    cudaError_t e = cudaMallocAsync((void**)&d_mm, 16, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_mm, h_mm, 16, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) {
+      DevColumn dc{c->values, c->validity, dtype, sz};
+      unsigned blocks = (unsigned)std::min<uint64_t>((rows + 255) / 256, (uint64_t)ds->sms * 8);
+      column_minmax<<<std::max(1u, blocks), 256, 0, stream>>>(dc, rows, d_mm);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_mm, d_mm, 16, cudaMemcpyDeviceToHost, stream);
+    if (d_mm) cudaFreeAsync(d_mm, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "column statistics"));
+    c->min_enc = h_mm[0];
+    c->max_enc = h_mm[1];
+    c->have_range = h_mm[0] <= h_mm[1];
+  } else {
+    cudaError_t e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "column upload"));
+  }
+  *out = c;
+  return DFC_OK;
+}
+
+DFC_API dfc_status dfc_column_release(dfc_column* column) {
+  if (!column) return DFC_OK;
+  DeviceGuard guard(column->device);
+  // Stream-ordered: queued work on this thread's stream that reads the column
+  // finishes before the memory is reused.
+  cudaStream_t stream = thread_stream(column->device);
+  if (column->owns_values && column->values) cudaFreeAsync(column->values, stream);
+  if (column->validity) cudaFreeAsync(column->validity, stream);
+  delete column;
+  return DFC_OK;
+}
+
+DFC_API uint64_t dfc_column_rows(const dfc_column* column) { return column ? column->rows : 0; }
+DFC_API int32_t dfc_column_null_count(const dfc_column* column) {
+  return column ? (int32_t)std::min<uint64_t>(column->null_count, INT32_MAX) : 0;
+}
+
+DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
+  if (!out) return fail(DFC_INVALID, "null output");
+  *out = nullptr;
+  t_timings = dfc_timings{};
+  const auto t0 = std::chrono::steady_clock::now();
+  Plan P;
+  dfc_status st = plan_query(query, P);
+  if (st) return st;
+  DeviceState* ds;
+  st = device_ready(P.device, &ds);
+  if (st) return st;
+  DeviceGuard guard(P.device);
+  cudaStream_t stream = query->stream ? static_cast<cudaStream_t>(query->stream) : thread_stream(P.device);
+  thread_local Control* host_ctl = nullptr;
+  if (!host_ctl) CK(cudaMallocHost((void**)&host_ctl, sizeof(Control)), "pinned control block");
+  uint64_t est = estimate_groups(query, P);
+  uint64_t slots = next_pow2(std::max<uint64_t>(1024, est * 2));
+  const uint64_t max_slots = next_pow2(std::max<uint64_t>(1024, P.rows * 2));
+  slots = std::min(slots, max_slots);
+  for (int attempt = 0; attempt < 6; ++attempt) {
+    bool grow = false;
+    st = run_attempt(query, P, ds, stream, slots, out, &grow, host_ctl);
+    if (!grow) break;
+    t_timings.retries += 1;
+    if (slots >= max_slots) return fail(DFC_CAPACITY, "group table could not grow further");
+    slots = std::min(slots * 8, max_slots);
+  }
+  if (st == DFC_CAPACITY) return fail(DFC_CAPACITY, "group table capacity exhausted after regrowth");
+  if (st) return st;
+  learn_groups(P, (*out)->rows);
+  t_timings.groups = (*out)->rows;
+  t_timings.regime = 0;
+  t_timings.total_ns = std::chrono::duration<double, std::nano>(std::chrono::steady_clock::now() - t0).count();
+  return DFC_OK;
+}
+
+DFC_API uint64_t dfc_result_rows(const dfc_result* result) { return result ? result->rows : 0; }
+DFC_API int32_t dfc_result_columns(const dfc_result* result) { return result ? (int32_t)result->cols.size() : 0; }
+
+DFC_API dfc_status dfc_result_column(const dfc_result* result, int32_t i, dfc_dtype* dtype, const void** device_values,
+                                     const uint8_t** device_validity) {
+  if (!result || i < 0 || i >= (int32_t)result->cols.size()) return fail(DFC_INVALID, "bad result column");
+  const ResultCol& c = result->cols[i];
+  if (dtype) *dtype = c.dtype;
+  if (device_values) *device_values = c.values;
+  if (device_validity) *device_validity = c.has_nulls ? reinterpret_cast<const uint8_t*>(c.validity) : nullptr;
+  return DFC_OK;
+}
+
+DFC_API dfc_status dfc_result_copy_to_host(const dfc_result* result, int32_t i, void* values, uint8_t* validity) {
+  if (!result || i < 0 || i >= (int32_t)result->cols.size()) return fail(DFC_INVALID, "bad result column");
+  const ResultCol& c = result->cols[i];
+  DeviceGuard guard(result->device);
+  cudaStream_t stream = thread_stream(result->device);
+  const size_t n = result->rows;
+  if (values && n) CK(cudaMemcpyAsync(values, c.values, n * dtype_size(c.dtype), cudaMemcpyDeviceToHost, stream), "result copy");
+  if (validity && n) {
+    if (c.has_nulls) CK(cudaMemcpyAsync(validity, c.validity, (n + 7) / 8, cudaMemcpyDeviceToHost, stream), "result copy");
+    else memset(validity, 0xFF, (n + 7) / 8);
+  }
+  CK(cudaStreamSynchronize(stream), "result copy");
+  return DFC_OK;
+}
+
+DFC_API void dfc_result_free(dfc_result* result) {
+  if (!result) return;
+  if (result->refs.fetch_sub(1) != 1) return;
+  DeviceGuard guard(result->device);
+  cudaStream_t stream = thread_stream(result->device);
+  for (auto& c : result->cols) {
+    if (c.values) cudaFreeAsync(c.values, stream);
+    if (c.validity) cudaFreeAsync(c.validity, stream);
+  }
+  delete result;
+}
+
+struct Residence {
+  dfc_result* result;
+  int32_t column;
+};
+
+DFC_API void* dfc_result_residence(dfc_result* result, int32_t i) {
+  if (!result || i < 0 || i >= (int32_t)result->cols.size()) return nullptr;
+  result->refs.fetch_add(1);
+  return new Residence{result, i};
+}
+
+DFC_API int32_t dfc_residence_to_host(void* ctx, void* host_dst, int64_t bytes) {
+  auto* r = static_cast<Residence*>(ctx);
+  if (!r || !host_dst || bytes < 0) return 1;
+  const ResultCol& c = r->result->cols[r->column];
+  const int64_t have = (int64_t)(r->result->rows * dtype_size(c.dtype));
+  if (bytes > have) return 1;
+  DeviceGuard guard(r->result->device);
+  if (bytes && cudaMemcpy(host_dst, c.values, (size_t)bytes, cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+  return 0;
+}
+
+DFC_API void dfc_residence_release(void* ctx) {
+  auto* r = static_cast<Residence*>(ctx);
+  if (!r) return;
+  dfc_result_free(r->result);
+  delete r;
+}
+
+DFC_API dfc_status dfc_last_timings(dfc_timings* out) {
+  if (!out) return fail(DFC_INVALID, "null output");
+  *out = t_timings;
+  return DFC_OK;
+}
+
+DFC_API dfc_status dfc_set_thread_stream(int32_t device, void* stream) {
+  if (device < 0) return fail(DFC_INVALID, "bad device");
+  if (stream) t_chosen[device] = static_cast<cudaStream_t>(stream);
+  else t_chosen.erase(device);
+  return DFC_OK;
+}
+
+DFC_API const char* dfc_last_error(void) { return t_error.c_str(); }
+
+DFC_API const char* dfc_status_name(dfc_status status) {
+  switch (status) {
+    case DFC_OK: return "ok";
+    case DFC_UNSUPPORTED: return "unsupported";
+    case DFC_INVALID: return "invalid";
+    case DFC_DATA_OVERFLOW: return "data overflow";
+    case DFC_DATA_FAULT: return "data fault";
+    case DFC_CAPACITY: return "capacity";
+    case DFC_OOM: return "out of device memory";
+    case DFC_TIMEOUT: return "timeout";
+    case DFC_DEVICE: return "device error";
+    case DFC_NO_DEVICE: return "no device";
+  }
+  return "unknown";
+}
+
+}  // extern "C"

@@ -1,0 +1,441 @@
+"""Host-side frames, expressions and plans: the shapes the reference's core
+hands a provider, restated just far enough for the filtered group-by region.
+
+Reference shapes:
+  * ``DataFrame`` of ``Series`` = typed values + validity
+    (dataframe/storage/column.mojo:1-32).
+  * ``LazyFrame.filter(pred).group_by(keys, maintain_order).agg(exprs)``
+    (dataframe/lazy_api.mojo:418-419, 3135-3256): a SCAN -> FILTER* -> AGG
+    region (dataframe/query_execution/placement.mojo:74-94).
+  * ``collect(engine="accel")`` reaches the provider's ``execute``
+    (dataframe/lazy_api.mojo:1763-1766).  The CPU engine is not part of this
+    package: ``engine="cpu"`` raises here.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Iterable, Sequence
+
+import numpy as np
+
+from . import _native as N
+
+_NP_TO_DFC = {
+    np.dtype(np.int8): N.INT8,
+    np.dtype(np.int16): N.INT16,
+    np.dtype(np.int32): N.INT32,
+    np.dtype(np.int64): N.INT64,
+    np.dtype(np.uint8): N.UINT8,
+    np.dtype(np.uint16): N.UINT16,
+    np.dtype(np.uint32): N.UINT32,
+    np.dtype(np.uint64): N.UINT64,
+    np.dtype(np.float32): N.FLOAT32,
+    np.dtype(np.float64): N.FLOAT64,
+}
+_DFC_TO_NP = {v: k for k, v in _NP_TO_DFC.items()}
+
+
+def dfc_dtype(dtype: np.dtype) -> int:
+    try:
+        return _NP_TO_DFC[np.dtype(dtype)]
+    except KeyError:
+        raise TypeError(f"unsupported column type {dtype}") from None
+
+
+def np_dtype(code: int) -> np.dtype:
+    return _DFC_TO_NP[code]
+
+
+class Series:
+    """A named column: values plus an optional validity mask (True = valid)."""
+
+    def __init__(self, name: str, values, valid=None, dtype=None):
+        arr = np.asarray(values, dtype=dtype)
+        if arr.ndim != 1:
+            raise ValueError("a Series is one-dimensional")
+        dfc_dtype(arr.dtype)
+        self.name = name
+        self.values = np.ascontiguousarray(arr)
+        if valid is not None:
+            valid = np.asarray(valid, dtype=bool)
+            if valid.shape != self.values.shape:
+                raise ValueError("validity length differs from values")
+            if valid.all():
+                valid = None
+        self.valid = valid
+
+    def __len__(self) -> int:
+        return len(self.values)
+
+    @property
+    def dtype(self) -> np.dtype:
+        return self.values.dtype
+
+    def is_valid(self, i: int) -> bool:
+        return self.valid is None or bool(self.valid[i])
+
+    def item(self, i: int):
+        return self.values[i].item() if self.is_valid(i) else None
+
+    def to_list(self) -> list:
+        return [self.item(i) for i in range(len(self))]
+
+    def slice(self, offset: int, length: int) -> "Series":
+        v = None if self.valid is None else self.valid[offset : offset + length]
+        return Series(self.name, self.values[offset : offset + length], v)
+
+    def equals(self, other: "Series") -> bool:
+        """Same name, dtype, length, nulls and values (NaN equals NaN)."""
+        if self.name != other.name or self.dtype != other.dtype or len(self) != len(other):
+            return False
+        va = np.ones(len(self), bool) if self.valid is None else self.valid
+        vb = np.ones(len(other), bool) if other.valid is None else other.valid
+        if not np.array_equal(va, vb):
+            return False
+        a, b = self.values[va], other.values[vb]
+        if self.dtype.kind == "f":
+            return bool(np.all((a == b) | (np.isnan(a) & np.isnan(b))))
+        return bool(np.array_equal(a, b))
+
+    def __repr__(self) -> str:
+        return f"Series({self.name!r}, {self.dtype}, {self.to_list()[:8]}{'...' if len(self) > 8 else ''})"
+
+
+class DataFrame:
+    def __init__(self, columns: Iterable[Series] | dict):
+        if isinstance(columns, dict):
+            columns = [s if isinstance(s, Series) else Series(k, s) for k, s in columns.items()]
+        self._cols: list[Series] = list(columns)
+        names = [c.name for c in self._cols]
+        if len(set(names)) != len(names):
+            raise ValueError("duplicate column names")
+        lens = {len(c) for c in self._cols}
+        if len(lens) > 1:
+            raise ValueError("columns differ in length")
+
+    @property
+    def columns(self) -> list[str]:
+        return [c.name for c in self._cols]
+
+    @property
+    def height(self) -> int:
+        return len(self._cols[0]) if self._cols else 0
+
+    def column(self, name: str) -> Series:
+        for c in self._cols:
+            if c.name == name:
+                return c
+        raise KeyError(name)
+
+    def __getitem__(self, name: str) -> Series:
+        return self.column(name)
+
+    def item(self, row: int, name: str):
+        return self.column(name).item(row)
+
+    def lazy(self) -> "LazyFrame":
+        return LazyFrame(self)
+
+    def slice(self, offset: int, length: int) -> "DataFrame":
+        return DataFrame([c.slice(offset, length) for c in self._cols])
+
+    def group_by(self, keys, maintain_order: bool = False) -> "LazyGroupBy":
+        """Eager form (dataframe/aggregation/group_by.mojo:235-356): a
+        one-node lazy plan collected at once by ``agg``."""
+        return _EagerGroupBy(self.lazy().group_by(keys, maintain_order=maintain_order))
+
+    def equals(self, other: "DataFrame") -> bool:
+        return self.columns == other.columns and all(a.equals(b) for a, b in zip(self._cols, other._cols))
+
+    def __repr__(self) -> str:
+        return f"DataFrame({self.height} rows: {', '.join(f'{c.name}:{c.dtype}' for c in self._cols)})"
+
+
+# ---------------------------------------------------------------------------
+# Expressions.
+# ---------------------------------------------------------------------------
+_CMP = {"<": N.LT, "<=": N.LE, ">": N.GT, ">=": N.GE, "==": N.EQ, "!=": N.NE}
+
+
+@dataclass(frozen=True)
+class Pred:
+    """A filter predicate: a tree of comparisons and Kleene connectives."""
+
+    kind: str  # cmp / is_null / is_not_null / and / or / not / true
+    column: str | None = None
+    op: str | None = None
+    literal: object = None
+    args: tuple = ()
+
+    def __and__(self, other: "Pred") -> "Pred":
+        return Pred("and", args=(self, other))
+
+    def __or__(self, other: "Pred") -> "Pred":
+        return Pred("or", args=(self, other))
+
+    def __invert__(self) -> "Pred":
+        return Pred("not", args=(self,))
+
+
+@dataclass(frozen=True)
+class AggExpr:
+    op: int
+    column: str
+    name: str
+    ddof: int = 1
+    min_count: int = 0
+
+    def alias(self, name: str) -> "AggExpr":
+        return AggExpr(self.op, self.column, name, self.ddof, self.min_count)
+
+
+@dataclass(frozen=True)
+class Col:
+    name: str
+
+    def _cmp(self, op: str, lit) -> Pred:
+        return Pred("cmp", column=self.name, op=op, literal=lit)
+
+    def __lt__(self, lit):
+        return self._cmp("<", lit)
+
+    def __le__(self, lit):
+        return self._cmp("<=", lit)
+
+    def __gt__(self, lit):
+        return self._cmp(">", lit)
+
+    def __ge__(self, lit):
+        return self._cmp(">=", lit)
+
+    def __eq__(self, lit):  # type: ignore[override]
+        return self._cmp("==", lit)
+
+    def __ne__(self, lit):  # type: ignore[override]
+        return self._cmp("!=", lit)
+
+    __hash__ = object.__hash__
+
+    def is_null(self) -> Pred:
+        return Pred("is_null", column=self.name)
+
+    def is_not_null(self) -> Pred:
+        return Pred("is_not_null", column=self.name)
+
+    def sum(self, min_count: int = 0) -> AggExpr:
+        return AggExpr(N.AGG_SUM, self.name, self.name, min_count=min_count)
+
+    def mean(self) -> AggExpr:
+        return AggExpr(N.AGG_MEAN, self.name, self.name)
+
+    def min(self) -> AggExpr:
+        return AggExpr(N.AGG_MIN, self.name, self.name)
+
+    def max(self) -> AggExpr:
+        return AggExpr(N.AGG_MAX, self.name, self.name)
+
+    def count(self) -> AggExpr:
+        return AggExpr(N.AGG_COUNT, self.name, self.name)
+
+    def len(self) -> AggExpr:
+        return AggExpr(N.AGG_LEN, self.name, self.name)
+
+    def null_count(self) -> AggExpr:
+        return AggExpr(N.AGG_NULL_COUNT, self.name, self.name)
+
+    def var(self, ddof: int = 1) -> AggExpr:
+        return AggExpr(N.AGG_VAR, self.name, self.name, ddof=ddof)
+
+    def std(self, ddof: int = 1) -> AggExpr:
+        return AggExpr(N.AGG_STD, self.name, self.name, ddof=ddof)
+
+
+def col(name: str) -> Col:
+    return Col(name)
+
+
+def lit(value):
+    return value
+
+
+# ---------------------------------------------------------------------------
+# Plans.
+# ---------------------------------------------------------------------------
+@dataclass
+class Plan:
+    """SCAN_FRAME -> FILTER* -> AGG, the region a provider receives."""
+
+    source: DataFrame
+    filters: list[Pred] = field(default_factory=list)
+    keys: list[str] | None = None
+    aggs: list[AggExpr] | None = None
+    maintain_order: bool = False
+
+    def describe(self) -> str:
+        parts = [f"SCAN_FRAME {self.source.columns}"]
+        parts += [f"FILTER {f}" for f in self.filters]
+        if self.keys is not None:
+            parts.append(f"AGG keys={self.keys} maintain_order={self.maintain_order} aggs={[a.name for a in self.aggs]}")
+        return " -> ".join(parts)
+
+
+class LazyFrame:
+    def __init__(self, source: DataFrame, plan: Plan | None = None):
+        self._plan = plan or Plan(source)
+
+    @property
+    def plan(self) -> Plan:
+        return self._plan
+
+    def filter(self, pred: Pred) -> "LazyFrame":
+        if self._plan.keys is not None:
+            raise ValueError("a filter after the aggregation is not part of this region")
+        p = Plan(self._plan.source, self._plan.filters + [pred])
+        return LazyFrame(p.source, p)
+
+    def group_by(self, keys, maintain_order: bool = False) -> "LazyGroupBy":
+        if isinstance(keys, str):
+            keys = [keys]
+        keys = list(keys)
+        if not keys:
+            raise ValueError("group_by needs at least one key")
+        if len(set(keys)) != len(keys):
+            raise ValueError("duplicate key column")
+        for k in keys:
+            self._plan.source.column(k)
+        return LazyGroupBy(self, keys, maintain_order)
+
+    def collect(self, engine: str = "accel") -> DataFrame:
+        if engine != "accel":
+            raise ValueError("this package holds only the accelerator provider: engine must be 'accel'")
+        from . import provider
+
+        return provider.execute(self)[0]
+
+
+class LazyGroupBy:
+    def __init__(self, frame: LazyFrame, keys: list[str], maintain_order: bool):
+        self._frame = frame
+        self._keys = keys
+        self._maintain_order = maintain_order
+
+    def agg(self, exprs: AggExpr | Sequence[AggExpr]) -> LazyFrame:
+        if isinstance(exprs, AggExpr):
+            exprs = [exprs]
+        exprs = list(exprs)
+        for e in exprs:
+            self._frame.plan.source.column(e.column)
+        names = list(self._keys) + [e.name for e in exprs]
+        if len(set(names)) != len(names):
+            raise ValueError("duplicate output column names")
+        p = self._frame.plan
+        plan = Plan(p.source, list(p.filters), list(self._keys), exprs, self._maintain_order)
+        return LazyFrame(p.source, plan)
+
+    def len(self, name: str = "len") -> LazyFrame:
+        return self.agg([AggExpr(N.AGG_LEN, self._keys[0], name)])
+
+
+class _EagerGroupBy:
+    def __init__(self, lazy: LazyGroupBy):
+        self._lazy = lazy
+
+    def agg(self, exprs) -> DataFrame:
+        return self._lazy.agg(exprs).collect()
+
+    def len(self, name: str = "len") -> DataFrame:
+        return self._lazy.len(name).collect()
+
+
+# ---------------------------------------------------------------------------
+# Binding: a plan as the column list, filter program and aggregation list the
+# C ABI takes (binding happens before a backend is chosen in the reference,
+# docs/design/accelerator-contract.md:75).
+# ---------------------------------------------------------------------------
+@dataclass
+class Bound:
+    names: list[str]                 # input column names, in `inputs` order
+    series: list[Series]
+    keys: list[int]
+    pred: list[tuple]                # (kind, column index, cmp, literal) postfix
+    aggs: list[tuple]                # (op, column index, ddof, min_count)
+    out_names: list[str]
+    maintain_order: bool
+
+
+def _bind_literal(series: Series, value):
+    """A literal cast to the column's type (the core's literal coercion)."""
+    kind = series.dtype.kind
+    if kind == "f":
+        return ("f", float(value))
+    if isinstance(value, float):
+        if value != value:
+            raise TypeError("NaN literal against an integer column")
+        if not float(value).is_integer():
+            raise TypeError("fractional literal against an integer column")
+        value = int(value)
+    info = np.iinfo(series.dtype)
+    if not info.min <= int(value) <= info.max:
+        raise TypeError(f"literal {value} out of range for {series.dtype}")
+    return ("u", int(value)) if series.dtype == np.uint64 else ("i", int(value))
+
+
+def bind(plan: Plan) -> Bound:
+    if plan.keys is None:
+        raise ValueError("the plan has no aggregation")
+    src = plan.source
+    names: list[str] = []
+
+    def idx(name: str) -> int:
+        if name not in names:
+            src.column(name)
+            names.append(name)
+        return names.index(name)
+
+    keys = [idx(k) for k in plan.keys]
+    prog: list[tuple] = []
+
+    def emit(p: Pred):
+        if p.kind == "cmp":
+            i = idx(p.column)
+            prog.append((N.PRED_CMP, i, _CMP[p.op], _bind_literal(src.column(p.column), p.literal)))
+        elif p.kind == "is_null":
+            prog.append((N.PRED_IS_NULL, idx(p.column), 0, ("i", 0)))
+        elif p.kind == "is_not_null":
+            prog.append((N.PRED_IS_NOT_NULL, idx(p.column), 0, ("i", 0)))
+        elif p.kind == "true":
+            prog.append((N.PRED_TRUE, 0, 0, ("i", 0)))
+        elif p.kind == "not":
+            emit(p.args[0])
+            prog.append((N.PRED_NOT, 0, 0, ("i", 0)))
+        elif p.kind in ("and", "or"):
+            emit(p.args[0])
+            emit(p.args[1])
+            prog.append((N.PRED_AND if p.kind == "and" else N.PRED_OR, 0, 0, ("i", 0)))
+        else:
+            raise ValueError(f"unknown predicate {p.kind}")
+
+    for i, f in enumerate(plan.filters):
+        emit(f)
+        if i > 0:
+            prog.append((N.PRED_AND, 0, 0, ("i", 0)))
+    aggs = [(a.op, idx(a.column), a.ddof, a.min_count) for a in plan.aggs]
+    return Bound(
+        names=names,
+        series=[src.column(n) for n in names],
+        keys=keys,
+        pred=prog,
+        aggs=aggs,
+        out_names=list(plan.keys) + [a.name for a in plan.aggs],
+        maintain_order=plan.maintain_order,
+    )
+
+
+def pack_validity(valid: np.ndarray | None) -> np.ndarray | None:
+    if valid is None:
+        return None
+    return np.packbits(valid.astype(np.uint8), bitorder="little")
+
+
+def unpack_validity(bits: np.ndarray, rows: int) -> np.ndarray:
+    return np.unpackbits(bits, bitorder="little")[:rows].astype(bool)

@@ -1,0 +1,500 @@
+"""The provider interface, mirrored: the thirteen functions the reference core
+calls through dataframe/_accel_provider.mojo:10-27, with the behaviour the
+contract gives them (docs/design/accelerator-contract.md:22-70), backed by
+libdfcuda.so.
+
+    installed execute describe execute_profiled
+    handoff_supports handoff_execute handoff_estimate
+    devices transfer_model pipeline_supports pipeline_estimate pipeline_costs run_pipeline
+
+Plus the resident-table form (columns registered once, queried many times),
+which is what `run_pipeline` over device-resident inputs means for a
+discrete device (dataframe/storage/residence.mojo:33-147).
+
+Errors: unsupported work raises ``UnsupportedError`` before anything is
+submitted; checked-sum overflow raises ``ProviderError`` with the CPU
+provider's exact text; a data fault (``DataFaultError``) asks the caller to
+let the CPU adjudicate, as the reference's data-fault marker does
+(dataframe_metal/accelerator/faults.mojo:1-18).  The provider itself never
+runs anything on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from .frame import Bound, DataFrame, LazyFrame, Plan, Series, bind, dfc_dtype, np_dtype, pack_validity, unpack_validity
+
+BACKEND = "cuda"
+MEMORY_DISCRETE = 1
+MEMORY_UNIFIED = 2
+
+
+class ProviderError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+class UnsupportedError(ProviderError):
+    pass
+
+
+class DataFaultError(ProviderError):
+    pass
+
+
+def _check(status: int) -> None:
+    if status == N.OK:
+        return
+    msg = N.last_error() or N.lib().dfc_status_name(status).decode()
+    if status in (N.UNSUPPORTED, N.INVALID):
+        raise UnsupportedError(status, msg)
+    if status == N.DATA_FAULT:
+        raise DataFaultError(status, msg)
+    raise ProviderError(status, msg)
+
+
+def _device_from_env() -> int:
+    """DATAFRAME_ACCEL_DEVICE, the name the reference's providers read
+    (docs/design/accelerator-contract.md:168-171); a bad value raises."""
+    raw = os.environ.get("DATAFRAME_ACCEL_DEVICE", "")
+    if raw == "":
+        return 0
+    try:
+        dev = int(raw)
+    except ValueError:
+        raise ValueError(f"DATAFRAME_ACCEL_DEVICE={raw!r} is not a device ordinal") from None
+    if dev < 0:
+        raise ValueError(f"DATAFRAME_ACCEL_DEVICE={raw!r} is negative")
+    return dev
+
+
+def _memory_limit() -> int:
+    raw = os.environ.get("DATAFRAME_ACCEL_MEMORY_LIMIT", "")
+    if raw == "":
+        return -1
+    try:
+        v = int(raw)
+    except ValueError:
+        raise ValueError(f"DATAFRAME_ACCEL_MEMORY_LIMIT={raw!r} is not a byte count") from None
+    if v <= 0:
+        raise ValueError(f"DATAFRAME_ACCEL_MEMORY_LIMIT={raw!r} must be positive")
+    return v
+
+
+# ---------------------------------------------------------------------------
+# Device columns and results.
+# ---------------------------------------------------------------------------
+class DeviceColumn:
+    """A column resident in HBM (values + normalised validity bitmap)."""
+
+    def __init__(self, series: Series, device: int = 0, *, device_pointer: int | None = None):
+        lib = N.lib()
+        self.name = series.name
+        self.dtype = series.dtype
+        self.rows = len(series)
+        self.device = device
+        bits = pack_validity(series.valid)
+        handle = C.c_void_p()
+        if device_pointer is None:
+            values = series.values
+            _check(
+                lib.dfc_column_register(
+                    device,
+                    dfc_dtype(values.dtype),
+                    self.rows,
+                    values.ctypes.data if self.rows else None,
+                    bits.ctypes.data if bits is not None else None,
+                    0,
+                    N.COLUMN_HOST,
+                    C.byref(handle),
+                )
+            )
+        else:
+            if bits is not None:
+                raise UnsupportedError(N.UNSUPPORTED, "device columns take a device validity pointer")
+            _check(
+                lib.dfc_column_register(
+                    device, dfc_dtype(series.dtype), self.rows, device_pointer, None, 0, N.COLUMN_DEVICE, C.byref(handle)
+                )
+            )
+        self.handle = handle
+
+    @classmethod
+    def from_host_pointer(cls, name: str, dtype, rows: int, values_ptr: int, validity_ptr: int | None = None,
+                          bit_offset: int = 0, device: int = 0) -> "DeviceColumn":
+        """Registers host memory (pinned or pageable) without a numpy copy."""
+        self = cls.__new__(cls)
+        self.name, self.dtype, self.rows, self.device = name, np.dtype(dtype), rows, device
+        handle = C.c_void_p()
+        _check(
+            N.lib().dfc_column_register(
+                device, dfc_dtype(dtype), rows, values_ptr, validity_ptr, bit_offset, N.COLUMN_HOST, C.byref(handle)
+            )
+        )
+        self.handle = handle
+        return self
+
+    @property
+    def null_count(self) -> int:
+        return int(N.lib().dfc_column_null_count(self.handle)) if self.handle else 0
+
+    def release(self) -> None:
+        if self.handle:
+            N.lib().dfc_column_release(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+class DeviceResult:
+    """A query result resident on the device: key columns then one column per
+    aggregation.  ``to_frame`` copies it to the host."""
+
+    def __init__(self, handle: C.c_void_p, names: list[str]):
+        self.handle = handle
+        self.names = names
+        self.rows = int(N.lib().dfc_result_rows(handle))
+
+    def column_info(self, i: int) -> tuple[np.dtype, int, int | None]:
+        dt = C.c_int()
+        vals = C.c_void_p()
+        valid = C.c_void_p()
+        _check(N.lib().dfc_result_column(self.handle, i, C.byref(dt), C.byref(vals), C.byref(valid)))
+        return np_dtype(dt.value), vals.value, valid.value
+
+    def to_frame(self) -> DataFrame:
+        lib = N.lib()
+        cols = []
+        for i, name in enumerate(self.names):
+            dtype, _, dvalid = self.column_info(i)
+            values = np.empty(self.rows, dtype=dtype)
+            bits = np.empty((self.rows + 7) // 8, dtype=np.uint8) if dvalid else None
+            _check(
+                lib.dfc_result_copy_to_host(
+                    self.handle,
+                    i,
+                    values.ctypes.data if self.rows else None,
+                    bits.ctypes.data if bits is not None and self.rows else None,
+                )
+            )
+            valid = unpack_validity(bits, self.rows) if bits is not None else None
+            cols.append(Series(name, values, valid))
+        return DataFrame(cols)
+
+    def free(self) -> None:
+        if self.handle:
+            N.lib().dfc_result_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def _query_struct(bound: Bound, handles: list, stream: int | None, flags: int = 0):
+    n = len(handles)
+    inputs = (C.c_void_p * n)(*[h.value for h in handles])
+    keys = (C.c_int32 * len(bound.keys))(*bound.keys)
+    pred = (N.PredOp * max(1, len(bound.pred)))()
+    for i, (kind, column, cmp, (lk, lv)) in enumerate(bound.pred):
+        pred[i].kind, pred[i].column, pred[i].cmp = kind, column, cmp
+        if lk == "f":
+            pred[i].lit.f = lv
+        elif lk == "u":
+            pred[i].lit.u = lv
+        else:
+            pred[i].lit.i = lv
+    aggs = (N.Agg * max(1, len(bound.aggs)))()
+    for i, (op, column, ddof, min_count) in enumerate(bound.aggs):
+        aggs[i].op, aggs[i].column, aggs[i].ddof, aggs[i].min_count = op, column, ddof, min_count
+    q = N.Query()
+    q.abi_version = N.ABI_VERSION
+    q.flags = flags | (N.Q_MAINTAIN_ORDER if bound.maintain_order else 0)
+    q.n_inputs = n
+    q.n_keys = len(bound.keys)
+    q.inputs = C.cast(inputs, C.POINTER(C.c_void_p))
+    q.keys = C.cast(keys, C.POINTER(C.c_int32))
+    q.n_pred = len(bound.pred)
+    q.n_aggs = len(bound.aggs)
+    q.pred = C.cast(pred, C.POINTER(N.PredOp))
+    q.aggs = C.cast(aggs, C.POINTER(N.Agg))
+    q.stream = stream
+    # Keep the arrays alive with the struct.
+    q._keep = (inputs, keys, pred, aggs)
+    return q
+
+
+def run_bound(bound: Bound, columns: list[DeviceColumn], stream: int | None = None, flags: int = 0) -> DeviceResult:
+    """Runs a bound region over registered columns; the result stays on the device."""
+    q = _query_struct(bound, [c.handle for c in columns], stream, flags)
+    out = C.c_void_p()
+    _check(N.lib().dfc_groupby(C.byref(q), C.byref(out)))
+    return DeviceResult(out, bound.out_names)
+
+
+def last_timings() -> dict:
+    t = N.Timings()
+    _check(N.lib().dfc_last_timings(C.byref(t)))
+    return {
+        "scan_ns": t.scan_ns,
+        "finish_ns": t.finish_ns,
+        "total_ns": t.total_ns,
+        "groups": int(t.groups),
+        "table_slots": int(t.table_slots),
+        "regime": int(t.regime),
+        "retries": int(t.retries),
+        "launches": int(t.launches),
+    }
+
+
+def set_thread_stream(device: int, stream: int | None) -> None:
+    """Routes this thread's library calls on `device` through `stream`."""
+    _check(N.lib().dfc_set_thread_stream(device, stream))
+
+
+class ResidentTable:
+    """Columns of a DataFrame registered once and kept resident in HBM, so
+    repeated queries move no input bytes (config 5's tables)."""
+
+    def __init__(self, frame: DataFrame, device: int | None = None):
+        self.device = _device_from_env() if device is None else device
+        self.frame = frame
+        self.columns = {name: DeviceColumn(frame.column(name), self.device) for name in frame.columns}
+
+    def run(self, lazy: LazyFrame | Plan, stream: int | None = None, flags: int = 0) -> DeviceResult:
+        plan = lazy.plan if isinstance(lazy, LazyFrame) else lazy
+        bound = bind(plan)
+        return run_bound(bound, [self.columns[n] for n in bound.names], stream, flags)
+
+    def release(self) -> None:
+        for c in self.columns.values():
+            c.release()
+        self.columns = {}
+
+
+def _region_plan(plan) -> Plan:
+    return plan.plan if isinstance(plan, LazyFrame) else plan
+
+
+def _execute_plan(plan: Plan, device: int) -> DataFrame:
+    bound = bind(plan)
+    cols = [DeviceColumn(s, device) for s in bound.series]
+    try:
+        result = run_bound(bound, cols)
+        try:
+            return result.to_frame()
+        finally:
+            result.free()
+    finally:
+        for c in cols:
+            c.release()
+
+
+def _unsupported_reason(plan: Plan) -> str | None:
+    if plan.keys is None:
+        return "the region has no grouped aggregation"
+    try:
+        bound = bind(plan)
+    except (TypeError, ValueError, KeyError) as e:
+        return str(e)
+    if len(bound.keys) > 4:
+        return "more than four keys"
+    if len(bound.names) > 16:
+        return "more than sixteen input columns"
+    if len(bound.aggs) > 32:
+        return "more than thirty-two aggregations"
+    if plan.source.height >= 0xFFFFFFFF:
+        return "more than 2^32-2 rows"
+    return None
+
+
+# ---------------------------------------------------------------------------
+# The thirteen provider functions.
+# ---------------------------------------------------------------------------
+def installed() -> bool:
+    """Whether the backend could run here; opens no driver and creates no context."""
+    if not N.library_present():
+        return False
+    try:
+        return bool(N.lib().dfc_installed())
+    except OSError:
+        return False
+
+
+def describe(plan) -> str:
+    """``ENGINE accel: ...`` text for explain; never raises and never touches a device."""
+    try:
+        p = _region_plan(plan)
+        reason = _unsupported_reason(p)
+        if reason:
+            return f"ENGINE accel: rejected ({reason})"
+        return f"ENGINE accel: {BACKEND} filtered hash group-by: {p.describe()}"
+    except Exception as e:  # describe does not raise
+        return f"ENGINE accel: rejected ({e})"
+
+
+def execute(plan) -> tuple[DataFrame, DataFrame]:
+    """Runs the whole plan; returns (result, report).  Unsupported plans raise
+    before anything is submitted."""
+    p = _region_plan(plan)
+    reason = _unsupported_reason(p)
+    if reason:
+        raise UnsupportedError(N.UNSUPPORTED, f"accelerator cannot run this plan: {reason}")
+    device = _device_from_env()
+    _memory_limit()
+    t0 = time.perf_counter_ns()
+    result = _execute_plan(p, device)
+    wall = time.perf_counter_ns() - t0
+    t = last_timings()
+    report = DataFrame(
+        [
+            Series("engine", np.array([0], np.int32)),
+            Series("device", np.array([device], np.int32)),
+            Series("groups", np.array([t["groups"]], np.int64)),
+            Series("scan_ns", np.array([t["scan_ns"]], np.float64)),
+            Series("finish_ns", np.array([t["finish_ns"]], np.float64)),
+            Series("wall_ns", np.array([wall], np.float64)),
+        ]
+    )
+    return result, report
+
+
+def execute_profiled(plan) -> tuple[DataFrame, DataFrame]:
+    return execute(plan)
+
+
+def handoff_supports(region) -> bool:
+    """False: the contract asks a provider for a discrete device to decline
+    node hand-off (docs/design/accelerator-contract.md:31); whole plans go
+    through `execute` and placed pipelines through `run_pipeline`."""
+    return False
+
+
+def handoff_execute(region) -> DataFrame:
+    p = _region_plan(region)
+    reason = _unsupported_reason(p)
+    if reason:
+        raise UnsupportedError(N.UNSUPPORTED, f"accelerator cannot run this region: {reason}")
+    return _execute_plan(p, _device_from_env())
+
+
+def handoff_estimate(region, rows: int) -> tuple[str, float]:
+    """(calibration key, estimated ns for `rows` input rows, moves included); -1: not measured."""
+    p = _region_plan(region)
+    key = "cuda:groupby:v1:" + describe(p)
+    return key, -1.0
+
+
+@dataclass
+class DeviceInfo:
+    backend: str
+    ordinal: int
+    name: str
+    memory: int
+    budget_bytes: int
+    total_bytes: int
+    sm_count: int
+
+
+@dataclass
+class TransferModel:
+    host_to_device_bytes_per_ns: float = -1.0
+    device_to_host_bytes_per_ns: float = -1.0
+    context_ns: float = -1.0
+
+
+@dataclass
+class PipelineFeatures:
+    rows: int = 0
+    input_bytes: int = 0
+    groups: int = -1
+
+
+def devices() -> list[DeviceInfo]:
+    """Each sm_100 device; reads driver metadata only, creates no context."""
+    if not installed():
+        return []
+    lib = N.lib()
+    out = []
+    for i in range(lib.dfc_device_count()):
+        info = N.DeviceInfo()
+        if lib.dfc_device_info_get(i, C.byref(info)) != N.OK:
+            continue
+        budget = _memory_limit()
+        out.append(
+            DeviceInfo(
+                BACKEND,
+                info.ordinal,
+                info.name.decode(),
+                MEMORY_DISCRETE,
+                budget if budget > 0 else int(info.budget_bytes),
+                int(info.total_bytes),
+                int(info.sm_count),
+            )
+        )
+    return out
+
+
+_transfer: dict[int, TransferModel] = {}
+
+
+def calibrate_transfer(device: int, nbytes: int = 1 << 28) -> TransferModel:
+    """Measures pinned host<->device copy rates once (torch pinned buffers)."""
+    import torch
+
+    with torch.cuda.device(device):
+        h = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        d = torch.empty(nbytes, dtype=torch.uint8, device=f"cuda:{device}")
+        d.copy_(h, non_blocking=True)
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter_ns()
+        d.copy_(h, non_blocking=True)
+        torch.cuda.synchronize(device)
+        t1 = time.perf_counter_ns()
+        h.copy_(d, non_blocking=True)
+        torch.cuda.synchronize(device)
+        t2 = time.perf_counter_ns()
+    m = TransferModel(nbytes / max(1, t1 - t0), nbytes / max(1, t2 - t1), -1.0)
+    _transfer[device] = m
+    return m
+
+
+def transfer_model(device: int) -> TransferModel:
+    return _transfer.get(device, TransferModel())
+
+
+def pipeline_supports(pipeline, device: int) -> bool:
+    try:
+        return installed() and _unsupported_reason(_region_plan(pipeline)) is None
+    except Exception:
+        return False
+
+
+def pipeline_estimate(pipeline, device: int, features: PipelineFeatures | None = None) -> float:
+    """Estimated device ns excluding input/output moves; -1 when unmeasured."""
+    return -1.0
+
+
+def pipeline_costs(pipeline, device: int, features: PipelineFeatures | None = None) -> tuple[float, float]:
+    return -1.0, pipeline_estimate(pipeline, device, features)
+
+
+def run_pipeline(pipeline, device: int) -> DataFrame:
+    p = _region_plan(pipeline)
+    reason = _unsupported_reason(p)
+    if reason:
+        raise UnsupportedError(N.UNSUPPORTED, f"accelerator cannot run this pipeline: {reason}")
+    return _execute_plan(p, device)

@@ -1,0 +1,283 @@
+/*
+ * dfcuda.h — C ABI of libdfcuda.so, a B200 (sm_100a) accelerator provider for
+ * dataframe_mojo's filtered hash group-by:
+ *
+ *     filter(predicate) -> group_by(keys, maintain_order) -> agg(...)
+ *
+ * The reference reaches an accelerator through thirteen provider functions
+ * re-exported by dataframe/_accel_provider.mojo:10-27 (contract:
+ * docs/design/accelerator-contract.md:22-70).  Those functions take Mojo
+ * objects (LazyFrame, DataFrame).  A provider package written in Mojo
+ * marshals them into the plain descriptors below and calls this library
+ * through external_call / OwnedDLHandle, the pattern the reference already
+ * uses for its native Parquet shim (dataframe/io/native_library.mojo:38-90,
+ * native/dfparquet/dfparquet.sym).  Nothing here names a Mojo or torch type.
+ *
+ * Threading: every entry point is thread-safe.  One CUDA context per device
+ * (the primary context); a query runs on the caller's stream or on a stream
+ * owned by the library; the resident-column registry is guarded by a lock.
+ *
+ * Errors: every call that can fail returns a dfc_status; the text of the last
+ * failure on the calling thread is dfc_last_error().  Checked integer sums
+ * report DFC_DATA_OVERFLOW with the reference CPU's exact message
+ * ("Int64 expression sum overflow", "int32 expression sum overflow", ...:
+ * dataframe/aggregation/function.mojo:2798, 2914).
+ */
+#ifndef DFCUDA_H
+#define DFCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DFC_ABI_VERSION 1u
+
+#if defined(__GNUC__)
+#define DFC_API __attribute__((visibility("default")))
+#else
+#define DFC_API
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes.                                                             */
+/* ------------------------------------------------------------------------ */
+typedef enum dfc_status {
+  DFC_OK = 0,
+  /* Rejected before anything was submitted (contract: "Raises for
+   * unsupported work before submitting anything",
+   * docs/design/accelerator-contract.md:28). */
+  DFC_UNSUPPORTED = 1,
+  /* Malformed arguments (null pointers, mismatched row counts, ...). */
+  DFC_INVALID = 2,
+  /* A checked integer sum does not fit its result type; dfc_last_error()
+   * holds the CPU provider's message. */
+  DFC_DATA_OVERFLOW = 3,
+  /* A value-dependent result the CPU must adjudicate (the reference's data
+   * fault, dataframe_metal/accelerator/faults.mojo:1-18). */
+  DFC_DATA_FAULT = 4,
+  /* The group table could not grow far enough (after the bounded retries). */
+  DFC_CAPACITY = 5,
+  /* Device memory could not be allocated. */
+  DFC_OOM = 6,
+  /* A bounded device wait gave up. */
+  DFC_TIMEOUT = 7,
+  /* A CUDA call failed. */
+  DFC_DEVICE = 8,
+  /* No usable sm_100 device. */
+  DFC_NO_DEVICE = 9
+} dfc_status;
+
+/* ------------------------------------------------------------------------ */
+/* Column types (numeric storage types of dataframe/dtype.mojo).             */
+/* ------------------------------------------------------------------------ */
+typedef enum dfc_dtype {
+  DFC_INT8 = 1,
+  DFC_INT16 = 2,
+  DFC_INT32 = 3,
+  DFC_INT64 = 4,
+  DFC_UINT8 = 5,
+  DFC_UINT16 = 6,
+  DFC_UINT32 = 7, /* also a categorical's dictionary codes */
+  DFC_UINT64 = 8,
+  DFC_FLOAT32 = 9,
+  DFC_FLOAT64 = 10
+} dfc_dtype;
+
+/* ------------------------------------------------------------------------ */
+/* Devices (reference: dataframe/devices.mojo:64-141; provider functions     */
+/* devices() and transfer_model()).  Neither call creates a context.        */
+/* ------------------------------------------------------------------------ */
+typedef struct dfc_device_info {
+  int32_t ordinal;
+  int32_t sm_count;
+  int32_t cc_major;
+  int32_t cc_minor;
+  uint64_t total_bytes;  /* HBM capacity */
+  int64_t budget_bytes;  /* bytes the planner may hold there; -1 = no limit */
+  char name[96];
+} dfc_device_info;
+
+/* Library ABI version (DFC_ABI_VERSION).  Mirrors the version probe of the
+ * reference's native shim (native/dfparquet/dfparquet.sym). */
+DFC_API uint32_t dfc_version(void);
+
+/* Whether this library can run here: built for sm_100a and an NVIDIA device
+ * node is present.  Opens no driver and creates no context (provider
+ * installed(), dataframe/_accel_provider.mojo:11;
+ * docs/design/accelerator-contract.md:27). */
+DFC_API int32_t dfc_installed(void);
+
+/* Number of sm_100 devices; reads driver metadata only (provider devices(),
+ * docs/design/accelerator-contract.md:40). */
+DFC_API int32_t dfc_device_count(void);
+DFC_API dfc_status dfc_device_info_get(int32_t ordinal, dfc_device_info* out);
+
+/* ------------------------------------------------------------------------ */
+/* Device column handoff: typed values plus an Arrow LSB-first validity     */
+/* bitmap, resident in HBM across queries.                                  */
+/* Reference: Column[T] = value buffer + validity bits + offset window,     */
+/* dataframe/storage/column.mojo:1-32, dataframe/storage/bitmap.mojo:1-76;  */
+/* device residence: dataframe/storage/residence.mojo:20-72.                */
+/* ------------------------------------------------------------------------ */
+typedef struct dfc_column dfc_column;
+
+/* values/validity point to host memory: the library copies them into HBM
+ * (validity normalised to bit offset 0) and keeps them resident. */
+#define DFC_COLUMN_HOST 0u
+/* values points to device memory the caller owns and keeps alive until
+ * dfc_column_release; only the validity bitmap is copied (normalised). */
+#define DFC_COLUMN_DEVICE 1u
+
+/* validity may be NULL (every row valid).  validity_bit_offset is the bit
+ * of row 0 inside validity (an Arrow window's offset). */
+DFC_API dfc_status dfc_column_register(int32_t device, dfc_dtype dtype,
+                                       uint64_t rows, const void* values,
+                                       const uint8_t* validity,
+                                       uint64_t validity_bit_offset,
+                                       uint32_t flags, dfc_column** out);
+DFC_API dfc_status dfc_column_release(dfc_column* column);
+DFC_API uint64_t dfc_column_rows(const dfc_column* column);
+DFC_API int32_t dfc_column_null_count(const dfc_column* column);
+
+/* ------------------------------------------------------------------------ */
+/* The query: a bound SCAN -> FILTER* -> AGG region                          */
+/* (dataframe/query_execution/placement.mojo:74-94).                        */
+/* ------------------------------------------------------------------------ */
+
+/* Predicate program, postfix.  Comparisons follow IEEE rules for floats
+ * (NaN compares false except !=) and a null operand makes the comparison
+ * null; AND/OR/NOT are Kleene; a row is kept only when the program is true
+ * (dataframe/kernels/fused_compare.mojo:31-183; kernels/binary.mojo:2172). */
+typedef enum dfc_pred_kind {
+  DFC_PRED_CMP = 1,         /* inputs[column] <cmp> literal */
+  DFC_PRED_IS_NULL = 2,     /* inputs[column] is null */
+  DFC_PRED_IS_NOT_NULL = 3, /* inputs[column] is not null */
+  DFC_PRED_AND = 4,
+  DFC_PRED_OR = 5,
+  DFC_PRED_NOT = 6,
+  DFC_PRED_TRUE = 7
+} dfc_pred_kind;
+
+typedef enum dfc_cmp { DFC_LT = 1, DFC_LE = 2, DFC_GT = 3, DFC_GE = 4, DFC_EQ = 5, DFC_NE = 6 } dfc_cmp;
+
+/* The literal is already bound to the column's type (binding happens in the
+ * core before a backend is chosen, docs/design/accelerator-contract.md:75):
+ * integer columns read lit.i (signed) or lit.u (UINT64), float columns lit.f. */
+typedef struct dfc_pred_op {
+  int32_t kind;   /* dfc_pred_kind */
+  int32_t column; /* index into dfc_query.inputs (CMP / IS_NULL / IS_NOT_NULL) */
+  int32_t cmp;    /* dfc_cmp (CMP) */
+  int32_t reserved;
+  union {
+    int64_t i;
+    uint64_t u;
+    double f;
+  } lit;
+} dfc_pred_op;
+
+/* Aggregations (dataframe/expr.mojo reduction ops; state kinds
+ * dataframe/aggregation/function.mojo:187-254). */
+typedef enum dfc_agg_op {
+  DFC_AGG_COUNT = 1,      /* valid values, Int64, never null */
+  DFC_AGG_SUM = 2,        /* sum type of the input; null when count < min_count */
+  DFC_AGG_MEAN = 3,       /* Float64; null when count == 0 */
+  DFC_AGG_MIN = 4,        /* input type; NaN only when every valid value is NaN */
+  DFC_AGG_MAX = 5,
+  DFC_AGG_VAR = 6,        /* Float64, M2 / (n - ddof); null when n <= ddof */
+  DFC_AGG_STD = 7,
+  DFC_AGG_LEN = 8,        /* rows of the group, Int64 */
+  DFC_AGG_NULL_COUNT = 9  /* null values, Int64 */
+} dfc_agg_op;
+
+typedef struct dfc_agg {
+  int32_t op;        /* dfc_agg_op */
+  int32_t column;    /* index into dfc_query.inputs */
+  int32_t ddof;      /* VAR / STD (reference default 1, dataframe/expr.mojo:2904-2910) */
+  int32_t min_count; /* SUM (reference default 0) */
+} dfc_agg;
+
+/* Query flags. */
+#define DFC_Q_MAINTAIN_ORDER 1u    /* groups in first-occurrence order of the rows the filter kept */
+#define DFC_Q_FORCE_GLOBAL 2u      /* skip the shared-memory table regime */
+#define DFC_Q_FORCE_SHARED 4u      /* use the shared-memory table regime regardless of estimates */
+#define DFC_Q_FLOAT32_FP64 8u      /* Float32 values: plain FP64 accumulation instead of compensated FP32 */
+
+typedef struct dfc_query {
+  uint32_t abi_version; /* DFC_ABI_VERSION */
+  uint32_t flags;       /* DFC_Q_* */
+  int32_t n_inputs;     /* columns the query reads; all have the same row count */
+  int32_t n_keys;       /* 1..4 */
+  dfc_column* const* inputs;
+  const int32_t* keys;  /* n_keys indices into inputs */
+  int32_t n_pred;       /* 0 keeps every row */
+  int32_t n_aggs;       /* 0..32 */
+  const dfc_pred_op* pred;
+  const dfc_agg* aggs;
+  void* stream;         /* cudaStream_t, or NULL for the library's per-thread stream */
+} dfc_query;
+
+/* ------------------------------------------------------------------------ */
+/* Results: n_keys key columns then one column per aggregation, resident    */
+/* on the device until dfc_result_free.                                     */
+/* ------------------------------------------------------------------------ */
+typedef struct dfc_result dfc_result;
+
+/* Runs the query and waits for it.  On DFC_OK *out holds the result.
+ * Provider execute()/handoff_execute() (docs/design/accelerator-contract.md:
+ * 28, 32) reduce to this call. */
+DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out);
+
+DFC_API uint64_t dfc_result_rows(const dfc_result* result);
+DFC_API int32_t dfc_result_columns(const dfc_result* result);
+/* Device pointers of column i; *device_validity is NULL when the column has
+ * no nulls. */
+DFC_API dfc_status dfc_result_column(const dfc_result* result, int32_t i, dfc_dtype* dtype,
+                                     const void** device_values,
+                                     const uint8_t** device_validity);
+/* Copies column i to host memory: values (rows * size of dtype bytes) and,
+ * when validity is not NULL, an LSB-first bitmap of ceil(rows / 8) bytes
+ * (all ones when the column has no nulls). */
+DFC_API dfc_status dfc_result_copy_to_host(const dfc_result* result, int32_t i, void* values,
+                                           uint8_t* validity);
+DFC_API void dfc_result_free(dfc_result* result);
+
+/* Residence callbacks in the shape of the reference's _DeviceResidence
+ * (dataframe/storage/residence.mojo:20-22): ctx is a dfc_result column
+ * handle made by dfc_result_residence(result, i). to_host returns 0 on
+ * success; release frees the handle (the result keeps its own reference). */
+DFC_API void* dfc_result_residence(dfc_result* result, int32_t i);
+DFC_API int32_t dfc_residence_to_host(void* ctx, void* host_dst, int64_t bytes);
+DFC_API void dfc_residence_release(void* ctx);
+
+/* Per-phase device timings of the last query on this thread, nanoseconds
+ * (the provider's report frame; dataframe/execution_observation.mojo:6-83). */
+typedef struct dfc_timings {
+  double scan_ns;
+  double finish_ns;
+  double total_ns;
+  uint64_t groups;
+  uint64_t table_slots;
+  int32_t regime;   /* 0 global table, 1 shared-memory tables */
+  int32_t retries;  /* capacity regrowths */
+  int32_t launches; /* kernels this library launched for the query */
+  int32_t reserved;
+} dfc_timings;
+DFC_API dfc_status dfc_last_timings(dfc_timings* out);
+
+/* Makes `stream` (a cudaStream_t; NULL restores the library's own) the
+ * stream this thread's calls on `device` use when they are not given one:
+ * column registration, queries without dfc_query.stream, result copies. */
+DFC_API dfc_status dfc_set_thread_stream(int32_t device, void* stream);
+
+/* Text of the last failing call on this thread ("" when none). */
+DFC_API const char* dfc_last_error(void);
+DFC_API const char* dfc_status_name(dfc_status status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DFCUDA_H */

@@ -1,0 +1,83 @@
+// column.cu — device side of the column handoff: validity normalisation and
+// value ranges of resident columns.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dfc_device.cuh"
+#include "dfc_internal.h"
+#include "kernels.h"
+
+namespace dfc {
+
+// Normalises an Arrow LSB-first bitmap window starting at bit `off` into
+// 32-bit words from bit 0 (bits past `rows` cleared) and counts valid rows.
+// `nbytes` bounds the source: ceil((off + rows) / 8).
+__global__ void normalize_validity(const uint8_t* src, uint64_t nbytes, uint64_t off, uint64_t rows, uint32_t* dst,
+                                   unsigned long long* valid_rows) {
+  const uint64_t words = (rows + 31) / 32;
+  unsigned long long local = 0;
+  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < words; w += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t bit = off + w * 32;
+    const uint64_t b0 = bit >> 3;
+    uint64_t window = 0;
+    for (int k = 0; k < 5; ++k)
+      if (b0 + k < nbytes) window |= (uint64_t)src[b0 + k] << (8 * k);
+    uint32_t out = (uint32_t)(window >> (bit & 7));
+    const uint64_t left = rows - w * 32;
+    if (left < 32) out &= (1u << left) - 1u;
+    dst[w] = out;
+    local += __popc(out);
+  }
+  for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(valid_rows, local);
+}
+
+// Order-encoded minimum and maximum of the valid values of a column
+// (out[0] = min, out[1] = max; NaN skipped).  Bounds a key's domain when the
+// planner sizes the group table.
+__global__ void column_minmax(DevColumn c, uint64_t rows, unsigned long long* out) {
+  unsigned long long lo = ~0ull, hi = 0ull;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < rows; i += (uint64_t)gridDim.x * blockDim.x) {
+    if (c.validity && !bit_valid(c.validity, i)) continue;
+    const uint64_t b = load_bits(c.values, c.size, i);
+    if (dt_float(c.dtype)) {
+      const double d = bits_to_f64(b, c.dtype);
+      if (d != d) continue;
+    }
+    const uint64_t e = order_encode(b, c.dtype);
+    lo = e < lo ? e : lo;
+    hi = e > hi ? e : hi;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long a = __shfl_xor_sync(0xffffffffu, lo, o);
+    const unsigned long long b = __shfl_xor_sync(0xffffffffu, hi, o);
+    lo = a < lo ? a : lo;
+    hi = b > hi ? b : hi;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&out[0], lo);
+    atomicMax(&out[1], hi);
+  }
+}
+
+// HyperLogLog sketch (2^kHllBits registers) of a column's distinct valid
+// values under group equality (floats canonical).  Each block keeps its
+// registers in shared memory and merges them into `regs` with atomicMax.
+__global__ void column_hll(DevColumn c, uint64_t rows, uint32_t* regs) {
+  __shared__ uint32_t local[1u << kHllBits];
+  for (uint32_t i = threadIdx.x; i < (1u << kHllBits); i += blockDim.x) local[i] = 0;
+  __syncthreads();
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < rows; i += (uint64_t)gridDim.x * blockDim.x) {
+    if (c.validity && !bit_valid(c.validity, i)) continue;
+    const uint64_t h = mix64(key_cell(load_bits(c.values, c.size, i), c.dtype) ^ 0xD6E8FEB86659FD93ull);
+    const uint32_t reg = (uint32_t)(h >> (64 - kHllBits));
+    const uint64_t rest = h << kHllBits;
+    const uint32_t rho = rest == 0 ? (65 - kHllBits) : (uint32_t)__clzll(rest) + 1;
+    if (rho > local[reg]) atomicMax(&local[reg], rho);
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < (1u << kHllBits); i += blockDim.x)
+    if (local[i]) atomicMax(&regs[i], local[i]);
+}
+
+}  // namespace dfc

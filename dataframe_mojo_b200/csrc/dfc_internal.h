@@ -13,7 +13,7 @@
 
 #include <stdint.h>
 
-#include "../../include/dfcuda.h"
+#include "dfcuda.h"
 
 namespace dfc {
 
@@ -26,31 +26,34 @@ constexpr int kMaxOut = kMaxKeys + kMaxAggs;
 constexpr int kMaxRecWords = 64;  // 512-byte records at most
 
 constexpr uint64_t kEmpty = ~0ull;
-constexpr uint32_t kNoRow = 0xFFFFFFFFu;
-// Shift K of the shifted second moment before any value set it: a signalling
-// NaN payload; data NaNs are stored canonical (0x7FF8...) so they never match.
-constexpr uint64_t kShiftUnset = 0x7FF40000000D0FC5ull;
+// The shift K of the shifted second moment is stored xor this tag, so an
+// all-zero record means "unset".  The tag is a signalling-NaN payload; data
+// NaNs are stored canonical (0x7FF8...), so no value stores as zero.
+constexpr uint64_t kShiftTag = 0x7FF40000000D0FC5ull;
 constexpr uint64_t kCanonNaN = 0x7FF8000000000000ull;
 
 // Status bits raised by kernels.
 enum StatusBits : uint32_t {
-  ST_CAPACITY = 1u,   // a CTA ran out of records or a probe wrapped
-  ST_TIMEOUT = 2u,    // a bounded wait gave up
-  ST_OVERFLOW = 4u,   // a checked integer sum does not fit
-  ST_FAULT = 8u,      // ill-conditioned moments: CPU adjudicates
+  ST_CAPACITY = 1u,    // records or table slots ran out
+  ST_TIMEOUT = 2u,     // a bounded wait gave up
+  ST_OVERFLOW = 4u,    // a checked integer sum does not fit
+  ST_FAULT = 8u,       // ill-conditioned moments: the CPU adjudicates
+  ST_ZERO_FAULT = 16u, // a zero extremum seen with both signs: the CPU adjudicates
 };
 
 enum KeyMode : int32_t { KEY_PACKED = 0, KEY_TICKET = 1 };
 
 enum SumKind : int32_t { SUM_NONE = 0, SUM_I64 = 1, SUM_I128 = 2, SUM_F64 = 3 };
 
-// Record header (bytes).
+// Group record (bytes).  Every field's identity is zero, so records are
+// initialised by a memset: first row stored as ~row and the minimum as ~code
+// (both raised by atomicMax), the maximum as its code, K xor kShiftTag.
+// Value fields follow the header: u32 length and counts, then per aggregated
+// column the read-set (K, min, max) and the sums.
 constexpr int kRecKey = 0;    // u64 key word (packed key or 64-bit hash)
-constexpr int kRecFirst = 8;  // u32 first row (claim row until updated)
-constexpr int kRecFlags = 12; // u32 per-value NaN-seen bits
-constexpr int kRecLen = 16;   // u32 rows of the group
-constexpr int kRecClaim = 20; // u32 row that claimed the group
-constexpr int kRecHeader = 24;
+constexpr int kRecFirst = 8;  // u32 ~first row; 0 = a hole (reserved, never claimed)
+constexpr int kRecFlags = 12; // u32, per value column v: bit 3v NaN seen, 3v+1 +0 seen, 3v+2 -0 seen
+constexpr int kRecHeader = 16;
 
 struct DevColumn {
   const void* values;
@@ -76,11 +79,8 @@ struct ValField {
   int32_t off_sum;    // i64 / i128 (lo, hi) / f64, -1 absent
   int32_t off_min;    // u64 order-preserving encoding, -1 absent
   int32_t off_max;
-  int32_t off_zero;   // u64 (row << 1 | sign) of the first zero, float min/max only
   int32_t off_m2;     // f64 sum of (x - K)^2, -1 absent
-  int32_t off_shift;  // f64 K
-  int32_t nan_bit;    // bit in the record flags
-  int32_t pad;
+  int32_t off_shift;  // f64 K, the first value the group saw
 };
 
 struct PredOp {
@@ -105,7 +105,6 @@ struct ScanParams {
   int32_t n_cols;
   // Columns staged per tile: values at stage_off, validity words at stage_voff.
   int32_t n_stage;
-  int32_t stage_col[kMaxInputs];
   int32_t stage_off[kMaxInputs];
   int32_t stage_voff[kMaxInputs];  // -1: no validity
   int32_t stage_bytes;  // ring stride (128-byte aligned)
@@ -128,11 +127,16 @@ struct ScanParams {
   int32_t n_vals;
   int32_t rec_stride;
   ValField vals[kMaxVals];
-  int32_t track_first;  // maintain_order: first row by atomic min
-  int32_t track_len;
+  // Shared-memory regime: CTA key table (smem_slots, power of two; 0 = off)
+  // and records at these byte offsets of the dynamic shared memory.
+  uint32_t smem_slots;
+  uint32_t smem_keys_off;
+  uint32_t smem_recs_off;
+  uint32_t pad2;
+  int32_t track_first;  // maintain_order: first row lowered by atomic min
+  int32_t off_len;      // u32 rows of the group, -1 absent
   int32_t rec_words;    // stride / 8
   int32_t pad1;
-  unsigned long long rec_template[kMaxRecWords];
   // Tables.
   KeyEntry* table;
   uint64_t table_mask;

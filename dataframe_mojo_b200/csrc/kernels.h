@@ -5,6 +5,7 @@
 
 namespace dfc {
 
+constexpr int kScanRowsPerThread = 4;  // rows each consumer thread holds in flight
 constexpr int kScanConsumerWarps = 8;
 constexpr int kScanConsumerThreads = kScanConsumerWarps * 32;
 constexpr int kScanThreads = kScanConsumerThreads + 32;  // + one producer warp
@@ -25,4 +26,6 @@ namespace dfc {
 __global__ void normalize_validity(const uint8_t* src, uint64_t nbytes, uint64_t off, uint64_t rows, uint32_t* dst,
                                    unsigned long long* valid_rows);
 __global__ void column_minmax(DevColumn c, uint64_t rows, unsigned long long* out);
+constexpr int kHllBits = 12;
+__global__ void column_hll(DevColumn c, uint64_t rows, uint32_t* regs);
 }  // namespace dfc

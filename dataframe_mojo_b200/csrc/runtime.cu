@@ -24,7 +24,7 @@
 #include <unordered_map>
 #include <vector>
 
-#include "../../include/dfcuda.h"
+#include "dfcuda.h"
 #include "dfc_internal.h"
 #include "kernels.h"
 
@@ -38,8 +38,11 @@ struct dfc_column {
   bool owns_values = false;
   uint32_t* validity = nullptr;  // device, normalised; nullptr when no row is null
   uint64_t null_count = 0;
-  uint64_t min_enc = ~0ull, max_enc = 0;  // order-encoded value range (integers)
-  bool have_range = false;
+  // Statistics, computed the first time the column is a key: order-encoded
+  // value range and a HyperLogLog estimate of its distinct valid values.
+  bool have_stats = false;
+  uint64_t min_enc = ~0ull, max_enc = 0;
+  double distinct = 0;
 };
 
 struct ResultCol {
@@ -397,9 +400,18 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
       default: break;
     }
   }
+  // Group record: header, u32 length and counts, then per column the
+  // read-set (K, min, max: read before the atomics that may improve them)
+  // and the sums.  The common single-column float record (count, sum, K,
+  // min, max, S2) is exactly 64 bytes: one pair of 32-byte sectors.
   sp.n_vals = (int)needs.size();
   int off = kRecHeader;
-  for (int j = 0; j < sp.n_vals; ++j) {  // counts first (u32 each)
+  sp.off_len = -1;
+  if (track_len) {
+    sp.off_len = off;
+    off += 4;
+  }
+  for (int j = 0; j < sp.n_vals; ++j) {
     ValField& f = sp.vals[j];
     f.input = use(needs[j].input);
     f.dtype = q->inputs[needs[j].input]->dtype;
@@ -411,9 +423,11 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
     ValField& f = sp.vals[j];
     const Need& n = needs[j];
     const int sz = dtype_size(f.dtype);
-    f.nan_bit = j;
     f.sum_kind = SUM_NONE;
-    f.off_sum = f.off_min = f.off_max = f.off_zero = f.off_m2 = f.off_shift = -1;
+    f.off_sum = f.off_min = f.off_max = f.off_m2 = f.off_shift = -1;
+    if (n.m2) { f.off_shift = off; off += 8; }
+    if (n.mn) { f.off_min = off; off += 8; }
+    if (n.mx) { f.off_max = off; off += 8; }
     if (n.sum) {
       if (is_float(f.dtype)) f.sum_kind = SUM_F64;
       else if (sz <= 2 || (sz == 4 && P.rows < (1ull << 31))) f.sum_kind = SUM_I64;
@@ -422,32 +436,12 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
       f.off_sum = off;
       off += f.sum_kind == SUM_I128 ? 16 : 8;
     }
-    if (n.mn) { f.off_min = off; off += 8; }
-    if (n.mx) { f.off_max = off; off += 8; }
-    if ((n.mn || n.mx) && is_float(f.dtype)) { f.off_zero = off; off += 8; }
-    if (n.m2) {
-      f.off_m2 = off; off += 8;
-      f.off_shift = off; off += 8;
-    }
+    if (n.m2) { f.off_m2 = off; off += 8; }
   }
   sp.rec_stride = (off + 15) & ~15;
   if (sp.rec_stride > kMaxRecWords * 8) return fail(DFC_UNSUPPORTED, "group record too wide");
   sp.rec_words = sp.rec_stride / 8;
-  sp.track_first = 1;  // groups are always emitted in first-row order
-  sp.track_len = track_len ? 1 : 0;
-  // Identity record.
-  std::vector<uint8_t> tpl(sp.rec_stride, 0);
-  auto put64 = [&](int o, uint64_t v) { memcpy(tpl.data() + o, &v, 8); };
-  auto put32 = [&](int o, uint32_t v) { memcpy(tpl.data() + o, &v, 4); };
-  put32(kRecFirst, kNoRow);
-  for (int j = 0; j < sp.n_vals; ++j) {
-    const ValField& f = sp.vals[j];
-    if (f.off_min >= 0) put64(f.off_min, ~0ull);
-    if (f.off_max >= 0) put64(f.off_max, 0ull);
-    if (f.off_zero >= 0) put64(f.off_zero, ~0ull);
-    if (f.off_shift >= 0) put64(f.off_shift, kShiftUnset);
-  }
-  memcpy(sp.rec_template, tpl.data(), sp.rec_stride);
+  sp.track_first = (q->flags & DFC_Q_MAINTAIN_ORDER) ? 1 : 0;
 
   // Output columns: keys, then one per aggregation.
   FinishParams& fp = P.fp;
@@ -524,7 +518,56 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
 
 // Estimated number of groups: what the last query on these keys found, else
 // the product of the key columns' value ranges, capped by the row count.
-uint64_t estimate_groups(const dfc_query* q, const Plan& P) {
+// Column statistics, computed once per column on its first use as a key.
+std::mutex g_stats_mu;
+
+dfc_status ensure_stats(dfc_column* c, DeviceState* ds, cudaStream_t stream) {
+  std::lock_guard<std::mutex> lk(g_stats_mu);
+  if (c->have_stats || c->rows == 0) return DFC_OK;
+  const uint32_t nreg = 1u << kHllBits;
+  unsigned long long* d_mm = nullptr;
+  uint32_t* d_regs = nullptr;
+  unsigned long long h_mm[2] = {~0ull, 0ull};
+  std::vector<uint32_t> regs(nreg);
+  cudaError_t e = cudaMallocAsync((void**)&d_mm, 16, stream);
+  if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_regs, nreg * 4, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_mm, h_mm, 16, cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_regs, 0, nreg * 4, stream);
+  if (e == cudaSuccess) {
+    DevColumn dc{c->values, c->validity, c->dtype, dtype_size(c->dtype)};
+    const unsigned blocks = (unsigned)std::min<uint64_t>((c->rows + 255) / 256, (uint64_t)ds->sms * 4);
+    column_minmax<<<std::max(1u, blocks), 256, 0, stream>>>(dc, c->rows, d_mm);
+    column_hll<<<std::max(1u, blocks), 256, 0, stream>>>(dc, c->rows, d_regs);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h_mm, d_mm, 16, cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(regs.data(), d_regs, nreg * 4, cudaMemcpyDeviceToHost, stream);
+  if (d_mm) cudaFreeAsync(d_mm, stream);
+  if (d_regs) cudaFreeAsync(d_regs, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return cuda_fail(e, "column statistics");
+  // HyperLogLog estimate (Flajolet et al. 2007) with the linear-counting
+  // correction for small cardinalities.
+  double sum = 0;
+  int zeros = 0;
+  for (uint32_t r : regs) {
+    sum += std::ldexp(1.0, -(int)r);
+    zeros += r == 0;
+  }
+  const double m = nreg, alpha = 0.7213 / (1.0 + 1.079 / m);
+  double est = alpha * m * m / sum;
+  if (est <= 2.5 * m && zeros > 0) est = m * std::log(m / zeros);
+  c->min_enc = h_mm[0];
+  c->max_enc = h_mm[1];
+  c->distinct = est;
+  c->have_stats = true;
+  return DFC_OK;
+}
+
+// Estimated number of groups: what the last query on these keys found, else
+// the product of the key columns' distinct estimates (capped by their value
+// ranges), capped by the row count.
+uint64_t estimate_groups(const dfc_query* q, const Plan& P, DeviceState* ds, cudaStream_t stream) {
   {
     std::lock_guard<std::mutex> lk(g_learn_mu);
     auto it = g_learned.find(P.key_sig);
@@ -532,11 +575,15 @@ uint64_t estimate_groups(const dfc_query* q, const Plan& P) {
   }
   double prod = 1.0;
   for (int k = 0; k < q->n_keys; ++k) {
-    const dfc_column* c = q->inputs[q->keys[k]];
+    dfc_column* c = q->inputs[q->keys[k]];
     double d = (double)c->rows;
-    if (c->have_range && !is_float(c->dtype)) {
-      __int128 span = order_value(c->max_enc, c->dtype) - order_value(c->min_enc, c->dtype) + 1;
-      if (span > 0 && (double)span < d) d = (double)span;
+    if (ensure_stats(c, ds, stream) == DFC_OK && c->have_stats) {
+      // HyperLogLog's standard error at 4096 registers is ~1.6%: keep a margin.
+      d = std::min(d, c->distinct * 1.1 + 16);
+      if (!is_float(c->dtype) && c->min_enc <= c->max_enc) {
+        const __int128 span = order_value(c->max_enc, c->dtype) - order_value(c->min_enc, c->dtype) + 1;
+        if (span > 0 && (double)span < d) d = (double)span;
+      }
     }
     if (c->validity) d += 1;
     prod *= d;
@@ -593,7 +640,8 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   const uint64_t groups_cap = std::min<uint64_t>(P.rows, slots / 2);
   uint64_t chunk = 64;
   while (chunk < 1024 && chunk * ncta * 8 < groups_cap) chunk <<= 1;
-  const uint64_t recs = groups_cap + chunk * ncta;
+  // Slack for holes: records reserved by claims that lost a race.
+  const uint64_t recs = groups_cap + groups_cap / 8 + chunk * ncta;
   if (recs >= 0xFFFFFFFFull) return fail(DFC_CAPACITY, "group capacity exceeds 2^32 records");
 
   void *table, *records, *ctl, *bits, *prefix, *bsums, *perm;
@@ -634,6 +682,8 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
 
   Control* dctl = static_cast<Control*>(ctl);
   cudaError_t e = cudaMemsetAsync(table, 0xFF, (slots + 1) * sizeof(KeyEntry), stream);
+  // Group records start all-zero: every field's identity (dfc_internal.h).
+  if (e == cudaSuccess) e = cudaMemsetAsync(records, 0, recs * sp.rec_stride, stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(ctl, 0, sizeof(Control), stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(&dctl->overflow_agg, 0xFF, 4, stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(bits, 0, words * 4 + 16, stream);
@@ -725,6 +775,10 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
     free_outputs();
     return fail(DFC_DATA_FAULT,
                 "Mojo GPU data fault: variance of a group whose mean is far from its spread; the CPU adjudicates");
+  }
+  if (status & ST_ZERO_FAULT) {
+    free_outputs();
+    return fail(DFC_DATA_FAULT, "Mojo GPU data fault: mixed signed-zero extrema; the CPU adjudicates");
   }
   auto* r = new dfc_result();
   r->device = P.device;
@@ -860,29 +914,8 @@ DFC_API dfc_status dfc_column_register(int32_t device, dfc_dtype dtype, uint64_t
       c->validity = nullptr;
     }
   }
-  // Value range of integer columns (bounds a key's domain for table sizing).
-  if (!is_float(dtype) && rows > 0) {
-    unsigned long long* d_mm = nullptr;
-    unsigned long long h_mm[2] = {~0ull, 0ull};
-    cudaError_t e = cudaMallocAsync((void**)&d_mm, 16, stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_mm, h_mm, 16, cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess) {
-      DevColumn dc{c->values, c->validity, dtype, sz};
-      unsigned blocks = (unsigned)std::min<uint64_t>((rows + 255) / 256, (uint64_t)ds->sms * 8);
-      column_minmax<<<std::max(1u, blocks), 256, 0, stream>>>(dc, rows, d_mm);
-      e = cudaGetLastError();
-    }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h_mm, d_mm, 16, cudaMemcpyDeviceToHost, stream);
-    if (d_mm) cudaFreeAsync(d_mm, stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    if (e != cudaSuccess) return bail(cuda_fail(e, "column statistics"));
-    c->min_enc = h_mm[0];
-    c->max_enc = h_mm[1];
-    c->have_range = h_mm[0] <= h_mm[1];
-  } else {
-    cudaError_t e = cudaStreamSynchronize(stream);
-    if (e != cudaSuccess) return bail(cuda_fail(e, "column upload"));
-  }
+  cudaError_t e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "column upload"));
   *out = c;
   return DFC_OK;
 }
@@ -919,7 +952,25 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
   cudaStream_t stream = query->stream ? static_cast<cudaStream_t>(query->stream) : thread_stream(P.device);
   thread_local Control* host_ctl = nullptr;
   if (!host_ctl) CK(cudaMallocHost((void**)&host_ctl, sizeof(Control)), "pinned control block");
-  uint64_t est = estimate_groups(query, P);
+  uint64_t est = estimate_groups(query, P, ds, stream);
+  // Regime: per-CTA shared-memory tables when the estimated groups fit in
+  // shared memory at load <= 1/2 (two CTAs per SM if possible, else one);
+  // otherwise the global table alone.  Rows whose key finds no room in a CTA
+  // table take the global path, so a low estimate costs speed, not results.
+  P.sp.smem_slots = 0;
+  if (!(query->flags & DFC_Q_FORCE_GLOBAL) && P.sp.key_mode == KEY_PACKED &&
+      ((query->flags & DFC_Q_FORCE_SHARED) || est <= 4096)) {
+    const uint64_t sslots = next_pow2(std::max<uint64_t>(64, std::min<uint64_t>(est, 4096) * 2));
+    const size_t keys_off = (P.smem + 15) & ~(size_t)15;
+    const size_t recs_off = (keys_off + sslots * 8 + 15) & ~(size_t)15;
+    const size_t total = recs_off + sslots * (size_t)P.sp.rec_stride;
+    if (total + 1024 <= ds->smem_optin) {
+      P.sp.smem_slots = (uint32_t)sslots;
+      P.sp.smem_keys_off = (uint32_t)keys_off;
+      P.sp.smem_recs_off = (uint32_t)recs_off;
+      P.smem = total;
+    }
+  }
   uint64_t slots = next_pow2(std::max<uint64_t>(1024, est * 2));
   const uint64_t max_slots = next_pow2(std::max<uint64_t>(1024, P.rows * 2));
   slots = std::min(slots, max_slots);
@@ -935,7 +986,7 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
   if (st) return st;
   learn_groups(P, (*out)->rows);
   t_timings.groups = (*out)->rows;
-  t_timings.regime = 0;
+  t_timings.regime = P.sp.smem_slots ? 1 : 0;
   t_timings.total_ns = std::chrono::duration<double, std::nano>(std::chrono::steady_clock::now() - t0).count();
   return DFC_OK;
 }

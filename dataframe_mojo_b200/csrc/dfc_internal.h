@@ -168,6 +168,7 @@ struct FinishParams {
   uint32_t* word_prefix;   // exclusive popcount prefix per 32-bit word
   uint32_t* block_sums;    // scratch of the prefix scan
   uint32_t* perm;          // rank -> gid
+  uint32_t* firsts;        // first row per record (~0: hole)
   uint32_t* groups;        // [0] number of groups
   uint32_t* has_nulls;     // per output column
   uint32_t* overflow_agg;  // [0] lowest aggregation index that overflowed

@@ -32,12 +32,17 @@ __device__ __forceinline__ bool live_record(const ScanParams& p, uint64_t i, uin
   return enc != 0;
 }
 
+// Marks each live record's first row in the bitmap and keeps the first rows
+// densely (firsts[i], ~0 for a hole) so the rank pass reads 4 bytes per
+// record instead of a record sector.
 __global__ void finish_mark(const __grid_constant__ FinishParams f) {
   const ScanParams& p = f.scan;
   const uint64_t n = records_handed_out(p);
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     uint32_t first;
-    if (live_record(p, i, first)) atomicOr(&f.order_bits[first >> 5], 1u << (first & 31));
+    const bool live = live_record(p, i, first);
+    f.firsts[i] = live ? first : 0xFFFFFFFFu;
+    if (live) atomicOr(&f.order_bits[first >> 5], 1u << (first & 31));
   }
 }
 
@@ -117,8 +122,8 @@ __global__ void finish_rank(const __grid_constant__ FinishParams f) {
   const ScanParams& p = f.scan;
   const uint64_t n = records_handed_out(p);
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t first;
-    if (!live_record(p, i, first)) continue;
+    const uint32_t first = f.firsts[i];
+    if (first == 0xFFFFFFFFu) continue;
     const uint32_t w = first >> 5;
     const uint32_t rank = f.word_prefix[w] + __popc(f.order_bits[w] & ((1u << (first & 31)) - 1u));
     f.perm[rank] = (uint32_t)i;

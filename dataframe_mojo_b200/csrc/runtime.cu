@@ -154,7 +154,11 @@ dfc_status device_ready(int dev, DeviceState** out) {
     CK(cudaDeviceGetDefaultMemPool(&pool, dev), "cudaDeviceGetDefaultMemPool");
     uint64_t threshold = UINT64_MAX;
     CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold), "cudaMemPoolSetAttribute");
-    CK(cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin - 1024),
+    // Dynamic shared memory may use what the kernel's static buffers leave.
+    cudaFuncAttributes fa;
+    CK(cudaFuncGetAttributes(&fa, scan_kernel), "cudaFuncGetAttributes");
+    d.smem_optin = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;
+    CK(cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin),
        "cudaFuncSetAttribute");
     d.ready = true;
   }
@@ -644,7 +648,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   const uint64_t recs = groups_cap + groups_cap / 8 + chunk * ncta;
   if (recs >= 0xFFFFFFFFull) return fail(DFC_CAPACITY, "group capacity exceeds 2^32 records");
 
-  void *table, *records, *ctl, *bits, *prefix, *bsums, *perm;
+  void *table, *records, *ctl, *bits, *prefix, *bsums, *perm, *firsts;
   const uint64_t words = (P.rows + 31) / 32;
   const uint64_t chunks = std::max<uint64_t>(1, (words + kFinishChunk - 1) / kFinishChunk);
   dfc_status st;
@@ -655,6 +659,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   if ((st = S.alloc(&prefix, words * 4 + 16, "order prefix"))) return S.release(), st;
   if ((st = S.alloc(&bsums, chunks * 4, "prefix chunks"))) return S.release(), st;
   if ((st = S.alloc(&perm, recs * 4, "group permutation"))) return S.release(), st;
+  if ((st = S.alloc(&firsts, recs * 4, "first rows"))) return S.release(), st;
   // Output columns sized for the group capacity (the group count is known
   // only on the device; the host reads it once, at the end).
   const uint64_t out_rows = std::min<uint64_t>(P.rows, recs);
@@ -715,6 +720,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   fp.word_prefix = static_cast<uint32_t*>(prefix);
   fp.block_sums = static_cast<uint32_t*>(bsums);
   fp.perm = static_cast<uint32_t*>(perm);
+  fp.firsts = static_cast<uint32_t*>(firsts);
   fp.groups = &dctl->groups;
   fp.has_nulls = dctl->has_nulls;
   fp.overflow_agg = &dctl->overflow_agg;
@@ -964,7 +970,8 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
     const size_t keys_off = (P.smem + 15) & ~(size_t)15;
     const size_t recs_off = (keys_off + sslots * 8 + 15) & ~(size_t)15;
     const size_t total = recs_off + sslots * (size_t)P.sp.rec_stride;
-    if (total + 1024 <= ds->smem_optin) {
+    // smem_optin already excludes the kernel's static shared memory.
+    if (total <= ds->smem_optin) {
       P.sp.smem_slots = (uint32_t)sslots;
       P.sp.smem_keys_off = (uint32_t)keys_off;
       P.sp.smem_recs_off = (uint32_t)recs_off;

@@ -5,18 +5,21 @@
 // `tile_rows` rows it streams each column the query touches (values and
 // validity words) into a ring of shared-memory stages with 1-D TMA bulk
 // copies (cp.async.bulk, no multicast) that complete on mbarriers.  The other
-// warps consume a stage with every thread holding kScanRowsPerThread rows at
-// once, so the rows' independent probes and record reads overlap:
-//   1. the filter program (postfix, Kleene logic) over the thread's rows;
-//   2. the key word (packed key columns, or a 64-bit hash in ticket mode);
-//   3. with few groups, the CTA's shared-memory table: duplicate keys of a
-//      warp collapse with __match_any_sync into one leader update;
-//   4. otherwise one 16-byte probe load per row in the global open-addressing
-//      table; misses resolve in warp-synchronous rounds in which new groups
-//      are claimed by a 128-bit CAS that publishes key and group id together;
-//   5. the group record's read-set (first row, K, min, max), then
-//      fire-and-forget atomics: counts, sums, the shifted square sum; first
-//      row / min / max only when the row improves them.
+// eight warps consume two tiles per step, column at a time:
+//   1. selection: the filter program per row, one warp ballot per 32 rows;
+//   2. compaction: the selected rows' indices, densely, in shared memory, so
+//      every lane of the later phases holds a selected row;
+//   3. keys: each key column packed into the rows' key words (packed mode) or
+//      hashed (ticket mode);
+//   4. groups: with few groups a CTA-local shared-memory table, duplicate keys
+//      of a warp collapsed with __match_any_sync into one leader update;
+//      otherwise the global open-addressing table, probed two entries per
+//      round in warp-synchronous rounds, new groups claimed by a 128-bit CAS
+//      that publishes key and group id together;
+//   5. states: each aggregated column's read-set (first row, K, min, max) for
+//      all rows, then fire-and-forget atomics (counts, sums, the shifted
+//      square sum; first row / min / max only when the row improves them).
+// Type dispatch happens once per column per step, outside the row loops.
 // Group records start all-zero (stream-ordered memset), so a claim needs no
 // initialisation and no fence: first row is stored as ~row, the minimum as
 // ~code (both raised by atomicMax), K xor a tag (0 = unset).
@@ -29,6 +32,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "dfc_device.cuh"
 #include "dfc_internal.h"
 #include "kernels.h"
@@ -38,23 +43,45 @@ namespace dfc {
 constexpr uint32_t kWaitLimit = 1u << 22;  // try_wait polls before a stage wait gives up
 constexpr uint32_t kSpinLimit = 1u << 20;  // re-reads before a publication wait gives up
 constexpr uint32_t kNoGid = 0xFFFFFFFFu;
-constexpr int kR = kScanRowsPerThread;
+constexpr int kR = kScanRowsPerThread;                  // rows a thread holds per pass
+constexpr int kTilesPerStep = 2;                         // tiles a consumer step covers
+constexpr int kMaxTileRows = 1024;
+constexpr int kStepRows = kTilesPerStep * kMaxTileRows;  // compacted rows at most per step
+constexpr int kPassRows = kScanConsumerThreads * kR;     // compacted rows per pass
 
-// Where a tile's data is: a shared-memory stage (staged) or global memory.
-struct Tile {
-  const unsigned char* stage;
-  uint64_t start;
-  bool staged;
-};
-
-__device__ __forceinline__ const unsigned char* col_values(const ScanParams& p, const Tile& t, int c) {
-  return t.staged ? t.stage + p.stage_off[c]
-                  : static_cast<const unsigned char*>(p.cols[c].values) + t.start * (uint64_t)p.cols[c].size;
+// Barrier of the consumer warps only (named barrier 1); returns whether any
+// of them passed `flag`, so every consumer warp takes the same decision.
+__device__ __forceinline__ bool consumer_sync_or(bool flag) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(out)
+      : "r"((uint32_t)flag), "n"(kScanConsumerThreads)
+      : "memory");
+  return out != 0;
 }
 
-__device__ __forceinline__ const uint32_t* col_valid(const ScanParams& p, const Tile& t, int c) {
-  if (t.staged) return p.stage_voff[c] >= 0 ? reinterpret_cast<const uint32_t*>(t.stage + p.stage_voff[c]) : nullptr;
-  return p.cols[c].validity ? p.cols[c].validity + t.start / 32 : nullptr;
+// The tiles of one consumer step: each in a shared-memory stage or, for the
+// ragged last tile, in global memory.
+struct Step {
+  const unsigned char* stage[kTilesPerStep];
+  uint64_t start[kTilesPerStep];
+  bool staged[kTilesPerStep];
+  uint32_t n[kTilesPerStep];  // rows of each tile (0: absent)
+};
+
+__device__ __forceinline__ const unsigned char* col_values(const ScanParams& p, const Step& s, int tile, int c) {
+  return s.staged[tile] ? s.stage[tile] + p.stage_off[c]
+                        : static_cast<const unsigned char*>(p.cols[c].values) + s.start[tile] * (uint64_t)p.cols[c].size;
+}
+
+__device__ __forceinline__ const uint32_t* col_valid(const ScanParams& p, const Step& s, int tile, int c) {
+  if (s.staged[tile])
+    return p.stage_voff[c] >= 0 ? reinterpret_cast<const uint32_t*>(s.stage[tile] + p.stage_voff[c]) : nullptr;
+  return p.cols[c].validity ? p.cols[c].validity + s.start[tile] / 32 : nullptr;
 }
 
 __device__ __forceinline__ bool valid_at(const uint32_t* w, uint32_t r) {
@@ -65,9 +92,43 @@ __device__ __forceinline__ unsigned char* record_at(const ScanParams& p, uint32_
   return p.records + (size_t)gid * (size_t)p.rec_stride;
 }
 
+template <typename T>
+__device__ __forceinline__ T load_as(const unsigned char* base, uint32_t r) {
+  return reinterpret_cast<const T*>(base)[r];
+}
+
+// A row of the step: tile index and row inside the tile.
+struct RowRef {
+  uint32_t tile;
+  uint32_t r;
+  bool on;
+};
+
+// Per-column pointers of the step, resolved once per column.
+struct ColRef {
+  const unsigned char* vals[kTilesPerStep];
+  const uint32_t* valid[kTilesPerStep];
+};
+
+__device__ __forceinline__ ColRef col_ref(const ScanParams& p, const Step& s, int c) {
+  ColRef cr;
+#pragma unroll
+  for (int t = 0; t < kTilesPerStep; ++t) {
+    cr.vals[t] = col_values(p, s, t, c);
+    cr.valid[t] = col_valid(p, s, t, c);
+  }
+  return cr;
+}
+
+__device__ __forceinline__ const unsigned char* rv(const ColRef& cr, const RowRef& x) {
+  return x.tile ? cr.vals[1] : cr.vals[0];
+}
+__device__ __forceinline__ bool rvalid(const ColRef& cr, const RowRef& x) {
+  return valid_at(x.tile ? cr.valid[1] : cr.valid[0], x.r);
+}
+
 // ---------------------------------------------------------------------------
-// Filter program over the thread's rows: value and known bits as two
-// register stacks per row.
+// 1. Selection.
 // ---------------------------------------------------------------------------
 template <typename F>
 __device__ __forceinline__ bool cmp_op(int op, F a, F b) {
@@ -81,61 +142,51 @@ __device__ __forceinline__ bool cmp_op(int op, F a, F b) {
   }
 }
 
-__device__ __forceinline__ void filter_rows(const ScanParams& p, const Tile& t, const uint32_t (&rr)[kR],
-                                            bool (&sel)[kR]) {
-  if (p.n_pred == 0) return;
-  uint32_t sv[kR], sk[kR];
-#pragma unroll
-  for (int j = 0; j < kR; ++j) sv[j] = sk[j] = 0;
+// One comparison on a row (known = not null).
+__device__ __forceinline__ bool cmp_row(const PredOp& op, int dt, int size, const unsigned char* vals, uint32_t r) {
+  const uint64_t b = load_bits(vals, size, r);
+  if (dt == DFC_FLOAT64) return cmp_op<double>(op.cmp, __longlong_as_double((long long)b), op.lit.f);
+  if (dt == DFC_FLOAT32) return cmp_op<float>(op.cmp, __uint_as_float((uint32_t)b), (float)op.lit.f);
+  if (dt == DFC_UINT64) return cmp_op<uint64_t>(op.cmp, b, op.lit.u);
+  return cmp_op<int64_t>(op.cmp, bits_to_i64(b, dt), op.lit.i);
+}
+
+// The general filter program for one row: value and known bits as two
+// register stacks (postfix, Kleene logic).
+__device__ bool program_row(const ScanParams& p, const Step& s, int tile, uint32_t r) {
+  uint32_t sv = 0, sk = 0;
   for (int i = 0; i < p.n_pred; ++i) {
     const PredOp& op = p.pred[i];
-    if (op.kind == DFC_PRED_CMP) {
-      const int c = op.input, dt = p.cols[c].dtype, size = p.cols[c].size;
-      const unsigned char* vals = col_values(p, t, c);
-      const uint32_t* valid = col_valid(p, t, c);
-#pragma unroll
-      for (int j = 0; j < kR; ++j) {
-        bool known = false, v = false;
-        if (sel[j]) {
-          known = valid_at(valid, rr[j]);
-          const uint64_t b = load_bits(vals, size, rr[j]);
-          if (dt == DFC_FLOAT64) v = cmp_op<double>(op.cmp, __longlong_as_double((long long)b), op.lit.f);
-          else if (dt == DFC_FLOAT32) v = cmp_op<float>(op.cmp, __uint_as_float((uint32_t)b), (float)op.lit.f);
-          else if (dt == DFC_UINT64) v = cmp_op<uint64_t>(op.cmp, b, op.lit.u);
-          else v = cmp_op<int64_t>(op.cmp, bits_to_i64(b, dt), op.lit.i);
-          v = v && known;
-        }
-        sv[j] = (sv[j] << 1) | (uint32_t)v;
-        sk[j] = (sk[j] << 1) | (uint32_t)known;
+    switch (op.kind) {
+      case DFC_PRED_CMP: {
+        const int c = op.input;
+        const bool known = valid_at(col_valid(p, s, tile, c), r);
+        const bool v = known && cmp_row(op, p.cols[c].dtype, p.cols[c].size, col_values(p, s, tile, c), r);
+        sv = (sv << 1) | (uint32_t)v;
+        sk = (sk << 1) | (uint32_t)known;
+        break;
       }
-    } else if (op.kind == DFC_PRED_IS_NULL || op.kind == DFC_PRED_IS_NOT_NULL) {
-      const uint32_t* valid = col_valid(p, t, op.input);
-      const bool want_null = op.kind == DFC_PRED_IS_NULL;
-#pragma unroll
-      for (int j = 0; j < kR; ++j) {
-        const bool is_valid = sel[j] ? valid_at(valid, rr[j]) : true;
-        sv[j] = (sv[j] << 1) | (uint32_t)(want_null ? !is_valid : is_valid);
-        sk[j] = (sk[j] << 1) | 1u;
+      case DFC_PRED_IS_NULL:
+      case DFC_PRED_IS_NOT_NULL: {
+        const bool is_valid = valid_at(col_valid(p, s, tile, op.input), r);
+        sv = (sv << 1) | (uint32_t)(op.kind == DFC_PRED_IS_NULL ? !is_valid : is_valid);
+        sk = (sk << 1) | 1u;
+        break;
       }
-    } else if (op.kind == DFC_PRED_TRUE) {
-#pragma unroll
-      for (int j = 0; j < kR; ++j) {
-        sv[j] = (sv[j] << 1) | 1u;
-        sk[j] = (sk[j] << 1) | 1u;
-      }
-    } else if (op.kind == DFC_PRED_NOT) {
-#pragma unroll
-      for (int j = 0; j < kR; ++j) sv[j] ^= sk[j] & 1u;
-    } else {  // AND / OR
-      const bool is_and = op.kind == DFC_PRED_AND;
-#pragma unroll
-      for (int j = 0; j < kR; ++j) {
-        const uint32_t bv = sv[j] & 1u, bk = sk[j] & 1u;
-        sv[j] >>= 1;
-        sk[j] >>= 1;
-        const uint32_t av = sv[j] & 1u, ak = sk[j] & 1u;
+      case DFC_PRED_TRUE:
+        sv = (sv << 1) | 1u;
+        sk = (sk << 1) | 1u;
+        break;
+      case DFC_PRED_NOT:
+        sv ^= sk & 1u;
+        break;
+      default: {  // AND / OR
+        const uint32_t bv = sv & 1u, bk = sk & 1u;
+        sv >>= 1;
+        sk >>= 1;
+        const uint32_t av = sv & 1u, ak = sk & 1u;
         uint32_t rv, rk;
-        if (is_and) {
+        if (op.kind == DFC_PRED_AND) {
           const uint32_t false_known = (ak & (av ^ 1u)) | (bk & (bv ^ 1u));
           rk = false_known | (ak & bk);
           rv = (false_known ^ 1u) & ak & bk & av & bv;
@@ -144,40 +195,99 @@ __device__ __forceinline__ void filter_rows(const ScanParams& p, const Tile& t, 
           rk = true_known | (ak & bk);
           rv = true_known;
         }
-        sv[j] = (sv[j] & ~1u) | rv;
-        sk[j] = (sk[j] & ~1u) | rk;
+        sv = (sv & ~1u) | rv;
+        sk = (sk & ~1u) | rk;
       }
     }
   }
-#pragma unroll
-  for (int j = 0; j < kR; ++j) sel[j] = sel[j] && ((sv[j] & sk[j] & 1u) != 0);
+  return (sv & sk & 1u) != 0;
+}
+
+template <typename T>
+__device__ __forceinline__ uint32_t select_word_cmp(const PredOp& op, const unsigned char* vals, const uint32_t* valid,
+                                                    uint32_t r, bool in) {
+  bool v = false;
+  if (in && valid_at(valid, r)) {
+    const T x = load_as<T>(vals, r);
+    if constexpr (sizeof(T) == 8 && T(-1) > T(0)) v = cmp_op<uint64_t>(op.cmp, (uint64_t)x, op.lit.u);
+    else if constexpr (std::is_floating_point<T>::value) v = cmp_op<T>(op.cmp, x, (T)op.lit.f);
+    else v = cmp_op<int64_t>(op.cmp, (int64_t)x, op.lit.i);
+  }
+  return __ballot_sync(0xffffffffu, v);
+}
+
+// The selection words of a tile: warp w computes words w, w + 8, ...; each
+// lane holds one row of a word.  Returns, per word, the bits of selected rows.
+__device__ __forceinline__ uint32_t select_word(const ScanParams& p, const Step& s, int tile, uint32_t word) {
+  const uint32_t r = word * 32 + (threadIdx.x & 31);
+  const bool in = r < s.n[tile];
+  if (p.n_pred == 0) return __ballot_sync(0xffffffffu, in);
+  const PredOp& op = p.pred[0];
+  if (p.n_pred == 1 && op.kind == DFC_PRED_CMP) {
+    const int c = op.input;
+    const unsigned char* vals = col_values(p, s, tile, c);
+    const uint32_t* valid = col_valid(p, s, tile, c);
+    switch (p.cols[c].dtype) {
+      case DFC_INT8: return select_word_cmp<int8_t>(op, vals, valid, r, in);
+      case DFC_INT16: return select_word_cmp<int16_t>(op, vals, valid, r, in);
+      case DFC_INT32: return select_word_cmp<int32_t>(op, vals, valid, r, in);
+      case DFC_INT64: return select_word_cmp<int64_t>(op, vals, valid, r, in);
+      case DFC_UINT8: return select_word_cmp<uint8_t>(op, vals, valid, r, in);
+      case DFC_UINT16: return select_word_cmp<uint16_t>(op, vals, valid, r, in);
+      case DFC_UINT32: return select_word_cmp<uint32_t>(op, vals, valid, r, in);
+      case DFC_UINT64: return select_word_cmp<uint64_t>(op, vals, valid, r, in);
+      case DFC_FLOAT32: return select_word_cmp<float>(op, vals, valid, r, in);
+      default: return select_word_cmp<double>(op, vals, valid, r, in);
+    }
+  }
+  return __ballot_sync(0xffffffffu, in && program_row(p, s, tile, r));
 }
 
 // ---------------------------------------------------------------------------
-// Keys.
+// 3. Keys.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void key_words(const ScanParams& p, const Tile& t, const uint32_t (&rr)[kR],
-                                          const bool (&sel)[kR], uint64_t (&kw)[kR]) {
+template <typename T>
+__device__ __forceinline__ void key_field(const ColRef& cr, const RowRef (&x)[kR], bool packed, const KeyField& f,
+                                          int k, uint64_t (&kw)[kR]) {
+#pragma unroll
+  for (int j = 0; j < kR; ++j) {
+    if (!x[j].on) continue;
+    const bool ok = rvalid(cr, x[j]);
+    uint64_t cell = 0;
+    if (ok) {
+      const T v = load_as<T>(rv(cr, x[j]), x[j].r);
+      if constexpr (std::is_same<T, float>::value) cell = key_cell(__float_as_uint(v), DFC_FLOAT32);
+      else if constexpr (std::is_same<T, double>::value) cell = key_cell((uint64_t)__double_as_longlong(v), DFC_FLOAT64);
+      else cell = (uint64_t)(typename std::make_unsigned<T>::type)v;
+    }
+    if (packed) {
+      if (!ok) kw[j] |= 1ull << f.null_bit;
+      else kw[j] |= (sizeof(T) == 8) ? cell : (cell << f.shift);
+    } else {
+      const uint64_t c = ok ? cell + 1 : 0x9E3779B97F4A7C15ull;
+      kw[j] = mix64(kw[j] ^ (c * 0x9E3779B97F4A7C15ull + (uint64_t)k));
+    }
+  }
+}
+
+__device__ __forceinline__ void key_words(const ScanParams& p, const Step& s, const RowRef (&x)[kR], uint64_t (&kw)[kR]) {
   const bool packed = p.key_mode == KEY_PACKED;
 #pragma unroll
   for (int j = 0; j < kR; ++j) kw[j] = packed ? 0ull : 0x243F6A8885A308D3ull;
   for (int k = 0; k < p.n_keys; ++k) {
     const KeyField& f = p.keys[k];
-    const int size = p.cols[f.input].size;
-    const unsigned char* vals = col_values(p, t, f.input);
-    const uint32_t* valid = col_valid(p, t, f.input);
-#pragma unroll
-    for (int j = 0; j < kR; ++j) {
-      if (!sel[j]) continue;
-      const bool ok = valid_at(valid, rr[j]);
-      const uint64_t cell = ok ? key_cell(load_bits(vals, size, rr[j]), f.dtype) : 0ull;
-      if (packed) {
-        if (!ok) kw[j] |= 1ull << f.null_bit;
-        else kw[j] |= (f.bits == 64) ? cell : (cell << f.shift);
-      } else {
-        const uint64_t c = ok ? cell + 1 : 0x9E3779B97F4A7C15ull;
-        kw[j] = mix64(kw[j] ^ (c * 0x9E3779B97F4A7C15ull + (uint64_t)k));
-      }
+    const ColRef cr = col_ref(p, s, f.input);
+    switch (f.dtype) {
+      case DFC_INT8: key_field<int8_t>(cr, x, packed, f, k, kw); break;
+      case DFC_INT16: key_field<int16_t>(cr, x, packed, f, k, kw); break;
+      case DFC_INT32: key_field<int32_t>(cr, x, packed, f, k, kw); break;
+      case DFC_INT64: key_field<int64_t>(cr, x, packed, f, k, kw); break;
+      case DFC_UINT8: key_field<uint8_t>(cr, x, packed, f, k, kw); break;
+      case DFC_UINT16: key_field<uint16_t>(cr, x, packed, f, k, kw); break;
+      case DFC_UINT32: key_field<uint32_t>(cr, x, packed, f, k, kw); break;
+      case DFC_UINT64: key_field<uint64_t>(cr, x, packed, f, k, kw); break;
+      case DFC_FLOAT32: key_field<float>(cr, x, packed, f, k, kw); break;
+      default: key_field<double>(cr, x, packed, f, k, kw); break;
     }
   }
   if (!packed) {
@@ -206,7 +316,7 @@ __device__ __forceinline__ uint64_t slot_of(const ScanParams& p, uint64_t kw) {
 }
 
 // ---------------------------------------------------------------------------
-// Claims.
+// 4. Groups: claims in the global table.
 // ---------------------------------------------------------------------------
 // Record numbers are handed out by CTA tickets: ticket t falls in the CTA's
 // chunk k = t / chunk, whose base the holder of the chunk's first ticket draws
@@ -264,7 +374,8 @@ __device__ __forceinline__ uint64_t entry_meta(const ScanParams& p, const KeyEnt
 
 // The group of key word kw at row `row`, claiming a new record if the key is
 // new: the per-lane path for ticket keys, the all-ones key word and merges.
-// kNoGid when records or table slots ran out (ST_CAPACITY set).
+// Visits slots in the same order as the lock-step rounds.  kNoGid when
+// records or table slots ran out (ST_CAPACITY set).
 __device__ __noinline__ uint32_t find_or_claim(const ScanParams& p, uint64_t kw, uint32_t row, ClaimState* cs) {
   const uint64_t slots = p.table_mask + 1;
   if (kw == kEmpty) {  // the all-ones key word has its own entry after the table
@@ -309,14 +420,14 @@ __device__ __noinline__ uint32_t find_or_claim(const ScanParams& p, uint64_t kw,
   return kNoGid;
 }
 
-// Packed keys: every lane's rows resolved together.  Each round a pending
-// row looks at its current entry: its key -> found; empty -> claim it (CAS);
-// another key -> step to the next slot and reload.  All lanes run the rounds
-// in lock-step, so a warp's claims share their latency.
+// Packed keys: all rows of the warp resolved together.  Each round a pending
+// row looks at two consecutive entries of its probe sequence: its key ->
+// found; empty -> claim it (CAS); both others -> the next two.  Rounds run in
+// lock-step so the warp's loads and claims overlap.
 __device__ __forceinline__ void resolve_packed(const ScanParams& p, const uint32_t (&rows)[kR], bool (&sel)[kR],
                                                const uint64_t (&kw)[kR], uint32_t (&gid)[kR], ClaimState* cs) {
   uint64_t slot[kR];
-  unsigned long long ek[kR], em[kR];
+  ulonglong2 e0[kR], e1[kR];
   bool pend[kR];
   uint32_t res[kR];
 #pragma unroll
@@ -325,16 +436,14 @@ __device__ __forceinline__ void resolve_packed(const ScanParams& p, const uint32
     res[j] = kNoGid;
     pend[j] = sel[j];
     slot[j] = 0;
-    ek[j] = em[j] = 0;
     if (pend[j] && kw[j] == kEmpty) {
       gid[j] = find_or_claim(p, kw[j], rows[j], cs);
       pend[j] = false;
     }
     if (pend[j]) {
       slot[j] = slot_of(p, kw[j]);
-      const ulonglong2 e = __ldcg(reinterpret_cast<const ulonglong2*>(p.table + slot[j]));
-      ek[j] = e.x;
-      em[j] = e.y;
+      e0[j] = __ldcg(reinterpret_cast<const ulonglong2*>(p.table + slot[j]));
+      e1[j] = __ldcg(reinterpret_cast<const ulonglong2*>(p.table + ((slot[j] + 1) & p.table_mask)));
     }
   }
   for (uint32_t round = 0;; ++round) {
@@ -342,7 +451,7 @@ __device__ __forceinline__ void resolve_packed(const ScanParams& p, const uint32
 #pragma unroll
     for (int j = 0; j < kR; ++j) any |= pend[j];
     if (!__any_sync(0xffffffffu, any)) break;
-    if (round > p.table_mask + 2) {  // every slot seen: the table is full
+    if (round > (p.table_mask >> 1) + 2) {  // every slot seen: the table is full
 #pragma unroll
       for (int j = 0; j < kR; ++j) pend[j] = false;
       atomicOr(p.status, ST_CAPACITY);
@@ -351,44 +460,46 @@ __device__ __forceinline__ void resolve_packed(const ScanParams& p, const uint32
 #pragma unroll
     for (int j = 0; j < kR; ++j) {
       if (!pend[j]) continue;
-      bool reload = false;
-      if (ek[j] == kw[j]) {
-        if (em[j] != kEmpty) {
-          gid[j] = (uint32_t)em[j];
-          pend[j] = false;
-        } else {
-          reload = true;  // torn read of a fresh claim
+      int step = 0;  // entries of this round consumed without a result
+      for (int h = 0; h < 2 && pend[j]; ++h) {
+        const ulonglong2 e = h ? e1[j] : e0[j];
+        const uint64_t s = (slot[j] + h) & p.table_mask;
+        if (e.x == kw[j]) {
+          if (e.y != kEmpty) {
+            gid[j] = (uint32_t)e.y;
+            pend[j] = false;
+          }
+          break;  // a torn read of a fresh claim: look at this entry again
         }
-      } else if (ek[j] == kEmpty) {
-        // A record reserved for a claim that lost its race is kept for this
-        // row's next attempt; one never used stays all-zero (a hole).
-        if (res[j] == kNoGid) res[j] = reserve_record(p, cs);
-        const uint32_t r = res[j];
-        if (r == kNoGid) {
-          pend[j] = false;
-          continue;
+        if (e.x == kEmpty) {
+          // A record reserved for a claim that lost its race is kept for this
+          // row's next attempt; one never used stays all-zero (a hole).
+          if (res[j] == kNoGid) res[j] = reserve_record(p, cs);
+          if (res[j] == kNoGid) {
+            pend[j] = false;
+            break;
+          }
+          uint64_t ok, om;
+          cas128(p.table + s, kEmpty, kEmpty, kw[j], (uint64_t)res[j] | ((uint64_t)rows[j] << 32), ok, om);
+          if (ok == kEmpty && om == kEmpty) {
+            claimed(p, res[j], kw[j], rows[j]);
+            gid[j] = res[j];
+            pend[j] = false;
+          } else if (ok == kw[j]) {
+            gid[j] = (uint32_t)om;
+            pend[j] = false;
+          } else {
+            step = h + 1;  // taken by another key: go on past it
+            continue;
+          }
+          break;
         }
-        uint64_t ok, om;
-        cas128(p.table + slot[j], kEmpty, kEmpty, kw[j], (uint64_t)r | ((uint64_t)rows[j] << 32), ok, om);
-        if (ok == kEmpty && om == kEmpty) {
-          claimed(p, r, kw[j], rows[j]);
-          gid[j] = r;
-          pend[j] = false;
-        } else if (ok == kw[j]) {
-          gid[j] = (uint32_t)om;
-          pend[j] = false;
-        } else {
-          slot[j] = (slot[j] + 1) & p.table_mask;
-          reload = true;
-        }
-      } else {
-        slot[j] = (slot[j] + 1) & p.table_mask;
-        reload = true;
+        step = h + 1;
       }
-      if (reload) {
-        const ulonglong2 e = __ldcg(reinterpret_cast<const ulonglong2*>(p.table + slot[j]));
-        ek[j] = e.x;
-        em[j] = e.y;
+      if (pend[j]) {
+        slot[j] = (slot[j] + step) & p.table_mask;
+        e0[j] = __ldcg(reinterpret_cast<const ulonglong2*>(p.table + slot[j]));
+        e1[j] = __ldcg(reinterpret_cast<const ulonglong2*>(p.table + ((slot[j] + 1) & p.table_mask)));
       }
     }
   }
@@ -397,7 +508,7 @@ __device__ __forceinline__ void resolve_packed(const ScanParams& p, const uint32
 }
 
 // ---------------------------------------------------------------------------
-// Shared-memory regime (few groups): each CTA keeps its own key table and
+// 4'. Shared-memory regime (few groups): each CTA keeps its own key table and
 // all-zero group records in shared memory; duplicate keys inside a warp are
 // collapsed with __match_any_sync so one leader lane applies the combined
 // update; the CTA's records are merged into the global table when it exits.
@@ -448,8 +559,9 @@ __device__ __forceinline__ V group_reduce(uint32_t grp, int maxpop, V mine, V id
   return acc;
 }
 
-__device__ __forceinline__ void smem_rows(const ScanParams& p, const Tile& t, const SmemTable& st,
-                                          const uint32_t (&rr)[kR], bool (&sel)[kR], const uint64_t (&kw)[kR]) {
+__device__ __forceinline__ void smem_rows(const ScanParams& p, const Step& s, const SmemTable& st,
+                                          const RowRef (&x)[kR], const uint32_t (&rows)[kR], bool (&sel)[kR],
+                                          const uint64_t (&kw)[kR]) {
   const int lane = threadIdx.x & 31;
 #pragma unroll
   for (int j = 0; j < kR; ++j) {
@@ -461,19 +573,21 @@ __device__ __forceinline__ void smem_rows(const ScanParams& p, const Tile& t, co
     if (maxpop == 0) continue;
     const bool leader = loc && lane == __ffs(grp) - 1;
     unsigned char* rec = loc ? st.recs + (size_t)ls * p.rec_stride : nullptr;
+    // The group's earliest row.  The CTA record always keeps its first row:
+    // it is the claim row when the record is merged into the global table.
+    const uint32_t first =
+        group_reduce<uint32_t>(grp, maxpop, rows[j], 0xFFFFFFFFu, loc, [](uint32_t a, uint32_t b2) { return a < b2 ? a : b2; });
     if (leader) {
-      // The leader is the group's lowest lane, hence its earliest row.  The
-      // CTA record always keeps its first row: it is the claim row when the
-      // record is merged into the global table.
-      atomicMax(reinterpret_cast<uint32_t*>(rec + kRecFirst), ~(uint32_t)(t.start + rr[j]));
+      atomicMax(reinterpret_cast<uint32_t*>(rec + kRecFirst), ~first);
       if (p.off_len >= 0) atomicAdd(reinterpret_cast<uint32_t*>(rec + p.off_len), (uint32_t)__popc(grp));
     }
     for (int v = 0; v < p.n_vals; ++v) {
       const ValField& f = p.vals[v];
       const int c = f.input, dt = f.dtype;
       const bool isf = dt_float(dt);
-      const bool ok = loc && valid_at(col_valid(p, t, c), rr[j]);
-      const uint64_t b = ok ? load_bits(col_values(p, t, c), p.cols[c].size, rr[j]) : 0ull;
+      const ColRef cr = col_ref(p, s, c);
+      const bool ok = loc && rvalid(cr, x[j]);
+      const uint64_t b = ok ? load_bits(rv(cr, x[j]), p.cols[c].size, x[j].r) : 0ull;
       const double xd = isf ? bits_to_f64(b, dt) : bits_as_double(b, dt);
       const bool nan = ok && isf && xd != xd;
       const uint32_t vmask = grp & __ballot_sync(0xffffffffu, ok);
@@ -483,17 +597,17 @@ __device__ __forceinline__ void smem_rows(const ScanParams& p, const Tile& t, co
       if (leader && vmask) atomicAdd(reinterpret_cast<uint32_t*>(rec + f.off_count), (uint32_t)__popc(vmask));
       if (f.off_sum >= 0) {
         if (f.sum_kind == SUM_F64) {
-          const double s = group_reduce<double>(grp, maxpop, xd, 0.0, ok, [](double a, double b2) { return a + b2; });
-          if (leader && vmask) atomicAdd(reinterpret_cast<double*>(rec + f.off_sum), s);
+          const double sm = group_reduce<double>(grp, maxpop, xd, 0.0, ok, [](double a, double b2) { return a + b2; });
+          if (leader && vmask) atomicAdd(reinterpret_cast<double*>(rec + f.off_sum), sm);
         } else {
           // The group's partial sum, exact in 128 bits.
           const bool uns = dt == DFC_UINT64;
-          const uint64_t x = ok ? (uns ? b : (uint64_t)bits_to_i64(b, dt)) : 0ull;
-          const uint64_t xhi = (!uns && (int64_t)x < 0) ? ~0ull : 0ull;
+          const uint64_t xv = ok ? (uns ? b : (uint64_t)bits_to_i64(b, dt)) : 0ull;
+          const uint64_t xhi = (!uns && (int64_t)xv < 0) ? ~0ull : 0ull;
           __int128 exact = 0;
           for (int i = 0; i < maxpop; ++i) {
             const int src = nth_lane(grp, i);
-            const uint64_t vlo = __shfl_sync(0xffffffffu, x, src);
+            const uint64_t vlo = __shfl_sync(0xffffffffu, xv, src);
             const uint64_t vhi = __shfl_sync(0xffffffffu, xhi, src);
             if (i < __popc(grp)) exact += (__int128)(((unsigned __int128)vhi << 64) | vlo);
           }
@@ -552,25 +666,102 @@ __device__ __forceinline__ void smem_rows(const ScanParams& p, const Tile& t, co
   }
 }
 
+// ---------------------------------------------------------------------------
+// 5. States in the global records.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void update_column(const ScanParams& p, const ValField& f, int v, const ColRef& cr,
+                                              const RowRef (&x)[kR], const bool (&sel)[kR], const uint32_t (&gid)[kR]) {
+  constexpr bool kFloat = std::is_floating_point<T>::value;
+  bool ok[kR];
+  T val[kR];
+  uint64_t lo[kR], hi[kR], ks[kR];
+  // Values and the read-set of every row, loads in flight together.
+#pragma unroll
+  for (int j = 0; j < kR; ++j) {
+    ok[j] = sel[j] && rvalid(cr, x[j]);
+    val[j] = ok[j] ? load_as<T>(rv(cr, x[j]), x[j].r) : T(0);
+    lo[j] = hi[j] = ks[j] = 0;
+    if (!ok[j]) continue;
+    const unsigned char* rec = record_at(p, gid[j]);
+    if (f.off_min >= 0) lo[j] = ld_cg_u64(rec + f.off_min);
+    if (f.off_max >= 0) hi[j] = ld_cg_u64(rec + f.off_max);
+    if (f.off_m2 >= 0) ks[j] = ld_cg_u64(rec + f.off_shift);
+  }
+#pragma unroll
+  for (int j = 0; j < kR; ++j) {
+    if (!ok[j]) continue;
+    unsigned char* rec = record_at(p, gid[j]);
+    red_add_u32(rec + f.off_count, 1u);
+    const double xd = (double)val[j];
+    const bool nan = kFloat && xd != xd;
+    if (f.off_sum >= 0) {
+      if constexpr (kFloat) {
+        red_add_f64(rec + f.off_sum, xd);
+      } else if (std::is_same<T, uint64_t>::value) {
+        const uint64_t xv = (uint64_t)val[j];
+        const uint64_t old = atomicAdd(reinterpret_cast<unsigned long long*>(rec + f.off_sum), xv);
+        if (old + xv < old) red_add_u64(rec + f.off_sum + 8, 1ull);
+      } else {
+        const int64_t xv = (int64_t)val[j];
+        if (f.sum_kind == SUM_I64) {
+          red_add_u64(rec + f.off_sum, (uint64_t)xv);
+        } else {
+          const uint64_t old = atomicAdd(reinterpret_cast<unsigned long long*>(rec + f.off_sum), (uint64_t)xv);
+          const uint64_t hi_add = (xv < 0 ? ~0ull : 0ull) + ((old + (uint64_t)xv) < old ? 1ull : 0ull);
+          if (hi_add) red_add_u64(rec + f.off_sum + 8, hi_add);
+        }
+      }
+    }
+    if (f.off_min >= 0 || f.off_max >= 0) {
+      if (nan) {
+        red_or_u32(rec + kRecFlags, 1u << (3 * v));
+      } else {
+        uint64_t bits;
+        if constexpr (std::is_same<T, float>::value) bits = __float_as_uint(val[j]);
+        else if constexpr (std::is_same<T, double>::value) bits = (uint64_t)__double_as_longlong(val[j]);
+        else bits = (uint64_t)(typename std::make_unsigned<T>::type)val[j];
+        const uint64_t e = order_encode(bits, f.dtype);
+        if (f.off_min >= 0 && ~e > lo[j]) red_max_u64(rec + f.off_min, ~e);
+        if (f.off_max >= 0 && e > hi[j]) red_max_u64(rec + f.off_max, e);
+        if (kFloat && xd == 0.0) red_or_u32(rec + kRecFlags, 1u << (3 * v + (signbit(xd) ? 2 : 1)));
+      }
+    }
+    if (f.off_m2 >= 0) {
+      const uint64_t xbits = nan ? kCanonNaN : (uint64_t)__double_as_longlong(xd);
+      uint64_t k = ks[j];
+      if (k == 0) {
+        const uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long*>(rec + f.off_shift), 0ull, xbits ^ kShiftTag);
+        k = prev == 0 ? (xbits ^ kShiftTag) : prev;
+      }
+      const double d = xd - __longlong_as_double((long long)(k ^ kShiftTag));
+      red_add_f64(rec + f.off_m2, d * d);
+    }
+  }
+}
+
 __device__ void merge_record(const ScanParams& p, const unsigned char* src, uint64_t kw, ClaimState* cs);
 
-// ---------------------------------------------------------------------------
-// A tile's rows for one consumer thread.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void consume_tile(const ScanParams& p, const Tile& t, uint32_t n, uint32_t ct,
-                                             ClaimState* cs, const SmemTable* st) {
-  uint32_t rr[kR], rows[kR];
+// One pass over up to kPassRows compacted rows of a step.
+__device__ __forceinline__ void consume_rows(const ScanParams& p, const Step& s, const uint16_t* idx, uint32_t nsel,
+                                             uint32_t base, uint32_t shift, ClaimState* cs, const SmemTable* st) {
+  const uint32_t ct = threadIdx.x - 32;
+  RowRef x[kR];
+  uint32_t rows[kR];
   bool sel[kR];
 #pragma unroll
   for (int j = 0; j < kR; ++j) {
-    rr[j] = ct + (uint32_t)j * kScanConsumerThreads;
-    rows[j] = (uint32_t)(t.start + rr[j]);
-    sel[j] = rr[j] < n;
+    const uint32_t i = base + ct + (uint32_t)j * kScanConsumerThreads;
+    x[j].on = i < nsel;
+    const uint32_t e = x[j].on ? idx[i] : 0u;
+    x[j].tile = e >> shift;
+    x[j].r = e & ((1u << shift) - 1u);
+    rows[j] = (uint32_t)(s.start[x[j].tile] + x[j].r);
+    sel[j] = x[j].on;
   }
-  filter_rows(p, t, rr, sel);
   uint64_t kw[kR];
-  key_words(p, t, rr, sel, kw);
-  if (st) smem_rows(p, t, *st, rr, sel, kw);
+  key_words(p, s, x, kw);
+  if (st) smem_rows(p, s, *st, x, rows, sel, kw);
 
   uint32_t gid[kR];
   if (p.key_mode == KEY_PACKED) {
@@ -583,82 +774,33 @@ __device__ __forceinline__ void consume_tile(const ScanParams& p, const Tile& t,
     }
   }
 
-  // Read-set of every row (first row, then per column K, min, max), loads in
-  // flight together, then the atomics.
-  uint32_t first[kR];
+  if (p.track_first) {
+    uint32_t first[kR];
 #pragma unroll
-  for (int j = 0; j < kR; ++j) first[j] = (sel[j] && p.track_first) ? ld_cg_u32(record_at(p, gid[j]) + kRecFirst) : ~0u;
+    for (int j = 0; j < kR; ++j) first[j] = sel[j] ? ld_cg_u32(record_at(p, gid[j]) + kRecFirst) : ~0u;
 #pragma unroll
-  for (int j = 0; j < kR; ++j) {
-    if (!sel[j]) continue;
-    unsigned char* rec = record_at(p, gid[j]);
-    if (p.track_first && ~rows[j] > first[j]) atomicMax(reinterpret_cast<uint32_t*>(rec + kRecFirst), ~rows[j]);
-    if (p.off_len >= 0) red_add_u32(rec + p.off_len, 1u);
+    for (int j = 0; j < kR; ++j)
+      if (sel[j] && ~rows[j] > first[j]) atomicMax(reinterpret_cast<uint32_t*>(record_at(p, gid[j]) + kRecFirst), ~rows[j]);
   }
-
+  if (p.off_len >= 0) {
+#pragma unroll
+    for (int j = 0; j < kR; ++j)
+      if (sel[j]) red_add_u32(record_at(p, gid[j]) + p.off_len, 1u);
+  }
   for (int v = 0; v < p.n_vals; ++v) {
     const ValField& f = p.vals[v];
-    const int c = f.input, dt = f.dtype, size = p.cols[c].size;
-    const unsigned char* vals = col_values(p, t, c);
-    const uint32_t* valid = col_valid(p, t, c);
-    const bool isf = dt_float(dt);
-    bool ok[kR];
-    uint64_t b[kR], lo[kR], hi[kR], ks[kR];
-#pragma unroll
-    for (int j = 0; j < kR; ++j) {
-      ok[j] = sel[j] && valid_at(valid, rr[j]);
-      b[j] = ok[j] ? load_bits(vals, size, rr[j]) : 0ull;
-      lo[j] = ~0ull;
-      hi[j] = ~0ull;
-      ks[j] = 1ull;
-      if (!ok[j]) continue;
-      const unsigned char* rec = record_at(p, gid[j]);
-      if (f.off_min >= 0) lo[j] = ld_cg_u64(rec + f.off_min);
-      if (f.off_max >= 0) hi[j] = ld_cg_u64(rec + f.off_max);
-      if (f.off_m2 >= 0) ks[j] = ld_cg_u64(rec + f.off_shift);
-    }
-#pragma unroll
-    for (int j = 0; j < kR; ++j) {
-      if (!ok[j]) continue;
-      unsigned char* rec = record_at(p, gid[j]);
-      red_add_u32(rec + f.off_count, 1u);
-      const double xd = isf ? bits_to_f64(b[j], dt) : 0.0;
-      if (f.off_sum >= 0) {
-        if (f.sum_kind == SUM_F64) {
-          red_add_f64(rec + f.off_sum, xd);
-        } else if (f.sum_kind == SUM_I64) {
-          red_add_u64(rec + f.off_sum, (uint64_t)bits_to_i64(b[j], dt));
-        } else {
-          const bool uns = dt == DFC_UINT64;
-          const uint64_t x = uns ? b[j] : (uint64_t)bits_to_i64(b[j], dt);
-          const uint64_t neg = (!uns && (int64_t)x < 0) ? ~0ull : 0ull;
-          const uint64_t old = atomicAdd(reinterpret_cast<unsigned long long*>(rec + f.off_sum), x);
-          const uint64_t hi_add = neg + ((old + x) < old ? 1ull : 0ull);
-          if (hi_add) red_add_u64(rec + f.off_sum + 8, hi_add);
-        }
-      }
-      if (f.off_min >= 0 || f.off_max >= 0) {
-        if (isf && xd != xd) {
-          red_or_u32(rec + kRecFlags, 1u << (3 * v));
-        } else {
-          const uint64_t e = order_encode(b[j], dt);
-          if (f.off_min >= 0 && ~e > lo[j]) red_max_u64(rec + f.off_min, ~e);
-          if (f.off_max >= 0 && (e > hi[j] || hi[j] == ~0ull)) red_max_u64(rec + f.off_max, e);
-          if (isf && xd == 0.0)
-            red_or_u32(rec + kRecFlags, 1u << (3 * v + ((__double_as_longlong(xd) < 0) ? 2 : 1)));
-        }
-      }
-      if (f.off_m2 >= 0) {
-        const double x = isf ? xd : bits_as_double(b[j], dt);
-        const uint64_t xbits = (x != x) ? kCanonNaN : (uint64_t)__double_as_longlong(x);
-        uint64_t k = ks[j];
-        if (k == 0) {
-          const uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long*>(rec + f.off_shift), 0ull, xbits ^ kShiftTag);
-          k = prev == 0 ? (xbits ^ kShiftTag) : prev;
-        }
-        const double d = x - __longlong_as_double((long long)(k ^ kShiftTag));
-        red_add_f64(rec + f.off_m2, d * d);
-      }
+    const ColRef cr = col_ref(p, s, f.input);
+    switch (f.dtype) {
+      case DFC_INT8: update_column<int8_t>(p, f, v, cr, x, sel, gid); break;
+      case DFC_INT16: update_column<int16_t>(p, f, v, cr, x, sel, gid); break;
+      case DFC_INT32: update_column<int32_t>(p, f, v, cr, x, sel, gid); break;
+      case DFC_INT64: update_column<int64_t>(p, f, v, cr, x, sel, gid); break;
+      case DFC_UINT8: update_column<uint8_t>(p, f, v, cr, x, sel, gid); break;
+      case DFC_UINT16: update_column<uint16_t>(p, f, v, cr, x, sel, gid); break;
+      case DFC_UINT32: update_column<uint32_t>(p, f, v, cr, x, sel, gid); break;
+      case DFC_UINT64: update_column<uint64_t>(p, f, v, cr, x, sel, gid); break;
+      case DFC_FLOAT32: update_column<float>(p, f, v, cr, x, sel, gid); break;
+      default: update_column<double>(p, f, v, cr, x, sel, gid); break;
     }
   }
 }
@@ -671,6 +813,10 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
   __shared__ ClaimState s_claim;
   __shared__ volatile uint32_t s_abort;
   __shared__ uint32_t s_used;
+  // Compacted rows of a step, three buffers: a step's count is reset two
+  // steps ahead of its reuse, between barriers.
+  __shared__ uint32_t s_nsel[3];
+  __shared__ uint16_t s_idx[3][kStepRows];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
@@ -681,6 +827,7 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
     s_claim.ticket = 0;
     s_abort = 0;
     s_used = 0;
+    s_nsel[0] = s_nsel[1] = s_nsel[2] = 0;
   }
   if (threadIdx.x < kChunkRing) s_claim.ring[threadIdx.x] = ~0ull;
   SmemTable st{nullptr, nullptr, &s_used};
@@ -727,23 +874,65 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
       }
     }
   } else {
-    const uint32_t ct = threadIdx.x - 32;
-    uint32_t it = 0;
-    for (uint64_t t = blockIdx.x; t < p.tiles; t += gridDim.x, ++it) {
-      const uint32_t s = it % S, ph = (it / S) & 1u;
-      if (!mbar_wait_bounded(&full[s], ph, kWaitLimit)) {
-        atomicOr(p.status, ST_TIMEOUT);
+    const uint32_t shift = 31 - __clz((uint32_t)p.tile_rows);
+    const uint32_t words = (uint32_t)(T / 32);
+    uint32_t it = 0;   // tiles consumed
+    uint32_t stp = 0;  // steps
+    for (uint64_t t = blockIdx.x; t < p.tiles; t += (uint64_t)kTilesPerStep * gridDim.x, ++stp) {
+      Step s;
+      int nt = 0;
+      bool failed = false;
+#pragma unroll
+      for (int k = 0; k < kTilesPerStep; ++k) {
+        const uint64_t tk = t + (uint64_t)k * gridDim.x;
+        s.n[k] = 0;
+        s.start[k] = 0;
+        s.staged[k] = false;
+        s.stage[k] = smem;
+        if (tk >= p.tiles || failed) continue;
+        const uint32_t sid = (it + k) % S, ph = ((it + k) / S) & 1u;
+        if (!mbar_wait_bounded(&full[sid], ph, kWaitLimit)) {
+          atomicOr(p.status, ST_TIMEOUT);
+          s_abort = 1;
+          failed = true;
+          continue;
+        }
+        s.stage[k] = smem + (size_t)sid * p.stage_bytes;
+        s.start[k] = tk * T;
+        s.staged[k] = p.use_tma && tk < p.full_tiles;
+        const uint64_t left = p.rows - s.start[k];
+        s.n[k] = (uint32_t)(left < T ? left : T);
+        ++nt;
+      }
+      // 1 + 2: selection words and compaction into s_idx[b].
+      const uint32_t b = stp % 3u;
+      if (!failed) {
+        for (int k = 0; k < nt; ++k) {
+          for (uint32_t w = (uint32_t)(warp - 1); w < words; w += kScanConsumerWarps) {
+            const uint32_t bits = select_word(p, s, k, w);
+            uint32_t off = 0;
+            if (lane == 0 && bits) off = atomicAdd(&s_nsel[b], (uint32_t)__popc(bits));
+            off = __shfl_sync(0xffffffffu, off, 0);
+            if ((bits >> lane) & 1u)
+              s_idx[b][off + __popc(bits & ((1u << lane) - 1u))] = (uint16_t)(((uint32_t)k << shift) | (w * 32 + lane));
+          }
+        }
+      }
+      // Every consumer warp takes the same exit decision at this barrier.
+      const bool stop = consumer_sync_or(failed || s_abort);
+      const uint32_t nsel = s_nsel[b];
+      if (threadIdx.x == 32) s_nsel[(b + 2u) % 3u] = 0;  // read last step, written two steps on
+      if (stop) {
         s_abort = 1;
         break;
       }
-      const Tile tile{smem + (size_t)s * p.stage_bytes, t * T, p.use_tma && t < p.full_tiles};
-      const uint64_t left = p.rows - tile.start;
-      const uint32_t n = (uint32_t)(left < T ? left : T);
-      for (uint32_t base = 0; base < n; base += kScanConsumerThreads * kR)
-        consume_tile(p, tile, n, ct + base, &s_claim, p.smem_slots ? &st : nullptr);
+      // 3 - 5 over the compacted rows.
+      for (uint32_t base = 0; base < nsel; base += kPassRows)
+        consume_rows(p, s, s_idx[b], nsel, base, shift, &s_claim, p.smem_slots ? &st : nullptr);
       __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[s]);
-      if (s_abort) break;
+      for (int k = 0; k < nt; ++k)
+        if (lane == 0) mbar_arrive(&empty[(it + k) % S]);
+      it += nt;
     }
   }
   __syncthreads();

@@ -98,6 +98,22 @@ class Timings(C.Structure):
     ]
 
 
+class DeviceColumnDesc(C.Structure):
+    """dfc_device_column: a column in device memory, read in place."""
+
+    _fields_ = [("dtype", C.c_int32), ("reserved", C.c_int32), ("values", C.c_void_p), ("validity", C.c_void_p)]
+
+
+class DeviceOutput(C.Structure):
+    """dfc_device_output: caller-owned device buffers of one output column."""
+
+    _fields_ = [("values", C.c_void_p), ("validity", C.c_void_p), ("dtype", C.c_int32), ("has_nulls", C.c_int32)]
+
+
+# Bytes of the fixed working-memory array behind dfc_groupby_noalloc.
+NOALLOC_SCRATCH_BYTES = 64 << 20
+
+
 # (name, restype, argtypes) of every entry point include/dfcuda.h declares.
 SIGNATURES = [
     ("dfc_version", C.c_uint32, []),
@@ -113,6 +129,12 @@ SIGNATURES = [
     ("dfc_column_rows", C.c_uint64, [C.c_void_p]),
     ("dfc_column_null_count", C.c_int32, [C.c_void_p]),
     ("dfc_groupby", C.c_int, [C.POINTER(Query), C.POINTER(C.c_void_p)]),
+    (
+        "dfc_groupby_noalloc",
+        C.c_int,
+        [C.POINTER(Query), C.c_int32, C.c_uint64, C.POINTER(DeviceColumnDesc), C.c_uint64, C.POINTER(DeviceOutput),
+         C.POINTER(C.c_uint64)],
+    ),
     ("dfc_result_rows", C.c_uint64, [C.c_void_p]),
     ("dfc_result_columns", C.c_int32, [C.c_void_p]),
     (

@@ -1099,3 +1099,266 @@ DFC_API const char* dfc_status_name(dfc_status status) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// dfc_groupby_noalloc: the query with all of its working memory in one fixed
+// array, for callers that cannot allocate device memory.
+// ---------------------------------------------------------------------------
+
+// The array every GPU that loads this library holds until the process exits.
+// In host code its name is only a stand-in for the symbol, not a device
+// address: noalloc_scratch() asks the runtime for the address once per device.
+static __device__ __align__(256) unsigned char dfc_noalloc_scratch[DFC_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_addr_mu;
+unsigned char* g_noalloc_base[kNoAllocMaxDevices] = {};
+// One call at a time per device: the calls share the array.
+std::mutex g_noalloc_run_mu[kNoAllocMaxDevices];
+
+// Device address of the array on `dev`; `dev` must be the current device.
+dfc_status noalloc_scratch(int dev, unsigned char** out) {
+  std::lock_guard<std::mutex> lk(g_noalloc_addr_mu);
+  if (!g_noalloc_base[dev]) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, dfc_noalloc_scratch), "cudaGetSymbolAddress of the fixed scratch array");
+    g_noalloc_base[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = g_noalloc_base[dev];
+  return DFC_OK;
+}
+
+// Bounded wait for `stream` that creates nothing (no event).
+dfc_status noalloc_wait(cudaStream_t stream) {
+  const auto t0 = std::chrono::steady_clock::now();
+  const double limit = wait_limit_seconds();
+  for (int spins = 0;; ++spins) {
+    const cudaError_t e = cudaStreamQuery(stream);
+    if (e == cudaSuccess) return DFC_OK;
+    if (e != cudaErrorNotReady) return cuda_fail(e, "query execution");
+    if (spins > 64) std::this_thread::sleep_for(std::chrono::microseconds(20));
+    if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > limit)
+      return fail(DFC_TIMEOUT, "device work did not finish within the wait limit");
+  }
+}
+
+// Hands out 256-byte-aligned pieces of the array; `used` is the total asked
+// for, which may exceed the array (checked before any piece is used).
+struct Carve {
+  unsigned char* base;
+  size_t used = 0;
+  void* take(size_t bytes) {
+    void* p = base + used;
+    used += (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255;
+    return p;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+DFC_API dfc_status dfc_groupby_noalloc(const dfc_query* query, int32_t device, uint64_t rows,
+                                       const dfc_device_column* columns, uint64_t capacity,
+                                       dfc_device_output* outputs, uint64_t* groups) {
+  if (!query || !columns || !outputs || !groups) return fail(DFC_INVALID, "null argument");
+  *groups = 0;
+  t_timings = dfc_timings{};
+  if (device < 0 || device >= kNoAllocMaxDevices) return fail(DFC_INVALID, "device ordinal out of range");
+  if (query->n_inputs < 1 || query->n_inputs > kMaxInputs)
+    return fail(DFC_UNSUPPORTED, "between 1 and 16 input columns are supported");
+  // Host-side descriptors over the caller's device memory (no copies).
+  dfc_column cols[kMaxInputs];
+  dfc_column* col_ptrs[kMaxInputs];
+  for (int i = 0; i < query->n_inputs; ++i) {
+    const dfc_device_column& d = columns[i];
+    if (dtype_size(d.dtype) == 0) return fail(DFC_UNSUPPORTED, "unsupported column type");
+    if (rows > 0 && !d.values) return fail(DFC_INVALID, "null values");
+    if (((uintptr_t)d.values & 15u) != 0 || ((uintptr_t)d.validity & 15u) != 0)
+      return fail(DFC_INVALID, "column values and validity must be 16-byte aligned");
+    cols[i].device = device;
+    cols[i].dtype = (dfc_dtype)d.dtype;
+    cols[i].rows = rows;
+    cols[i].values = const_cast<void*>(d.values);
+    cols[i].validity = const_cast<uint32_t*>(d.validity);
+    col_ptrs[i] = &cols[i];
+  }
+  dfc_query q = *query;
+  q.inputs = col_ptrs;
+  Plan P;
+  dfc_status st = plan_query(&q, P);
+  if (st) return st;
+  for (int c = 0; c < P.n_out; ++c)
+    if (capacity > 0 && (!outputs[c].values || !outputs[c].validity)) return fail(DFC_INVALID, "null output buffer");
+  DeviceState* ds;
+  if ((st = device_ready(P.device, &ds))) return st;
+  DeviceGuard guard(P.device);
+  std::lock_guard<std::mutex> run_lock(g_noalloc_run_mu[device]);
+  unsigned char* base;
+  if ((st = noalloc_scratch(P.device, &base))) return st;
+  cudaStream_t stream = query->stream ? static_cast<cudaStream_t>(query->stream) : cudaStreamPerThread;
+  ScanParams& sp = P.sp;
+  FinishParams& fp = P.fp;
+
+  // Regime and table size from the caller's capacity (no statistics pass).
+  const uint64_t est = std::min<uint64_t>(capacity, P.rows);
+  sp.smem_slots = 0;
+  if (!(query->flags & DFC_Q_FORCE_GLOBAL) && sp.key_mode == KEY_PACKED &&
+      ((query->flags & DFC_Q_FORCE_SHARED) || est <= 4096)) {
+    const uint64_t sslots = next_pow2(std::max<uint64_t>(64, std::min<uint64_t>(est, 4096) * 2));
+    const size_t keys_off = (P.smem + 15) & ~(size_t)15;
+    const size_t recs_off = (keys_off + sslots * 8 + 15) & ~(size_t)15;
+    const size_t total = recs_off + sslots * (size_t)sp.rec_stride;
+    if (total <= ds->smem_optin) {
+      sp.smem_slots = (uint32_t)sslots;
+      sp.smem_keys_off = (uint32_t)keys_off;
+      sp.smem_recs_off = (uint32_t)recs_off;
+      P.smem = total;
+    }
+  }
+  const uint64_t slots = std::min(next_pow2(std::max<uint64_t>(1024, est * 2)),
+                                  next_pow2(std::max<uint64_t>(1024, P.rows * 2)));
+  int occ = 1;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_kernel, kScanThreads, P.smem), "occupancy");
+  occ = std::max(1, occ);
+  uint64_t ncta = (uint64_t)ds->sms * (uint64_t)occ;
+  ncta = std::max<uint64_t>(1, std::min<uint64_t>(ncta, std::max<uint64_t>(1, sp.tiles)));
+  const uint64_t groups_cap = std::min<uint64_t>(P.rows, slots / 2);
+  uint64_t chunk = 64;
+  while (chunk < 1024 && chunk * ncta * 8 < groups_cap) chunk <<= 1;
+  const uint64_t words = (P.rows + 31) / 32;
+  const uint64_t chunks = std::max<uint64_t>(1, (words + kFinishChunk - 1) / kFinishChunk);
+  // Every group holds a table entry, so the table bounds the group count.
+  const uint64_t out_rows = std::min<uint64_t>(P.rows, slots + 1);
+
+  // Working memory, carved from the array: the fixed parts, then as many
+  // group records as the rest holds.  Besides the groups, records go to
+  // claims that lost a race (many with hot keys) and to partly used chunks;
+  // a row reserves one record at most, so more than rows + chunks of slack
+  // is never needed.  Outputs are staged here and copied out once the group
+  // count is known to fit the caller's buffers.
+  Carve cv{base};
+  void* table = cv.take((slots + 1) * sizeof(KeyEntry));
+  Control* dctl = static_cast<Control*>(cv.take(sizeof(Control)));
+  void* bits = cv.take(words * 4 + 16);
+  void* prefix = cv.take(words * 4 + 16);
+  void* bsums = cv.take(chunks * 4);
+  void* perm = cv.take(out_rows * 4);
+  void* out_vals[kMaxOut];
+  uint32_t* out_valid[kMaxOut];
+  for (int c = 0; c < P.n_out; ++c) {
+    out_vals[c] = cv.take(out_rows * 8);
+    out_valid[c] = static_cast<uint32_t*>(cv.take(((out_rows + 31) / 32) * 4));
+  }
+  const uint64_t per_record = (uint64_t)sp.rec_stride + 4;  // record + its first row
+  const uint64_t min_recs = groups_cap + groups_cap / 8 + chunk * ncta;
+  const uint64_t left = cv.used + 512 < DFC_NOALLOC_SCRATCH_BYTES ? DFC_NOALLOC_SCRATCH_BYTES - cv.used - 512 : 0;
+  const uint64_t useful = std::max<uint64_t>(min_recs, P.rows + chunk * ncta);
+  const uint64_t recs = std::min<uint64_t>({useful, left / per_record, 0xFFFFFFF0ull});
+  if (recs < min_recs) {
+    char msg[256];
+    snprintf(msg, sizeof msg,
+             "dfc_groupby_noalloc: this query needs %llu bytes of working memory; the fixed scratch array holds %llu "
+             "(fewer rows or a smaller capacity fit)",
+             (unsigned long long)(cv.used + 512 + min_recs * per_record), (unsigned long long)DFC_NOALLOC_SCRATCH_BYTES);
+    return fail(DFC_CAPACITY, msg);
+  }
+  void* records = cv.take(recs * sp.rec_stride);
+  void* firsts = cv.take(recs * 4);
+
+  // The array keeps the previous call's contents: clear what starts known.
+  cudaError_t e = cudaMemsetAsync(table, 0xFF, (slots + 1) * sizeof(KeyEntry), stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(records, 0, recs * sp.rec_stride, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dctl, 0, sizeof(Control), stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(&dctl->overflow_agg, 0xFF, 4, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(bits, 0, words * 4 + 16, stream);
+  if (e != cudaSuccess) return cuda_fail(e, "scratch initialisation");
+
+  sp.table = static_cast<KeyEntry*>(table);
+  sp.table_mask = slots - 1;
+  sp.records = static_cast<unsigned char*>(records);
+  sp.recs_total = (uint32_t)recs;
+  sp.chunk = (uint32_t)chunk;
+  sp.alloc = &dctl->alloc;
+  sp.status = dctl->status;
+  if (P.rows > 0) {
+    scan_kernel<<<(unsigned)ncta, kScanThreads, P.smem, stream>>>(sp);
+    t_timings.launches += 1;
+  }
+  fp.scan = sp;
+  fp.order_bits = static_cast<uint32_t*>(bits);
+  fp.word_prefix = static_cast<uint32_t*>(prefix);
+  fp.block_sums = static_cast<uint32_t*>(bsums);
+  fp.perm = static_cast<uint32_t*>(perm);
+  fp.firsts = static_cast<uint32_t*>(firsts);
+  fp.groups = &dctl->groups;
+  fp.has_nulls = dctl->has_nulls;
+  fp.overflow_agg = &dctl->overflow_agg;
+  fp.words = words;
+  for (int c = 0; c < P.n_out; ++c) {
+    fp.out[c].values = out_vals[c];
+    fp.out[c].validity = out_valid[c];
+  }
+  const unsigned rec_blocks = (unsigned)std::min<uint64_t>((recs + kFinishThreads - 1) / kFinishThreads, (uint64_t)ds->sms * 16);
+  finish_mark<<<std::max(1u, rec_blocks), kFinishThreads, 0, stream>>>(fp);
+  finish_chunk_sums<<<(unsigned)chunks, kFinishThreads, 0, stream>>>(fp);
+  finish_scan_chunks<<<1, 1024, 0, stream>>>(fp, (uint32_t)chunks);
+  finish_word_prefix<<<(unsigned)chunks, 1024, 0, stream>>>(fp);
+  finish_rank<<<std::max(1u, rec_blocks), kFinishThreads, 0, stream>>>(fp);
+  const unsigned out_blocks = (unsigned)std::min<uint64_t>((out_rows + kFinishThreads - 1) / kFinishThreads, (uint64_t)ds->sms * 16);
+  finish_output<<<std::max(1u, out_blocks), kFinishThreads, 0, stream>>>(fp);
+  t_timings.launches += 6;
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  if ((st = noalloc_wait(stream))) return st;
+  Control hc;
+  CK(cudaMemcpyAsync(&hc, dctl, sizeof(Control), cudaMemcpyDeviceToHost, stream), "control block");
+  if ((st = noalloc_wait(stream))) return st;
+
+  const uint32_t status = hc.status[0];
+  if (status & ST_TIMEOUT) return fail(DFC_TIMEOUT, "a bounded device wait gave up");
+  if (status & ST_CAPACITY) {
+    char msg[200];
+    snprintf(msg, sizeof msg,
+             "dfc_groupby_noalloc: more groups than the table sized for this capacity holds "
+             "(%u of %llu records handed out, %llu table slots)",
+             hc.alloc, (unsigned long long)recs, (unsigned long long)slots);
+    return fail(DFC_CAPACITY, msg);
+  }
+  if (status & ST_OVERFLOW) {
+    const uint32_t a = hc.overflow_agg;
+    const int idt = (a < (uint32_t)query->n_aggs) ? P.out_agg_input_dtype[a] : DFC_INT64;
+    return fail(DFC_DATA_OVERFLOW, overflow_message(idt));
+  }
+  if (status & ST_FAULT)
+    return fail(DFC_DATA_FAULT,
+                "Mojo GPU data fault: variance of a group whose mean is far from its spread; the CPU adjudicates");
+  if (status & ST_ZERO_FAULT)
+    return fail(DFC_DATA_FAULT, "Mojo GPU data fault: mixed signed-zero extrema; the CPU adjudicates");
+  const uint64_t G = hc.groups;
+  if (G > capacity) {
+    char msg[160];
+    snprintf(msg, sizeof msg, "dfc_groupby_noalloc: the query has %llu groups; the outputs hold %llu",
+             (unsigned long long)G, (unsigned long long)capacity);
+    return fail(DFC_CAPACITY, msg);
+  }
+  for (int c = 0; c < P.n_out; ++c) {
+    outputs[c].dtype = P.out_dtype[c];
+    outputs[c].has_nulls = hc.has_nulls[c] != 0 ? 1 : 0;
+    if (G == 0) continue;
+    e = cudaMemcpyAsync(outputs[c].values, out_vals[c], G * dtype_size(P.out_dtype[c]), cudaMemcpyDeviceToDevice, stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(outputs[c].validity, out_valid[c], ((G + 31) / 32) * 4, cudaMemcpyDeviceToDevice, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "output copy");
+  }
+  if ((st = noalloc_wait(stream))) return st;
+  *groups = G;
+  t_timings.groups = G;
+  t_timings.table_slots = slots;
+  t_timings.regime = sp.smem_slots ? 1 : 0;
+  return DFC_OK;
+}
+
+}  // extern "C"

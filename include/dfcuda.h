@@ -230,6 +230,64 @@ typedef struct dfc_result dfc_result;
  * 28, 32) reduce to this call. */
 DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out);
 
+/* ------------------------------------------------------------------------ */
+/* The same query without any device allocation.  No counterpart in the    */
+/* reference: it is for callers that cannot call cudaMalloc -- code running  */
+/* under an allocator that owns the device heap (a host framework's caching */
+/* pool or a fixed memory budget), or code that must not allocate while it  */
+/* holds a lock or serves latency-bound requests.  They pass device inputs  */
+/* and device output buffers they already own; the working memory (key      */
+/* table, group records, order bitmaps, staged outputs) comes from one       */
+/* fixed array of DFC_NOALLOC_SCRATCH_BYTES that every GPU loading this     */
+/* library holds until the process exits.                                   */
+/*                                                                          */
+/* - A query whose working memory exceeds the array is rejected with        */
+/*   DFC_CAPACITY and a message giving the bytes it needs; nothing runs.    */
+/*   Roughly: rows/4 bytes of bitmaps plus, per group of capacity, 32 to 64 */
+/*   bytes of table, 16 to 32 bytes per output column and one group record; */
+/*   what is left of the array goes to records for claims that lose a race. */
+/*   A query whose racing claims use up those records fails with           */
+/*   DFC_CAPACITY too (hot keys over many groups); dfc_groupby regrows.     */
+/* - The first call on a device looks up the array's device address (with  */
+/*   that device current); make that first call before any stream capture. */
+/* - Every call shares the array, which keeps the last call's contents;     */
+/*   each call clears what must start at zero.  The library runs one call   */
+/*   per device at a time and waits for its work, but work that is still on */
+/*   the GPU when the next call starts (after a DFC_TIMEOUT, say) races     */
+/*   with it and corrupts both: calls must not overlap on the GPU.          */
+/* - Results are the same as dfc_groupby's.  Groups come back in the same   */
+/*   order; floating sums and moments may differ in the last bits, as      */
+/*   between two dfc_groupby calls.  No timings are recorded.               */
+/* ------------------------------------------------------------------------ */
+#define DFC_NOALLOC_SCRATCH_BYTES (64ull << 20)
+
+/* A column in device memory, read in place. */
+typedef struct dfc_device_column {
+  int32_t dtype;            /* dfc_dtype */
+  int32_t reserved;         /* 0 */
+  const void* values;       /* rows values, 16-byte aligned */
+  const uint32_t* validity; /* LSB-first bitmap at bit offset 0 in ceil(rows/32) 32-bit words,
+                               16-byte aligned; NULL when every row is valid */
+} dfc_device_column;
+
+/* An output column in device memory the caller owns. */
+typedef struct dfc_device_output {
+  void* values;       /* capacity * 8 bytes at least (any output type fits) */
+  uint32_t* validity; /* ceil(capacity / 32) 32-bit words, LSB first */
+  int32_t dtype;      /* set by the call: the column's dfc_dtype */
+  int32_t has_nulls;  /* set by the call: 1 when some validity bit is 0 */
+} dfc_device_output;
+
+/* Runs `query` over `columns` (query->n_inputs entries, all `rows` long, on
+ * `device`; query->inputs is not read) and writes n_keys + n_aggs columns
+ * (keys, then one per aggregation) into `outputs`, *groups rows each.
+ * `capacity` is the most groups the outputs hold: more groups fail with
+ * DFC_CAPACITY.  It waits for the work on query->stream, or on the calling
+ * thread's default stream when that is NULL. */
+DFC_API dfc_status dfc_groupby_noalloc(const dfc_query* query, int32_t device, uint64_t rows,
+                                       const dfc_device_column* columns, uint64_t capacity,
+                                       dfc_device_output* outputs, uint64_t* groups);
+
 DFC_API uint64_t dfc_result_rows(const dfc_result* result);
 DFC_API int32_t dfc_result_columns(const dfc_result* result);
 /* Device pointers of column i; *device_validity is NULL when the column has

@@ -30,7 +30,7 @@ def test_library_exports_every_declared_symbol():
     for name in declared_symbols():
         assert hasattr(lib, name), name
     bound = {s[0] for s in N.SIGNATURES}
-    assert set(declared_symbols()) <= bound | {"dfc_groupby_noalloc"}
+    assert set(declared_symbols()) <= bound
 
 
 def test_version_and_status_names():

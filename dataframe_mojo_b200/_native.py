@@ -32,6 +32,7 @@ AGG_COUNT, AGG_SUM, AGG_MEAN, AGG_MIN, AGG_MAX, AGG_VAR, AGG_STD, AGG_LEN, AGG_N
 Q_MAINTAIN_ORDER = 1
 Q_FORCE_GLOBAL = 2
 Q_FORCE_SHARED = 4
+Q_FORCE_PARTITIONED = 16
 Q_FLOAT32_FP64 = 8
 
 COLUMN_HOST = 0
@@ -94,7 +95,8 @@ class Timings(C.Structure):
         ("regime", C.c_int32),
         ("retries", C.c_int32),
         ("launches", C.c_int32),
-        ("reserved", C.c_int32),
+        ("partitions", C.c_int32),
+        ("aggregate_ns", C.c_double),
     ]
 
 

@@ -83,6 +83,12 @@ __device__ __forceinline__ void cas128(void* addr, uint64_t cmp_lo, uint64_t cmp
 __device__ __forceinline__ uint64_t ld_cg_u64(const void* p) {
   return __ldcg(reinterpret_cast<const unsigned long long*>(p));
 }
+// A load every iteration of a spin wait issues afresh (never hoisted).
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const void* p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
 __device__ __forceinline__ uint32_t ld_cg_u32(const void* p) {
   return __ldcg(reinterpret_cast<const unsigned int*>(p));
 }

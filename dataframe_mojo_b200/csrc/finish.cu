@@ -41,8 +41,16 @@ __global__ void finish_mark(const __grid_constant__ FinishParams f) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     uint32_t first;
     const bool live = live_record(p, i, first);
+    if (live && first >= p.rows) {
+      atomicOr(p.status + 2, CHK_FIRST);
+      f.firsts[i] = 0xFFFFFFFFu;
+      continue;
+    }
     f.firsts[i] = live ? first : 0xFFFFFFFFu;
-    if (live) atomicOr(&f.order_bits[first >> 5], 1u << (first & 31));
+    if (live) {
+      const uint32_t bit = 1u << (first & 31);
+      if (atomicOr(&f.order_bits[first >> 5], bit) & bit) atomicOr(p.status + 2, CHK_DUP);
+    }
   }
 }
 
@@ -166,6 +174,11 @@ __device__ uint64_t output_cell(const FinishParams& f, const OutCol& oc, const u
     const bool gather = p.key_mode == KEY_TICKET || kf.dtype == DFC_FLOAT32 || kf.dtype == DFC_FLOAT64;
     if (gather) {
       const uint32_t row = ~*reinterpret_cast<const uint32_t*>(rec + kRecFirst);
+      if (row >= p.rows) {
+        atomicOr(p.status + 2, CHK_FIRST);
+        *ok = false;
+        return 0;
+      }
       if (col.validity && !bit_valid(col.validity, row)) {
         *ok = false;
         return 0;
@@ -292,8 +305,13 @@ __global__ void finish_output(const __grid_constant__ FinishParams f) {
   const int lane = threadIdx.x & 31;
   for (uint64_t wbase = gwarp * 32; wbase < G; wbase += warps * 32) {
     const uint64_t i = wbase + lane;
-    const bool active = i < G;
-    const unsigned char* rec = active ? record_at(p, f.perm[i]) : nullptr;
+    bool active = i < G;
+    const uint32_t gid = active ? f.perm[i] : 0u;
+    if (active && gid >= records_handed_out(p)) {
+      atomicOr(p.status + 2, CHK_PERM);
+      active = false;
+    }
+    const unsigned char* rec = active ? record_at(p, gid) : nullptr;
     for (int c = 0; c < f.n_out; ++c) {
       const OutCol& oc = f.out[c];
       bool ok = false;

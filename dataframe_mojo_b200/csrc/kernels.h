@@ -13,6 +13,15 @@ constexpr int kFinishThreads = 256;
 constexpr int kFinishChunk = 4096;  // bitmap words per prefix-scan block
 
 __global__ void scan_kernel(const __grid_constant__ ScanParams p);
+// Radix-partitioned regime: pass A (filter, keys, partition) and pass B
+// (per-partition aggregation by clusters of kAggCluster CTAs).
+constexpr int kAggCluster = 8;
+constexpr int kAggThreads = 512;
+constexpr int kPartMax = 1024;  // partitions at most
+__global__ void partition_count(const __grid_constant__ ScanParams p);
+__global__ void partition_offsets(const __grid_constant__ ScanParams p, uint32_t ctas);
+__global__ void partition_kernel(const __grid_constant__ ScanParams p);
+__global__ void partition_aggregate(const __grid_constant__ ScanParams p);
 __global__ void finish_mark(const __grid_constant__ FinishParams f);
 __global__ void finish_chunk_sums(const __grid_constant__ FinishParams f);
 __global__ void finish_scan_chunks(const __grid_constant__ FinishParams f, uint32_t chunks);

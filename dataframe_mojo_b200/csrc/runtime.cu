@@ -31,6 +31,7 @@
 using namespace dfc;
 
 struct dfc_column {
+  uint64_t serial = 0;  // registration number: identifies the column for learned group counts
   int32_t device = 0;
   dfc_dtype dtype = DFC_INT64;
   uint64_t rows = 0;
@@ -127,7 +128,9 @@ std::string overflow_message(int input_dtype) {
 struct DeviceState {
   bool ready = false;
   int sms = 0;
-  size_t smem_optin = 0;
+  size_t smem_optin = 0;       // scan_kernel's dynamic shared memory limit
+  size_t part_smem_optin = 0;  // partition_kernel's
+  int agg_clusters = 0;        // partition_aggregate clusters resident at once
   int scan_occupancy = 1;
 };
 std::mutex g_dev_mu;
@@ -137,7 +140,8 @@ std::map<int, DeviceState> g_dev;
 // its table from them (the reference sizes from column statistics,
 // dataframe/aggregation/hash_table.mojo:699-714).
 std::mutex g_learn_mu;
-std::map<std::vector<const void*>, uint64_t> g_learned;
+std::map<std::vector<uint64_t>, uint64_t> g_learned;
+std::atomic<uint64_t> g_column_serial{0};
 
 dfc_status device_ready(int dev, DeviceState** out) {
   std::lock_guard<std::mutex> lk(g_dev_mu);
@@ -160,6 +164,32 @@ dfc_status device_ready(int dev, DeviceState** out) {
     d.smem_optin = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;
     CK(cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin),
        "cudaFuncSetAttribute");
+    CK(cudaFuncGetAttributes(&fa, partition_kernel), "cudaFuncGetAttributes");
+    d.part_smem_optin = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;
+    CK(cudaFuncSetAttribute(partition_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.part_smem_optin),
+       "cudaFuncSetAttribute");
+    // The counting pass uses the scan's ring (smaller static shared memory).
+    CK(cudaFuncGetAttributes(&fa, partition_count), "cudaFuncGetAttributes");
+    CK(cudaFuncSetAttribute(partition_count, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)(prop.sharedMemPerBlockOptin - fa.sharedSizeBytes)),
+       "cudaFuncSetAttribute");
+    // Clusters of kAggCluster CTAs for the per-partition aggregation.
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kAggCluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(kAggCluster * 64);
+    cfg.blockDim = dim3(kAggThreads);
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, partition_aggregate, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      clusters = 0;
+    }
+    d.agg_clusters = clusters;
     d.ready = true;
   }
   *out = &d;
@@ -257,7 +287,7 @@ struct Plan {
   int device = 0;
   uint64_t rows = 0;
   uint64_t est_groups = 0;
-  std::vector<const void*> key_sig;
+  std::vector<uint64_t> key_sig;  // registration numbers of the key columns
 };
 
 dfc_status plan_query(const dfc_query* q, Plan& P) {
@@ -314,7 +344,7 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
     f.dtype = c->dtype;
     f.bits = 8 * dtype_size(c->dtype);
     total_bits += f.bits + (c->validity ? 1 : 0);
-    P.key_sig.push_back(c);
+    P.key_sig.push_back(c->serial);
   }
   if (total_bits <= 64) {
     sp.key_mode = KEY_PACKED;
@@ -371,6 +401,9 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
     if (depth > 32) return fail(DFC_UNSUPPORTED, "filter program too deep");
   }
   if (q->n_pred > 0 && depth != 1) return fail(DFC_INVALID, "malformed filter program");
+  // Key and filter columns hold the first slots: the partition counting pass
+  // stages only those.
+  sp.n_stage_count = n_slots;
 
   // Value states: one ValField per distinct aggregated column.
   struct Need {
@@ -487,12 +520,13 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
   for (int c = 0; c < n_slots; ++c)
     if (((uintptr_t)sp.cols[c].values & 15u) != 0) aligned = false;
   int tile = 1024;
-  size_t stage_bytes = 0, stage_tx = 0;
+  size_t stage_bytes = 0, stage_tx = 0, stage_tx_count = 0;
   for (; tile >= 128; tile >>= 1) {
     // tile >= 128: every values block (tile * size) and validity block
     // (tile / 8) is a multiple of 16 bytes, as bulk copies require.
     size_t b = 0;
     for (int c = 0; c < n_slots; ++c) {
+      if (c == sp.n_stage_count) stage_tx_count = b;
       sp.stage_off[c] = (int)b;
       b += (size_t)tile * sp.cols[c].size;
       if (sp.cols[c].validity) {
@@ -503,6 +537,7 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
       }
     }
     stage_tx = b;
+    if (sp.n_stage_count == n_slots) stage_tx_count = b;
     b = (b + 127) & ~(size_t)127;
     stage_bytes = b;
     if (b * 4 <= 96 * 1024) break;
@@ -511,6 +546,7 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
   sp.tile_rows = tile;
   sp.stage_bytes = (int)stage_bytes;
   sp.stage_tx = (int)stage_tx;
+  sp.stage_tx_count = (int)stage_tx_count;
   sp.stages = 4;
   sp.use_tma = aligned ? 1 : 0;
   sp.tiles = (P.rows + tile - 1) / tile;
@@ -568,11 +604,11 @@ dfc_status ensure_stats(dfc_column* c, DeviceState* ds, cudaStream_t stream) {
   return DFC_OK;
 }
 
-// Estimated number of groups: what the last query on these keys found, else
-// the product of the key columns' distinct estimates (capped by their value
-// ranges), capped by the row count.
-uint64_t estimate_groups(const dfc_query* q, const Plan& P, DeviceState* ds, cudaStream_t stream) {
-  {
+// Estimated number of groups: what the last query on these key columns
+// found (when `learned`), else the product of the key columns' distinct
+// estimates (capped by their value ranges), capped by the row count.
+uint64_t estimate_groups(const dfc_query* q, const Plan& P, DeviceState* ds, cudaStream_t stream, bool learned = true) {
+  if (learned) {
     std::lock_guard<std::mutex> lk(g_learn_mu);
     auto it = g_learned.find(P.key_sig);
     if (it != g_learned.end()) return it->second;
@@ -618,16 +654,76 @@ struct Scratch {
 
 // Control block copied back after every attempt.
 struct Control {
-  uint32_t status[4];
+  uint32_t status[4];  // [0] StatusBits, [1] CapacityBits, [2] partition-pass index checks
   uint32_t groups;
   uint32_t overflow_agg;
   uint32_t alloc;
-  uint32_t pad;
+  uint32_t part_next;
+  uint32_t pad[4];
   uint32_t has_nulls[kMaxOut];
 };
 
+// Radix-partitioned regime sizing (the ScanParams fields of that name).
+struct PartPlan {
+  uint32_t bits = 0;
+  uint32_t words = 0;
+  uint32_t flush = 0;
+  uint32_t stage_off = 0;
+  uint32_t agg_slots = 0;
+  uint64_t recs = 0;
+  size_t smem = 0;        // pass A dynamic shared memory
+  size_t count_smem = 0;  // counting pass dynamic shared memory
+  int clusters = 0;
+};
+
+// L2 bytes the clusters' tables may take together (of 126 MB): the rest
+// serves the streamed partition rows and the records being written.
+constexpr double kAggL2Budget = 40.0 * 1024 * 1024;
+
+// Sizes the regime for `est` groups; false when it does not apply (keys
+// wider than 64 bits, too little shared memory, no cluster launch).
+bool plan_partitions(const Plan& P, const DeviceState* ds, uint64_t est, PartPlan& pp) {
+  const ScanParams& sp = P.sp;
+  if (sp.key_mode != KEY_PACKED || ds->agg_clusters < 1 || P.rows == 0 || P.rows >= 0xFFFFFFFFull) return false;
+  pp.words = 2 + (uint32_t)sp.n_vals;
+  pp.clusters = ds->agg_clusters;
+  // Staging area: what the ring leaves, a power of two of rows, split into
+  // one region per consumer warp of at least 128 rows (a warp stages up to
+  // 128 rows a tile); at most 2^15 rows (flush positions are 16-bit).
+  const size_t ring = (size_t)sp.stages * sp.stage_bytes + 2 * sp.stages * sizeof(uint64_t);
+  pp.count_smem = ring;
+  pp.stage_off = (uint32_t)((ring + 15) & ~(size_t)15);
+  if (ds->part_smem_optin <= pp.stage_off) return false;
+  const size_t per_row = (size_t)pp.words * 8 + 4;
+  size_t rows_fit = (ds->part_smem_optin - pp.stage_off) / per_row;
+  rows_fit = std::min<size_t>(rows_fit, 32768);
+  uint32_t flush = 1;
+  while ((size_t)flush * 2 <= rows_fit) flush <<= 1;
+  if (flush < 1024u) return false;
+  pp.flush = flush;
+  pp.smem = pp.stage_off + (size_t)flush * per_row;
+  // Partitions: the fewest (>= 16) whose tables, at load <= 1/2, fit the L2
+  // budget together.
+  const uint64_t groups = std::max<uint64_t>(est, 1);
+  uint32_t bits = 4;
+  uint64_t slots = 0;
+  for (;; ++bits) {
+    slots = next_pow2(std::max<uint64_t>(256, 2 * ((groups >> bits) + 1)));
+    if (bits >= 10 || (double)pp.clusters * (double)(slots + 1) * sp.rec_stride <= kAggL2Budget) break;
+  }
+  pp.bits = bits;
+  pp.agg_slots = (uint32_t)slots;
+  pp.recs = std::min<uint64_t>(P.rows, groups + groups / 4 + 4096);
+  return true;
+}
+
+// One attempt of the query at the given capacities: the global or
+// shared-memory regime (`pp` null; `slots` key-table entries) or the
+// radix-partitioned regime (`pp`).  *grow: a capacity ran out; the caller
+// regrows it (host_ctl->status[1] says which in the partitioned regime) and
+// retries.
 dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_t stream, uint64_t slots,
-                       dfc_result** out, bool* grow, Control* host_ctl) {
+                       const PartPlan* pp, dfc_result** out, bool* grow, Control* host_ctl) {
   *grow = false;
   ScanParams& sp = P.sp;
   FinishParams& fp = P.fp;
@@ -635,24 +731,47 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   S.stream = stream;
 
   int occ = 1;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_kernel, kScanThreads, P.smem), "occupancy");
+  if (pp) {
+    // The counting pass and pass A must see the same tiles per CTA: one grid.
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, partition_kernel, kScanThreads, pp->smem), "occupancy");
+    occ = 1;
+  } else {
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_kernel, kScanThreads, P.smem), "occupancy");
+  }
   occ = std::max(1, occ);
   uint64_t ncta = (uint64_t)ds->sms * (uint64_t)occ;
   ncta = std::max<uint64_t>(1, std::min<uint64_t>(ncta, std::max<uint64_t>(1, sp.tiles)));
-  // Records: the groups the table may hold (load factor <= 1/2) plus every
-  // CTA's partly used last chunk.
-  const uint64_t groups_cap = std::min<uint64_t>(P.rows, slots / 2);
-  uint64_t chunk = 64;
-  while (chunk < 1024 && chunk * ncta * 8 < groups_cap) chunk <<= 1;
-  // Slack for holes: records reserved by claims that lost a race.
-  const uint64_t recs = groups_cap + groups_cap / 8 + chunk * ncta;
+  uint64_t chunk = 64, recs;
+  if (pp) {
+    // Pass B appends every group exactly once: no holes, no chunks.
+    recs = std::max<uint64_t>(1, pp->recs);
+  } else {
+    // Records: the groups the table may hold (load factor <= 1/2) plus every
+    // CTA's partly used last chunk.
+    const uint64_t groups_cap = std::min<uint64_t>(P.rows, slots / 2);
+    while (chunk < 1024 && chunk * ncta * 8 < groups_cap) chunk <<= 1;
+    // Slack for holes: records reserved by claims that lost a race.
+    recs = groups_cap + groups_cap / 8 + chunk * ncta;
+  }
   if (recs >= 0xFFFFFFFFull) return fail(DFC_CAPACITY, "group capacity exceeds 2^32 records");
 
-  void *table, *records, *ctl, *bits, *prefix, *bsums, *perm, *firsts;
+  void *table = nullptr, *records, *ctl, *bits, *prefix, *bsums, *perm, *firsts;
+  void *part_buf = nullptr, *part_counts = nullptr, *part_totals = nullptr, *part_start = nullptr, *agg_tables = nullptr;
   const uint64_t words = (P.rows + 31) / 32;
   const uint64_t chunks = std::max<uint64_t>(1, (words + kFinishChunk - 1) / kFinishChunk);
+  const uint64_t nparts = pp ? (1ull << pp->bits) : 0;
   dfc_status st;
-  if ((st = S.alloc(&table, (slots + 1) * sizeof(KeyEntry), "key table"))) return S.release(), st;
+  if (pp) {
+    // Every row may pass the filter: part_buf holds all of them.
+    if ((st = S.alloc(&part_buf, P.rows * pp->words * 8, "partition rows"))) return S.release(), st;
+    if ((st = S.alloc(&part_counts, ncta * nparts * 4, "partition counts"))) return S.release(), st;
+    if ((st = S.alloc(&part_totals, nparts * 4, "partition totals"))) return S.release(), st;
+    if ((st = S.alloc(&part_start, nparts * 4, "partition starts"))) return S.release(), st;
+    if ((st = S.alloc(&agg_tables, (uint64_t)pp->clusters * (pp->agg_slots + 1ull) * sp.rec_stride, "partition tables")))
+      return S.release(), st;
+  } else {
+    if ((st = S.alloc(&table, (slots + 1) * sizeof(KeyEntry), "key table"))) return S.release(), st;
+  }
   if ((st = S.alloc(&records, recs * sp.rec_stride, "group records"))) return S.release(), st;
   if ((st = S.alloc(&ctl, sizeof(Control), "control block"))) return S.release(), st;
   if ((st = S.alloc(&bits, words * 4 + 16, "order bitmap"))) return S.release(), st;
@@ -686,9 +805,16 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   };
 
   Control* dctl = static_cast<Control*>(ctl);
-  cudaError_t e = cudaMemsetAsync(table, 0xFF, (slots + 1) * sizeof(KeyEntry), stream);
-  // Group records start all-zero: every field's identity (dfc_internal.h).
-  if (e == cudaSuccess) e = cudaMemsetAsync(records, 0, recs * sp.rec_stride, stream);
+  cudaError_t e;
+  if (pp) {
+    // The partition kernels write everything they read; pass B writes every
+    // record it hands out.
+    e = cudaSuccess;
+  } else {
+    e = cudaMemsetAsync(table, 0xFF, (slots + 1) * sizeof(KeyEntry), stream);
+    // Group records start all-zero: every field's identity (dfc_internal.h).
+    if (e == cudaSuccess) e = cudaMemsetAsync(records, 0, recs * sp.rec_stride, stream);
+  }
   if (e == cudaSuccess) e = cudaMemsetAsync(ctl, 0, sizeof(Control), stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(&dctl->overflow_agg, 0xFF, 4, stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(bits, 0, words * 4 + 16, stream);
@@ -699,19 +825,65 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   }
 
   sp.table = static_cast<KeyEntry*>(table);
-  sp.table_mask = slots - 1;
+  sp.table_mask = pp ? 0 : slots - 1;
   sp.records = static_cast<unsigned char*>(records);
   sp.recs_total = (uint32_t)recs;
   sp.chunk = (uint32_t)chunk;
   sp.alloc = &dctl->alloc;
   sp.status = dctl->status;
+  sp.part_bits = pp ? pp->bits : 0;
+  if (pp) {
+    sp.part_words = pp->words;
+    sp.part_buf = static_cast<unsigned long long*>(part_buf);
+    sp.part_cap = P.rows;
+    sp.part_counts = static_cast<uint32_t*>(part_counts);
+    sp.part_totals = static_cast<uint32_t*>(part_totals);
+    sp.part_start = static_cast<uint32_t*>(part_start);
+    sp.part_flush = pp->flush;
+    sp.part_stage_off = pp->stage_off;
+    sp.agg_slots = pp->agg_slots;
+    sp.agg_tables_n = (uint32_t)pp->clusters;
+    sp.agg_tables = static_cast<unsigned char*>(agg_tables);
+    sp.part_next = &dctl->part_next;
+  }
 
-  cudaEvent_t ev[3];
+  cudaEvent_t ev[6];
   for (auto& x : ev) cudaEventCreate(&x);
   cudaEventRecord(ev[0], stream);
-  if (P.rows > 0) {
-    scan_kernel<<<(unsigned)ncta, kScanThreads, P.smem, stream>>>(sp);
-    t_timings.launches += 1;
+  if (pp) {
+    partition_count<<<(unsigned)ncta, kScanThreads, pp->count_smem, stream>>>(sp);
+    cudaEventRecord(ev[4], stream);
+    partition_offsets<<<(unsigned)((nparts + 255) / 256), 256, 0, stream>>>(sp, (uint32_t)ncta);
+    cudaEventRecord(ev[5], stream);
+    partition_kernel<<<(unsigned)ncta, kScanThreads, pp->smem, stream>>>(sp);
+    cudaEventRecord(ev[3], stream);
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kAggCluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    const uint64_t clusters = std::min<uint64_t>((uint64_t)pp->clusters, nparts);
+    cfg.gridDim = dim3((unsigned)(clusters * kAggCluster));
+    cfg.blockDim = dim3(kAggThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, partition_aggregate, sp);
+    if (e != cudaSuccess) {
+      free_outputs();
+      S.release();
+      for (auto& x : ev) cudaEventDestroy(x);
+      return cuda_fail(e, "partition aggregation launch");
+    }
+    t_timings.launches += 4;
+  } else {
+    if (P.rows > 0) {
+      scan_kernel<<<(unsigned)ncta, kScanThreads, P.smem, stream>>>(sp);
+      t_timings.launches += 1;
+    }
+    cudaEventRecord(ev[3], stream);
   }
   cudaEventRecord(ev[1], stream);
 
@@ -753,13 +925,37 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
     free_outputs();
     return st;
   }
-  float ms_scan = 0, ms_finish = 0;
-  cudaEventElapsedTime(&ms_scan, ev[0], ev[1]);
+  float ms_scan = 0, ms_agg = 0, ms_finish = 0, ms_count = 0, ms_offsets = 0;
+  cudaEventElapsedTime(&ms_scan, ev[0], ev[3]);
+  if (pp) {
+    cudaEventElapsedTime(&ms_count, ev[0], ev[4]);
+    cudaEventElapsedTime(&ms_offsets, ev[4], ev[5]);
+  }
+  cudaEventElapsedTime(&ms_agg, ev[3], ev[1]);
   cudaEventElapsedTime(&ms_finish, ev[1], ev[2]);
   for (auto& x : ev) cudaEventDestroy(x);
   t_timings.scan_ns += ms_scan * 1e6;
+  t_timings.aggregate_ns += ms_agg * 1e6;
   t_timings.finish_ns += ms_finish * 1e6;
-  t_timings.table_slots = slots;
+  t_timings.table_slots = pp ? (uint64_t)pp->agg_slots : slots;
+  t_timings.partitions = pp ? (int32_t)nparts : 0;
+  if (getenv("DFC_TRACE")) {
+    fprintf(stderr,
+            "dfc attempt: rows=%llu regime=%s slots=%llu recs=%llu smem_slots=%u ctas=%llu parts=%llu agg_slots=%u "
+            "clusters=%d flush=%u | status=%#x cap=%#x check=%#x alloc=%u groups=%u ms scan=%.3f (count=%.3f offsets=%.3f) "
+            "agg=%.3f fin=%.3f\n",
+            (unsigned long long)P.rows, pp ? "partitioned" : "table", (unsigned long long)slots,
+            (unsigned long long)recs, sp.smem_slots, (unsigned long long)ncta, (unsigned long long)nparts,
+            pp ? pp->agg_slots : 0u, pp ? pp->clusters : 0, pp ? pp->flush : 0u, host_ctl->status[0],
+            host_ctl->status[1], host_ctl->status[2], host_ctl->alloc, host_ctl->groups, ms_scan, ms_count, ms_offsets,
+            ms_agg, ms_finish);
+  }
+  if (host_ctl->status[2] && !(host_ctl->status[0] & ST_TIMEOUT)) {
+    free_outputs();
+    char msg[128];
+    snprintf(msg, sizeof msg, "an internal index or consistency check failed (code %#x)", host_ctl->status[2]);
+    return fail(DFC_DEVICE, msg);
+  }
 
   const uint32_t status = host_ctl->status[0];
   if (status & ST_TIMEOUT) {
@@ -865,6 +1061,7 @@ DFC_API dfc_status dfc_column_register(int32_t device, dfc_dtype dtype, uint64_t
   DeviceGuard guard(device);
   cudaStream_t stream = thread_stream(device);
   auto* c = new dfc_column();
+  c->serial = ++g_column_serial;
   c->device = device;
   c->dtype = dtype;
   c->rows = rows;
@@ -964,7 +1161,13 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
   // otherwise the global table alone.  Rows whose key finds no room in a CTA
   // table take the global path, so a low estimate costs speed, not results.
   P.sp.smem_slots = 0;
-  if (!(query->flags & DFC_Q_FORCE_GLOBAL) && P.sp.key_mode == KEY_PACKED &&
+  // Radix-partitioned when the groups' table and records would outgrow L2.
+  PartPlan pp;
+  bool partitioned = false;
+  if (!(query->flags & (DFC_Q_FORCE_GLOBAL | DFC_Q_FORCE_SHARED)) &&
+      ((query->flags & DFC_Q_FORCE_PARTITIONED) || (double)est * (P.sp.rec_stride + 32) > kAggL2Budget))
+    partitioned = plan_partitions(P, ds, est, pp);
+  if (!partitioned && !(query->flags & DFC_Q_FORCE_GLOBAL) && P.sp.key_mode == KEY_PACKED &&
       ((query->flags & DFC_Q_FORCE_SHARED) || est <= 4096)) {
     const uint64_t sslots = next_pow2(std::max<uint64_t>(64, std::min<uint64_t>(est, 4096) * 2));
     const size_t keys_off = (P.smem + 15) & ~(size_t)15;
@@ -983,9 +1186,24 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
   slots = std::min(slots, max_slots);
   for (int attempt = 0; attempt < 6; ++attempt) {
     bool grow = false;
-    st = run_attempt(query, P, ds, stream, slots, out, &grow, host_ctl);
+    st = run_attempt(query, P, ds, stream, slots, partitioned ? &pp : nullptr, out, &grow, host_ctl);
     if (!grow) break;
     t_timings.retries += 1;
+    if (partitioned) {
+      // Re-plan from the column statistics (a learned count may come from a
+      // query with another filter), at least 8x the last estimate and twice
+      // the groups already seen; the table and records at least double.
+      const uint32_t why = host_ctl->status[1];
+      const PartPlan last = pp;
+      const uint64_t stats = estimate_groups(query, P, ds, stream, false);
+      est = std::min<uint64_t>(P.rows, std::max<uint64_t>({stats, est * 8, (uint64_t)host_ctl->alloc * 2}));
+      if (!plan_partitions(P, ds, est, pp)) return fail(DFC_CAPACITY, "partition capacity could not grow further");
+      if (why & CAP_AGG_TABLE) pp.agg_slots = std::max(pp.agg_slots, std::min(last.agg_slots * 2, 1u << 28));
+      if (why & CAP_RECORDS) pp.recs = std::max<uint64_t>(pp.recs, std::min<uint64_t>(P.rows, last.recs * 2));
+      if (pp.agg_slots == last.agg_slots && pp.recs == last.recs && pp.bits == last.bits)
+        return fail(DFC_CAPACITY, "partition capacity could not grow further");
+      continue;
+    }
     if (slots >= max_slots) return fail(DFC_CAPACITY, "group table could not grow further");
     slots = std::min(slots * 8, max_slots);
   }
@@ -993,7 +1211,7 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
   if (st) return st;
   learn_groups(P, (*out)->rows);
   t_timings.groups = (*out)->rows;
-  t_timings.regime = P.sp.smem_slots ? 1 : 0;
+  t_timings.regime = partitioned ? 2 : (P.sp.smem_slots ? 1 : 0);
   t_timings.total_ns = std::chrono::duration<double, std::nano>(std::chrono::steady_clock::now() - t0).count();
   return DFC_OK;
 }
@@ -1318,6 +1536,11 @@ DFC_API dfc_status dfc_groupby_noalloc(const dfc_query* query, int32_t device, u
   if ((st = noalloc_wait(stream))) return st;
 
   const uint32_t status = hc.status[0];
+  if (hc.status[2]) {
+    char msg[128];
+    snprintf(msg, sizeof msg, "an internal index or consistency check failed (code %#x)", hc.status[2]);
+    return fail(DFC_DEVICE, msg);
+  }
   if (status & ST_TIMEOUT) return fail(DFC_TIMEOUT, "a bounded device wait gave up");
   if (status & ST_CAPACITY) {
     char msg[200];

@@ -365,7 +365,7 @@ __device__ __forceinline__ void claimed(const ScanParams& p, uint32_t gid, uint6
 // in one 128-bit CAS, so this only loops on a torn read).
 __device__ __forceinline__ uint64_t entry_meta(const ScanParams& p, const KeyEntry* e) {
   for (uint32_t i = 0; i < kSpinLimit; ++i) {
-    const uint64_t m = ld_cg_u64(&e->meta);
+    const uint64_t m = ld_relaxed_u64(&e->meta);
     if (m != kEmpty) return m;
   }
   atomicOr(p.status, ST_TIMEOUT);
@@ -548,46 +548,51 @@ __device__ __forceinline__ int nth_lane(uint32_t grp, int i) {
   return grp ? __ffs(grp) - 1 : (int)(threadIdx.x & 31);
 }
 
-// Reduction over each lane's group; shuffles run on the full warp.
+// Reduction over each lane's group, members in lane order; shuffles run on
+// the full warp, one per member of the largest group.
 template <typename V, typename Op>
 __device__ __forceinline__ V group_reduce(uint32_t grp, int maxpop, V mine, V identity, bool take, Op op) {
   V acc = identity;
+  uint32_t left = grp;
+  const int lane = threadIdx.x & 31;
   for (int i = 0; i < maxpop; ++i) {
-    const V v = __shfl_sync(0xffffffffu, take ? mine : identity, nth_lane(grp, i));
-    if (i < __popc(grp)) acc = op(acc, v);
+    const V v = __shfl_sync(0xffffffffu, take ? mine : identity, left ? __ffs(left) - 1 : lane);
+    if (left) {
+      acc = op(acc, v);
+      left &= left - 1;
+    }
   }
   return acc;
 }
 
-__device__ __forceinline__ void smem_rows(const ScanParams& p, const Step& s, const SmemTable& st,
-                                          const RowRef (&x)[kR], const uint32_t (&rows)[kR], bool (&sel)[kR],
-                                          const uint64_t (&kw)[kR]) {
+// One warp's rows folded into their records, rows of one record first
+// reduced across lanes: `grp` the lanes sharing this lane's record `rec` (0
+// for a lane outside), `maxpop` the largest group in the warp.  The group's
+// lowest lane (the leader) applies one atomic per field.  `get(v, ok, b)`
+// gives the lane's validity and raw bits of value column v.  Works on shared
+// or global records (generic addresses).
+template <typename Get>
+__device__ __forceinline__ void group_update(const ScanParams& p, unsigned char* rec, uint32_t grp, int maxpop, bool loc,
+                                             uint32_t row, Get&& get) {
   const int lane = threadIdx.x & 31;
-#pragma unroll
-  for (int j = 0; j < kR; ++j) {
-    const int ls = sel[j] ? smem_probe(p, st, kw[j]) : -1;
-    const bool loc = ls >= 0;
-    uint32_t grp = __match_any_sync(0xffffffffu, kw[j]) & __ballot_sync(0xffffffffu, loc);
-    if (!loc) grp = 0;
-    const int maxpop = __reduce_max_sync(0xffffffffu, (unsigned)__popc(grp));
-    if (maxpop == 0) continue;
+  {
     const bool leader = loc && lane == __ffs(grp) - 1;
-    unsigned char* rec = loc ? st.recs + (size_t)ls * p.rec_stride : nullptr;
-    // The group's earliest row.  The CTA record always keeps its first row:
+    // The group's earliest row.  A CTA record always keeps its first row:
     // it is the claim row when the record is merged into the global table.
     const uint32_t first =
-        group_reduce<uint32_t>(grp, maxpop, rows[j], 0xFFFFFFFFu, loc, [](uint32_t a, uint32_t b2) { return a < b2 ? a : b2; });
+        group_reduce<uint32_t>(grp, maxpop, row, 0xFFFFFFFFu, loc, [](uint32_t a, uint32_t b2) { return a < b2 ? a : b2; });
     if (leader) {
       atomicMax(reinterpret_cast<uint32_t*>(rec + kRecFirst), ~first);
       if (p.off_len >= 0) atomicAdd(reinterpret_cast<uint32_t*>(rec + p.off_len), (uint32_t)__popc(grp));
     }
     for (int v = 0; v < p.n_vals; ++v) {
       const ValField& f = p.vals[v];
-      const int c = f.input, dt = f.dtype;
+      const int dt = f.dtype;
       const bool isf = dt_float(dt);
-      const ColRef cr = col_ref(p, s, c);
-      const bool ok = loc && rvalid(cr, x[j]);
-      const uint64_t b = ok ? load_bits(rv(cr, x[j]), p.cols[c].size, x[j].r) : 0ull;
+      bool ok = false;
+      uint64_t b = 0;
+      if (loc) get(v, ok, b);
+      if (!ok) b = 0;
       const double xd = isf ? bits_to_f64(b, dt) : bits_as_double(b, dt);
       const bool nan = ok && isf && xd != xd;
       const uint32_t vmask = grp & __ballot_sync(0xffffffffu, ok);
@@ -605,11 +610,15 @@ __device__ __forceinline__ void smem_rows(const ScanParams& p, const Step& s, co
           const uint64_t xv = ok ? (uns ? b : (uint64_t)bits_to_i64(b, dt)) : 0ull;
           const uint64_t xhi = (!uns && (int64_t)xv < 0) ? ~0ull : 0ull;
           __int128 exact = 0;
+          uint32_t left = grp;
           for (int i = 0; i < maxpop; ++i) {
-            const int src = nth_lane(grp, i);
+            const int src = left ? __ffs(left) - 1 : lane;
             const uint64_t vlo = __shfl_sync(0xffffffffu, xv, src);
             const uint64_t vhi = __shfl_sync(0xffffffffu, xhi, src);
-            if (i < __popc(grp)) exact += (__int128)(((unsigned __int128)vhi << 64) | vlo);
+            if (left) {
+              exact += (__int128)(((unsigned __int128)vhi << 64) | vlo);
+              left &= left - 1;
+            }
           }
           if (leader && vmask) {
             if (f.sum_kind == SUM_I64) {
@@ -662,6 +671,27 @@ __device__ __forceinline__ void smem_rows(const ScanParams& p, const Step& s, co
         if (leader && vmask) atomicAdd(reinterpret_cast<double*>(rec + f.off_m2), s2);
       }
     }
+  }
+}
+
+__device__ __forceinline__ void smem_rows(const ScanParams& p, const Step& s, const SmemTable& st,
+                                          const RowRef (&x)[kR], const uint32_t (&rows)[kR], bool (&sel)[kR],
+                                          const uint64_t (&kw)[kR]) {
+#pragma unroll
+  for (int j = 0; j < kR; ++j) {
+    const int ls = sel[j] ? smem_probe(p, st, kw[j]) : -1;
+    const bool loc = ls >= 0;
+    uint32_t grp = __match_any_sync(0xffffffffu, kw[j]) & __ballot_sync(0xffffffffu, loc);
+    if (!loc) grp = 0;
+    const int maxpop = __reduce_max_sync(0xffffffffu, (unsigned)__popc(grp));
+    if (maxpop == 0) continue;
+    unsigned char* rec = loc ? st.recs + (size_t)ls * p.rec_stride : nullptr;
+    group_update(p, rec, grp, maxpop, loc, rows[j], [&](int v, bool& ok, uint64_t& b) {
+      const int c = p.vals[v].input;
+      const ColRef cr = col_ref(p, s, c);
+      ok = rvalid(cr, x[j]);
+      b = ok ? load_bits(rv(cr, x[j]), p.cols[c].size, x[j].r) : 0ull;
+    });
     sel[j] = sel[j] && !loc;  // the rest take the global path
   }
 }
@@ -670,20 +700,27 @@ __device__ __forceinline__ void smem_rows(const ScanParams& p, const Step& s, co
 // 5. States in the global records.
 // ---------------------------------------------------------------------------
 template <typename T>
-__device__ __forceinline__ void update_column(const ScanParams& p, const ValField& f, int v, const ColRef& cr,
-                                              const RowRef (&x)[kR], const bool (&sel)[kR], const uint32_t (&gid)[kR]) {
+__device__ __forceinline__ T from_bits(uint64_t b) {
+  if constexpr (std::is_same<T, float>::value) return __uint_as_float((uint32_t)b);
+  else if constexpr (std::is_same<T, double>::value) return __longlong_as_double((long long)b);
+  else return (T)b;
+}
+
+// The rows' updates of one aggregated column: `recs` the rows' group records,
+// `ok` whether the row holds a valid value, `vb` the value's raw bits.
+template <typename T>
+__device__ __forceinline__ void update_rows(const ScanParams& p, const ValField& f, int v, unsigned char* const (&recs)[kR],
+                                            const bool (&ok)[kR], const uint64_t (&vb)[kR]) {
   constexpr bool kFloat = std::is_floating_point<T>::value;
-  bool ok[kR];
   T val[kR];
   uint64_t lo[kR], hi[kR], ks[kR];
   // Values and the read-set of every row, loads in flight together.
 #pragma unroll
   for (int j = 0; j < kR; ++j) {
-    ok[j] = sel[j] && rvalid(cr, x[j]);
-    val[j] = ok[j] ? load_as<T>(rv(cr, x[j]), x[j].r) : T(0);
+    val[j] = ok[j] ? from_bits<T>(vb[j]) : T(0);
     lo[j] = hi[j] = ks[j] = 0;
     if (!ok[j]) continue;
-    const unsigned char* rec = record_at(p, gid[j]);
+    const unsigned char* rec = recs[j];
     if (f.off_min >= 0) lo[j] = ld_cg_u64(rec + f.off_min);
     if (f.off_max >= 0) hi[j] = ld_cg_u64(rec + f.off_max);
     if (f.off_m2 >= 0) ks[j] = ld_cg_u64(rec + f.off_shift);
@@ -691,7 +728,7 @@ __device__ __forceinline__ void update_column(const ScanParams& p, const ValFiel
 #pragma unroll
   for (int j = 0; j < kR; ++j) {
     if (!ok[j]) continue;
-    unsigned char* rec = record_at(p, gid[j]);
+    unsigned char* rec = recs[j];
     red_add_u32(rec + f.off_count, 1u);
     const double xd = (double)val[j];
     const bool nan = kFloat && xd != xd;
@@ -738,6 +775,28 @@ __device__ __forceinline__ void update_column(const ScanParams& p, const ValFiel
       red_add_f64(rec + f.off_m2, d * d);
     }
   }
+}
+
+// The rows' values of one aggregated column from the step, then update_rows.
+template <typename T>
+__device__ __forceinline__ void update_column(const ScanParams& p, const ValField& f, int v, const ColRef& cr,
+                                              const RowRef (&x)[kR], const bool (&sel)[kR], const uint32_t (&gid)[kR]) {
+  unsigned char* recs[kR];
+  bool ok[kR];
+  uint64_t vb[kR];
+#pragma unroll
+  for (int j = 0; j < kR; ++j) {
+    ok[j] = sel[j] && rvalid(cr, x[j]);
+    recs[j] = ok[j] ? record_at(p, gid[j]) : p.records;
+    vb[j] = 0;
+    if (ok[j]) {
+      const T val = load_as<T>(rv(cr, x[j]), x[j].r);
+      if constexpr (std::is_same<T, float>::value) vb[j] = __float_as_uint(val);
+      else if constexpr (std::is_same<T, double>::value) vb[j] = (uint64_t)__double_as_longlong(val);
+      else vb[j] = (uint64_t)(typename std::make_unsigned<T>::type)val;
+    }
+  }
+  update_rows<T>(p, f, v, recs, ok, vb);
 }
 
 __device__ void merge_record(const ScanParams& p, const unsigned char* src, uint64_t kw, ClaimState* cs);
@@ -805,6 +864,46 @@ __device__ __forceinline__ void consume_rows(const ScanParams& p, const Step& s,
   }
 }
 
+// The producer (one thread): every tile of this CTA (t = blockIdx.x, +
+// gridDim.x, ...) into the ring of S stages, as bulk copies of the first
+// n_stage staged columns (tile_tx bytes a full tile) completing on full[s];
+// a stage is refilled after its consumers arrive on empty[s].  All
+// waits are bounded; on a timeout the producer raises ST_TIMEOUT, sets
+// *abort and waits for the copies it issued before returning.
+__device__ void produce_tiles(const ScanParams& p, unsigned char* smem, uint64_t* full, uint64_t* empty,
+                              volatile uint32_t* abort, int n_stage, uint32_t tile_tx) {
+  const int S = p.stages;
+  const uint64_t T = (uint64_t)p.tile_rows;
+  uint32_t it = 0;
+  for (uint64_t t = blockIdx.x; t < p.tiles; t += gridDim.x, ++it) {
+    const uint32_t s = it % S, ph = (it / S) & 1u;
+    if (it >= (uint32_t)S && !mbar_wait_bounded(&empty[s], ph ^ 1u, kWaitLimit)) {
+      atomicOr(p.status, ST_TIMEOUT);
+      *abort = 1;
+      break;
+    }
+    if (*abort) break;
+    if (p.use_tma && t < p.full_tiles) {
+      unsigned char* stage = smem + (size_t)s * p.stage_bytes;
+      mbar_arrive_expect_tx(&full[s], tile_tx);
+      for (int c = 0; c < n_stage; ++c) {
+        const DevColumn& col = p.cols[c];
+        bulk_g2s(stage + p.stage_off[c], static_cast<const unsigned char*>(col.values) + t * T * col.size,
+                 (uint32_t)(T * col.size), &full[s]);
+        if (p.stage_voff[c] >= 0)
+          bulk_g2s(stage + p.stage_voff[c], col.validity + t * (T / 32), (uint32_t)(T / 8), &full[s]);
+      }
+    } else {
+      mbar_arrive(&full[s]);  // ragged tail: consumers read global memory
+    }
+  }
+  // Every issued stage must have landed before the CTA may exit.
+  if (*abort) {
+    const uint32_t first = it > (uint32_t)S ? it - S : 0;
+    for (uint32_t j = first; j < it; ++j) mbar_wait_bounded(&full[j % S], (j / S) & 1u, kWaitLimit);
+  }
+}
+
 __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_constant__ ScanParams p) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int S = p.stages;
@@ -843,36 +942,7 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
 
   const uint64_t T = (uint64_t)p.tile_rows;
   if (warp == 0) {
-    if (lane == 0) {
-      uint32_t it = 0;
-      for (uint64_t t = blockIdx.x; t < p.tiles; t += gridDim.x, ++it) {
-        const uint32_t s = it % S, ph = (it / S) & 1u;
-        if (it >= (uint32_t)S && !mbar_wait_bounded(&empty[s], ph ^ 1u, kWaitLimit)) {
-          atomicOr(p.status, ST_TIMEOUT);
-          s_abort = 1;
-          break;
-        }
-        if (s_abort) break;
-        if (p.use_tma && t < p.full_tiles) {
-          unsigned char* stage = smem + (size_t)s * p.stage_bytes;
-          mbar_arrive_expect_tx(&full[s], (uint32_t)p.stage_tx);
-          for (int c = 0; c < p.n_stage; ++c) {
-            const DevColumn& col = p.cols[c];
-            bulk_g2s(stage + p.stage_off[c], static_cast<const unsigned char*>(col.values) + t * T * col.size,
-                     (uint32_t)(T * col.size), &full[s]);
-            if (p.stage_voff[c] >= 0)
-              bulk_g2s(stage + p.stage_voff[c], col.validity + t * (T / 32), (uint32_t)(T / 8), &full[s]);
-          }
-        } else {
-          mbar_arrive(&full[s]);  // ragged tail: consumers read global memory
-        }
-      }
-      // Every issued stage must have landed before the CTA may exit.
-      if (s_abort) {
-        const uint32_t first = it > (uint32_t)S ? it - S : 0;
-        for (uint32_t j = first; j < it; ++j) mbar_wait_bounded(&full[j % S], (j / S) & 1u, kWaitLimit);
-      }
-    }
+    if (lane == 0) produce_tiles(p, smem, full, empty, &s_abort, p.n_stage, (uint32_t)p.stage_tx);
   } else {
     const uint32_t shift = 31 - __clz((uint32_t)p.tile_rows);
     const uint32_t words = (uint32_t)(T / 32);
@@ -1005,6 +1075,599 @@ __device__ void merge_record(const ScanParams& p, const unsigned char* src, uint
       const double s2 = *reinterpret_cast<const double*>(src + f.off_m2);
       red_add_f64(dst + f.off_m2, d == 0.0 ? s2 : s2 + 2.0 * d * s1 + dn * d * d);
     }
+  }
+}
+
+// ===========================================================================
+// Radix-partitioned regime (many groups).
+//
+// With millions of groups the global table and records outgrow L2, and every
+// probe, read-set load and atomic becomes an HBM round trip: HBM serves about
+// 50 G random 16-byte loads and 25 G random atomics a second, L2 about 284 G
+// and 187 G.  So the scan only partitions, in three streaming kernels:
+//   count    the key and filter columns only: each CTA's selected rows per
+//            partition (shared-memory counters);
+//   offsets  per partition, the CTAs' exclusive prefix and the total;
+//   pass A   every staged column; each selected row is staged in shared
+//            memory and, partition-sorted, appended to its CTA's exact range
+//            of part_buf with coalesced writes -- no global atomics, so a
+//            flush costs shared-memory work and the writes only.
+// Pass B then hands each partition to a cluster of CTAs whose table
+// (agg_slots records, a few MB) stays L2-resident while the cluster folds the
+// partition into it; the live records are appended densely to `records`.
+// Both kernels see the same tiles per CTA (t = blockIdx.x + k * gridDim.x),
+// so pass A's rows of a partition fill exactly the range the count gave;
+// pass A checks that, and failed checks record a code in status word 2.
+// ===========================================================================
+constexpr int kPartPerThread = kPartMax / kScanConsumerThreads;
+
+__device__ __forceinline__ void part_check(const ScanParams& p, uint32_t code) { atomicOr(p.status + 2, code); }
+
+__device__ __forceinline__ uint32_t partition_of(const ScanParams& p, uint64_t kw) {
+  return (uint32_t)(mix64(kw ^ 0xA0761D6478BD642Full) >> (64 - p.part_bits));
+}
+
+__device__ __forceinline__ void raise_capacity(const ScanParams& p, uint32_t what) {
+  atomicOr(p.status, ST_CAPACITY);
+  atomicOr(p.status + 1, what);
+}
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_ranks() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_index() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+  return r;
+}
+// Every thread of every CTA of the cluster; release/acquire at cluster scope
+// orders the CTAs' global-memory work on the shared table across phases.
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ uint32_t ld_cluster_u32(const void* local, uint32_t rank) {
+  uint32_t a, v;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(local)), "r"(rank));
+  asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
+  return v;
+}
+
+// Exclusive prefix of one value per consumer thread (256 threads) and the
+// total; consumer warps only.
+__device__ __forceinline__ uint32_t consumer_exclusive_scan(uint32_t v, uint32_t* warp_tot, uint32_t* total) {
+  const int lane = threadIdx.x & 31, cw = (threadIdx.x >> 5) - 1;
+  uint32_t x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[cw] = x;
+  consumer_sync_or(false);
+  uint32_t before = 0, all = 0;
+  for (int w = 0; w < kScanConsumerWarps; ++w) {
+    const uint32_t t = warp_tot[w];
+    if (w < cw) before += t;
+    all += t;
+  }
+  *total = all;
+  consumer_sync_or(false);
+  return before + x - v;
+}
+
+// The partition kernels need no compaction: consumer warp w owns words
+// w, w + 8, ... of every tile (kR of them at most), and each lane handles
+// its own row of each word.  Selection is a ballot per word; unselected rows
+// are masked off.  Between flushes the warps pass no CTA barrier, so their
+// latencies overlap freely.
+constexpr int kWordsPerWarp = kMaxTileRows / 32 / kScanConsumerWarps;
+static_assert(kWordsPerWarp == kR, "a lane holds one row per owned word");
+
+__device__ __forceinline__ void tile_rows(const ScanParams& p, const Step& s, RowRef (&x)[kR], uint32_t (&bits)[kR]) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t words = (uint32_t)p.tile_rows / 32;
+#pragma unroll
+  for (int j = 0; j < kR; ++j) {
+    const uint32_t w = (uint32_t)(warp - 1) + (uint32_t)j * kScanConsumerWarps;
+    bits[j] = w < words ? select_word(p, s, 0, w) : 0u;
+    x[j].tile = 0;
+    x[j].r = w * 32 + lane;
+    x[j].on = (bits[j] >> lane) & 1u;
+  }
+}
+
+// The step of tile t (this CTA's it-th tile) once its stage has landed.
+__device__ __forceinline__ Step tile_step(const ScanParams& p, unsigned char* smem, uint64_t t, uint32_t sid, bool failed) {
+  const uint64_t T = (uint64_t)p.tile_rows;
+  Step s;
+  s.stage[0] = smem + (size_t)sid * p.stage_bytes;
+  s.start[0] = t * T;
+  s.staged[0] = p.use_tma && t < p.full_tiles;
+  const uint64_t left = p.rows - s.start[0];
+  s.n[0] = failed ? 0u : (uint32_t)(left < T ? left : T);
+  s.stage[1] = s.stage[0];
+  s.start[1] = 0;
+  s.staged[1] = false;
+  s.n[1] = 0;
+  return s;
+}
+
+// Ring set-up shared by the counting pass and pass A.
+__device__ __forceinline__ void ring_init(int S, uint64_t* full, uint64_t* empty, volatile uint32_t* s_abort) {
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kScanConsumerWarps);
+    }
+    fence_mbar_init();
+    *s_abort = 0;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kScanThreads, 1) partition_count(const __grid_constant__ ScanParams p) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int S = p.stages;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)S * p.stage_bytes);
+  uint64_t* empty = full + S;
+  __shared__ volatile uint32_t s_abort;
+  __shared__ uint32_t s_count[kPartMax];
+  const uint32_t nparts = 1u << p.part_bits;
+  for (uint32_t q = threadIdx.x; q < nparts; q += blockDim.x) s_count[q] = 0;
+  ring_init(S, full, empty, &s_abort);
+  if ((threadIdx.x >> 5) == 0) {
+    if ((threadIdx.x & 31) == 0) produce_tiles(p, smem, full, empty, &s_abort, p.n_stage_count, (uint32_t)p.stage_tx_count);
+  } else {
+    uint32_t it = 0;
+    for (uint64_t t = blockIdx.x; t < p.tiles; t += gridDim.x, ++it) {
+      const uint32_t sid = it % S, ph = (it / S) & 1u;
+      if (s_abort || !mbar_wait_bounded(&full[sid], ph, kWaitLimit)) {
+        atomicOr(p.status, ST_TIMEOUT);
+        s_abort = 1;
+        break;
+      }
+      const Step s = tile_step(p, smem, t, sid, false);
+      RowRef x[kR];
+      uint32_t bits[kR];
+      uint64_t kw[kR];
+      tile_rows(p, s, x, bits);
+      key_words(p, s, x, kw);
+      __syncwarp();
+      if ((threadIdx.x & 31) == 0) mbar_arrive(&empty[sid]);  // this warp no longer reads the stage
+#pragma unroll
+      for (int j = 0; j < kR; ++j)
+        if (x[j].on) atomicAdd(&s_count[partition_of(p, kw[j])], 1u);
+    }
+  }
+  __syncthreads();
+  for (uint32_t q = threadIdx.x; q < nparts; q += blockDim.x) p.part_counts[(size_t)blockIdx.x * nparts + q] = s_count[q];
+}
+
+// Per partition (one thread each): the CTAs' counts become their exclusive
+// prefix; the total goes to part_totals.
+__global__ void partition_offsets(const __grid_constant__ ScanParams p, uint32_t ctas) {
+  const uint32_t nparts = 1u << p.part_bits;
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nparts) return;
+  uint32_t run = 0;
+  for (uint32_t c = 0; c < ctas; ++c) {
+    uint32_t* e = p.part_counts + (size_t)c * nparts + q;
+    const uint32_t v = *e;
+    *e = run;
+    run += v;
+  }
+  p.part_totals[q] = run;
+}
+
+struct PartSmem {
+  uint32_t cur[kPartMax];   // counts, then scatter cursors
+  uint32_t off[kPartMax];   // first sorted position of each partition in the flush
+  uint32_t base[kPartMax];  // part_buf row of that position (all ones: not stored)
+  uint32_t next[kPartMax];  // this CTA's next part_buf row of each partition
+  uint32_t end[kPartMax];   // the end of this CTA's range of each partition
+  uint32_t wfill[kScanConsumerWarps];  // rows each warp's staging region holds
+  uint32_t warp_tot[kScanConsumerWarps];
+};
+
+// Pass A's flush: the staged rows of every warp region (region rows each,
+// ps.wfill[w] used) sorted by partition through shared-memory counters and
+// appended to this CTA's ranges, consecutive threads writing consecutive
+// rows.  Every consumer thread calls it.
+__device__ void flush_staged(const ScanParams& p, const unsigned long long* staged, uint16_t* order,
+                             const uint16_t* rpart, uint32_t region_shift, PartSmem& ps) {
+  const uint32_t ct = threadIdx.x - 32;
+  const uint32_t nparts = 1u << p.part_bits;
+  const uint32_t cap = (uint32_t)kScanConsumerWarps << region_shift;
+  const uint32_t rmask = (1u << region_shift) - 1u;
+  for (uint32_t q = ct; q < nparts; q += kScanConsumerThreads) ps.cur[q] = 0;
+  consumer_sync_or(false);
+  uint32_t rows = 0;
+  for (int w = 0; w < kScanConsumerWarps; ++w) rows += ps.wfill[w];
+  for (uint32_t u = ct; u < cap; u += kScanConsumerThreads)
+    if ((u & rmask) < ps.wfill[u >> region_shift]) atomicAdd(&ps.cur[rpart[u]], 1u);
+  consumer_sync_or(false);
+  uint32_t h[kPartPerThread], sum = 0;
+#pragma unroll
+  for (int k = 0; k < kPartPerThread; ++k) {
+    const uint32_t q = ct * kPartPerThread + k;
+    h[k] = q < nparts ? ps.cur[q] : 0u;
+    sum += h[k];
+  }
+  uint32_t total;
+  uint32_t off = consumer_exclusive_scan(sum, ps.warp_tot, &total);
+#pragma unroll
+  for (int k = 0; k < kPartPerThread; ++k) {
+    const uint32_t q = ct * kPartPerThread + k;
+    if (q < nparts) {
+      ps.off[q] = off;
+      ps.cur[q] = off;
+      const uint32_t at = ps.next[q];
+      if (h[k] && (at > ps.end[q] || ps.end[q] - at < h[k])) {
+        part_check(p, CHK_RANGE);
+        ps.base[q] = ~0u;
+      } else {
+        ps.base[q] = at;
+        ps.next[q] = at + h[k];
+      }
+    }
+    off += h[k];
+  }
+  consumer_sync_or(false);
+  for (uint32_t u = ct; u < cap; u += kScanConsumerThreads)
+    if ((u & rmask) < ps.wfill[u >> region_shift]) order[atomicAdd(&ps.cur[rpart[u]], 1u)] = (uint16_t)u;
+  consumer_sync_or(false);
+  const uint32_t W = p.part_words;
+  for (uint32_t s = ct; s < rows; s += kScanConsumerThreads) {
+    const uint32_t u = order[s];
+    const uint32_t q = rpart[u];
+    const uint32_t base = ps.base[q];
+    if (base == ~0u) continue;
+    const uint64_t x = (uint64_t)base + (s - ps.off[q]);
+    if (x >= p.part_cap) {
+      part_check(p, CHK_RANGE);
+      continue;
+    }
+    const unsigned long long* src = staged + (size_t)u * W;
+    unsigned long long* dst = p.part_buf + x * W;
+    for (uint32_t j = 0; j < W; ++j) dst[j] = src[j];
+  }
+  consumer_sync_or(false);
+}
+
+__global__ void __launch_bounds__(kScanThreads, 1) partition_kernel(const __grid_constant__ ScanParams p) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int S = p.stages;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)S * p.stage_bytes);
+  uint64_t* empty = full + S;
+  unsigned long long* staged = reinterpret_cast<unsigned long long*>(smem + p.part_stage_off);
+  uint16_t* order = reinterpret_cast<uint16_t*>(staged + (size_t)p.part_flush * p.part_words);
+  uint16_t* rpart = order + p.part_flush;
+  __shared__ volatile uint32_t s_abort;
+  __shared__ PartSmem s_part;
+  ring_init(S, full, empty, &s_abort);
+  if ((threadIdx.x >> 5) == 0) {
+    if ((threadIdx.x & 31) == 0) produce_tiles(p, smem, full, empty, &s_abort, p.n_stage, (uint32_t)p.stage_tx);
+    return;
+  }
+  const uint32_t ct = threadIdx.x - 32;
+  const int cw = (threadIdx.x >> 5) - 1, lane = threadIdx.x & 31;
+  const uint32_t nparts = 1u << p.part_bits;
+  const uint32_t W = p.part_words;
+  // Staging: one region per consumer warp; a warp stages at most kR * 32
+  // rows a tile, so flushing every `every` tiles never overflows a region.
+  uint32_t region_shift = 0;
+  while ((kScanConsumerWarps << (region_shift + 1)) <= p.part_flush) ++region_shift;
+  const uint32_t every = (1u << region_shift) / (kR * 32);
+  // This CTA's range of each partition: the partition's start (prefix of the
+  // totals) plus the CTA's prefix among the CTAs.
+  {
+    uint32_t tot[kPartPerThread], sum = 0;
+#pragma unroll
+    for (int k = 0; k < kPartPerThread; ++k) {
+      const uint32_t q = ct * kPartPerThread + k;
+      tot[k] = q < nparts ? p.part_totals[q] : 0u;
+      sum += tot[k];
+    }
+    uint32_t all;
+    uint32_t start = consumer_exclusive_scan(sum, s_part.warp_tot, &all);
+#pragma unroll
+    for (int k = 0; k < kPartPerThread; ++k) {
+      const uint32_t q = ct * kPartPerThread + k;
+      if (q < nparts) {
+        const uint32_t mine = p.part_counts[(size_t)blockIdx.x * nparts + q];
+        const uint32_t upto = blockIdx.x + 1 < gridDim.x ? p.part_counts[(size_t)(blockIdx.x + 1) * nparts + q] : tot[k];
+        s_part.next[q] = start + mine;
+        s_part.end[q] = start + upto;
+        if (blockIdx.x == 0) p.part_start[q] = start;
+      }
+      start += tot[k];
+    }
+  }
+  const uint32_t rbase = (uint32_t)cw << region_shift;
+  uint32_t wfill = 0;  // this warp's staged rows (the same in all its lanes)
+  bool aborted = false;
+  uint32_t it = 0;
+  for (uint64_t t = blockIdx.x; t < p.tiles; t += gridDim.x, ++it) {
+    const uint32_t sid = it % S, ph = (it / S) & 1u;
+    if (!aborted && (s_abort || !mbar_wait_bounded(&full[sid], ph, kWaitLimit))) {
+      atomicOr(p.status, ST_TIMEOUT);
+      s_abort = 1;
+      aborted = true;
+    }
+    if (!aborted) {
+      const Step s = tile_step(p, smem, t, sid, false);
+      RowRef x[kR];
+      uint32_t bits[kR];
+      uint64_t kw[kR];
+      tile_rows(p, s, x, bits);
+      key_words(p, s, x, kw);
+      // Positions in this warp's region: words in order, lanes in order.
+      uint32_t at[kR];
+      uint32_t run = wfill;
+#pragma unroll
+      for (int j = 0; j < kR; ++j) {
+        at[j] = rbase + run + __popc(bits[j] & ((1u << lane) - 1u));
+        run += __popc(bits[j]);
+      }
+      uint32_t vflags[kR] = {};
+      for (int v = 0; v < p.n_vals; ++v) {
+        const int c = p.vals[v].input;
+        const ColRef cr = col_ref(p, s, c);
+        const int size = p.cols[c].size;
+#pragma unroll
+        for (int j = 0; j < kR; ++j) {
+          if (!x[j].on) continue;
+          const bool ok = rvalid(cr, x[j]);
+          vflags[j] |= (uint32_t)ok << v;
+          staged[(size_t)at[j] * W + 2 + v] = ok ? load_bits(rv(cr, x[j]), size, x[j].r) : 0ull;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[sid]);  // this warp no longer reads the stage
+#pragma unroll
+      for (int j = 0; j < kR; ++j) {
+        if (!x[j].on) continue;
+        staged[(size_t)at[j] * W] = kw[j];
+        staged[(size_t)at[j] * W + 1] = (uint64_t)(uint32_t)(s.start[0] + x[j].r) | ((uint64_t)vflags[j] << 32);
+        rpart[at[j]] = (uint16_t)partition_of(p, kw[j]);
+      }
+      wfill = run;
+    }
+    if ((it + 1) % every == 0) {
+      if (lane == 0) s_part.wfill[cw] = wfill;
+      if (consumer_sync_or(aborted)) {
+        aborted = true;
+        break;
+      }
+      flush_staged(p, staged, order, rpart, region_shift, s_part);
+      wfill = 0;
+    }
+  }
+  if (lane == 0) s_part.wfill[cw] = wfill;
+  if (consumer_sync_or(aborted)) return;
+  flush_staged(p, staged, order, rpart, region_shift, s_part);
+  // Every range filled exactly as counted.
+  for (uint32_t q = ct; q < nparts; q += kScanConsumerThreads)
+    if (s_part.next[q] != s_part.end[q]) part_check(p, CHK_RANGE);
+}
+
+// ---------------------------------------------------------------------------
+// Pass B.  A cluster's table is initialised once (key words all ones, fields
+// zero: every field's identity); then per partition taken from p.part_next
+// its CTAs fold the partition's rows into it with lock-step probe rounds and
+// the read-set/atomic updates of the global regime, all L2 hits, and append
+// the live records densely to `records`, resetting each slot as it is read.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void reset_record(unsigned char* rec, size_t rs) {
+  uint4* r = reinterpret_cast<uint4*>(rec);
+  r[0] = make_uint4(~0u, ~0u, 0u, 0u);
+  for (size_t q = 1; q < rs / 16; ++q) r[q] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+__device__ __forceinline__ void fold_rows(const ScanParams& p, unsigned char* table, const unsigned long long* rows,
+                                          uint32_t n, uint64_t first, uint64_t stride) {
+  const uint32_t W = p.part_words;
+  const uint64_t mask = p.agg_slots - 1;
+  const size_t rs = (size_t)p.rec_stride;
+  const int lane = threadIdx.x & 31;
+  bool on[kR], pend[kR];
+  uint64_t kw[kR], slot[kR], ek[kR];
+  uint32_t row[kR], vf[kR], ef[kR];
+  const unsigned long long* src[kR];
+#pragma unroll
+  for (int j = 0; j < kR; ++j) {
+    const uint64_t i = first + (uint64_t)j * stride;
+    on[j] = i < n;
+    src[j] = rows + (on[j] ? i : 0) * W;
+    kw[j] = slot[j] = 0;
+    row[j] = vf[j] = 0;
+    if (!on[j]) continue;
+    kw[j] = __ldcs(src[j]);
+    const uint64_t w1 = __ldcs(src[j] + 1);
+    row[j] = (uint32_t)w1;
+    vf[j] = (uint32_t)(w1 >> 32);
+    slot[j] = kw[j] == kEmpty ? (uint64_t)p.agg_slots : (mix64(kw[j] ^ 0x632BE59BD9B4E019ull) & mask);
+  }
+  // Probe rounds; the first 16 bytes of a record are {key word, ~first row, flags}.
+#pragma unroll
+  for (int j = 0; j < kR; ++j) {
+    pend[j] = on[j] && kw[j] != kEmpty;
+    ek[j] = 0;
+    ef[j] = 0;
+    if (on[j]) {
+      const ulonglong2 e = __ldcg(reinterpret_cast<const ulonglong2*>(table + slot[j] * rs));
+      ek[j] = e.x;
+      ef[j] = (uint32_t)e.y;
+    }
+  }
+  const uint32_t limit = (uint32_t)(mask < 1024 ? mask + 1 : 1024);
+  for (uint32_t round = 0;; ++round) {
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < kR; ++j) any |= pend[j];
+    if (!__any_sync(0xffffffffu, any)) break;
+    if (round > limit) {  // a full table: the host grows it
+#pragma unroll
+      for (int j = 0; j < kR; ++j) {
+        if (pend[j]) on[j] = false;
+        pend[j] = false;
+      }
+      if (any) raise_capacity(p, CAP_AGG_TABLE);
+      break;
+    }
+#pragma unroll
+    for (int j = 0; j < kR; ++j) {
+      if (!pend[j]) continue;
+      if (ek[j] == kw[j]) {
+        pend[j] = false;
+        continue;
+      }
+      if (ek[j] == kEmpty) {
+        const unsigned long long prev =
+            atomicCAS(reinterpret_cast<unsigned long long*>(table + slot[j] * rs), kEmpty, kw[j]);
+        if (prev == kEmpty || prev == kw[j]) {
+          pend[j] = false;
+          continue;
+        }
+      }
+      slot[j] = (slot[j] + 1) & mask;
+      const ulonglong2 e = __ldcg(reinterpret_cast<const ulonglong2*>(table + slot[j] * rs));
+      ek[j] = e.x;
+      ef[j] = (uint32_t)e.y;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kR; ++j) {
+    if (on[j] && slot[j] > p.agg_slots) {
+      part_check(p, CHK_SLOT);
+      on[j] = false;
+    }
+    if (!on[j]) slot[j] = 0;
+  }
+  // Rows of one record within the warp (hot keys) are reduced across lanes
+  // first: one atomic per field and group instead of one per row.
+#pragma unroll
+  for (int j = 0; j < kR; ++j) {
+    const uint64_t tag = on[j] ? slot[j] : (0x8000000000000000ull | (uint64_t)lane);
+    uint32_t grp = __match_any_sync(0xffffffffu, tag) & __ballot_sync(0xffffffffu, on[j]);
+    if (!on[j]) grp = 0;
+    const int maxpop = __reduce_max_sync(0xffffffffu, (unsigned)__popc(grp));
+    if (maxpop <= 1) continue;
+    unsigned char* rec = table + slot[j] * rs;
+    const unsigned long long* sp = src[j];
+    const uint32_t flags = vf[j];
+    group_update(p, rec, grp, maxpop, on[j], row[j], [&](int v, bool& ok, uint64_t& b) {
+      ok = (flags >> v) & 1u;
+      b = ok ? __ldcs(sp + 2 + v) : 0ull;
+    });
+    on[j] = false;
+  }
+  unsigned char* recs[kR];
+#pragma unroll
+  for (int j = 0; j < kR; ++j) {
+    recs[j] = table + slot[j] * rs;
+    if (on[j] && ~row[j] > ef[j]) atomicMax(reinterpret_cast<uint32_t*>(recs[j] + kRecFirst), ~row[j]);
+    if (on[j] && p.off_len >= 0) red_add_u32(recs[j] + p.off_len, 1u);
+  }
+  for (int v = 0; v < p.n_vals; ++v) {
+    bool ok[kR];
+    uint64_t vb[kR];
+#pragma unroll
+    for (int j = 0; j < kR; ++j) {
+      ok[j] = on[j] && ((vf[j] >> v) & 1u);
+      vb[j] = ok[j] ? __ldcs(src[j] + 2 + v) : 0ull;
+    }
+    const ValField& f = p.vals[v];
+    switch (f.dtype) {
+      case DFC_INT8: update_rows<int8_t>(p, f, v, recs, ok, vb); break;
+      case DFC_INT16: update_rows<int16_t>(p, f, v, recs, ok, vb); break;
+      case DFC_INT32: update_rows<int32_t>(p, f, v, recs, ok, vb); break;
+      case DFC_INT64: update_rows<int64_t>(p, f, v, recs, ok, vb); break;
+      case DFC_UINT8: update_rows<uint8_t>(p, f, v, recs, ok, vb); break;
+      case DFC_UINT16: update_rows<uint16_t>(p, f, v, recs, ok, vb); break;
+      case DFC_UINT32: update_rows<uint32_t>(p, f, v, recs, ok, vb); break;
+      case DFC_UINT64: update_rows<uint64_t>(p, f, v, recs, ok, vb); break;
+      case DFC_FLOAT32: update_rows<float>(p, f, v, recs, ok, vb); break;
+      default: update_rows<double>(p, f, v, recs, ok, vb); break;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kAggThreads, 1) partition_aggregate(const __grid_constant__ ScanParams p) {
+  __shared__ uint32_t s_part;
+  __shared__ uint32_t s_warp[kAggThreads / 32];
+  __shared__ uint32_t s_base;
+  const uint32_t crank = cluster_rank(), csize = cluster_ranks();
+  const uint32_t cid = cluster_index();
+  if (cid >= p.agg_tables_n) {  // uniform over the cluster
+    if (threadIdx.x == 0) part_check(p, CHK_CLUSTER);
+    return;
+  }
+  const uint64_t slots = p.agg_slots;
+  const size_t rs = (size_t)p.rec_stride;
+  unsigned char* table = p.agg_tables + (size_t)cid * (slots + 1) * rs;
+  const uint32_t nparts = 1u << p.part_bits;
+  const uint64_t lt = (uint64_t)crank * blockDim.x + threadIdx.x, lstride = (uint64_t)csize * blockDim.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // This CTA's share of the slots (initialisation, extraction and reset).
+  const uint64_t per = (slots + 1 + csize - 1) / csize;
+  const uint64_t lo = (uint64_t)crank * per < slots + 1 ? (uint64_t)crank * per : slots + 1;
+  const uint64_t hi = lo + per < slots + 1 ? lo + per : slots + 1;
+  for (uint64_t s = lo + threadIdx.x; s < hi; s += blockDim.x) reset_record(table + s * rs, rs);
+  for (;;) {
+    if (crank == 0 && threadIdx.x == 0) s_part = atomicAdd(p.part_next, 1u);
+    cluster_sync_all();
+    const uint32_t part = ld_cluster_u32(&s_part, 0);
+    if (part >= nparts) {
+      cluster_sync_all();  // rank 0's shared memory outlives every read of it
+      break;
+    }
+    // Fold the partition's rows.
+    const uint64_t start = p.part_start[part];
+    const uint64_t total = p.part_totals[part];
+    const uint32_t n = (uint32_t)(start >= p.part_cap ? 0 : (total < p.part_cap - start ? total : p.part_cap - start));
+    const unsigned long long* rows = p.part_buf + start * p.part_words;
+    for (uint64_t base = 0; base < n; base += lstride * kR) fold_rows(p, table, rows, n, base + lt, lstride);
+    cluster_sync_all();
+    // Append the live records (first row set), one counter reservation per CTA.
+    uint32_t mine = 0;
+    for (uint64_t s = lo + threadIdx.x; s < hi; s += blockDim.x) mine += ld_cg_u32(table + s * rs + kRecFirst) != 0;
+    uint32_t x = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t tot = 0;
+      for (int w = 0; w < (int)(blockDim.x / 32); ++w) {
+        const uint32_t t = s_warp[w];
+        s_warp[w] = tot;
+        tot += t;
+      }
+      s_base = tot ? atomicAdd(p.alloc, tot) : 0u;
+      if (tot && (uint64_t)s_base + tot > p.recs_total) raise_capacity(p, CAP_RECORDS);
+    }
+    __syncthreads();
+    uint32_t dst = s_base + s_warp[warp] + x - mine;
+    for (uint64_t s = lo + threadIdx.x; s < hi; s += blockDim.x) {
+      unsigned char* rec = table + s * rs;
+      if (ld_cg_u32(rec + kRecFirst) == 0) continue;
+      if (dst < p.recs_total) {
+        uint4* out = reinterpret_cast<uint4*>(record_at(p, dst));
+        for (size_t q = 0; q < rs / 16; ++q) out[q] = __ldcg(reinterpret_cast<const uint4*>(rec) + q);
+      }
+      reset_record(rec, rs);
+      ++dst;
+    }
+    __syncthreads();  // s_warp and s_base are rewritten for the next partition
   }
 }
 

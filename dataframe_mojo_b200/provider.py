@@ -88,6 +88,19 @@ def _memory_limit() -> int:
     return v
 
 
+_REGIMES = {"": 0, "auto": 0, "global": N.Q_FORCE_GLOBAL, "shared": N.Q_FORCE_SHARED,
+            "partitioned": N.Q_FORCE_PARTITIONED}
+
+
+def _regime_flags() -> int:
+    """DATAFRAME_ACCEL_REGIME: auto (default; chosen from the estimated group
+    count), global, shared or partitioned.  A bad value raises."""
+    raw = os.environ.get("DATAFRAME_ACCEL_REGIME", "").strip().lower()
+    if raw not in _REGIMES:
+        raise ValueError(f"DATAFRAME_ACCEL_REGIME={raw!r} is not one of auto, global, shared, partitioned")
+    return _REGIMES[raw]
+
+
 # ---------------------------------------------------------------------------
 # Device columns and results.
 # ---------------------------------------------------------------------------
@@ -257,6 +270,8 @@ def last_timings() -> dict:
         "regime": int(t.regime),
         "retries": int(t.retries),
         "launches": int(t.launches),
+        "partitions": int(t.partitions),
+        "aggregate_ns": t.aggregate_ns,
     }
 
 
@@ -291,9 +306,10 @@ def _region_plan(plan) -> Plan:
 
 def _execute_plan(plan: Plan, device: int) -> DataFrame:
     bound = bind(plan)
+    flags = _regime_flags()
     cols = [DeviceColumn(s, device) for s in bound.series]
     try:
-        result = run_bound(bound, cols)
+        result = run_bound(bound, cols, flags=flags)
         try:
             return result.to_frame()
         finally:

@@ -204,6 +204,7 @@ typedef struct dfc_agg {
 #define DFC_Q_FORCE_GLOBAL 2u      /* skip the shared-memory table regime */
 #define DFC_Q_FORCE_SHARED 4u      /* use the shared-memory table regime regardless of estimates */
 #define DFC_Q_FLOAT32_FP64 8u      /* Float32 values: plain FP64 accumulation instead of compensated FP32 */
+#define DFC_Q_FORCE_PARTITIONED 16u /* use the radix-partitioned regime regardless of estimates (keys <= 64 bits) */
 
 typedef struct dfc_query {
   uint32_t abi_version; /* DFC_ABI_VERSION */
@@ -318,10 +319,11 @@ typedef struct dfc_timings {
   double total_ns;
   uint64_t groups;
   uint64_t table_slots;
-  int32_t regime;   /* 0 global table, 1 shared-memory tables */
+  int32_t regime;   /* 0 global table, 1 shared-memory tables, 2 radix-partitioned */
   int32_t retries;  /* capacity regrowths */
   int32_t launches; /* kernels this library launched for the query */
-  int32_t reserved;
+  int32_t partitions;  /* radix-partitioned regime: partitions (else 0) */
+  double aggregate_ns; /* radix-partitioned regime: the per-partition aggregation pass (scan_ns: the partition pass) */
 } dfc_timings;
 DFC_API dfc_status dfc_last_timings(dfc_timings* out);
 

@@ -88,6 +88,18 @@ def test_env_settings_validated():
             os.environ["DATAFRAME_ACCEL_DEVICE"] = old
 
 
+def test_regime_setting(monkeypatch):
+    monkeypatch.setenv("DATAFRAME_ACCEL_REGIME", "partitioned")
+    assert provider._regime_flags() == N.Q_FORCE_PARTITIONED
+    monkeypatch.setenv("DATAFRAME_ACCEL_REGIME", "Global")
+    assert provider._regime_flags() == N.Q_FORCE_GLOBAL
+    monkeypatch.setenv("DATAFRAME_ACCEL_REGIME", "")
+    assert provider._regime_flags() == 0
+    monkeypatch.setenv("DATAFRAME_ACCEL_REGIME", "radix")
+    with pytest.raises(ValueError):
+        provider._regime_flags()
+
+
 def test_cpu_engine_is_not_part_of_the_provider():
     plan = config1_plan(config1(rows=10))
     with pytest.raises(ValueError):

@@ -113,6 +113,60 @@ __device__ __forceinline__ void red_max_u64(void* p, uint64_t v) {
 }
 __device__ __forceinline__ void red_add_f64(void* p, double v) { atomicAdd(reinterpret_cast<double*>(p), v); }
 
+// Record updates in either space: kShared selects explicit shared-memory
+// atomics (a generic pointer into shared memory would take the generic path).
+__device__ __forceinline__ uint32_t shared_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+template <bool kShared>
+__device__ __forceinline__ void rec_add_u32(void* p, uint32_t v) {
+  if constexpr (kShared) asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(shared_addr(p)), "r"(v) : "memory");
+  else red_add_u32(p, v);
+}
+template <bool kShared>
+__device__ __forceinline__ void rec_or_u32(void* p, uint32_t v) {
+  if constexpr (kShared) asm volatile("red.shared.or.b32 [%0], %1;" ::"r"(shared_addr(p)), "r"(v) : "memory");
+  else red_or_u32(p, v);
+}
+template <bool kShared>
+__device__ __forceinline__ void rec_max_u32(void* p, uint32_t v) {
+  if constexpr (kShared) asm volatile("red.shared.max.u32 [%0], %1;" ::"r"(shared_addr(p)), "r"(v) : "memory");
+  else atomicMax(reinterpret_cast<unsigned int*>(p), v);
+}
+template <bool kShared>
+__device__ __forceinline__ void rec_add_u64(void* p, uint64_t v) {
+  if constexpr (kShared) asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(shared_addr(p)), "l"(v) : "memory");
+  else red_add_u64(p, v);
+}
+template <bool kShared>
+__device__ __forceinline__ uint64_t rec_fetch_add_u64(void* p, uint64_t v) {
+  if constexpr (kShared) {
+    uint64_t old;
+    asm volatile("atom.shared.add.u64 %0, [%1], %2;" : "=l"(old) : "r"(shared_addr(p)), "l"(v) : "memory");
+    return old;
+  } else {
+    return atomicAdd(reinterpret_cast<unsigned long long*>(p), (unsigned long long)v);
+  }
+}
+template <bool kShared>
+__device__ __forceinline__ void rec_max_u64(void* p, uint64_t v) {
+  if constexpr (kShared) asm volatile("red.shared.max.u64 [%0], %1;" ::"r"(shared_addr(p)), "l"(v) : "memory");
+  else red_max_u64(p, v);
+}
+template <bool kShared>
+__device__ __forceinline__ void rec_add_f64(void* p, double v) {
+  if constexpr (kShared) asm volatile("red.shared.add.f64 [%0], %1;" ::"r"(shared_addr(p)), "d"(v) : "memory");
+  else red_add_f64(p, v);
+}
+template <bool kShared>
+__device__ __forceinline__ uint64_t rec_cas_u64(void* p, uint64_t cmp, uint64_t val) {
+  if constexpr (kShared) {
+    uint64_t old;
+    asm volatile("atom.shared.cas.b64 %0, [%1], %2, %3;" : "=l"(old) : "r"(shared_addr(p)), "l"(cmp), "l"(val) : "memory");
+    return old;
+  } else {
+    return atomicCAS(reinterpret_cast<unsigned long long*>(p), (unsigned long long)cmp, (unsigned long long)val);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Values.
 // ---------------------------------------------------------------------------

@@ -18,6 +18,10 @@ __global__ void scan_kernel(const __grid_constant__ ScanParams p);
 constexpr int kAggCluster = 8;
 constexpr int kAggThreads = 512;
 constexpr int kPartMax = 1024;  // partitions at most
+// The partition passes: one producer warp and kPartWarps consumer warps.
+constexpr int kPartWarps = 16;
+constexpr int kPartConsumerThreads = kPartWarps * 32;
+constexpr int kPartThreads = kPartConsumerThreads + 32;
 __global__ void partition_count(const __grid_constant__ ScanParams p);
 __global__ void partition_offsets(const __grid_constant__ ScanParams p, uint32_t ctas);
 __global__ void partition_kernel(const __grid_constant__ ScanParams p);

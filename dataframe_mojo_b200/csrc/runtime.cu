@@ -130,7 +130,6 @@ struct DeviceState {
   int sms = 0;
   size_t smem_optin = 0;       // scan_kernel's dynamic shared memory limit
   size_t part_smem_optin = 0;  // partition_kernel's
-  int agg_clusters = 0;        // partition_aggregate clusters resident at once
   int scan_occupancy = 1;
 };
 std::mutex g_dev_mu;
@@ -173,23 +172,6 @@ dfc_status device_ready(int dev, DeviceState** out) {
     CK(cudaFuncSetAttribute(partition_count, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)(prop.sharedMemPerBlockOptin - fa.sharedSizeBytes)),
        "cudaFuncSetAttribute");
-    // Clusters of kAggCluster CTAs for the per-partition aggregation.
-    cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = kAggCluster;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.gridDim = dim3(kAggCluster * 64);
-    cfg.blockDim = dim3(kAggThreads);
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    int clusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&clusters, partition_aggregate, &cfg) != cudaSuccess) {
-      cudaGetLastError();
-      clusters = 0;
-    }
-    d.agg_clusters = clusters;
     d.ready = true;
   }
   *out = &d;
@@ -673,23 +655,47 @@ struct PartPlan {
   uint64_t recs = 0;
   size_t smem = 0;        // pass A dynamic shared memory
   size_t count_smem = 0;  // counting pass dynamic shared memory
-  int clusters = 0;
+  int clusters = 0;       // pass B clusters resident at once
 };
 
-// L2 bytes the clusters' tables may take together (of 126 MB): the rest
-// serves the streamed partition rows and the records being written.
+// Clusters of kAggCluster CTAs resident at once with `smem` bytes of
+// dynamic shared memory each (0: no cluster launch possible).
+int agg_clusters(size_t smem) {
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = kAggCluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(kAggCluster * 64);
+  cfg.blockDim = dim3(kAggThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, partition_aggregate, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return clusters;
+}
+
+// L2 bytes the clusters' pass B tables may take together: the rest serves
+// the streamed partition rows and the records being written.
 constexpr double kAggL2Budget = 40.0 * 1024 * 1024;
 
 // Sizes the regime for `est` groups; false when it does not apply (keys
 // wider than 64 bits, too little shared memory, no cluster launch).
 bool plan_partitions(const Plan& P, const DeviceState* ds, uint64_t est, PartPlan& pp) {
   const ScanParams& sp = P.sp;
-  if (sp.key_mode != KEY_PACKED || ds->agg_clusters < 1 || P.rows == 0 || P.rows >= 0xFFFFFFFFull) return false;
+  if (sp.key_mode != KEY_PACKED || P.rows == 0 || P.rows >= 0xFFFFFFFFull) return false;
   pp.words = 2 + (uint32_t)sp.n_vals;
-  pp.clusters = ds->agg_clusters;
+  pp.clusters = agg_clusters(0);
+  if (pp.clusters < 1) return false;
   // Staging area: what the ring leaves, a power of two of rows, split into
-  // one region per consumer warp of at least 128 rows (a warp stages up to
-  // 128 rows a tile); at most 2^15 rows (flush positions are 16-bit).
+  // one region per consumer warp of at least one step's share (a warp stages
+  // up to 128 rows a two-tile step); at most 2^15 rows (flush positions are
+  // 16-bit).
   const size_t ring = (size_t)sp.stages * sp.stage_bytes + 2 * sp.stages * sizeof(uint64_t);
   pp.count_smem = ring;
   pp.stage_off = (uint32_t)((ring + 15) & ~(size_t)15);
@@ -699,7 +705,7 @@ bool plan_partitions(const Plan& P, const DeviceState* ds, uint64_t est, PartPla
   rows_fit = std::min<size_t>(rows_fit, 32768);
   uint32_t flush = 1;
   while ((size_t)flush * 2 <= rows_fit) flush <<= 1;
-  if (flush < 1024u) return false;
+  if (flush < (uint32_t)kPartWarps * 128u) return false;
   pp.flush = flush;
   pp.smem = pp.stage_off + (size_t)flush * per_row;
   // Partitions: the fewest (>= 16) whose tables, at load <= 1/2, fit the L2
@@ -733,7 +739,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   int occ = 1;
   if (pp) {
     // The counting pass and pass A must see the same tiles per CTA: one grid.
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, partition_kernel, kScanThreads, pp->smem), "occupancy");
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, partition_kernel, kPartThreads, pp->smem), "occupancy");
     occ = 1;
   } else {
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_kernel, kScanThreads, P.smem), "occupancy");
@@ -746,9 +752,10 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
     // Pass B appends every group exactly once: no holes, no chunks.
     recs = std::max<uint64_t>(1, pp->recs);
   } else {
-    // Records: the groups the table may hold (load factor <= 1/2) plus every
-    // CTA's partly used last chunk.
-    const uint64_t groups_cap = std::min<uint64_t>(P.rows, slots / 2);
+    // Records: the groups the table may hold (load factor <= 1/8: the lock-step
+    // probe rounds run as long as a warp's longest chain) plus every CTA's
+    // partly used last chunk.
+    const uint64_t groups_cap = std::min<uint64_t>(P.rows, slots / 8);
     while (chunk < 1024 && chunk * ncta * 8 < groups_cap) chunk <<= 1;
     // Slack for holes: records reserved by claims that lost a race.
     recs = groups_cap + groups_cap / 8 + chunk * ncta;
@@ -851,11 +858,11 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   for (auto& x : ev) cudaEventCreate(&x);
   cudaEventRecord(ev[0], stream);
   if (pp) {
-    partition_count<<<(unsigned)ncta, kScanThreads, pp->count_smem, stream>>>(sp);
+    partition_count<<<(unsigned)ncta, kPartThreads, pp->count_smem, stream>>>(sp);
     cudaEventRecord(ev[4], stream);
     partition_offsets<<<(unsigned)((nparts + 255) / 256), 256, 0, stream>>>(sp, (uint32_t)ncta);
     cudaEventRecord(ev[5], stream);
-    partition_kernel<<<(unsigned)ncta, kScanThreads, pp->smem, stream>>>(sp);
+    partition_kernel<<<(unsigned)ncta, kPartThreads, pp->smem, stream>>>(sp);
     cudaEventRecord(ev[3], stream);
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
@@ -1161,11 +1168,12 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
   // otherwise the global table alone.  Rows whose key finds no room in a CTA
   // table take the global path, so a low estimate costs speed, not results.
   P.sp.smem_slots = 0;
-  // Radix-partitioned when the groups' table and records would outgrow L2.
+  // The radix-partitioned regime on request.  Measured on B200 it does not
+  // yet beat the global table at load <= 1/8 (100M rows, 7.4M groups:
+  // about 14 ms against 8.7), so the automatic choice keeps the global table.
   PartPlan pp;
   bool partitioned = false;
-  if (!(query->flags & (DFC_Q_FORCE_GLOBAL | DFC_Q_FORCE_SHARED)) &&
-      ((query->flags & DFC_Q_FORCE_PARTITIONED) || (double)est * (P.sp.rec_stride + 32) > kAggL2Budget))
+  if ((query->flags & DFC_Q_FORCE_PARTITIONED) && !(query->flags & (DFC_Q_FORCE_GLOBAL | DFC_Q_FORCE_SHARED)))
     partitioned = plan_partitions(P, ds, est, pp);
   if (!partitioned && !(query->flags & DFC_Q_FORCE_GLOBAL) && P.sp.key_mode == KEY_PACKED &&
       ((query->flags & DFC_Q_FORCE_SHARED) || est <= 4096)) {
@@ -1181,8 +1189,8 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
       P.smem = total;
     }
   }
-  uint64_t slots = next_pow2(std::max<uint64_t>(1024, est * 2));
-  const uint64_t max_slots = next_pow2(std::max<uint64_t>(1024, P.rows * 2));
+  uint64_t slots = next_pow2(std::max<uint64_t>(1024, est * 8));
+  const uint64_t max_slots = next_pow2(std::max<uint64_t>(1024, P.rows * 8));
   slots = std::min(slots, max_slots);
   for (int attempt = 0; attempt < 6; ++attempt) {
     bool grow = false;
@@ -1193,15 +1201,19 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
       // Re-plan from the column statistics (a learned count may come from a
       // query with another filter), at least 8x the last estimate and twice
       // the groups already seen; the table and records at least double.
+      // A full table asks for more partitions or slots; when the plan cannot
+      // grow, the global regime takes the query.
       const uint32_t why = host_ctl->status[1];
       const PartPlan last = pp;
       const uint64_t stats = estimate_groups(query, P, ds, stream, false);
       est = std::min<uint64_t>(P.rows, std::max<uint64_t>({stats, est * 8, (uint64_t)host_ctl->alloc * 2}));
-      if (!plan_partitions(P, ds, est, pp)) return fail(DFC_CAPACITY, "partition capacity could not grow further");
-      if (why & CAP_AGG_TABLE) pp.agg_slots = std::max(pp.agg_slots, std::min(last.agg_slots * 2, 1u << 28));
-      if (why & CAP_RECORDS) pp.recs = std::max<uint64_t>(pp.recs, std::min<uint64_t>(P.rows, last.recs * 2));
-      if (pp.agg_slots == last.agg_slots && pp.recs == last.recs && pp.bits == last.bits)
-        return fail(DFC_CAPACITY, "partition capacity could not grow further");
+      if (plan_partitions(P, ds, est, pp)) {
+        if ((why & CAP_AGG_TABLE) && pp.agg_slots <= last.agg_slots) pp.agg_slots = std::min(last.agg_slots * 2, 1u << 28);
+        if (why & CAP_RECORDS) pp.recs = std::max<uint64_t>(pp.recs, std::min<uint64_t>(P.rows, last.recs * 2));
+        if (pp.bits != last.bits || pp.recs != last.recs || pp.agg_slots != last.agg_slots) continue;
+      }
+      partitioned = false;
+      slots = std::min(next_pow2(std::max<uint64_t>(1024, est * 8)), max_slots);
       continue;
     }
     if (slots >= max_slots) return fail(DFC_CAPACITY, "group table could not grow further");

@@ -246,11 +246,11 @@ __device__ __forceinline__ uint32_t select_word(const ScanParams& p, const Step&
 // ---------------------------------------------------------------------------
 // 3. Keys.
 // ---------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ void key_field(const ColRef& cr, const RowRef (&x)[kR], bool packed, const KeyField& f,
-                                          int k, uint64_t (&kw)[kR]) {
+template <typename T, int R>
+__device__ __forceinline__ void key_field(const ColRef& cr, const RowRef (&x)[R], bool packed, const KeyField& f,
+                                          int k, uint64_t (&kw)[R]) {
 #pragma unroll
-  for (int j = 0; j < kR; ++j) {
+  for (int j = 0; j < R; ++j) {
     if (!x[j].on) continue;
     const bool ok = rvalid(cr, x[j]);
     uint64_t cell = 0;
@@ -270,29 +270,30 @@ __device__ __forceinline__ void key_field(const ColRef& cr, const RowRef (&x)[kR
   }
 }
 
-__device__ __forceinline__ void key_words(const ScanParams& p, const Step& s, const RowRef (&x)[kR], uint64_t (&kw)[kR]) {
+template <int R = kR>
+__device__ __forceinline__ void key_words(const ScanParams& p, const Step& s, const RowRef (&x)[R], uint64_t (&kw)[R]) {
   const bool packed = p.key_mode == KEY_PACKED;
 #pragma unroll
-  for (int j = 0; j < kR; ++j) kw[j] = packed ? 0ull : 0x243F6A8885A308D3ull;
+  for (int j = 0; j < R; ++j) kw[j] = packed ? 0ull : 0x243F6A8885A308D3ull;
   for (int k = 0; k < p.n_keys; ++k) {
     const KeyField& f = p.keys[k];
     const ColRef cr = col_ref(p, s, f.input);
     switch (f.dtype) {
-      case DFC_INT8: key_field<int8_t>(cr, x, packed, f, k, kw); break;
-      case DFC_INT16: key_field<int16_t>(cr, x, packed, f, k, kw); break;
-      case DFC_INT32: key_field<int32_t>(cr, x, packed, f, k, kw); break;
-      case DFC_INT64: key_field<int64_t>(cr, x, packed, f, k, kw); break;
-      case DFC_UINT8: key_field<uint8_t>(cr, x, packed, f, k, kw); break;
-      case DFC_UINT16: key_field<uint16_t>(cr, x, packed, f, k, kw); break;
-      case DFC_UINT32: key_field<uint32_t>(cr, x, packed, f, k, kw); break;
-      case DFC_UINT64: key_field<uint64_t>(cr, x, packed, f, k, kw); break;
-      case DFC_FLOAT32: key_field<float>(cr, x, packed, f, k, kw); break;
-      default: key_field<double>(cr, x, packed, f, k, kw); break;
+      case DFC_INT8: key_field<int8_t, R>(cr, x, packed, f, k, kw); break;
+      case DFC_INT16: key_field<int16_t, R>(cr, x, packed, f, k, kw); break;
+      case DFC_INT32: key_field<int32_t, R>(cr, x, packed, f, k, kw); break;
+      case DFC_INT64: key_field<int64_t, R>(cr, x, packed, f, k, kw); break;
+      case DFC_UINT8: key_field<uint8_t, R>(cr, x, packed, f, k, kw); break;
+      case DFC_UINT16: key_field<uint16_t, R>(cr, x, packed, f, k, kw); break;
+      case DFC_UINT32: key_field<uint32_t, R>(cr, x, packed, f, k, kw); break;
+      case DFC_UINT64: key_field<uint64_t, R>(cr, x, packed, f, k, kw); break;
+      case DFC_FLOAT32: key_field<float, R>(cr, x, packed, f, k, kw); break;
+      default: key_field<double, R>(cr, x, packed, f, k, kw); break;
     }
   }
   if (!packed) {
 #pragma unroll
-    for (int j = 0; j < kR; ++j)
+    for (int j = 0; j < R; ++j)
       if (kw[j] == kEmpty) kw[j] = kEmpty - 1;
   }
 }
@@ -708,7 +709,8 @@ __device__ __forceinline__ T from_bits(uint64_t b) {
 
 // The rows' updates of one aggregated column: `recs` the rows' group records,
 // `ok` whether the row holds a valid value, `vb` the value's raw bits.
-template <typename T>
+// kShared: the records are in shared memory (generic loads, not .cg).
+template <typename T, bool kShared = false>
 __device__ __forceinline__ void update_rows(const ScanParams& p, const ValField& f, int v, unsigned char* const (&recs)[kR],
                                             const bool (&ok)[kR], const uint64_t (&vb)[kR]) {
   constexpr bool kFloat = std::is_floating_point<T>::value;
@@ -721,58 +723,62 @@ __device__ __forceinline__ void update_rows(const ScanParams& p, const ValField&
     lo[j] = hi[j] = ks[j] = 0;
     if (!ok[j]) continue;
     const unsigned char* rec = recs[j];
-    if (f.off_min >= 0) lo[j] = ld_cg_u64(rec + f.off_min);
-    if (f.off_max >= 0) hi[j] = ld_cg_u64(rec + f.off_max);
-    if (f.off_m2 >= 0) ks[j] = ld_cg_u64(rec + f.off_shift);
+    auto ld = [&](int off) -> uint64_t {
+      if constexpr (kShared) return *reinterpret_cast<const volatile unsigned long long*>(rec + off);
+      else return ld_cg_u64(rec + off);
+    };
+    if (f.off_min >= 0) lo[j] = ld(f.off_min);
+    if (f.off_max >= 0) hi[j] = ld(f.off_max);
+    if (f.off_m2 >= 0) ks[j] = ld(f.off_shift);
   }
 #pragma unroll
   for (int j = 0; j < kR; ++j) {
     if (!ok[j]) continue;
     unsigned char* rec = recs[j];
-    red_add_u32(rec + f.off_count, 1u);
+    rec_add_u32<kShared>(rec + f.off_count, 1u);
     const double xd = (double)val[j];
     const bool nan = kFloat && xd != xd;
     if (f.off_sum >= 0) {
       if constexpr (kFloat) {
-        red_add_f64(rec + f.off_sum, xd);
+        rec_add_f64<kShared>(rec + f.off_sum, xd);
       } else if (std::is_same<T, uint64_t>::value) {
         const uint64_t xv = (uint64_t)val[j];
-        const uint64_t old = atomicAdd(reinterpret_cast<unsigned long long*>(rec + f.off_sum), xv);
-        if (old + xv < old) red_add_u64(rec + f.off_sum + 8, 1ull);
+        const uint64_t old = rec_fetch_add_u64<kShared>(rec + f.off_sum, xv);
+        if (old + xv < old) rec_add_u64<kShared>(rec + f.off_sum + 8, 1ull);
       } else {
         const int64_t xv = (int64_t)val[j];
         if (f.sum_kind == SUM_I64) {
-          red_add_u64(rec + f.off_sum, (uint64_t)xv);
+          rec_add_u64<kShared>(rec + f.off_sum, (uint64_t)xv);
         } else {
-          const uint64_t old = atomicAdd(reinterpret_cast<unsigned long long*>(rec + f.off_sum), (uint64_t)xv);
+          const uint64_t old = rec_fetch_add_u64<kShared>(rec + f.off_sum, (uint64_t)xv);
           const uint64_t hi_add = (xv < 0 ? ~0ull : 0ull) + ((old + (uint64_t)xv) < old ? 1ull : 0ull);
-          if (hi_add) red_add_u64(rec + f.off_sum + 8, hi_add);
+          if (hi_add) rec_add_u64<kShared>(rec + f.off_sum + 8, hi_add);
         }
       }
     }
     if (f.off_min >= 0 || f.off_max >= 0) {
       if (nan) {
-        red_or_u32(rec + kRecFlags, 1u << (3 * v));
+        rec_or_u32<kShared>(rec + kRecFlags, 1u << (3 * v));
       } else {
         uint64_t bits;
         if constexpr (std::is_same<T, float>::value) bits = __float_as_uint(val[j]);
         else if constexpr (std::is_same<T, double>::value) bits = (uint64_t)__double_as_longlong(val[j]);
         else bits = (uint64_t)(typename std::make_unsigned<T>::type)val[j];
         const uint64_t e = order_encode(bits, f.dtype);
-        if (f.off_min >= 0 && ~e > lo[j]) red_max_u64(rec + f.off_min, ~e);
-        if (f.off_max >= 0 && e > hi[j]) red_max_u64(rec + f.off_max, e);
-        if (kFloat && xd == 0.0) red_or_u32(rec + kRecFlags, 1u << (3 * v + (signbit(xd) ? 2 : 1)));
+        if (f.off_min >= 0 && ~e > lo[j]) rec_max_u64<kShared>(rec + f.off_min, ~e);
+        if (f.off_max >= 0 && e > hi[j]) rec_max_u64<kShared>(rec + f.off_max, e);
+        if (kFloat && xd == 0.0) rec_or_u32<kShared>(rec + kRecFlags, 1u << (3 * v + (signbit(xd) ? 2 : 1)));
       }
     }
     if (f.off_m2 >= 0) {
       const uint64_t xbits = nan ? kCanonNaN : (uint64_t)__double_as_longlong(xd);
       uint64_t k = ks[j];
       if (k == 0) {
-        const uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long*>(rec + f.off_shift), 0ull, xbits ^ kShiftTag);
+        const uint64_t prev = rec_cas_u64<kShared>(rec + f.off_shift, 0ull, xbits ^ kShiftTag);
         k = prev == 0 ? (xbits ^ kShiftTag) : prev;
       }
       const double d = xd - __longlong_as_double((long long)(k ^ kShiftTag));
-      red_add_f64(rec + f.off_m2, d * d);
+      rec_add_f64<kShared>(rec + f.off_m2, d * d);
     }
   }
 }
@@ -1099,7 +1105,21 @@ __device__ void merge_record(const ScanParams& p, const unsigned char* src, uint
 // so pass A's rows of a partition fill exactly the range the count gave;
 // pass A checks that, and failed checks record a code in status word 2.
 // ===========================================================================
-constexpr int kPartPerThread = kPartMax / kScanConsumerThreads;
+constexpr int kPartPerThread = kPartMax / kPartConsumerThreads;
+
+// Barrier of the partition kernels' consumer warps (named barrier 1).
+__device__ __forceinline__ bool part_sync_or(bool flag) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(out)
+      : "r"((uint32_t)flag), "n"(kPartConsumerThreads)
+      : "memory");
+  return out != 0;
+}
 
 __device__ __forceinline__ void part_check(const ScanParams& p, uint32_t code) { atomicOr(p.status + 2, code); }
 
@@ -1139,7 +1159,7 @@ __device__ __forceinline__ uint32_t ld_cluster_u32(const void* local, uint32_t r
   return v;
 }
 
-// Exclusive prefix of one value per consumer thread (256 threads) and the
+// Exclusive prefix of one value per consumer thread (512 threads) and the
 // total; consumer warps only.
 __device__ __forceinline__ uint32_t consumer_exclusive_scan(uint32_t v, uint32_t* warp_tot, uint32_t* total) {
   const int lane = threadIdx.x & 31, cw = (threadIdx.x >> 5) - 1;
@@ -1149,53 +1169,80 @@ __device__ __forceinline__ uint32_t consumer_exclusive_scan(uint32_t v, uint32_t
     if (lane >= o) x += y;
   }
   if (lane == 31) warp_tot[cw] = x;
-  consumer_sync_or(false);
+  part_sync_or(false);
   uint32_t before = 0, all = 0;
-  for (int w = 0; w < kScanConsumerWarps; ++w) {
+  for (int w = 0; w < kPartWarps; ++w) {
     const uint32_t t = warp_tot[w];
     if (w < cw) before += t;
     all += t;
   }
   *total = all;
-  consumer_sync_or(false);
+  part_sync_or(false);
   return before + x - v;
 }
 
 // The partition kernels need no compaction: consumer warp w owns words
-// w, w + 8, ... of every tile (kR of them at most), and each lane handles
+// w, w + 16, ... of every tile (kPR of them at most), and each lane handles
 // its own row of each word.  Selection is a ballot per word; unselected rows
 // are masked off.  Between flushes the warps pass no CTA barrier, so their
 // latencies overlap freely.
-constexpr int kWordsPerWarp = kMaxTileRows / 32 / kScanConsumerWarps;
-static_assert(kWordsPerWarp == kR, "a lane holds one row per owned word");
+constexpr int kPR = kMaxTileRows / 32 / kPartWarps;  // rows a lane holds per tile
+static_assert(kPR >= 1, "a consumer warp owns whole words");
 
-__device__ __forceinline__ void tile_rows(const ScanParams& p, const Step& s, RowRef (&x)[kR], uint32_t (&bits)[kR]) {
+constexpr int kSR = kPR * kTilesPerStep;  // rows a lane holds per step (two tiles)
+
+// Waits for the tiles of one step (this CTA's tiles t and t + gridDim.x,
+// its it-th and it+1-th): false when a wait gave up (ST_TIMEOUT raised).
+__device__ __forceinline__ bool step_wait(const ScanParams& p, unsigned char* smem, uint64_t* full, uint64_t t,
+                                          uint32_t it, volatile uint32_t* s_abort, Step& s, int& nt) {
+  const int S = p.stages;
+  const uint64_t T = (uint64_t)p.tile_rows;
+  nt = 0;
+#pragma unroll
+  for (int k = 0; k < kTilesPerStep; ++k) {
+    const uint64_t tk = t + (uint64_t)k * gridDim.x;
+    s.n[k] = 0;
+    s.start[k] = 0;
+    s.staged[k] = false;
+    s.stage[k] = smem;
+    if (tk >= p.tiles) continue;
+    const uint32_t sid = (it + k) % S, ph = ((it + k) / S) & 1u;
+    if (*s_abort || !mbar_wait_bounded(&full[sid], ph, kWaitLimit)) {
+      atomicOr(p.status, ST_TIMEOUT);
+      *s_abort = 1;
+      return false;
+    }
+    s.stage[k] = smem + (size_t)sid * p.stage_bytes;
+    s.start[k] = tk * T;
+    s.staged[k] = p.use_tma && tk < p.full_tiles;
+    const uint64_t left = p.rows - s.start[k];
+    s.n[k] = (uint32_t)(left < T ? left : T);
+    ++nt;
+  }
+  return true;
+}
+
+// This lane's rows of the step: tile j / kPR, word (warp - 1) + (j % kPR) * 16.
+__device__ __forceinline__ void step_rows(const ScanParams& p, const Step& s, int nt, RowRef (&x)[kSR],
+                                          uint32_t (&bits)[kSR]) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t words = (uint32_t)p.tile_rows / 32;
 #pragma unroll
-  for (int j = 0; j < kR; ++j) {
-    const uint32_t w = (uint32_t)(warp - 1) + (uint32_t)j * kScanConsumerWarps;
-    bits[j] = w < words ? select_word(p, s, 0, w) : 0u;
-    x[j].tile = 0;
+  for (int j = 0; j < kSR; ++j) {
+    const int tile = j / kPR;
+    const uint32_t w = (uint32_t)(warp - 1) + (uint32_t)(j % kPR) * kPartWarps;
+    bits[j] = (w < words && tile < nt) ? select_word(p, s, tile, w) : 0u;
+    x[j].tile = (uint32_t)tile;
     x[j].r = w * 32 + lane;
     x[j].on = (bits[j] >> lane) & 1u;
   }
 }
 
-// The step of tile t (this CTA's it-th tile) once its stage has landed.
-__device__ __forceinline__ Step tile_step(const ScanParams& p, unsigned char* smem, uint64_t t, uint32_t sid, bool failed) {
-  const uint64_t T = (uint64_t)p.tile_rows;
-  Step s;
-  s.stage[0] = smem + (size_t)sid * p.stage_bytes;
-  s.start[0] = t * T;
-  s.staged[0] = p.use_tma && t < p.full_tiles;
-  const uint64_t left = p.rows - s.start[0];
-  s.n[0] = failed ? 0u : (uint32_t)(left < T ? left : T);
-  s.stage[1] = s.stage[0];
-  s.start[1] = 0;
-  s.staged[1] = false;
-  s.n[1] = 0;
-  return s;
+// Releases the step's stages (each consumer warp arrives once per tile).
+__device__ __forceinline__ void step_release(const ScanParams& p, uint64_t* empty, uint32_t it, int nt) {
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < nt; ++k) mbar_arrive(&empty[(it + k) % p.stages]);
 }
 
 // Ring set-up shared by the counting pass and pass A.
@@ -1203,7 +1250,7 @@ __device__ __forceinline__ void ring_init(int S, uint64_t* full, uint64_t* empty
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&empty[s], kScanConsumerWarps);
+      mbar_init(&empty[s], kPartWarps);
     }
     fence_mbar_init();
     *s_abort = 0;
@@ -1211,7 +1258,7 @@ __device__ __forceinline__ void ring_init(int S, uint64_t* full, uint64_t* empty
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kScanThreads, 1) partition_count(const __grid_constant__ ScanParams p) {
+__global__ void __launch_bounds__(kPartThreads, 1) partition_count(const __grid_constant__ ScanParams p) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int S = p.stages;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)S * p.stage_bytes);
@@ -1225,23 +1272,19 @@ __global__ void __launch_bounds__(kScanThreads, 1) partition_count(const __grid_
     if ((threadIdx.x & 31) == 0) produce_tiles(p, smem, full, empty, &s_abort, p.n_stage_count, (uint32_t)p.stage_tx_count);
   } else {
     uint32_t it = 0;
-    for (uint64_t t = blockIdx.x; t < p.tiles; t += gridDim.x, ++it) {
-      const uint32_t sid = it % S, ph = (it / S) & 1u;
-      if (s_abort || !mbar_wait_bounded(&full[sid], ph, kWaitLimit)) {
-        atomicOr(p.status, ST_TIMEOUT);
-        s_abort = 1;
-        break;
-      }
-      const Step s = tile_step(p, smem, t, sid, false);
-      RowRef x[kR];
-      uint32_t bits[kR];
-      uint64_t kw[kR];
-      tile_rows(p, s, x, bits);
-      key_words(p, s, x, kw);
-      __syncwarp();
-      if ((threadIdx.x & 31) == 0) mbar_arrive(&empty[sid]);  // this warp no longer reads the stage
+    for (uint64_t t = blockIdx.x; t < p.tiles; t += (uint64_t)kTilesPerStep * gridDim.x) {
+      Step s;
+      int nt;
+      if (!step_wait(p, smem, full, t, it, &s_abort, s, nt)) break;
+      RowRef x[kSR];
+      uint32_t bits[kSR];
+      uint64_t kw[kSR];
+      step_rows(p, s, nt, x, bits);
+      key_words<kSR>(p, s, x, kw);
+      step_release(p, empty, it, nt);
+      it += nt;
 #pragma unroll
-      for (int j = 0; j < kR; ++j)
+      for (int j = 0; j < kSR; ++j)
         if (x[j].on) atomicAdd(&s_count[partition_of(p, kw[j])], 1u);
     }
   }
@@ -1271,8 +1314,8 @@ struct PartSmem {
   uint32_t base[kPartMax];  // part_buf row of that position (all ones: not stored)
   uint32_t next[kPartMax];  // this CTA's next part_buf row of each partition
   uint32_t end[kPartMax];   // the end of this CTA's range of each partition
-  uint32_t wfill[kScanConsumerWarps];  // rows each warp's staging region holds
-  uint32_t warp_tot[kScanConsumerWarps];
+  uint32_t wfill[kPartWarps];  // rows each warp's staging region holds
+  uint32_t warp_tot[kPartWarps];
 };
 
 // Pass A's flush: the staged rows of every warp region (region rows each,
@@ -1283,15 +1326,15 @@ __device__ void flush_staged(const ScanParams& p, const unsigned long long* stag
                              const uint16_t* rpart, uint32_t region_shift, PartSmem& ps) {
   const uint32_t ct = threadIdx.x - 32;
   const uint32_t nparts = 1u << p.part_bits;
-  const uint32_t cap = (uint32_t)kScanConsumerWarps << region_shift;
+  const uint32_t cap = (uint32_t)kPartWarps << region_shift;
   const uint32_t rmask = (1u << region_shift) - 1u;
-  for (uint32_t q = ct; q < nparts; q += kScanConsumerThreads) ps.cur[q] = 0;
-  consumer_sync_or(false);
+  for (uint32_t q = ct; q < nparts; q += kPartConsumerThreads) ps.cur[q] = 0;
+  part_sync_or(false);
   uint32_t rows = 0;
-  for (int w = 0; w < kScanConsumerWarps; ++w) rows += ps.wfill[w];
-  for (uint32_t u = ct; u < cap; u += kScanConsumerThreads)
+  for (int w = 0; w < kPartWarps; ++w) rows += ps.wfill[w];
+  for (uint32_t u = ct; u < cap; u += kPartConsumerThreads)
     if ((u & rmask) < ps.wfill[u >> region_shift]) atomicAdd(&ps.cur[rpart[u]], 1u);
-  consumer_sync_or(false);
+  part_sync_or(false);
   uint32_t h[kPartPerThread], sum = 0;
 #pragma unroll
   for (int k = 0; k < kPartPerThread; ++k) {
@@ -1318,12 +1361,12 @@ __device__ void flush_staged(const ScanParams& p, const unsigned long long* stag
     }
     off += h[k];
   }
-  consumer_sync_or(false);
-  for (uint32_t u = ct; u < cap; u += kScanConsumerThreads)
+  part_sync_or(false);
+  for (uint32_t u = ct; u < cap; u += kPartConsumerThreads)
     if ((u & rmask) < ps.wfill[u >> region_shift]) order[atomicAdd(&ps.cur[rpart[u]], 1u)] = (uint16_t)u;
-  consumer_sync_or(false);
+  part_sync_or(false);
   const uint32_t W = p.part_words;
-  for (uint32_t s = ct; s < rows; s += kScanConsumerThreads) {
+  for (uint32_t s = ct; s < rows; s += kPartConsumerThreads) {
     const uint32_t u = order[s];
     const uint32_t q = rpart[u];
     const uint32_t base = ps.base[q];
@@ -1337,10 +1380,10 @@ __device__ void flush_staged(const ScanParams& p, const unsigned long long* stag
     unsigned long long* dst = p.part_buf + x * W;
     for (uint32_t j = 0; j < W; ++j) dst[j] = src[j];
   }
-  consumer_sync_or(false);
+  part_sync_or(false);
 }
 
-__global__ void __launch_bounds__(kScanThreads, 1) partition_kernel(const __grid_constant__ ScanParams p) {
+__global__ void __launch_bounds__(kPartThreads, 1) partition_kernel(const __grid_constant__ ScanParams p) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int S = p.stages;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)S * p.stage_bytes);
@@ -1359,11 +1402,11 @@ __global__ void __launch_bounds__(kScanThreads, 1) partition_kernel(const __grid
   const int cw = (threadIdx.x >> 5) - 1, lane = threadIdx.x & 31;
   const uint32_t nparts = 1u << p.part_bits;
   const uint32_t W = p.part_words;
-  // Staging: one region per consumer warp; a warp stages at most kR * 32
-  // rows a tile, so flushing every `every` tiles never overflows a region.
+  // Staging: one region per consumer warp; a warp stages at most kSR * 32
+  // rows a step, so flushing every `every` steps never overflows a region.
   uint32_t region_shift = 0;
-  while ((kScanConsumerWarps << (region_shift + 1)) <= p.part_flush) ++region_shift;
-  const uint32_t every = (1u << region_shift) / (kR * 32);
+  while ((kPartWarps << (region_shift + 1)) <= p.part_flush) ++region_shift;
+  const uint32_t every = (1u << region_shift) / (kSR * 32);
   // This CTA's range of each partition: the partition's start (prefix of the
   // totals) plus the CTA's prefix among the CTAs.
   {
@@ -1392,56 +1435,52 @@ __global__ void __launch_bounds__(kScanThreads, 1) partition_kernel(const __grid
   const uint32_t rbase = (uint32_t)cw << region_shift;
   uint32_t wfill = 0;  // this warp's staged rows (the same in all its lanes)
   bool aborted = false;
-  uint32_t it = 0;
-  for (uint64_t t = blockIdx.x; t < p.tiles; t += gridDim.x, ++it) {
-    const uint32_t sid = it % S, ph = (it / S) & 1u;
-    if (!aborted && (s_abort || !mbar_wait_bounded(&full[sid], ph, kWaitLimit))) {
-      atomicOr(p.status, ST_TIMEOUT);
-      s_abort = 1;
-      aborted = true;
-    }
+  uint32_t it = 0, step = 0;
+  for (uint64_t t = blockIdx.x; t < p.tiles; t += (uint64_t)kTilesPerStep * gridDim.x, ++step) {
+    Step s;
+    int nt = 0;
+    if (!aborted && !step_wait(p, smem, full, t, it, &s_abort, s, nt)) aborted = true;
     if (!aborted) {
-      const Step s = tile_step(p, smem, t, sid, false);
-      RowRef x[kR];
-      uint32_t bits[kR];
-      uint64_t kw[kR];
-      tile_rows(p, s, x, bits);
-      key_words(p, s, x, kw);
+      RowRef x[kSR];
+      uint32_t bits[kSR];
+      uint64_t kw[kSR];
+      step_rows(p, s, nt, x, bits);
+      key_words<kSR>(p, s, x, kw);
       // Positions in this warp's region: words in order, lanes in order.
-      uint32_t at[kR];
+      uint32_t at[kSR];
       uint32_t run = wfill;
 #pragma unroll
-      for (int j = 0; j < kR; ++j) {
+      for (int j = 0; j < kSR; ++j) {
         at[j] = rbase + run + __popc(bits[j] & ((1u << lane) - 1u));
         run += __popc(bits[j]);
       }
-      uint32_t vflags[kR] = {};
+      uint32_t vflags[kSR] = {};
       for (int v = 0; v < p.n_vals; ++v) {
         const int c = p.vals[v].input;
         const ColRef cr = col_ref(p, s, c);
         const int size = p.cols[c].size;
 #pragma unroll
-        for (int j = 0; j < kR; ++j) {
+        for (int j = 0; j < kSR; ++j) {
           if (!x[j].on) continue;
           const bool ok = rvalid(cr, x[j]);
           vflags[j] |= (uint32_t)ok << v;
           staged[(size_t)at[j] * W + 2 + v] = ok ? load_bits(rv(cr, x[j]), size, x[j].r) : 0ull;
         }
       }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[sid]);  // this warp no longer reads the stage
+      step_release(p, empty, it, nt);
+      it += nt;
 #pragma unroll
-      for (int j = 0; j < kR; ++j) {
+      for (int j = 0; j < kSR; ++j) {
         if (!x[j].on) continue;
         staged[(size_t)at[j] * W] = kw[j];
-        staged[(size_t)at[j] * W + 1] = (uint64_t)(uint32_t)(s.start[0] + x[j].r) | ((uint64_t)vflags[j] << 32);
+        staged[(size_t)at[j] * W + 1] = (uint64_t)(uint32_t)(s.start[x[j].tile] + x[j].r) | ((uint64_t)vflags[j] << 32);
         rpart[at[j]] = (uint16_t)partition_of(p, kw[j]);
       }
       wfill = run;
     }
-    if ((it + 1) % every == 0) {
+    if ((step + 1) % every == 0) {
       if (lane == 0) s_part.wfill[cw] = wfill;
-      if (consumer_sync_or(aborted)) {
+      if (part_sync_or(aborted)) {
         aborted = true;
         break;
       }
@@ -1450,12 +1489,138 @@ __global__ void __launch_bounds__(kScanThreads, 1) partition_kernel(const __grid
     }
   }
   if (lane == 0) s_part.wfill[cw] = wfill;
-  if (consumer_sync_or(aborted)) return;
+  if (part_sync_or(aborted)) return;
   flush_staged(p, staged, order, rpart, region_shift, s_part);
   // Every range filled exactly as counted.
-  for (uint32_t q = ct; q < nparts; q += kScanConsumerThreads)
+  for (uint32_t q = ct; q < nparts; q += kPartConsumerThreads)
     if (s_part.next[q] != s_part.end[q]) part_check(p, CHK_RANGE);
 }
+
+// Full-warp butterfly reductions (every lane gets the result).
+__device__ __forceinline__ double warp_sum_f64(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ uint64_t warp_max_u64(uint64_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const uint64_t w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = w > v ? w : v;
+  }
+  return v;
+}
+__device__ __forceinline__ __int128 warp_sum_i128(__int128 v) {
+  uint64_t lo = (uint64_t)v, hi = (uint64_t)((unsigned __int128)v >> 64);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const uint64_t olo = __shfl_xor_sync(0xffffffffu, lo, o), ohi = __shfl_xor_sync(0xffffffffu, hi, o);
+    const uint64_t nlo = lo + olo;
+    hi = hi + ohi + (nlo < lo ? 1ull : 0ull);
+    lo = nlo;
+  }
+  return (__int128)(((unsigned __int128)hi << 64) | lo);
+}
+
+// Folds the lanes of the warp's largest group -- `grp` is each lane's group
+// mask (0 outside), `maxpop` its size -- into the group's record (`rec`, the
+// lane's own record pointer) with one atomic per field: every field reduced
+// over the group by a five-step butterfly, whatever the group's size.  Same
+// state updates as group_update.  Every lane calls it; returns whether this
+// lane was folded.  `get(v, ok, b)` gives the lane's value of column v.
+template <typename Get>
+__device__ bool collapse_largest(const ScanParams& p, unsigned char* rec, uint32_t grp, int maxpop, bool on, uint32_t row,
+                                 Get&& get) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t cand = __ballot_sync(0xffffffffu, on && __popc(grp) == maxpop);
+  const int lead = __ffs(cand) - 1;  // the lowest lane of a largest group: its leader
+  const uint32_t big = __shfl_sync(0xffffffffu, grp, lead);
+  const bool in = (big >> lane) & 1u;
+  const bool leader = lane == lead;
+  unsigned char* const grec = reinterpret_cast<unsigned char*>(
+      __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(rec), lead));
+  const uint32_t first = __reduce_min_sync(0xffffffffu, in ? row : 0xFFFFFFFFu);
+  if (leader) {
+    atomicMax(reinterpret_cast<uint32_t*>(grec + kRecFirst), ~first);
+    if (p.off_len >= 0) atomicAdd(reinterpret_cast<uint32_t*>(grec + p.off_len), (uint32_t)__popc(big));
+  }
+  for (int v = 0; v < p.n_vals; ++v) {
+    const ValField& f = p.vals[v];
+    const int dt = f.dtype;
+    const bool isf = dt_float(dt);
+    bool ok = false;
+    uint64_t b = 0;
+    if (in) get(v, ok, b);
+    ok = ok && in;
+    if (!ok) b = 0;
+    const double xd = isf ? bits_to_f64(b, dt) : bits_as_double(b, dt);
+    const bool nan = ok && isf && xd != xd;
+    const uint32_t vmask = __ballot_sync(0xffffffffu, ok);
+    if (leader && vmask) atomicAdd(reinterpret_cast<uint32_t*>(grec + f.off_count), (uint32_t)__popc(vmask));
+    if (f.off_sum >= 0) {
+      if (f.sum_kind == SUM_F64) {
+        const double sm = warp_sum_f64(ok ? xd : 0.0);
+        if (leader && vmask) atomicAdd(reinterpret_cast<double*>(grec + f.off_sum), sm);
+      } else {
+        const bool uns = dt == DFC_UINT64;
+        const __int128 xv = !ok ? (__int128)0 : (uns ? (__int128)b : (__int128)bits_to_i64(b, dt));
+        const __int128 exact = warp_sum_i128(xv);
+        if (leader && vmask) {
+          if (f.sum_kind == SUM_I64) {
+            atomicAdd(reinterpret_cast<unsigned long long*>(grec + f.off_sum), (unsigned long long)(long long)exact);
+          } else {
+            const uint64_t add_lo = (uint64_t)exact, add_hi = (uint64_t)(exact >> 64);
+            const uint64_t old = atomicAdd(reinterpret_cast<unsigned long long*>(grec + f.off_sum), add_lo);
+            const uint64_t hi_add = add_hi + ((old + add_lo) < old ? 1ull : 0ull);
+            if (hi_add) atomicAdd(reinterpret_cast<unsigned long long*>(grec + f.off_sum + 8), hi_add);
+          }
+        }
+      }
+    }
+    if (f.off_min >= 0 || f.off_max >= 0) {
+      const bool ordinary = ok && !nan;
+      const uint64_t e = ordinary ? order_encode(b, dt) : 0ull;
+      if (f.off_min >= 0) {
+        const unsigned long long m = warp_max_u64(ordinary ? ~e : 0ull);
+        if (leader && m) atomicMax(reinterpret_cast<unsigned long long*>(grec + f.off_min), m);
+      }
+      if (f.off_max >= 0) {
+        const unsigned long long m = warp_max_u64(e);
+        if (leader && m) atomicMax(reinterpret_cast<unsigned long long*>(grec + f.off_max), m);
+      }
+      const uint32_t nanmask = __ballot_sync(0xffffffffu, nan);
+      const uint32_t pz = __ballot_sync(0xffffffffu, ok && isf && xd == 0.0 && __double_as_longlong(xd) >= 0);
+      const uint32_t nz = __ballot_sync(0xffffffffu, ok && isf && xd == 0.0 && __double_as_longlong(xd) < 0);
+      if (leader) {
+        uint32_t bits = 0;
+        if (nanmask) bits |= 1u << (3 * v);
+        if (pz) bits |= 1u << (3 * v + 1);
+        if (nz) bits |= 1u << (3 * v + 2);
+        if (bits) atomicOr(reinterpret_cast<uint32_t*>(grec + kRecFlags), bits);
+      }
+    }
+    if (f.off_m2 >= 0 && vmask) {
+      // The group's shift K: set once, by the first valid value of a leader.
+      const uint64_t xbits = (xd != xd) ? kCanonNaN : (uint64_t)__double_as_longlong(xd);
+      const uint64_t candk = __shfl_sync(0xffffffffu, xbits, __ffs(vmask) - 1);
+      uint64_t ks = 0;
+      if (leader) {
+        ks = *reinterpret_cast<volatile unsigned long long*>(grec + f.off_shift);
+        if (ks == 0) {
+          const uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long*>(grec + f.off_shift), 0ull, candk ^ kShiftTag);
+          ks = prev == 0 ? (candk ^ kShiftTag) : prev;
+        }
+      }
+      ks = __shfl_sync(0xffffffffu, ks, lead);
+      const double d = xd - __longlong_as_double((long long)(ks ^ kShiftTag));
+      const double s2 = warp_sum_f64(ok ? d * d : 0.0);
+      if (leader) atomicAdd(reinterpret_cast<double*>(grec + f.off_m2), s2);
+    }
+  }
+  return in;
+}
+
+constexpr int kCollapseMin = 4;  // group size from which a warp folds a group by butterfly
 
 // ---------------------------------------------------------------------------
 // Pass B.  A cluster's table is initialised once (key words all ones, fields
@@ -1550,23 +1715,27 @@ __device__ __forceinline__ void fold_rows(const ScanParams& p, unsigned char* ta
     }
     if (!on[j]) slot[j] = 0;
   }
-  // Rows of one record within the warp (hot keys) are reduced across lanes
-  // first: one atomic per field and group instead of one per row.
+  // Large groups of one record within the warp (hot keys) are folded by a
+  // butterfly first (up to two per row set): one atomic per field and group.
 #pragma unroll
   for (int j = 0; j < kR; ++j) {
     const uint64_t tag = on[j] ? slot[j] : (0x8000000000000000ull | (uint64_t)lane);
     uint32_t grp = __match_any_sync(0xffffffffu, tag) & __ballot_sync(0xffffffffu, on[j]);
     if (!on[j]) grp = 0;
-    const int maxpop = __reduce_max_sync(0xffffffffu, (unsigned)__popc(grp));
-    if (maxpop <= 1) continue;
-    unsigned char* rec = table + slot[j] * rs;
-    const unsigned long long* sp = src[j];
-    const uint32_t flags = vf[j];
-    group_update(p, rec, grp, maxpop, on[j], row[j], [&](int v, bool& ok, uint64_t& b) {
-      ok = (flags >> v) & 1u;
-      b = ok ? __ldcs(sp + 2 + v) : 0ull;
-    });
-    on[j] = false;
+    int maxpop = __reduce_max_sync(0xffffffffu, (unsigned)__popc(grp));
+    for (int round = 0; round < 2 && maxpop >= kCollapseMin; ++round) {
+      unsigned char* rec = table + slot[j] * rs;
+      const unsigned long long* sp = src[j];
+      const uint32_t flags = vf[j];
+      if (collapse_largest(p, rec, grp, maxpop, on[j], row[j], [&](int v, bool& ok, uint64_t& b) {
+            ok = (flags >> v) & 1u;
+            b = ok ? __ldcs(sp + 2 + v) : 0ull;
+          })) {
+        on[j] = false;
+        grp = 0;
+      }
+      maxpop = __reduce_max_sync(0xffffffffu, (unsigned)__popc(grp));
+    }
   }
   unsigned char* recs[kR];
 #pragma unroll

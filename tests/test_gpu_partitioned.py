@@ -53,12 +53,11 @@ def test_fixture_partitioned(case, partitioned):
     assert_frames_match(actual, expected_frame(case), rtol=1e-15, label=case["name"])
 
 
-def test_config2_many_groups_chooses_partitioned():
-    """4M rows over 1M x 64 key pairs: about 1.5M groups, past the L2 budget
-    of the global table, so the planner partitions on its own."""
+def test_config2_many_groups_partitioned(partitioned):
+    """4M rows over 1M x 64 key pairs: about 1.5M groups in 512 partitions."""
     frame = config2(rows=4_000_000, distinct=1_000_000)
     compare_with_oracle(
-        config2_plan(frame), "config2-4M-auto", float_cols=("sum", "mean"), var_cols=("var",),
+        config2_plan(frame), "config2-4M-partitioned", float_cols=("sum", "mean"), var_cols=("var",),
         scales=lambda ref: dict(zip(("sum", "mean"), magnitude(ref, "count", "min", "max"))),
     )
     assert regime() == 2

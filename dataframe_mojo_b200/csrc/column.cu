@@ -80,4 +80,39 @@ __global__ void column_hll(DevColumn c, uint64_t rows, uint32_t* regs) {
     if (local[i]) atomicMax(&regs[i], local[i]);
 }
 
+// HyperLogLog registers of the query's key words over all rows: the packed
+// key word (keys <= 64 bits) or the 64-bit key hash, both as the scan forms
+// them.  The group count of a multi-key query is estimated from these
+// directly instead of from the product of the columns' distinct counts.
+__global__ void keys_hll(const __grid_constant__ ScanParams p, uint32_t* regs) {
+  __shared__ uint32_t local[1u << kHllBits];
+  for (uint32_t i = threadIdx.x; i < (1u << kHllBits); i += blockDim.x) local[i] = 0;
+  __syncthreads();
+  const bool packed = p.key_mode == KEY_PACKED;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < p.rows; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t kw = packed ? 0ull : 0x243F6A8885A308D3ull;
+    for (int k = 0; k < p.n_keys; ++k) {
+      const KeyField& f = p.keys[k];
+      const DevColumn& c = p.cols[f.input];
+      const bool ok = !c.validity || bit_valid(c.validity, i);
+      const uint64_t cell = ok ? key_cell(load_bits(c.values, c.size, i), f.dtype) : 0ull;
+      if (packed) {
+        if (!ok) kw |= 1ull << f.null_bit;
+        else kw |= (f.bits == 64) ? cell : (cell << f.shift);
+      } else {
+        const uint64_t v = ok ? cell + 1 : 0x9E3779B97F4A7C15ull;
+        kw = mix64(kw ^ (v * 0x9E3779B97F4A7C15ull + (uint64_t)k));
+      }
+    }
+    const uint64_t h = mix64(kw ^ 0xD6E8FEB86659FD93ull);
+    const uint32_t reg = (uint32_t)(h >> (64 - kHllBits));
+    const uint64_t rest = h << kHllBits;
+    const uint32_t rho = rest == 0 ? (65 - kHllBits) : (uint32_t)__clzll(rest) + 1;
+    if (rho > local[reg]) atomicMax(&local[reg], rho);
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < (1u << kHllBits); i += blockDim.x)
+    if (local[i]) atomicMax(&regs[i], local[i]);
+}
+
 }  // namespace dfc

@@ -41,4 +41,5 @@ __global__ void normalize_validity(const uint8_t* src, uint64_t nbytes, uint64_t
 __global__ void column_minmax(DevColumn c, uint64_t rows, unsigned long long* out);
 constexpr int kHllBits = 12;
 __global__ void column_hll(DevColumn c, uint64_t rows, uint32_t* regs);
+__global__ void keys_hll(const __grid_constant__ ScanParams p, uint32_t* regs);
 }  // namespace dfc

@@ -543,6 +543,43 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
 // Column statistics, computed once per column on its first use as a key.
 std::mutex g_stats_mu;
 
+// HyperLogLog estimate (Flajolet et al. 2007) with the linear-counting
+// correction for small cardinalities.
+double hll_estimate(const std::vector<uint32_t>& regs) {
+  double sum = 0;
+  int zeros = 0;
+  for (uint32_t r : regs) {
+    sum += std::ldexp(1.0, -(int)r);
+    zeros += r == 0;
+  }
+  const double m = (double)regs.size(), alpha = 0.7213 / (1.0 + 1.079 / m);
+  double est = alpha * m * m / sum;
+  if (est <= 2.5 * m && zeros > 0) est = m * std::log(m / zeros);
+  return est;
+}
+
+// Distinct key words of the query over all rows (HyperLogLog; 0 on failure).
+double joint_key_estimate(const Plan& P, DeviceState* ds, cudaStream_t stream) {
+  const uint32_t nreg = 1u << kHllBits;
+  uint32_t* d_regs = nullptr;
+  std::vector<uint32_t> regs(nreg);
+  cudaError_t e = cudaMallocAsync((void**)&d_regs, nreg * 4, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_regs, 0, nreg * 4, stream);
+  if (e == cudaSuccess) {
+    const unsigned blocks = (unsigned)std::min<uint64_t>((P.rows + 255) / 256, (uint64_t)ds->sms * 4);
+    keys_hll<<<std::max(1u, blocks), 256, 0, stream>>>(P.sp, d_regs);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(regs.data(), d_regs, nreg * 4, cudaMemcpyDeviceToHost, stream);
+  if (d_regs) cudaFreeAsync(d_regs, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return hll_estimate(regs) * 1.05 + 16;  // ~1.6% standard error at 4096 registers: keep a margin
+}
+
 dfc_status ensure_stats(dfc_column* c, DeviceState* ds, cudaStream_t stream) {
   std::lock_guard<std::mutex> lk(g_stats_mu);
   if (c->have_stats || c->rows == 0) return DFC_OK;
@@ -568,17 +605,7 @@ dfc_status ensure_stats(dfc_column* c, DeviceState* ds, cudaStream_t stream) {
   if (d_regs) cudaFreeAsync(d_regs, stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
   if (e != cudaSuccess) return cuda_fail(e, "column statistics");
-  // HyperLogLog estimate (Flajolet et al. 2007) with the linear-counting
-  // correction for small cardinalities.
-  double sum = 0;
-  int zeros = 0;
-  for (uint32_t r : regs) {
-    sum += std::ldexp(1.0, -(int)r);
-    zeros += r == 0;
-  }
-  const double m = nreg, alpha = 0.7213 / (1.0 + 1.079 / m);
-  double est = alpha * m * m / sum;
-  if (est <= 2.5 * m && zeros > 0) est = m * std::log(m / zeros);
+  const double est = hll_estimate(regs);
   c->min_enc = h_mm[0];
   c->max_enc = h_mm[1];
   c->distinct = est;
@@ -609,6 +636,12 @@ uint64_t estimate_groups(const dfc_query* q, const Plan& P, DeviceState* ds, cud
     }
     if (c->validity) d += 1;
     prod *= d;
+  }
+  // Several keys: the product bounds the group count loosely (correlated
+  // keys, Zipf pairs); the key words' own distinct count is the estimate.
+  if (q->n_keys > 1 && prod > 65536 && P.rows > 0) {
+    const double joint = joint_key_estimate(P, ds, stream);
+    if (joint > 0) prod = std::min(prod, joint);
   }
   double est = std::min(prod, (double)P.rows);
   return (uint64_t)std::max(1.0, est);

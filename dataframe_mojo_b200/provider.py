@@ -186,13 +186,23 @@ class DeviceResult:
         _check(N.lib().dfc_result_column(self.handle, i, C.byref(dt), C.byref(vals), C.byref(valid)))
         return np_dtype(dt.value), vals.value, valid.value
 
-    def to_frame(self) -> DataFrame:
+    def to_frame(self, into: dict | None = None) -> DataFrame:
+        """Copies the result to host memory.  `into` maps column names to
+        (values, bits) host arrays of at least rows elements / ceil(rows/8)
+        bytes (pinned memory copies at full speed); the frame then views them."""
         lib = N.lib()
         cols = []
         for i, name in enumerate(self.names):
             dtype, _, dvalid = self.column_info(i)
-            values = np.empty(self.rows, dtype=dtype)
-            bits = np.empty((self.rows + 7) // 8, dtype=np.uint8) if dvalid else None
+            if into is not None:
+                vbuf, bbuf = into[name]
+                if vbuf.dtype != dtype or len(vbuf) < self.rows or len(bbuf) < (self.rows + 7) // 8:
+                    raise ValueError(f"buffer for {name!r} is too small or of the wrong type")
+                values = vbuf[: self.rows]
+                bits = bbuf[: (self.rows + 7) // 8] if dvalid else None
+            else:
+                values = np.empty(self.rows, dtype=dtype)
+                bits = np.empty((self.rows + 7) // 8, dtype=np.uint8) if dvalid else None
             _check(
                 lib.dfc_result_copy_to_host(
                     self.handle,

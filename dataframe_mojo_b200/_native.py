@@ -137,6 +137,8 @@ SIGNATURES = [
         [C.POINTER(Query), C.c_int32, C.c_uint64, C.POINTER(DeviceColumnDesc), C.c_uint64, C.POINTER(DeviceOutput),
          C.POINTER(C.c_uint64)],
     ),
+    ("dfc_groupby_batch", C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_int)]),
+    ("dfc_batch_error", C.c_char_p, [C.c_int32]),
     ("dfc_result_rows", C.c_uint64, [C.c_void_p]),
     ("dfc_result_columns", C.c_int32, [C.c_void_p]),
     (

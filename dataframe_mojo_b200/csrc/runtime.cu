@@ -1630,3 +1630,299 @@ DFC_API dfc_status dfc_groupby_noalloc(const dfc_query* query, int32_t device, u
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// dfc_groupby_batch: many queries in one submission.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kBatchStreams = 8;
+thread_local std::vector<std::string> t_batch_errors;
+
+// The batch's streams on `dev`, created once per thread.
+const std::vector<cudaStream_t>& batch_streams(int dev) {
+  thread_local std::map<int, std::vector<cudaStream_t>> streams;
+  auto& v = streams[dev];
+  if (v.empty()) {
+    v.resize(kBatchStreams);
+    for (auto& s : v) cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  }
+  return v;
+}
+
+// One query of a batch: its plan and where its working memory lies.
+struct BatchItem {
+  Plan P;
+  dfc_status st = DFC_OK;
+  uint64_t slots = 0, recs = 0, chunk = 64, ncta = 1, words = 0, chunks = 1, out_rows = 0;
+  size_t off_table = 0, off_records = 0, off_bits = 0, off_prefix = 0, off_bsums = 0, off_perm = 0, off_firsts = 0;
+  std::vector<ResultCol> rc;
+};
+
+size_t arena_take(size_t& used, size_t bytes) {
+  const size_t at = used;
+  used += (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255;
+  return at;
+}
+
+// The launches of one planned query (global or shared-memory regime) on
+// `stream`, working memory at `base`, control block `dctl`.
+void launch_item(BatchItem& it, DeviceState* ds, unsigned char* base, Control* dctl, cudaStream_t stream) {
+  ScanParams& sp = it.P.sp;
+  FinishParams& fp = it.P.fp;
+  void* table = base + it.off_table;
+  void* records = base + it.off_records;
+  cudaMemsetAsync(table, 0xFF, (it.slots + 1) * sizeof(KeyEntry), stream);
+  cudaMemsetAsync(records, 0, it.recs * sp.rec_stride, stream);
+  cudaMemsetAsync(dctl, 0, sizeof(Control), stream);
+  cudaMemsetAsync(&dctl->overflow_agg, 0xFF, 4, stream);
+  cudaMemsetAsync(base + it.off_bits, 0, it.words * 4 + 16, stream);
+  sp.table = static_cast<KeyEntry*>(table);
+  sp.table_mask = it.slots - 1;
+  sp.records = static_cast<unsigned char*>(records);
+  sp.recs_total = (uint32_t)it.recs;
+  sp.chunk = (uint32_t)it.chunk;
+  sp.alloc = &dctl->alloc;
+  sp.status = dctl->status;
+  sp.part_bits = 0;
+  if (it.P.rows > 0) scan_kernel<<<(unsigned)it.ncta, kScanThreads, it.P.smem, stream>>>(sp);
+  fp.scan = sp;
+  fp.order_bits = reinterpret_cast<uint32_t*>(base + it.off_bits);
+  fp.word_prefix = reinterpret_cast<uint32_t*>(base + it.off_prefix);
+  fp.block_sums = reinterpret_cast<uint32_t*>(base + it.off_bsums);
+  fp.perm = reinterpret_cast<uint32_t*>(base + it.off_perm);
+  fp.firsts = reinterpret_cast<uint32_t*>(base + it.off_firsts);
+  fp.groups = &dctl->groups;
+  fp.has_nulls = dctl->has_nulls;
+  fp.overflow_agg = &dctl->overflow_agg;
+  fp.words = it.words;
+  for (int c = 0; c < it.P.n_out; ++c) {
+    fp.out[c].values = it.rc[c].values;
+    fp.out[c].validity = it.rc[c].validity;
+  }
+  const unsigned rec_blocks = (unsigned)std::min<uint64_t>((it.recs + kFinishThreads - 1) / kFinishThreads, (uint64_t)ds->sms * 16);
+  finish_mark<<<std::max(1u, rec_blocks), kFinishThreads, 0, stream>>>(fp);
+  finish_chunk_sums<<<(unsigned)it.chunks, kFinishThreads, 0, stream>>>(fp);
+  finish_scan_chunks<<<1, 1024, 0, stream>>>(fp, (uint32_t)it.chunks);
+  finish_word_prefix<<<(unsigned)it.chunks, 1024, 0, stream>>>(fp);
+  finish_rank<<<std::max(1u, rec_blocks), kFinishThreads, 0, stream>>>(fp);
+  const unsigned out_blocks = (unsigned)std::min<uint64_t>((it.out_rows + kFinishThreads - 1) / kFinishThreads, (uint64_t)ds->sms * 16);
+  finish_output<<<std::max(1u, out_blocks), kFinishThreads, 0, stream>>>(fp);
+}
+
+}  // namespace
+
+extern "C" {
+
+DFC_API const char* dfc_batch_error(int32_t i) {
+  if (i < 0 || (size_t)i >= t_batch_errors.size()) return "";
+  return t_batch_errors[i].c_str();
+}
+
+DFC_API dfc_status dfc_groupby_batch(const dfc_query* const* queries, int32_t n, dfc_result** results,
+                                     dfc_status* statuses) {
+  if (n < 0 || (n > 0 && (!queries || !results || !statuses))) return fail(DFC_INVALID, "null argument");
+  t_batch_errors.assign((size_t)n, std::string());
+  const auto t0 = std::chrono::steady_clock::now();
+  dfc_timings bt{};
+  for (int i = 0; i < n; ++i) {
+    results[i] = nullptr;
+    statuses[i] = DFC_OK;
+  }
+  if (n == 0) return DFC_OK;
+  std::vector<BatchItem> items((size_t)n);
+  auto reject = [&](int i, dfc_status st) {
+    items[i].st = st;
+    statuses[i] = st;
+    t_batch_errors[i] = t_error;
+  };
+  int device = -1;
+  DeviceState* ds = nullptr;
+  for (int i = 0; i < n; ++i) {
+    dfc_status st = plan_query(queries[i], items[i].P);
+    if (st) {
+      reject(i, st);
+      continue;
+    }
+    if (device < 0) {
+      device = items[i].P.device;
+      if ((st = device_ready(device, &ds))) return st;
+    } else if (items[i].P.device != device) {
+      fail(DFC_UNSUPPORTED, "a batch runs on one device");
+      reject(i, DFC_UNSUPPORTED);
+    }
+  }
+  if (device < 0) return DFC_OK;  // nothing to run
+  DeviceGuard guard(device);
+  cudaStream_t main = thread_stream(device);
+  const auto& streams = batch_streams(device);
+
+  // Plans: regime and capacities per query, working memory in one arena.
+  size_t used = 0;
+  for (int i = 0; i < n; ++i) {
+    BatchItem& it = items[i];
+    if (it.st) continue;
+    Plan& P = it.P;
+    const dfc_query* q = queries[i];
+    const uint64_t est = estimate_groups(q, P, ds, main);
+    P.sp.smem_slots = 0;
+    if (!(q->flags & DFC_Q_FORCE_GLOBAL) && P.sp.key_mode == KEY_PACKED && ((q->flags & DFC_Q_FORCE_SHARED) || est <= 4096)) {
+      const uint64_t sslots = next_pow2(std::max<uint64_t>(64, std::min<uint64_t>(est, 4096) * 2));
+      const size_t keys_off = (P.smem + 15) & ~(size_t)15;
+      const size_t recs_off = (keys_off + sslots * 8 + 15) & ~(size_t)15;
+      const size_t total = recs_off + sslots * (size_t)P.sp.rec_stride;
+      if (total <= ds->smem_optin) {
+        P.sp.smem_slots = (uint32_t)sslots;
+        P.sp.smem_keys_off = (uint32_t)keys_off;
+        P.sp.smem_recs_off = (uint32_t)recs_off;
+        P.smem = total;
+      }
+    }
+    it.slots = std::min(next_pow2(std::max<uint64_t>(1024, est * 8)), next_pow2(std::max<uint64_t>(1024, P.rows * 8)));
+    int occ = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_kernel, kScanThreads, P.smem);
+    it.ncta = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ds->sms * std::max(1, occ), std::max<uint64_t>(1, P.sp.tiles)));
+    const uint64_t groups_cap = std::min<uint64_t>(P.rows, it.slots / 8);
+    while (it.chunk < 1024 && it.chunk * it.ncta * 8 < groups_cap) it.chunk <<= 1;
+    it.recs = groups_cap + groups_cap / 8 + it.chunk * it.ncta;
+    it.words = (P.rows + 31) / 32;
+    it.chunks = std::max<uint64_t>(1, (it.words + kFinishChunk - 1) / kFinishChunk);
+    it.out_rows = std::min<uint64_t>(P.rows, it.recs);
+    it.off_table = arena_take(used, (it.slots + 1) * sizeof(KeyEntry));
+    it.off_records = arena_take(used, it.recs * P.sp.rec_stride);
+    it.off_bits = arena_take(used, it.words * 4 + 16);
+    it.off_prefix = arena_take(used, it.words * 4 + 16);
+    it.off_bsums = arena_take(used, it.chunks * 4);
+    it.off_perm = arena_take(used, it.recs * 4);
+    it.off_firsts = arena_take(used, it.recs * 4);
+  }
+  unsigned char* arena = nullptr;
+  Control* dctl = nullptr;
+  cudaError_t e = cudaMallocAsync((void**)&arena, std::max<size_t>(used, 256), main);
+  if (e == cudaSuccess) e = cudaMallocAsync((void**)&dctl, (size_t)n * sizeof(Control), main);
+  if (e != cudaSuccess) {
+    if (arena) cudaFreeAsync(arena, main);
+    return cuda_fail(e, "batch working memory");
+  }
+  auto free_outputs = [&](BatchItem& it) {
+    for (auto& r : it.rc) {
+      if (r.values) cudaFreeAsync(r.values, main);
+      if (r.validity) cudaFreeAsync(r.validity, main);
+      r.values = nullptr;
+      r.validity = nullptr;
+    }
+  };
+  for (int i = 0; i < n; ++i) {
+    BatchItem& it = items[i];
+    if (it.st) continue;
+    it.rc.resize(it.P.n_out);
+    for (int c = 0; c < it.P.n_out; ++c) {
+      it.rc[c].dtype = (dfc_dtype)it.P.out_dtype[c];
+      e = cudaMallocAsync(&it.rc[c].values, std::max<uint64_t>(256, it.out_rows * dtype_size(it.P.out_dtype[c])), main);
+      if (e == cudaSuccess)
+        e = cudaMallocAsync((void**)&it.rc[c].validity, std::max<uint64_t>(256, ((it.out_rows + 31) / 32) * 4), main);
+      if (e != cudaSuccess) break;
+    }
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      free_outputs(it);
+      fail(DFC_OOM, "batch output columns");
+      reject(i, DFC_OOM);
+    }
+  }
+
+  // Launch: queries round-robin over the batch streams, forked from and
+  // joined back to the thread's stream; no synchronisation in between.
+  cudaEvent_t fork;
+  cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+  cudaEventRecord(fork, main);
+  std::vector<cudaEvent_t> joins(streams.size());
+  for (size_t s = 0; s < streams.size(); ++s) {
+    cudaStreamWaitEvent(streams[s], fork, 0);
+    cudaEventCreateWithFlags(&joins[s], cudaEventDisableTiming);
+  }
+  int k = 0;
+  for (int i = 0; i < n; ++i) {
+    if (items[i].st) continue;
+    launch_item(items[i], ds, arena, dctl + i, streams[k % streams.size()]);
+    bt.launches += items[i].P.rows > 0 ? 7 : 6;
+    ++k;
+  }
+  for (size_t s = 0; s < streams.size(); ++s) {
+    cudaEventRecord(joins[s], streams[s]);
+    cudaStreamWaitEvent(main, joins[s], 0);
+  }
+  thread_local std::vector<Control> hctl;
+  thread_local Control* pinned = nullptr;
+  thread_local size_t pinned_n = 0;
+  if (pinned_n < (size_t)n) {
+    if (pinned) cudaFreeHost(pinned);
+    pinned = nullptr;
+    if (cudaMallocHost((void**)&pinned, (size_t)n * sizeof(Control)) != cudaSuccess) pinned = nullptr;
+    pinned_n = pinned ? (size_t)n : 0;
+  }
+  e = cudaGetLastError();
+  if (e == cudaSuccess && pinned) e = cudaMemcpyAsync(pinned, dctl, (size_t)n * sizeof(Control), cudaMemcpyDeviceToHost, main);
+  dfc_status st = e == cudaSuccess ? wait_bounded(main) : cuda_fail(e, "batch launch");
+  if (st == DFC_OK && !pinned) st = fail(DFC_OOM, "pinned batch control blocks");
+  cudaEventDestroy(fork);
+  for (auto& j : joins) cudaEventDestroy(j);
+  cudaFreeAsync(arena, main);
+  cudaFreeAsync(dctl, main);
+  if (st) {
+    for (auto& it : items) free_outputs(it);
+    return st;
+  }
+
+  // Results; a query that ran out of capacity reruns alone with regrowth.
+  for (int i = 0; i < n; ++i) {
+    BatchItem& it = items[i];
+    if (it.st) continue;
+    const Control& c = pinned[i];
+    const uint32_t status = c.status[0];
+    dfc_status qs = DFC_OK;
+    if (c.status[2] && !(status & ST_TIMEOUT)) {
+      char msg[128];
+      snprintf(msg, sizeof msg, "an internal index or consistency check failed (code %#x)", c.status[2]);
+      qs = fail(DFC_DEVICE, msg);
+    } else if (status & ST_TIMEOUT) {
+      qs = fail(DFC_TIMEOUT, "a bounded device wait gave up");
+    } else if (status & ST_CAPACITY) {
+      free_outputs(it);
+      const dfc_timings keep = bt;
+      qs = dfc_groupby(queries[i], &results[i]);
+      bt = keep;
+      bt.retries += 1;
+      statuses[i] = qs;
+      if (qs) t_batch_errors[i] = t_error;
+      continue;
+    } else if (status & ST_OVERFLOW) {
+      const uint32_t a = c.overflow_agg;
+      const int idt = (a < (uint32_t)queries[i]->n_aggs) ? it.P.out_agg_input_dtype[a] : DFC_INT64;
+      qs = fail(DFC_DATA_OVERFLOW, overflow_message(idt));
+    } else if (status & ST_FAULT) {
+      qs = fail(DFC_DATA_FAULT, "Mojo GPU data fault: variance of a group whose mean is far from its spread; the CPU adjudicates");
+    } else if (status & ST_ZERO_FAULT) {
+      qs = fail(DFC_DATA_FAULT, "Mojo GPU data fault: mixed signed-zero extrema; the CPU adjudicates");
+    }
+    if (qs) {
+      free_outputs(it);
+      statuses[i] = qs;
+      t_batch_errors[i] = t_error;
+      continue;
+    }
+    auto* r = new dfc_result();
+    r->device = device;
+    r->rows = c.groups;
+    for (int col = 0; col < it.P.n_out; ++col) it.rc[col].has_nulls = c.has_nulls[col] != 0;
+    r->cols = std::move(it.rc);
+    results[i] = r;
+    bt.groups += c.groups;
+    learn_groups(it.P, c.groups);
+  }
+  bt.total_ns = std::chrono::duration<double, std::nano>(std::chrono::steady_clock::now() - t0).count();
+  t_timings = bt;
+  return DFC_OK;
+}
+
+}  // extern "C"

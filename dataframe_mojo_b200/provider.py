@@ -49,15 +49,19 @@ class DataFaultError(ProviderError):
     pass
 
 
+def _error(status: int, msg: str) -> ProviderError:
+    msg = msg or N.lib().dfc_status_name(status).decode()
+    if status in (N.UNSUPPORTED, N.INVALID):
+        return UnsupportedError(status, msg)
+    if status == N.DATA_FAULT:
+        return DataFaultError(status, msg)
+    return ProviderError(status, msg)
+
+
 def _check(status: int) -> None:
     if status == N.OK:
         return
-    msg = N.last_error() or N.lib().dfc_status_name(status).decode()
-    if status in (N.UNSUPPORTED, N.INVALID):
-        raise UnsupportedError(status, msg)
-    if status == N.DATA_FAULT:
-        raise DataFaultError(status, msg)
-    raise ProviderError(status, msg)
+    raise _error(status, N.last_error())
 
 
 def _device_from_env() -> int:
@@ -266,6 +270,25 @@ def run_bound(bound: Bound, columns: list[DeviceColumn], stream: int | None = No
     out = C.c_void_p()
     _check(N.lib().dfc_groupby(C.byref(q), C.byref(out)))
     return DeviceResult(out, bound.out_names)
+
+
+def run_batch(jobs: list, stream: int | None = None, flags: int = 0) -> list:
+    """Runs many bound regions in one submission (dfc_groupby_batch).  `jobs`
+    is a list of (Bound, [DeviceColumn]); returns, per job, a DeviceResult or
+    the ProviderError that query raised."""
+    qs = [_query_struct(b, [c.handle for c in cols], stream, flags) for b, cols in jobs]
+    n = len(qs)
+    ptrs = (C.c_void_p * max(1, n))(*[C.cast(C.pointer(q), C.c_void_p) for q in qs])
+    outs = (C.c_void_p * max(1, n))()
+    sts = (C.c_int * max(1, n))()
+    _check(N.lib().dfc_groupby_batch(ptrs, n, outs, sts))
+    res = []
+    for i, (b, _) in enumerate(jobs):
+        if sts[i] == N.OK:
+            res.append(DeviceResult(C.c_void_p(outs[i]), b.out_names))
+        else:
+            res.append(_error(sts[i], N.lib().dfc_batch_error(i).decode()))
+    return res
 
 
 def last_timings() -> dict:

@@ -232,6 +232,22 @@ typedef struct dfc_result dfc_result;
 DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out);
 
 /* ------------------------------------------------------------------------ */
+/* Many queries in one submission (the batched form).  The reference core   */
+/* issues one execute() per region; a server or a pipeline with many small  */
+/* regions pays a host round trip and a device synchronisation per query.   */
+/* This plans every query, takes their working memory from one arena,       */
+/* spreads their launches over several streams with no synchronisation in   */
+/* between, and reads every control block back at once.  statuses[i] and    */
+/* results[i] are query i's outcome (dfc_batch_error(i) its message); a     */
+/* query that outgrows its capacity estimate reruns alone with regrowth.    */
+/* Returns DFC_OK when the batch ran (look at statuses), else the failure   */
+/* that stopped all of it.  The radix-partitioned regime is not used here.  */
+/* ------------------------------------------------------------------------ */
+DFC_API dfc_status dfc_groupby_batch(const dfc_query* const* queries, int32_t n, dfc_result** results,
+                                     dfc_status* statuses);
+DFC_API const char* dfc_batch_error(int32_t i);
+
+/* ------------------------------------------------------------------------ */
 /* The same query without any device allocation.  No counterpart in the    */
 /* reference: it is for callers that cannot call cudaMalloc -- code running  */
 /* under an allocator that owns the device heap (a host framework's caching */

@@ -112,6 +112,32 @@ class DeviceOutput(C.Structure):
     _fields_ = [("values", C.c_void_p), ("validity", C.c_void_p), ("dtype", C.c_int32), ("has_nulls", C.c_int32)]
 
 
+class Completion(C.Structure):
+    """dfc_completion: one finished served request."""
+
+    _fields_ = [
+        ("tag", C.c_uint64),
+        ("status", C.c_int32),
+        ("reserved", C.c_int32),
+        ("result", C.c_void_p),
+        ("latency_ns", C.c_double),
+        ("queue_ns", C.c_double),
+        ("message", C.c_char * 160),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_uint64),
+        ("completed", C.c_uint64),
+        ("pending", C.c_uint64),
+        ("inflight", C.c_uint64),
+        ("max_inflight_seen", C.c_int64),
+        ("bytes_held", C.c_int64),
+        ("budget", C.c_int64),
+    ]
+
+
 # Bytes of the fixed working-memory array behind dfc_groupby_noalloc.
 NOALLOC_SCRATCH_BYTES = 64 << 20
 
@@ -139,6 +165,11 @@ SIGNATURES = [
     ),
     ("dfc_groupby_batch", C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_int)]),
     ("dfc_batch_error", C.c_char_p, [C.c_int32]),
+    ("dfc_server_create", C.c_int, [C.c_int32, C.c_int32, C.c_int64, C.POINTER(C.c_void_p)]),
+    ("dfc_server_submit", C.c_int, [C.c_void_p, C.POINTER(Query), C.c_uint64]),
+    ("dfc_server_poll", C.c_int32, [C.c_void_p, C.POINTER(Completion), C.c_int32, C.c_int32]),
+    ("dfc_server_stats_get", C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
+    ("dfc_server_destroy", None, [C.c_void_p]),
     ("dfc_result_rows", C.c_uint64, [C.c_void_p]),
     ("dfc_result_columns", C.c_int32, [C.c_void_p]),
     (

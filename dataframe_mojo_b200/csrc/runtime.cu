@@ -13,6 +13,8 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
+#include <deque>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -793,7 +795,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
     // Slack for holes: records reserved by claims that lost a race.
     recs = groups_cap + groups_cap / 8 + chunk * ncta;
   }
-  if (recs >= 0xFFFFFFFFull) return fail(DFC_CAPACITY, "group capacity exceeds 2^32 records");
+  if (recs >= 0xFFFFFFE0ull) return fail(DFC_CAPACITY, "group capacity exceeds 2^32 - 32 records");
 
   void *table = nullptr, *records, *ctl, *bits, *prefix, *bsums, *perm, *firsts;
   void *part_buf = nullptr, *part_counts = nullptr, *part_totals = nullptr, *part_start = nullptr, *agg_tables = nullptr;
@@ -1519,7 +1521,7 @@ DFC_API dfc_status dfc_groupby_noalloc(const dfc_query* query, int32_t device, u
   const uint64_t min_recs = groups_cap + groups_cap / 8 + chunk * ncta;
   const uint64_t left = cv.used + 512 < DFC_NOALLOC_SCRATCH_BYTES ? DFC_NOALLOC_SCRATCH_BYTES - cv.used - 512 : 0;
   const uint64_t useful = std::max<uint64_t>(min_recs, P.rows + chunk * ncta);
-  const uint64_t recs = std::min<uint64_t>({useful, left / per_record, 0xFFFFFFF0ull});
+  const uint64_t recs = std::min<uint64_t>({useful, left / per_record, 0xFFFFFFDFull});
   if (recs < min_recs) {
     char msg[256];
     snprintf(msg, sizeof msg,
@@ -1665,6 +1667,91 @@ size_t arena_take(size_t& used, size_t bytes) {
   return at;
 }
 
+// Regime and capacities of one planned query; its working memory is laid
+// out from `used` on (256-byte aligned pieces).
+dfc_status size_item(const dfc_query* q, BatchItem& it, DeviceState* ds, cudaStream_t stream, size_t& used) {
+  Plan& P = it.P;
+  const uint64_t est = estimate_groups(q, P, ds, stream);
+  P.sp.smem_slots = 0;
+  if (!(q->flags & DFC_Q_FORCE_GLOBAL) && P.sp.key_mode == KEY_PACKED && ((q->flags & DFC_Q_FORCE_SHARED) || est <= 4096)) {
+    const uint64_t sslots = next_pow2(std::max<uint64_t>(64, std::min<uint64_t>(est, 4096) * 2));
+    const size_t keys_off = (P.smem + 15) & ~(size_t)15;
+    const size_t recs_off = (keys_off + sslots * 8 + 15) & ~(size_t)15;
+    const size_t total = recs_off + sslots * (size_t)P.sp.rec_stride;
+    if (total <= ds->smem_optin) {
+      P.sp.smem_slots = (uint32_t)sslots;
+      P.sp.smem_keys_off = (uint32_t)keys_off;
+      P.sp.smem_recs_off = (uint32_t)recs_off;
+      P.smem = total;
+    }
+  }
+  it.slots = std::min(next_pow2(std::max<uint64_t>(1024, est * 8)), next_pow2(std::max<uint64_t>(1024, P.rows * 8)));
+  int occ = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_kernel, kScanThreads, P.smem);
+  it.ncta = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ds->sms * std::max(1, occ), std::max<uint64_t>(1, P.sp.tiles)));
+  const uint64_t groups_cap = std::min<uint64_t>(P.rows, it.slots / 8);
+  it.chunk = 64;
+  while (it.chunk < 1024 && it.chunk * it.ncta * 8 < groups_cap) it.chunk <<= 1;
+  it.recs = groups_cap + groups_cap / 8 + it.chunk * it.ncta;
+  if (it.recs >= 0xFFFFFFE0ull) return fail(DFC_CAPACITY, "group capacity exceeds 2^32 - 32 records");
+  it.words = (P.rows + 31) / 32;
+  it.chunks = std::max<uint64_t>(1, (it.words + kFinishChunk - 1) / kFinishChunk);
+  it.out_rows = std::min<uint64_t>(P.rows, it.recs);
+  it.off_table = arena_take(used, (it.slots + 1) * sizeof(KeyEntry));
+  it.off_records = arena_take(used, it.recs * P.sp.rec_stride);
+  it.off_bits = arena_take(used, it.words * 4 + 16);
+  it.off_prefix = arena_take(used, it.words * 4 + 16);
+  it.off_bsums = arena_take(used, it.chunks * 4);
+  it.off_perm = arena_take(used, it.recs * 4);
+  it.off_firsts = arena_take(used, it.recs * 4);
+  return DFC_OK;
+}
+
+// Output columns of a sized query (stream-ordered allocations).
+dfc_status alloc_outputs(BatchItem& it, cudaStream_t stream) {
+  it.rc.resize(it.P.n_out);
+  for (int c = 0; c < it.P.n_out; ++c) {
+    it.rc[c].dtype = (dfc_dtype)it.P.out_dtype[c];
+    cudaError_t e = cudaMallocAsync(&it.rc[c].values, std::max<uint64_t>(256, it.out_rows * dtype_size(it.P.out_dtype[c])), stream);
+    if (e == cudaSuccess)
+      e = cudaMallocAsync((void**)&it.rc[c].validity, std::max<uint64_t>(256, ((it.out_rows + 31) / 32) * 4), stream);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(DFC_OOM, "output columns");
+    }
+  }
+  return DFC_OK;
+}
+
+// The result of a finished query from its control block, or its error.
+dfc_status finish_item(const dfc_query* q, BatchItem& it, const Control& c, int device, dfc_result** out) {
+  const uint32_t status = c.status[0];
+  if (c.status[2] && !(status & ST_TIMEOUT)) {
+    char msg[128];
+    snprintf(msg, sizeof msg, "an internal index or consistency check failed (code %#x)", c.status[2]);
+    return fail(DFC_DEVICE, msg);
+  }
+  if (status & ST_TIMEOUT) return fail(DFC_TIMEOUT, "a bounded device wait gave up");
+  if (status & ST_CAPACITY) return DFC_CAPACITY;
+  if (status & ST_OVERFLOW) {
+    const uint32_t a = c.overflow_agg;
+    const int idt = (a < (uint32_t)q->n_aggs) ? it.P.out_agg_input_dtype[a] : DFC_INT64;
+    return fail(DFC_DATA_OVERFLOW, overflow_message(idt));
+  }
+  if (status & ST_FAULT)
+    return fail(DFC_DATA_FAULT, "Mojo GPU data fault: variance of a group whose mean is far from its spread; the CPU adjudicates");
+  if (status & ST_ZERO_FAULT)
+    return fail(DFC_DATA_FAULT, "Mojo GPU data fault: mixed signed-zero extrema; the CPU adjudicates");
+  auto* r = new dfc_result();
+  r->device = device;
+  r->rows = c.groups;
+  for (int col = 0; col < it.P.n_out; ++col) it.rc[col].has_nulls = c.has_nulls[col] != 0;
+  r->cols = std::move(it.rc);
+  *out = r;
+  learn_groups(it.P, c.groups);
+  return DFC_OK;
+}
+
 // The launches of one planned query (global or shared-memory regime) on
 // `stream`, working memory at `base`, control block `dctl`.
 void launch_item(BatchItem& it, DeviceState* ds, unsigned char* base, Control* dctl, cudaStream_t stream) {
@@ -1762,39 +1849,8 @@ DFC_API dfc_status dfc_groupby_batch(const dfc_query* const* queries, int32_t n,
   for (int i = 0; i < n; ++i) {
     BatchItem& it = items[i];
     if (it.st) continue;
-    Plan& P = it.P;
-    const dfc_query* q = queries[i];
-    const uint64_t est = estimate_groups(q, P, ds, main);
-    P.sp.smem_slots = 0;
-    if (!(q->flags & DFC_Q_FORCE_GLOBAL) && P.sp.key_mode == KEY_PACKED && ((q->flags & DFC_Q_FORCE_SHARED) || est <= 4096)) {
-      const uint64_t sslots = next_pow2(std::max<uint64_t>(64, std::min<uint64_t>(est, 4096) * 2));
-      const size_t keys_off = (P.smem + 15) & ~(size_t)15;
-      const size_t recs_off = (keys_off + sslots * 8 + 15) & ~(size_t)15;
-      const size_t total = recs_off + sslots * (size_t)P.sp.rec_stride;
-      if (total <= ds->smem_optin) {
-        P.sp.smem_slots = (uint32_t)sslots;
-        P.sp.smem_keys_off = (uint32_t)keys_off;
-        P.sp.smem_recs_off = (uint32_t)recs_off;
-        P.smem = total;
-      }
-    }
-    it.slots = std::min(next_pow2(std::max<uint64_t>(1024, est * 8)), next_pow2(std::max<uint64_t>(1024, P.rows * 8)));
-    int occ = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_kernel, kScanThreads, P.smem);
-    it.ncta = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ds->sms * std::max(1, occ), std::max<uint64_t>(1, P.sp.tiles)));
-    const uint64_t groups_cap = std::min<uint64_t>(P.rows, it.slots / 8);
-    while (it.chunk < 1024 && it.chunk * it.ncta * 8 < groups_cap) it.chunk <<= 1;
-    it.recs = groups_cap + groups_cap / 8 + it.chunk * it.ncta;
-    it.words = (P.rows + 31) / 32;
-    it.chunks = std::max<uint64_t>(1, (it.words + kFinishChunk - 1) / kFinishChunk);
-    it.out_rows = std::min<uint64_t>(P.rows, it.recs);
-    it.off_table = arena_take(used, (it.slots + 1) * sizeof(KeyEntry));
-    it.off_records = arena_take(used, it.recs * P.sp.rec_stride);
-    it.off_bits = arena_take(used, it.words * 4 + 16);
-    it.off_prefix = arena_take(used, it.words * 4 + 16);
-    it.off_bsums = arena_take(used, it.chunks * 4);
-    it.off_perm = arena_take(used, it.recs * 4);
-    it.off_firsts = arena_take(used, it.recs * 4);
+    const dfc_status st = size_item(queries[i], it, ds, main, used);
+    if (st) reject(i, st);
   }
   unsigned char* arena = nullptr;
   Control* dctl = nullptr;
@@ -1815,18 +1871,8 @@ DFC_API dfc_status dfc_groupby_batch(const dfc_query* const* queries, int32_t n,
   for (int i = 0; i < n; ++i) {
     BatchItem& it = items[i];
     if (it.st) continue;
-    it.rc.resize(it.P.n_out);
-    for (int c = 0; c < it.P.n_out; ++c) {
-      it.rc[c].dtype = (dfc_dtype)it.P.out_dtype[c];
-      e = cudaMallocAsync(&it.rc[c].values, std::max<uint64_t>(256, it.out_rows * dtype_size(it.P.out_dtype[c])), main);
-      if (e == cudaSuccess)
-        e = cudaMallocAsync((void**)&it.rc[c].validity, std::max<uint64_t>(256, ((it.out_rows + 31) / 32) * 4), main);
-      if (e != cudaSuccess) break;
-    }
-    if (e != cudaSuccess) {
-      cudaGetLastError();
+    if (alloc_outputs(it, main)) {
       free_outputs(it);
-      fail(DFC_OOM, "batch output columns");
       reject(i, DFC_OOM);
     }
   }
@@ -1879,50 +1925,349 @@ DFC_API dfc_status dfc_groupby_batch(const dfc_query* const* queries, int32_t n,
     BatchItem& it = items[i];
     if (it.st) continue;
     const Control& c = pinned[i];
-    const uint32_t status = c.status[0];
-    dfc_status qs = DFC_OK;
-    if (c.status[2] && !(status & ST_TIMEOUT)) {
-      char msg[128];
-      snprintf(msg, sizeof msg, "an internal index or consistency check failed (code %#x)", c.status[2]);
-      qs = fail(DFC_DEVICE, msg);
-    } else if (status & ST_TIMEOUT) {
-      qs = fail(DFC_TIMEOUT, "a bounded device wait gave up");
-    } else if (status & ST_CAPACITY) {
+    dfc_status qs = finish_item(queries[i], it, c, device, &results[i]);
+    if (qs == DFC_CAPACITY) {
+      // Ran out of capacity: alone, with regrowth.
       free_outputs(it);
       const dfc_timings keep = bt;
       qs = dfc_groupby(queries[i], &results[i]);
       bt = keep;
       bt.retries += 1;
-      statuses[i] = qs;
-      if (qs) t_batch_errors[i] = t_error;
-      continue;
-    } else if (status & ST_OVERFLOW) {
-      const uint32_t a = c.overflow_agg;
-      const int idt = (a < (uint32_t)queries[i]->n_aggs) ? it.P.out_agg_input_dtype[a] : DFC_INT64;
-      qs = fail(DFC_DATA_OVERFLOW, overflow_message(idt));
-    } else if (status & ST_FAULT) {
-      qs = fail(DFC_DATA_FAULT, "Mojo GPU data fault: variance of a group whose mean is far from its spread; the CPU adjudicates");
-    } else if (status & ST_ZERO_FAULT) {
-      qs = fail(DFC_DATA_FAULT, "Mojo GPU data fault: mixed signed-zero extrema; the CPU adjudicates");
-    }
-    if (qs) {
+    } else if (qs == DFC_OK) {
+      bt.groups += c.groups;
+    } else {
       free_outputs(it);
-      statuses[i] = qs;
-      t_batch_errors[i] = t_error;
-      continue;
     }
-    auto* r = new dfc_result();
-    r->device = device;
-    r->rows = c.groups;
-    for (int col = 0; col < it.P.n_out; ++col) it.rc[col].has_nulls = c.has_nulls[col] != 0;
-    r->cols = std::move(it.rc);
-    results[i] = r;
-    bt.groups += c.groups;
-    learn_groups(it.P, c.groups);
+    statuses[i] = qs;
+    if (qs) t_batch_errors[i] = t_error;
   }
   bt.total_ns = std::chrono::duration<double, std::nano>(std::chrono::steady_clock::now() - t0).count();
   t_timings = bt;
   return DFC_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The served form: a request loop with continuous batching.
+// ---------------------------------------------------------------------------
+namespace {
+
+// A query description the server owns (dfc_query holds borrowed pointers).
+struct OwnedQuery {
+  dfc_query q{};
+  std::vector<dfc_column*> inputs;
+  std::vector<int32_t> keys;
+  std::vector<dfc_pred_op> pred;
+  std::vector<dfc_agg> aggs;
+  void take(const dfc_query* src) {
+    q = *src;
+    inputs.assign(src->inputs, src->inputs + std::max(0, src->n_inputs));
+    keys.assign(src->keys, src->keys + std::max(0, src->n_keys));
+    pred.assign(src->pred, src->pred + std::max(0, src->n_pred));
+    aggs.assign(src->aggs, src->aggs + std::max(0, src->n_aggs));
+    q.inputs = inputs.data();
+    q.keys = keys.data();
+    q.pred = pred.empty() ? nullptr : pred.data();
+    q.aggs = aggs.empty() ? nullptr : aggs.data();
+    q.stream = nullptr;
+  }
+};
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+  uint64_t tag = 0;
+  OwnedQuery oq;
+  Clock::time_point submitted, admitted;
+  BatchItem item;
+  size_t bytes = 0;  // device memory it holds while in flight
+  unsigned char* arena = nullptr;
+  Control* dctl = nullptr;
+  int slot = -1;     // pinned control slot
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+};
+
+}  // namespace
+
+struct dfc_server {
+  int device = 0;
+  DeviceState* ds = nullptr;
+  int max_inflight = 64;
+  int64_t budget = 0;       // device bytes in flight at most
+  int64_t held = 0;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Request*> pending;
+  std::vector<Request*> inflight;
+  std::deque<dfc_completion> done;
+  std::vector<cudaStream_t> streams;
+  Control* pinned = nullptr;  // max_inflight control slots
+  std::vector<int> free_slots;
+  bool stop = false;
+  uint64_t submitted = 0, completed = 0, admitted_total = 0;
+  int max_seen_inflight = 0;
+  std::thread worker;
+};
+
+namespace {
+
+void server_complete(dfc_server* sv, Request* r, dfc_status st, dfc_result* res, const std::string& msg) {
+  dfc_completion c{};
+  c.tag = r->tag;
+  c.status = st;
+  c.result = res;
+  const auto now = Clock::now();
+  c.latency_ns = std::chrono::duration<double, std::nano>(now - r->submitted).count();
+  c.queue_ns = std::chrono::duration<double, std::nano>(r->admitted - r->submitted).count();
+  snprintf(c.message, sizeof c.message, "%s", msg.c_str());
+  std::lock_guard<std::mutex> lk(sv->mu);
+  sv->done.push_back(c);
+  sv->completed += 1;
+  sv->cv_done.notify_all();
+}
+
+// Plans, sizes and launches one request; false when it must wait for memory
+// (nothing done) or failed (completed with its error).
+bool server_launch(dfc_server* sv, Request* r, int k) {
+  r->item = BatchItem{};  // a request that waited for memory is planned afresh
+  BatchItem& it = r->item;
+  dfc_status st = plan_query(&r->oq.q, it.P);
+  if (!st && it.P.device != sv->device) st = fail(DFC_UNSUPPORTED, "the request's columns live on another device");
+  size_t used = 0;
+  cudaStream_t stream = sv->streams[k % sv->streams.size()];
+  if (!st) st = size_item(&r->oq.q, it, sv->ds, stream, used);
+  if (st) {
+    r->admitted = Clock::now();
+    server_complete(sv, r, st, nullptr, t_error);
+    delete r;
+    return true;
+  }
+  // Output bytes count against the budget too (they live until released).
+  size_t out_bytes = 0;
+  for (int c = 0; c < it.P.n_out; ++c) out_bytes += it.out_rows * 8 + ((it.out_rows + 31) / 32) * 4 + 512;
+  r->bytes = used + out_bytes + sizeof(Control);
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (sv->held > 0 && sv->held + (int64_t)r->bytes > sv->budget) return false;  // wait for memory
+    sv->held += (int64_t)r->bytes;
+  }
+  r->admitted = Clock::now();
+  r->stream = stream;
+  cudaError_t e = cudaMallocAsync((void**)&r->arena, std::max<size_t>(used, 256), stream);
+  if (e == cudaSuccess) e = cudaMallocAsync((void**)&r->dctl, sizeof(Control), stream);
+  if (e == cudaSuccess && alloc_outputs(it, stream)) e = cudaErrorMemoryAllocation;
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    for (auto& c : it.rc) {
+      if (c.values) cudaFreeAsync(c.values, stream);
+      if (c.validity) cudaFreeAsync(c.validity, stream);
+    }
+    if (r->arena) cudaFreeAsync(r->arena, stream);
+    if (r->dctl) cudaFreeAsync(r->dctl, stream);
+    {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      sv->held -= (int64_t)r->bytes;
+    }
+    server_complete(sv, r, DFC_OOM, nullptr, "device memory for the request");
+    delete r;
+    return true;
+  }
+  launch_item(it, sv->ds, r->arena, r->dctl, stream);
+  r->slot = sv->free_slots.back();
+  sv->free_slots.pop_back();
+  cudaMemcpyAsync(sv->pinned + r->slot, r->dctl, sizeof(Control), cudaMemcpyDeviceToHost, stream);
+  cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming);
+  cudaEventRecord(r->done, stream);
+  sv->inflight.push_back(r);
+  return true;
+}
+
+// Finishes a request whose work is done on the device.
+void server_finish(dfc_server* sv, Request* r) {
+  dfc_result* res = nullptr;
+  const Control c = sv->pinned[r->slot];
+  sv->free_slots.push_back(r->slot);
+  cudaEventDestroy(r->done);
+  cudaFreeAsync(r->arena, r->stream);
+  cudaFreeAsync(r->dctl, r->stream);
+  dfc_status st = finish_item(&r->oq.q, r->item, c, sv->device, &res);
+  std::string msg = st ? t_error : std::string();
+  if (st) {
+    for (auto& col : r->item.rc) {
+      if (col.values) cudaFreeAsync(col.values, r->stream);
+      if (col.validity) cudaFreeAsync(col.validity, r->stream);
+    }
+  }
+  if (st == DFC_CAPACITY) {  // alone, with regrowth
+    st = dfc_groupby(&r->oq.q, &res);
+    msg = st ? t_error : std::string();
+  }
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->held -= (int64_t)r->bytes;
+  }
+  server_complete(sv, r, st, res, msg);
+  delete r;
+}
+
+void server_loop(dfc_server* sv) {
+  DeviceGuard guard(sv->device);
+  int k = 0;
+  bool mem_blocked = false;  // the head request waits for memory: retry after a completion
+  for (;;) {
+    // Admit what arrived, as in-flight slots and memory allow.
+    std::vector<Request*> take;
+    {
+      std::unique_lock<std::mutex> lk(sv->mu);
+      if (sv->pending.empty() && sv->inflight.empty()) {
+        if (sv->stop) return;
+        sv->cv_work.wait_for(lk, std::chrono::milliseconds(5));
+      }
+      while (!mem_blocked && !sv->pending.empty() && (int)(sv->inflight.size() + take.size()) < sv->max_inflight) {
+        take.push_back(sv->pending.front());
+        sv->pending.pop_front();
+      }
+    }
+    for (size_t i = 0; i < take.size(); ++i) {
+      if (!server_launch(sv, take[i], k++)) {
+        // Not enough memory now: back to the front, in order.
+        std::lock_guard<std::mutex> lk(sv->mu);
+        for (size_t j = take.size(); j-- > i;) sv->pending.push_front(take[j]);
+        mem_blocked = true;
+        break;
+      }
+      std::lock_guard<std::mutex> lk(sv->mu);
+      sv->admitted_total += 1;
+      sv->max_seen_inflight = std::max(sv->max_seen_inflight, (int)sv->inflight.size());
+    }
+    // Finish what the device completed.
+    bool progressed = false;
+    for (size_t i = 0; i < sv->inflight.size();) {
+      Request* r = sv->inflight[i];
+      const cudaError_t q = cudaEventQuery(r->done);
+      if (q == cudaErrorNotReady) {
+        ++i;
+        continue;
+      }
+      sv->inflight.erase(sv->inflight.begin() + (long)i);
+      progressed = true;
+      if (q != cudaSuccess) {
+        {
+          std::lock_guard<std::mutex> lk(sv->mu);
+          sv->held -= (int64_t)r->bytes;
+        }
+        server_complete(sv, r, cuda_fail(q, "request execution"), nullptr, t_error);
+        delete r;
+        continue;
+      }
+      server_finish(sv, r);
+    }
+    if (progressed) mem_blocked = false;
+    if (!progressed && take.empty()) std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+DFC_API dfc_status dfc_server_create(int32_t device, int32_t max_inflight, int64_t memory_budget, dfc_server** out) {
+  if (!out) return fail(DFC_INVALID, "null output");
+  *out = nullptr;
+  DeviceState* ds;
+  dfc_status st = device_ready(device, &ds);
+  if (st) return st;
+  DeviceGuard guard(device);
+  auto* sv = new dfc_server();
+  sv->device = device;
+  sv->ds = ds;
+  sv->max_inflight = std::max(1, max_inflight);
+  if (memory_budget <= 0) {
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    memory_budget = (int64_t)(free_b * 0.8);
+  }
+  sv->budget = memory_budget;
+  sv->streams.resize(kBatchStreams);
+  for (auto& s : sv->streams) cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  if (cudaMallocHost((void**)&sv->pinned, sizeof(Control) * sv->max_inflight) != cudaSuccess) {
+    for (auto& s : sv->streams) cudaStreamDestroy(s);
+    delete sv;
+    return fail(DFC_OOM, "pinned control slots");
+  }
+  for (int i = sv->max_inflight - 1; i >= 0; --i) sv->free_slots.push_back(i);
+  sv->worker = std::thread(server_loop, sv);
+  *out = sv;
+  return DFC_OK;
+}
+
+DFC_API dfc_status dfc_server_submit(dfc_server* sv, const dfc_query* query, uint64_t tag) {
+  if (!sv || !query) return fail(DFC_INVALID, "null argument");
+  if (query->n_inputs < 0 || query->n_keys < 0 || query->n_pred < 0 || query->n_aggs < 0 ||
+      (query->n_inputs > 0 && !query->inputs) || (query->n_keys > 0 && !query->keys) ||
+      (query->n_pred > 0 && !query->pred) || (query->n_aggs > 0 && !query->aggs))
+    return fail(DFC_INVALID, "malformed query");
+  auto* r = new Request();
+  r->tag = tag;
+  r->oq.take(query);
+  r->submitted = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (sv->stop) {
+      delete r;
+      return fail(DFC_INVALID, "the server is stopping");
+    }
+    sv->pending.push_back(r);
+    sv->submitted += 1;
+  }
+  sv->cv_work.notify_one();
+  return DFC_OK;
+}
+
+DFC_API int32_t dfc_server_poll(dfc_server* sv, dfc_completion* out, int32_t max, int32_t wait_ms) {
+  if (!sv || !out || max <= 0) return 0;
+  std::unique_lock<std::mutex> lk(sv->mu);
+  if (sv->done.empty() && wait_ms > 0) sv->cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms));
+  int32_t n = 0;
+  while (n < max && !sv->done.empty()) {
+    out[n++] = sv->done.front();
+    sv->done.pop_front();
+  }
+  return n;
+}
+
+DFC_API dfc_status dfc_server_stats_get(dfc_server* sv, dfc_server_stats* out) {
+  if (!sv || !out) return fail(DFC_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(sv->mu);
+  out->submitted = sv->submitted;
+  out->completed = sv->completed;
+  out->pending = sv->pending.size();
+  out->inflight = sv->inflight.size();
+  out->max_inflight_seen = sv->max_seen_inflight;
+  out->bytes_held = sv->held;
+  out->budget = sv->budget;
+  return DFC_OK;
+}
+
+DFC_API void dfc_server_destroy(dfc_server* sv) {
+  if (!sv) return;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->stop = true;
+  }
+  sv->cv_work.notify_all();
+  sv->worker.join();  // the loop drains pending and in-flight requests first
+  for (auto& c : sv->done)
+    if (c.result) dfc_result_free(c.result);
+  DeviceGuard guard(sv->device);
+  for (auto& s : sv->streams) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
+  cudaFreeHost(sv->pinned);
+  delete sv;
 }
 
 }  // extern "C"

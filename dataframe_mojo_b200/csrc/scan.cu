@@ -697,6 +697,132 @@ __device__ __forceinline__ void smem_rows(const ScanParams& p, const Step& s, co
   }
 }
 
+// Full-warp butterfly reductions (every lane gets the result).
+__device__ __forceinline__ double warp_sum_f64(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ uint64_t warp_max_u64(uint64_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const uint64_t w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = w > v ? w : v;
+  }
+  return v;
+}
+__device__ __forceinline__ __int128 warp_sum_i128(__int128 v) {
+  uint64_t lo = (uint64_t)v, hi = (uint64_t)((unsigned __int128)v >> 64);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const uint64_t olo = __shfl_xor_sync(0xffffffffu, lo, o), ohi = __shfl_xor_sync(0xffffffffu, hi, o);
+    const uint64_t nlo = lo + olo;
+    hi = hi + ohi + (nlo < lo ? 1ull : 0ull);
+    lo = nlo;
+  }
+  return (__int128)(((unsigned __int128)hi << 64) | lo);
+}
+
+// Folds the lanes of the warp's largest group -- `grp` is each lane's group
+// mask (0 outside), `maxpop` its size -- into the group's record (`rec`, the
+// lane's own record pointer) with one atomic per field: every field reduced
+// over the group by a five-step butterfly, whatever the group's size.  Same
+// state updates as group_update.  Every lane calls it; returns whether this
+// lane was folded.  `get(v, ok, b)` gives the lane's value of column v.
+template <typename Get>
+__device__ bool collapse_largest(const ScanParams& p, unsigned char* rec, uint32_t grp, int maxpop, bool on, uint32_t row,
+                                 Get&& get) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t cand = __ballot_sync(0xffffffffu, on && __popc(grp) == maxpop);
+  const int lead = __ffs(cand) - 1;  // the lowest lane of a largest group: its leader
+  const uint32_t big = __shfl_sync(0xffffffffu, grp, lead);
+  const bool in = (big >> lane) & 1u;
+  const bool leader = lane == lead;
+  unsigned char* const grec = reinterpret_cast<unsigned char*>(
+      __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(rec), lead));
+  const uint32_t first = __reduce_min_sync(0xffffffffu, in ? row : 0xFFFFFFFFu);
+  if (leader) {
+    atomicMax(reinterpret_cast<uint32_t*>(grec + kRecFirst), ~first);
+    if (p.off_len >= 0) atomicAdd(reinterpret_cast<uint32_t*>(grec + p.off_len), (uint32_t)__popc(big));
+  }
+  for (int v = 0; v < p.n_vals; ++v) {
+    const ValField& f = p.vals[v];
+    const int dt = f.dtype;
+    const bool isf = dt_float(dt);
+    bool ok = false;
+    uint64_t b = 0;
+    if (in) get(v, ok, b);
+    ok = ok && in;
+    if (!ok) b = 0;
+    const double xd = isf ? bits_to_f64(b, dt) : bits_as_double(b, dt);
+    const bool nan = ok && isf && xd != xd;
+    const uint32_t vmask = __ballot_sync(0xffffffffu, ok);
+    if (leader && vmask) atomicAdd(reinterpret_cast<uint32_t*>(grec + f.off_count), (uint32_t)__popc(vmask));
+    if (f.off_sum >= 0) {
+      if (f.sum_kind == SUM_F64) {
+        const double sm = warp_sum_f64(ok ? xd : 0.0);
+        if (leader && vmask) atomicAdd(reinterpret_cast<double*>(grec + f.off_sum), sm);
+      } else {
+        const bool uns = dt == DFC_UINT64;
+        const __int128 xv = !ok ? (__int128)0 : (uns ? (__int128)b : (__int128)bits_to_i64(b, dt));
+        const __int128 exact = warp_sum_i128(xv);
+        if (leader && vmask) {
+          if (f.sum_kind == SUM_I64) {
+            atomicAdd(reinterpret_cast<unsigned long long*>(grec + f.off_sum), (unsigned long long)(long long)exact);
+          } else {
+            const uint64_t add_lo = (uint64_t)exact, add_hi = (uint64_t)(exact >> 64);
+            const uint64_t old = atomicAdd(reinterpret_cast<unsigned long long*>(grec + f.off_sum), add_lo);
+            const uint64_t hi_add = add_hi + ((old + add_lo) < old ? 1ull : 0ull);
+            if (hi_add) atomicAdd(reinterpret_cast<unsigned long long*>(grec + f.off_sum + 8), hi_add);
+          }
+        }
+      }
+    }
+    if (f.off_min >= 0 || f.off_max >= 0) {
+      const bool ordinary = ok && !nan;
+      const uint64_t e = ordinary ? order_encode(b, dt) : 0ull;
+      if (f.off_min >= 0) {
+        const unsigned long long m = warp_max_u64(ordinary ? ~e : 0ull);
+        if (leader && m) atomicMax(reinterpret_cast<unsigned long long*>(grec + f.off_min), m);
+      }
+      if (f.off_max >= 0) {
+        const unsigned long long m = warp_max_u64(e);
+        if (leader && m) atomicMax(reinterpret_cast<unsigned long long*>(grec + f.off_max), m);
+      }
+      const uint32_t nanmask = __ballot_sync(0xffffffffu, nan);
+      const uint32_t pz = __ballot_sync(0xffffffffu, ok && isf && xd == 0.0 && __double_as_longlong(xd) >= 0);
+      const uint32_t nz = __ballot_sync(0xffffffffu, ok && isf && xd == 0.0 && __double_as_longlong(xd) < 0);
+      if (leader) {
+        uint32_t bits = 0;
+        if (nanmask) bits |= 1u << (3 * v);
+        if (pz) bits |= 1u << (3 * v + 1);
+        if (nz) bits |= 1u << (3 * v + 2);
+        if (bits) atomicOr(reinterpret_cast<uint32_t*>(grec + kRecFlags), bits);
+      }
+    }
+    if (f.off_m2 >= 0 && vmask) {
+      // The group's shift K: set once, by the first valid value of a leader.
+      const uint64_t xbits = (xd != xd) ? kCanonNaN : (uint64_t)__double_as_longlong(xd);
+      const uint64_t candk = __shfl_sync(0xffffffffu, xbits, __ffs(vmask) - 1);
+      uint64_t ks = 0;
+      if (leader) {
+        ks = *reinterpret_cast<volatile unsigned long long*>(grec + f.off_shift);
+        if (ks == 0) {
+          const uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long*>(grec + f.off_shift), 0ull, candk ^ kShiftTag);
+          ks = prev == 0 ? (candk ^ kShiftTag) : prev;
+        }
+      }
+      ks = __shfl_sync(0xffffffffu, ks, lead);
+      const double d = xd - __longlong_as_double((long long)(ks ^ kShiftTag));
+      const double s2 = warp_sum_f64(ok ? d * d : 0.0);
+      if (leader) atomicAdd(reinterpret_cast<double*>(grec + f.off_m2), s2);
+    }
+  }
+  return in;
+}
+
+constexpr int kCollapseMin = 4;  // group size from which a warp folds a group by butterfly
+
 // ---------------------------------------------------------------------------
 // 5. States in the global records.
 // ---------------------------------------------------------------------------
@@ -836,6 +962,33 @@ __device__ __forceinline__ void consume_rows(const ScanParams& p, const Step& s,
     for (int j = 0; j < kR; ++j) {
       gid[j] = sel[j] ? find_or_claim(p, kw[j], rows[j], cs) : kNoGid;
       sel[j] = sel[j] && gid[j] != kNoGid;
+    }
+  }
+
+  // Hot keys: a warp's largest set of rows of one group (up to two sets per
+  // row slot) folds into the record by butterfly, one atomic per field.
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int j = 0; j < kR; ++j) {
+    // Record numbers stay below 2^32 - 32 (the planner caps them), so a lane
+    // without a row gets a tag no record has.
+    const uint32_t tag = sel[j] ? gid[j] : (0xFFFFFFE0u | (uint32_t)lane);
+    uint32_t grp = __match_any_sync(0xffffffffu, tag) & __ballot_sync(0xffffffffu, sel[j]);
+    if (!sel[j]) grp = 0;
+    int maxpop = __reduce_max_sync(0xffffffffu, (unsigned)__popc(grp));
+    for (int round = 0; round < 2 && maxpop >= kCollapseMin; ++round) {
+      unsigned char* rec = record_at(p, sel[j] ? gid[j] : 0u);
+      const RowRef xr = x[j];
+      if (collapse_largest(p, rec, grp, maxpop, sel[j], rows[j], [&](int v, bool& ok, uint64_t& b) {
+            const int c = p.vals[v].input;
+            const ColRef cr = col_ref(p, s, c);
+            ok = rvalid(cr, xr);
+            b = ok ? load_bits(rv(cr, xr), p.cols[c].size, xr.r) : 0ull;
+          })) {
+        sel[j] = false;
+        grp = 0;
+      }
+      maxpop = __reduce_max_sync(0xffffffffu, (unsigned)__popc(grp));
     }
   }
 
@@ -1496,131 +1649,6 @@ __global__ void __launch_bounds__(kPartThreads, 1) partition_kernel(const __grid
     if (s_part.next[q] != s_part.end[q]) part_check(p, CHK_RANGE);
 }
 
-// Full-warp butterfly reductions (every lane gets the result).
-__device__ __forceinline__ double warp_sum_f64(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-__device__ __forceinline__ uint64_t warp_max_u64(uint64_t v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const uint64_t w = __shfl_xor_sync(0xffffffffu, v, o);
-    v = w > v ? w : v;
-  }
-  return v;
-}
-__device__ __forceinline__ __int128 warp_sum_i128(__int128 v) {
-  uint64_t lo = (uint64_t)v, hi = (uint64_t)((unsigned __int128)v >> 64);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const uint64_t olo = __shfl_xor_sync(0xffffffffu, lo, o), ohi = __shfl_xor_sync(0xffffffffu, hi, o);
-    const uint64_t nlo = lo + olo;
-    hi = hi + ohi + (nlo < lo ? 1ull : 0ull);
-    lo = nlo;
-  }
-  return (__int128)(((unsigned __int128)hi << 64) | lo);
-}
-
-// Folds the lanes of the warp's largest group -- `grp` is each lane's group
-// mask (0 outside), `maxpop` its size -- into the group's record (`rec`, the
-// lane's own record pointer) with one atomic per field: every field reduced
-// over the group by a five-step butterfly, whatever the group's size.  Same
-// state updates as group_update.  Every lane calls it; returns whether this
-// lane was folded.  `get(v, ok, b)` gives the lane's value of column v.
-template <typename Get>
-__device__ bool collapse_largest(const ScanParams& p, unsigned char* rec, uint32_t grp, int maxpop, bool on, uint32_t row,
-                                 Get&& get) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t cand = __ballot_sync(0xffffffffu, on && __popc(grp) == maxpop);
-  const int lead = __ffs(cand) - 1;  // the lowest lane of a largest group: its leader
-  const uint32_t big = __shfl_sync(0xffffffffu, grp, lead);
-  const bool in = (big >> lane) & 1u;
-  const bool leader = lane == lead;
-  unsigned char* const grec = reinterpret_cast<unsigned char*>(
-      __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(rec), lead));
-  const uint32_t first = __reduce_min_sync(0xffffffffu, in ? row : 0xFFFFFFFFu);
-  if (leader) {
-    atomicMax(reinterpret_cast<uint32_t*>(grec + kRecFirst), ~first);
-    if (p.off_len >= 0) atomicAdd(reinterpret_cast<uint32_t*>(grec + p.off_len), (uint32_t)__popc(big));
-  }
-  for (int v = 0; v < p.n_vals; ++v) {
-    const ValField& f = p.vals[v];
-    const int dt = f.dtype;
-    const bool isf = dt_float(dt);
-    bool ok = false;
-    uint64_t b = 0;
-    if (in) get(v, ok, b);
-    ok = ok && in;
-    if (!ok) b = 0;
-    const double xd = isf ? bits_to_f64(b, dt) : bits_as_double(b, dt);
-    const bool nan = ok && isf && xd != xd;
-    const uint32_t vmask = __ballot_sync(0xffffffffu, ok);
-    if (leader && vmask) atomicAdd(reinterpret_cast<uint32_t*>(grec + f.off_count), (uint32_t)__popc(vmask));
-    if (f.off_sum >= 0) {
-      if (f.sum_kind == SUM_F64) {
-        const double sm = warp_sum_f64(ok ? xd : 0.0);
-        if (leader && vmask) atomicAdd(reinterpret_cast<double*>(grec + f.off_sum), sm);
-      } else {
-        const bool uns = dt == DFC_UINT64;
-        const __int128 xv = !ok ? (__int128)0 : (uns ? (__int128)b : (__int128)bits_to_i64(b, dt));
-        const __int128 exact = warp_sum_i128(xv);
-        if (leader && vmask) {
-          if (f.sum_kind == SUM_I64) {
-            atomicAdd(reinterpret_cast<unsigned long long*>(grec + f.off_sum), (unsigned long long)(long long)exact);
-          } else {
-            const uint64_t add_lo = (uint64_t)exact, add_hi = (uint64_t)(exact >> 64);
-            const uint64_t old = atomicAdd(reinterpret_cast<unsigned long long*>(grec + f.off_sum), add_lo);
-            const uint64_t hi_add = add_hi + ((old + add_lo) < old ? 1ull : 0ull);
-            if (hi_add) atomicAdd(reinterpret_cast<unsigned long long*>(grec + f.off_sum + 8), hi_add);
-          }
-        }
-      }
-    }
-    if (f.off_min >= 0 || f.off_max >= 0) {
-      const bool ordinary = ok && !nan;
-      const uint64_t e = ordinary ? order_encode(b, dt) : 0ull;
-      if (f.off_min >= 0) {
-        const unsigned long long m = warp_max_u64(ordinary ? ~e : 0ull);
-        if (leader && m) atomicMax(reinterpret_cast<unsigned long long*>(grec + f.off_min), m);
-      }
-      if (f.off_max >= 0) {
-        const unsigned long long m = warp_max_u64(e);
-        if (leader && m) atomicMax(reinterpret_cast<unsigned long long*>(grec + f.off_max), m);
-      }
-      const uint32_t nanmask = __ballot_sync(0xffffffffu, nan);
-      const uint32_t pz = __ballot_sync(0xffffffffu, ok && isf && xd == 0.0 && __double_as_longlong(xd) >= 0);
-      const uint32_t nz = __ballot_sync(0xffffffffu, ok && isf && xd == 0.0 && __double_as_longlong(xd) < 0);
-      if (leader) {
-        uint32_t bits = 0;
-        if (nanmask) bits |= 1u << (3 * v);
-        if (pz) bits |= 1u << (3 * v + 1);
-        if (nz) bits |= 1u << (3 * v + 2);
-        if (bits) atomicOr(reinterpret_cast<uint32_t*>(grec + kRecFlags), bits);
-      }
-    }
-    if (f.off_m2 >= 0 && vmask) {
-      // The group's shift K: set once, by the first valid value of a leader.
-      const uint64_t xbits = (xd != xd) ? kCanonNaN : (uint64_t)__double_as_longlong(xd);
-      const uint64_t candk = __shfl_sync(0xffffffffu, xbits, __ffs(vmask) - 1);
-      uint64_t ks = 0;
-      if (leader) {
-        ks = *reinterpret_cast<volatile unsigned long long*>(grec + f.off_shift);
-        if (ks == 0) {
-          const uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long*>(grec + f.off_shift), 0ull, candk ^ kShiftTag);
-          ks = prev == 0 ? (candk ^ kShiftTag) : prev;
-        }
-      }
-      ks = __shfl_sync(0xffffffffu, ks, lead);
-      const double d = xd - __longlong_as_double((long long)(ks ^ kShiftTag));
-      const double s2 = warp_sum_f64(ok ? d * d : 0.0);
-      if (leader) atomicAdd(reinterpret_cast<double*>(grec + f.off_m2), s2);
-    }
-  }
-  return in;
-}
-
-constexpr int kCollapseMin = 4;  // group size from which a warp folds a group by butterfly
 
 // ---------------------------------------------------------------------------
 // Pass B.  A cluster's table is initialised once (key words all ones, fields

@@ -291,6 +291,54 @@ def run_batch(jobs: list, stream: int | None = None, flags: int = 0) -> list:
     return res
 
 
+class Server:
+    """The served form (dfc_server_*): submit bound regions over registered
+    columns; a native worker admits them as in-flight slots and memory allow
+    and overlaps their work on the device; poll() returns completions as
+    (tag, DeviceResult or ProviderError, latency_ns, queue_ns)."""
+
+    def __init__(self, device: int = 0, max_inflight: int = 64, memory_budget: int = -1):
+        h = C.c_void_p()
+        _check(N.lib().dfc_server_create(device, max_inflight, memory_budget, C.byref(h)))
+        self.handle = h
+        self._names: dict[int, list[str]] = {}
+        self._buf = (N.Completion * 256)()
+
+    def submit(self, bound: Bound, columns: list, tag: int, flags: int = 0) -> None:
+        q = _query_struct(bound, [c.handle for c in columns], None, flags)
+        self._names[tag] = bound.out_names
+        _check(N.lib().dfc_server_submit(self.handle, C.byref(q), tag))
+
+    def poll(self, wait_ms: int = 0) -> list:
+        n = N.lib().dfc_server_poll(self.handle, self._buf, len(self._buf), wait_ms)
+        out = []
+        for i in range(n):
+            c = self._buf[i]
+            names = self._names.pop(int(c.tag))
+            if c.status == N.OK:
+                res = DeviceResult(C.c_void_p(c.result), names)
+            else:
+                res = _error(c.status, c.message.decode())
+            out.append((int(c.tag), res, c.latency_ns, c.queue_ns))
+        return out
+
+    def stats(self) -> dict:
+        s = N.ServerStats()
+        _check(N.lib().dfc_server_stats_get(self.handle, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in N.ServerStats._fields_}
+
+    def close(self) -> None:
+        if self.handle:
+            N.lib().dfc_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def last_timings() -> dict:
     t = N.Timings()
     _check(N.lib().dfc_last_timings(C.byref(t)))

@@ -248,6 +248,50 @@ DFC_API dfc_status dfc_groupby_batch(const dfc_query* const* queries, int32_t n,
 DFC_API const char* dfc_batch_error(int32_t i);
 
 /* ------------------------------------------------------------------------ */
+/* The served form: a request loop with continuous batching.  The reference */
+/* has no server (its core runs one query per collect()); this serves many  */
+/* clients over resident tables.  A worker thread admits submitted requests */
+/* while fewer than max_inflight are on the device and their working memory */
+/* fits memory_budget (<= 0: 80% of the free HBM at creation), launches     */
+/* each on one of several streams without waiting for the others, and       */
+/* finishes each as its device work completes: requests that arrive while   */
+/* others run are admitted as slots and memory free up, and their work      */
+/* overlaps.  The columns a request names must stay registered until its    */
+/* completion is polled.                                                    */
+/* ------------------------------------------------------------------------ */
+typedef struct dfc_server dfc_server;
+
+typedef struct dfc_completion {
+  uint64_t tag;          /* as submitted */
+  int32_t status;        /* dfc_status */
+  int32_t reserved;
+  dfc_result* result;    /* on DFC_OK: the caller frees it */
+  double latency_ns;     /* submission to completion */
+  double queue_ns;       /* submission to admission */
+  char message[160];     /* the error text when status != DFC_OK */
+} dfc_completion;
+
+typedef struct dfc_server_stats {
+  uint64_t submitted;
+  uint64_t completed;
+  uint64_t pending;
+  uint64_t inflight;
+  int64_t max_inflight_seen;
+  int64_t bytes_held;
+  int64_t budget;
+} dfc_server_stats;
+
+DFC_API dfc_status dfc_server_create(int32_t device, int32_t max_inflight, int64_t memory_budget,
+                                     dfc_server** out);
+/* Copies the query description; returns at once. */
+DFC_API dfc_status dfc_server_submit(dfc_server* server, const dfc_query* query, uint64_t tag);
+/* Up to max completions, waiting up to wait_ms for the first; returns how many. */
+DFC_API int32_t dfc_server_poll(dfc_server* server, dfc_completion* out, int32_t max, int32_t wait_ms);
+DFC_API dfc_status dfc_server_stats_get(dfc_server* server, dfc_server_stats* out);
+/* Finishes every submitted request, frees unpolled results, stops. */
+DFC_API void dfc_server_destroy(dfc_server* server);
+
+/* ------------------------------------------------------------------------ */
 /* The same query without any device allocation.  No counterpart in the    */
 /* reference: it is for callers that cannot call cudaMalloc -- code running  */
 /* under an allocator that owns the device heap (a host framework's caching */

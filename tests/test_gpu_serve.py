@@ -1,0 +1,79 @@
+"""The served form: requests submitted to the native server (continuous
+batching, memory admission) give the same results as each query run alone
+-- keys, integers, validity and group order bit for bit, floats within the
+summation and moments bounds of the other parity tests -- and errors stay
+with their request."""
+import time
+
+import numpy as np
+import pytest
+
+from dataframe_mojo_b200 import provider
+from test_gpu_batch import canonical, make_jobs, same
+
+pytestmark = pytest.mark.gpu
+
+
+def serve_all(server, jobs, gap_s=0.0):
+    for i, (bound, cols) in enumerate(jobs):
+        server.submit(bound, cols, i)
+        if gap_s:
+            time.sleep(gap_s)
+    got = {}
+    deadline = time.time() + 120
+    while len(got) < len(jobs) and time.time() < deadline:
+        for tag, res, lat, queue in server.poll(wait_ms=50):
+            assert lat >= queue >= 0
+            got[tag] = res
+    assert len(got) == len(jobs)
+    return got
+
+
+def check_against_alone(jobs, got):
+    for i, (bound, cols) in enumerate(jobs):
+        try:
+            alone = provider.run_bound(bound, cols)
+        except provider.ProviderError as e:
+            assert isinstance(got[i], provider.ProviderError), (i, got[i])
+            assert got[i].status == e.status and str(got[i]) == str(e)
+            continue
+        assert isinstance(got[i], provider.DeviceResult), (i, got[i])
+        x, y = got[i].to_frame(), alone.to_frame()
+        if not bound.maintain_order:
+            x, y = canonical(x, len(bound.keys)), canonical(y, len(bound.keys))
+        same(x, y, f"request {i}")
+        got[i].free()
+        alone.free()
+
+
+def test_served_requests_match_alone():
+    rng = np.random.default_rng(91)
+    jobs, keep = make_jobs(rng, 48)
+    server = provider.Server(max_inflight=16)
+    try:
+        got = serve_all(server, jobs, gap_s=0.0005)
+        assert server.stats()["completed"] == len(jobs)
+    finally:
+        server.close()
+    check_against_alone(jobs, got)
+    for cols in keep:
+        for c in cols:
+            c.release()
+
+
+def test_memory_admission_one_at_a_time():
+    """A budget below any request's working memory admits one request at a
+    time (the server never starves): every result still arrives, in order of
+    admission, and matches the query alone."""
+    rng = np.random.default_rng(5)
+    jobs, keep = make_jobs(rng, 10)
+    server = provider.Server(max_inflight=8, memory_budget=1)
+    try:
+        got = serve_all(server, jobs)
+        assert server.stats()["max_inflight_seen"] <= 1
+    finally:
+        server.close()
+    check_against_alone(jobs, got)
+    for cols in keep:
+        for c in cols:
+            c.release()

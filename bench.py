@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -282,6 +283,192 @@ def run_reference(args, rank: int, world: int) -> int:
     return 0
 
 
+def _register(tensor, dtype_code, rows, valid_bytes=None):
+    """A device column over a torch tensor (kept alive by the caller)."""
+    import ctypes as C
+
+    from dataframe_mojo_b200 import _native as native
+
+    h = C.c_void_p()
+    st = native.lib().dfc_column_register(0, dtype_code, rows, tensor.data_ptr(),
+                                          valid_bytes.data_ptr() if valid_bytes is not None else None, 0,
+                                          native.COLUMN_DEVICE, C.byref(h))
+    if st != native.OK:
+        raise RuntimeError(native.last_error())
+    return type("DeviceHandle", (), {"handle": h})()
+
+
+def batched_form(device: str, nq: int) -> dict:
+    """The batched configuration: nq independent queries (rows log-uniform
+    1K-20M; one Int64 key, cardinality log-uniform 1-2M, uniform or Zipf
+    s=1.2; Int64 and Float32 values with 2% nulls; filter on the Int64
+    value against a random threshold), seeds 4 + query id.  Times the plain
+    path (one dfc_groupby per query) and the batched one (dfc_groupby_batch),
+    both after a warm-up pass of each."""
+    import torch
+    from dataframe_mojo_b200 import _native as native
+    from dataframe_mojo_b200 import provider
+    from dataframe_mojo_b200.frame import bind
+    from dataframe_mojo_b200.frame import DataFrame, Series, col
+
+    rng = np.random.default_rng(4)
+    shape = DataFrame([Series("k", np.zeros(1, np.int64)), Series("a", np.zeros(1, np.int64)),
+                       Series("b", np.zeros(1, np.float32))])
+    jobs, keep, total = [], [], 0
+    for q in range(nq):
+        rows = int(math.exp(rng.uniform(math.log(1e3), math.log(2e7))))
+        card = max(1, int(math.exp(rng.uniform(0.0, math.log(2e6)))))
+        zipf = bool(rng.integers(0, 2))
+        thr = int(rng.integers(-1000, 1000))
+        g = torch.Generator(device=device)
+        g.manual_seed(4 + q)
+        if zipf:
+            w = torch.arange(1, card + 1, device=device, dtype=torch.float64).pow(-1.2)
+            cdf = torch.cumsum(w, 0)
+            cdf /= cdf[-1].clone()
+            u = torch.rand(rows, generator=g, device=device, dtype=torch.float64)
+            k = torch.searchsorted(cdf, u).clamp_(max=card - 1)
+        else:
+            k = torch.randint(0, card, (rows,), generator=g, device=device)
+        a = torch.randint(-1000, 1001, (rows,), generator=g, device=device)
+        b = torch.randn(rows, generator=g, device=device, dtype=torch.float32)
+        va = pack_bits_torch(torch.rand(rows, generator=g, device=device) >= 0.02)
+        vb = pack_bits_torch(torch.rand(rows, generator=g, device=device) >= 0.02)
+        plan = shape.lazy().filter(col("a") > thr).group_by("k", maintain_order=True).agg(
+            [col("a").sum().alias("sa"), col("b").mean().alias("mb"), col("a").min().alias("lo"),
+             col("b").max().alias("hi"), col("b").count().alias("n")])
+        bound = bind(plan.plan)
+        hs = {"k": _register(k, native.INT64, rows), "a": _register(a, native.INT64, rows, va),
+              "b": _register(b, native.FLOAT32, rows, vb)}
+        keep.append((k, a, b, va, vb, hs))
+        jobs.append((bound, [hs[n] for n in bound.names]))
+        total += rows
+    torch.cuda.synchronize()
+
+    def plain():
+        for bd, cl in jobs:
+            r = provider.run_bound(bd, cl)
+            r.free()
+
+    def batched():
+        for r in provider.run_batch(jobs):
+            if isinstance(r, Exception):
+                raise r
+            r.free()
+
+    times = {}
+    for name, fn in (("plain", plain), ("batched", batched), ("plain", plain), ("batched", batched)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        times[name] = time.perf_counter() - t0  # the second (warm) pass counts
+    for *_, hs in keep:
+        for h in hs.values():
+            native.lib().dfc_column_release(h.handle)
+    return {
+        "config": "batched: %d queries, rows log-uniform 1K-20M (%d rows), Int64 key cardinality log-uniform 1-2M "
+                  "(uniform or Zipf 1.2), Int64 + Float32 values 2%% nulls, filter on the Int64 value" % (nq, total),
+        "queries": nq,
+        "rows": total,
+        "plain_ms": times["plain"] * 1e3,
+        "batched_ms": times["batched"] * 1e3,
+        "plain_rows_per_s": total / times["plain"],
+        "batched_rows_per_s": total / times["batched"],
+        "speedup": times["plain"] / times["batched"],
+    }
+
+
+def served_form(device: str, nreq: int, rate: float = 2000.0) -> dict:
+    """The served configuration: 8 resident tables of 10M-200M rows (the
+    100M-row workload's schema, seeds 5 + table id), nreq requests arriving
+    as a Poisson process at `rate` per second, each a group-by with a random
+    threshold (p < t), key subset ({k1}, {k2} or {k1, k2}) and aggregation
+    list.  The plain path serves them first-in first-out with one
+    dfc_groupby at a time; the served path submits them to the native server
+    (continuous batching).  Latency = completion - arrival."""
+    import torch
+    from dataframe_mojo_b200 import _native as native
+    from dataframe_mojo_b200 import provider
+    from dataframe_mojo_b200.frame import bind
+    from dataframe_mojo_b200.frame import DataFrame, Series, col
+
+    sizes = [int(x) for x in np.geomspace(1e7, 2e8, 8)]
+    tables = []
+    for t, n in enumerate(sizes):
+        c = generate(n, 5 + t, device)
+        vb = pack_bits_torch(c["v_valid"])
+        hs = {"k1": _register(c["k1"], native.INT32, n), "k2": _register(c["k2"], native.UINT32, n),
+              "v": _register(c["v"], native.FLOAT64, n, vb), "p": _register(c["p"], native.INT32, n)}
+        tables.append((c, vb, hs))
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(5)
+    shape = DataFrame([Series("k1", np.zeros(1, np.int32)), Series("k2", np.zeros(1, np.uint32)),
+                       Series("v", np.zeros(1)), Series("p", np.zeros(1, np.int32))])
+    aggs_all = [("sum", lambda v: v.sum()), ("mean", lambda v: v.mean()), ("min", lambda v: v.min()),
+                ("max", lambda v: v.max()), ("count", lambda v: v.count()), ("var", lambda v: v.var())]
+    reqs = []
+    for i in range(nreq):
+        t = int(rng.integers(0, len(tables)))
+        keys = [["k1"], ["k2"], ["k1", "k2"]][int(rng.integers(0, 3))]
+        pick = [a for a in aggs_all if rng.random() < 0.5] or [aggs_all[0]]
+        plan = shape.lazy().filter(col("p") < int(rng.integers(1, 100))).group_by(keys, maintain_order=True).agg(
+            [f(col("v")).alias(n) for n, f in pick])
+        bound = bind(plan.plan)
+        reqs.append((bound, [tables[t][2][n] for n in bound.names]))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
+
+    # Warm-up: every table once (statistics, learned group counts).
+    for bound, cl in reqs[: min(nreq, 16)]:
+        provider.run_bound(bound, cl).free()
+
+    def plain():
+        lat = []
+        t0 = time.perf_counter()
+        for (bound, cl), at in zip(reqs, arrivals):
+            while time.perf_counter() - t0 < at:
+                pass
+            r = provider.run_bound(bound, cl)
+            r.free()
+            lat.append(time.perf_counter() - t0 - at)
+        return np.array(lat), time.perf_counter() - t0
+
+    def served():
+        server = provider.Server(max_inflight=32)
+        lat = {}
+        t0 = time.perf_counter()
+        i = 0
+        while len(lat) < nreq:
+            now = time.perf_counter() - t0
+            while i < nreq and arrivals[i] <= now:
+                server.submit(reqs[i][0], reqs[i][1], i)
+                i += 1
+            for tag, res, _, _ in server.poll(wait_ms=0):
+                if isinstance(res, Exception):
+                    raise res
+                res.free()
+                lat[tag] = time.perf_counter() - t0 - arrivals[tag]
+        span = time.perf_counter() - t0
+        server.close()
+        return np.array([lat[j] for j in range(nreq)]), span
+
+    lp, sp_ = plain()
+    ls, ss = served()
+    for c, vb, hs in tables:
+        for h in hs.values():
+            native.lib().dfc_column_release(h.handle)
+    return {
+        "config": "served: 8 resident tables of 10M-200M rows (%d rows), %d requests, Poisson arrivals at %.0f/s, "
+                  "random threshold, key subset and aggregation list" % (sum(sizes), nreq, rate),
+        "requests": nreq,
+        "plain": {"p50_ms": float(np.percentile(lp, 50) * 1e3), "p99_ms": float(np.percentile(lp, 99) * 1e3),
+                  "queries_per_s": nreq / sp_},
+        "served": {"p50_ms": float(np.percentile(ls, 50) * 1e3), "p99_ms": float(np.percentile(ls, 99) * 1e3),
+                   "queries_per_s": nreq / ss},
+        "throughput_ratio": (nreq / ss) / (nreq / sp_),
+    }
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -292,6 +479,8 @@ def main() -> int:
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--sample-rows", type=int, default=10_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-queries", type=int, default=512, help="batched form: queries (0: skip)")
+    ap.add_argument("--served-requests", type=int, default=400, help="served form: requests (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("at least 3 warm-up steps")
@@ -488,6 +677,15 @@ def main() -> int:
 
     for h in handles.values():
         lib.dfc_column_release(h)
+    del cols
+    torch.cuda.empty_cache()
+    batched = served = None
+    if world == 1 and args.batch_queries > 0:
+        batched = batched_form(f"cuda:{local}", args.batch_queries)
+        torch.cuda.empty_cache()
+    if world == 1 and args.served_requests > 0:
+        served = served_form(f"cuda:{local}", args.served_requests)
+        torch.cuda.empty_cache()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -518,6 +716,10 @@ def main() -> int:
             "gpu_launches": launches,
             "clocks": clk,
         }
+        if batched is not None:
+            line["batched"] = batched
+        if served is not None:
+            line["served"] = served
         print(json.dumps(line), flush=True)
     return 0
 

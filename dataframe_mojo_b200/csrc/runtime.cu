@@ -137,11 +137,13 @@ struct DeviceState {
 std::mutex g_dev_mu;
 std::map<int, DeviceState> g_dev;
 
-// Group counts seen per key-column set: the next query on the same keys sizes
-// its table from them (the reference sizes from column statistics,
-// dataframe/aggregation/hash_table.mojo:699-714).
+// Group counts seen per query shape (key columns and filter program, literals
+// included): a repeat of the same query sizes its table from them (the
+// reference sizes from column statistics, dataframe/aggregation/hash_table.mojo:699-714).
+// Joint distinct counts of multi-key sets over all rows, per key-column set.
 std::mutex g_learn_mu;
 std::map<std::vector<uint64_t>, uint64_t> g_learned;
+std::map<std::vector<uint64_t>, double> g_joint;
 std::atomic<uint64_t> g_column_serial{0};
 
 dfc_status device_ready(int dev, DeviceState** out) {
@@ -272,6 +274,7 @@ struct Plan {
   uint64_t rows = 0;
   uint64_t est_groups = 0;
   std::vector<uint64_t> key_sig;  // registration numbers of the key columns
+  std::vector<uint64_t> shape_sig;  // key_sig, then the filter program (columns by registration number)
 };
 
 dfc_status plan_query(const dfc_query* q, Plan& P) {
@@ -385,6 +388,15 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
     if (depth > 32) return fail(DFC_UNSUPPORTED, "filter program too deep");
   }
   if (q->n_pred > 0 && depth != 1) return fail(DFC_INVALID, "malformed filter program");
+  P.shape_sig = P.key_sig;
+  P.shape_sig.push_back(~0ull);
+  for (int i = 0; i < q->n_pred; ++i) {
+    const dfc_pred_op& op = q->pred[i];
+    const bool has_col = op.kind == DFC_PRED_CMP || op.kind == DFC_PRED_IS_NULL || op.kind == DFC_PRED_IS_NOT_NULL;
+    P.shape_sig.push_back(((uint64_t)(uint32_t)op.kind << 32) | (uint32_t)op.cmp);
+    P.shape_sig.push_back(has_col ? q->inputs[op.column]->serial : 0);
+    P.shape_sig.push_back(op.kind == DFC_PRED_CMP ? op.lit.u : 0);
+  }
   // Key and filter columns hold the first slots: the partition counting pass
   // stages only those.
   sp.n_stage_count = n_slots;
@@ -615,13 +627,19 @@ dfc_status ensure_stats(dfc_column* c, DeviceState* ds, cudaStream_t stream) {
   return DFC_OK;
 }
 
-// Estimated number of groups: what the last query on these key columns
-// found (when `learned`), else the product of the key columns' distinct
-// estimates (capped by their value ranges), capped by the row count.
+// Estimated number of groups: what the last query of the same shape found
+// (when `learned`), else the product of the key columns' distinct estimates
+// (capped by their value ranges), capped by the row count.  The statistics
+// describe all rows, so for a filtered query they bound the count from above.
 uint64_t estimate_groups(const dfc_query* q, const Plan& P, DeviceState* ds, cudaStream_t stream, bool learned = true) {
   if (learned) {
+    // DFC_GROUPS_ESTIMATE=<n> replaces the first estimate (capacity regrowth tests).
+    if (const char* env = getenv("DFC_GROUPS_ESTIMATE")) {
+      const long long v = atoll(env);
+      if (v > 0) return (uint64_t)v;
+    }
     std::lock_guard<std::mutex> lk(g_learn_mu);
-    auto it = g_learned.find(P.key_sig);
+    auto it = g_learned.find(P.shape_sig);
     if (it != g_learned.end()) return it->second;
   }
   double prod = 1.0;
@@ -642,7 +660,17 @@ uint64_t estimate_groups(const dfc_query* q, const Plan& P, DeviceState* ds, cud
   // Several keys: the product bounds the group count loosely (correlated
   // keys, Zipf pairs); the key words' own distinct count is the estimate.
   if (q->n_keys > 1 && prod > 65536 && P.rows > 0) {
-    const double joint = joint_key_estimate(P, ds, stream);
+    double joint = 0;
+    {
+      std::lock_guard<std::mutex> lk(g_learn_mu);
+      auto it = g_joint.find(P.key_sig);
+      if (it != g_joint.end()) joint = it->second;
+    }
+    if (joint <= 0) {
+      joint = joint_key_estimate(P, ds, stream);
+      std::lock_guard<std::mutex> lk(g_learn_mu);
+      if (joint > 0) g_joint[P.key_sig] = joint;
+    }
     if (joint > 0) prod = std::min(prod, joint);
   }
   double est = std::min(prod, (double)P.rows);
@@ -651,7 +679,7 @@ uint64_t estimate_groups(const dfc_query* q, const Plan& P, DeviceState* ds, cud
 
 void learn_groups(const Plan& P, uint64_t groups) {
   std::lock_guard<std::mutex> lk(g_learn_mu);
-  g_learned[P.key_sig] = groups;
+  g_learned[P.shape_sig] = groups;
 }
 
 struct Scratch {
@@ -1657,9 +1685,18 @@ struct BatchItem {
   Plan P;
   dfc_status st = DFC_OK;
   uint64_t slots = 0, recs = 0, chunk = 64, ncta = 1, words = 0, chunks = 1, out_rows = 0;
+  bool full_grid = false;  // the scan's grid fills every SM
   size_t off_table = 0, off_records = 0, off_bits = 0, off_prefix = 0, off_bsums = 0, off_perm = 0, off_firsts = 0;
   std::vector<ResultCol> rc;
 };
+
+// The stream of a sized query: a scan whose grid fills every SM runs on
+// stream 0, one after another (two such scans side by side only interleave
+// and share L2 between their tables); smaller queries spread over the rest.
+int item_stream(const BatchItem& it, int& k) {
+  if (it.full_grid) return 0;
+  return 1 + (k++ % (kBatchStreams - 1));
+}
 
 size_t arena_take(size_t& used, size_t bytes) {
   const size_t at = used;
@@ -1689,6 +1726,7 @@ dfc_status size_item(const dfc_query* q, BatchItem& it, DeviceState* ds, cudaStr
   int occ = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_kernel, kScanThreads, P.smem);
   it.ncta = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ds->sms * std::max(1, occ), std::max<uint64_t>(1, P.sp.tiles)));
+  it.full_grid = it.ncta >= (uint64_t)ds->sms * std::max(1, occ);
   const uint64_t groups_cap = std::min<uint64_t>(P.rows, it.slots / 8);
   it.chunk = 64;
   while (it.chunk < 1024 && it.chunk * it.ncta * 8 < groups_cap) it.chunk <<= 1;
@@ -1890,9 +1928,8 @@ DFC_API dfc_status dfc_groupby_batch(const dfc_query* const* queries, int32_t n,
   int k = 0;
   for (int i = 0; i < n; ++i) {
     if (items[i].st) continue;
-    launch_item(items[i], ds, arena, dctl + i, streams[k % streams.size()]);
+    launch_item(items[i], ds, arena, dctl + i, streams[item_stream(items[i], k)]);
     bt.launches += items[i].P.rows > 0 ? 7 : 6;
-    ++k;
   }
   for (size_t s = 0; s < streams.size(); ++s) {
     cudaEventRecord(joins[s], streams[s]);
@@ -2003,6 +2040,7 @@ struct dfc_server {
   std::vector<Request*> inflight;
   std::deque<dfc_completion> done;
   std::vector<cudaStream_t> streams;
+  cudaStream_t plan_stream = nullptr;
   Control* pinned = nullptr;  // max_inflight control slots
   std::vector<int> free_slots;
   bool stop = false;
@@ -2030,14 +2068,16 @@ void server_complete(dfc_server* sv, Request* r, dfc_status st, dfc_result* res,
 
 // Plans, sizes and launches one request; false when it must wait for memory
 // (nothing done) or failed (completed with its error).
-bool server_launch(dfc_server* sv, Request* r, int k) {
+bool server_launch(dfc_server* sv, Request* r, int& k) {
   r->item = BatchItem{};  // a request that waited for memory is planned afresh
   BatchItem& it = r->item;
   dfc_status st = plan_query(&r->oq.q, it.P);
   if (!st && it.P.device != sv->device) st = fail(DFC_UNSUPPORTED, "the request's columns live on another device");
   size_t used = 0;
-  cudaStream_t stream = sv->streams[k % sv->streams.size()];
-  if (!st) st = size_item(&r->oq.q, it, sv->ds, stream, used);
+  // Statistics kernels (first use of a key column) run on their own stream,
+  // so waiting for them does not wait for requests in flight.
+  if (!st) st = size_item(&r->oq.q, it, sv->ds, sv->plan_stream, used);
+  cudaStream_t stream = sv->streams[st ? 0 : item_stream(it, k)];
   if (st) {
     r->admitted = Clock::now();
     server_complete(sv, r, st, nullptr, t_error);
@@ -2131,7 +2171,7 @@ void server_loop(dfc_server* sv) {
       }
     }
     for (size_t i = 0; i < take.size(); ++i) {
-      if (!server_launch(sv, take[i], k++)) {
+      if (!server_launch(sv, take[i], k)) {
         // Not enough memory now: back to the front, in order.
         std::lock_guard<std::mutex> lk(sv->mu);
         for (size_t j = take.size(); j-- > i;) sv->pending.push_front(take[j]);
@@ -2192,8 +2232,10 @@ DFC_API dfc_status dfc_server_create(int32_t device, int32_t max_inflight, int64
   sv->budget = memory_budget;
   sv->streams.resize(kBatchStreams);
   for (auto& s : sv->streams) cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  cudaStreamCreateWithFlags(&sv->plan_stream, cudaStreamNonBlocking);
   if (cudaMallocHost((void**)&sv->pinned, sizeof(Control) * sv->max_inflight) != cudaSuccess) {
     for (auto& s : sv->streams) cudaStreamDestroy(s);
+    cudaStreamDestroy(sv->plan_stream);
     delete sv;
     return fail(DFC_OOM, "pinned control slots");
   }
@@ -2266,6 +2308,8 @@ DFC_API void dfc_server_destroy(dfc_server* sv) {
     cudaStreamSynchronize(s);
     cudaStreamDestroy(s);
   }
+  cudaStreamSynchronize(sv->plan_stream);
+  cudaStreamDestroy(sv->plan_stream);
   cudaFreeHost(sv->pinned);
   delete sv;
 }

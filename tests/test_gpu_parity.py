@@ -2,6 +2,7 @@
 the reference), through the C ABI.  Integers, keys, nulls and group order are
 bit-exact; floating results carry the tolerance written beside each check."""
 import math
+import os
 
 import numpy as np
 import pytest
@@ -230,7 +231,13 @@ def test_capacity_regrowth_after_small_learned_estimate():
         small = table.run(frame.lazy().filter(col("p") < 100).group_by("k").agg(col("v").sum()))
         assert small.rows == 100
         small.free()
-        big = table.run(frame.lazy().group_by("k", maintain_order=True).agg(col("v").sum()))
+        # The first estimate for a new query shape comes from column
+        # statistics; pin it to 100 groups so the table must regrow.
+        os.environ["DFC_GROUPS_ESTIMATE"] = "100"
+        try:
+            big = table.run(frame.lazy().group_by("k", maintain_order=True).agg(col("v").sum()))
+        finally:
+            del os.environ["DFC_GROUPS_ESTIMATE"]
         t = provider.last_timings()
         assert t["retries"] >= 1
         out = big.to_frame()

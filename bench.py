@@ -298,23 +298,22 @@ def _register(tensor, dtype_code, rows, valid_bytes=None):
     return type("DeviceHandle", (), {"handle": h})()
 
 
-def batched_form(device: str, nq: int) -> dict:
-    """The batched configuration: nq independent queries (rows log-uniform
-    1K-20M; one Int64 key, cardinality log-uniform 1-2M, uniform or Zipf
-    s=1.2; Int64 and Float32 values with 2% nulls; filter on the Int64
-    value against a random threshold), seeds 4 + query id.  Times the plain
-    path (one dfc_groupby per query) and the batched one (dfc_groupby_batch),
-    both after a warm-up pass of each."""
+def batched_jobs(device: str, nq: int):
+    """The batched configuration's queries: nq independent queries (rows
+    log-uniform 1K-20M; one Int64 key, cardinality log-uniform 1-2M, uniform
+    or Zipf s=1.2; Int64 and Float32 values with 2% nulls; filter on the Int64
+    value against a random threshold), seeds 4 + query id.  Returns the jobs
+    (bound plan, registered columns), what keeps their buffers alive, the
+    total rows and per query (rows, cardinality, zipf)."""
     import torch
     from dataframe_mojo_b200 import _native as native
-    from dataframe_mojo_b200 import provider
     from dataframe_mojo_b200.frame import bind
     from dataframe_mojo_b200.frame import DataFrame, Series, col
 
     rng = np.random.default_rng(4)
     shape = DataFrame([Series("k", np.zeros(1, np.int64)), Series("a", np.zeros(1, np.int64)),
                        Series("b", np.zeros(1, np.float32))])
-    jobs, keep, total = [], [], 0
+    jobs, keep, total, info = [], [], 0, []
     for q in range(nq):
         rows = int(math.exp(rng.uniform(math.log(1e3), math.log(2e7))))
         card = max(1, int(math.exp(rng.uniform(0.0, math.log(2e6)))))
@@ -342,8 +341,21 @@ def batched_form(device: str, nq: int) -> dict:
               "b": _register(b, native.FLOAT32, rows, vb)}
         keep.append((k, a, b, va, vb, hs))
         jobs.append((bound, [hs[n] for n in bound.names]))
+        info.append((rows, card, zipf))
         total += rows
     torch.cuda.synchronize()
+    return jobs, keep, total, info
+
+
+def batched_form(device: str, nq: int) -> dict:
+    """The batched configuration (batched_jobs): times the plain path (one
+    dfc_groupby per query) and the batched one (dfc_groupby_batch), both
+    after a warm-up pass of each."""
+    import torch
+    from dataframe_mojo_b200 import _native as native
+    from dataframe_mojo_b200 import provider
+
+    jobs, keep, total, _ = batched_jobs(device, nq)
 
     def plain():
         for bd, cl in jobs:
@@ -469,6 +481,96 @@ def served_form(device: str, nreq: int, rate: float = 2000.0) -> dict:
     }
 
 
+def precision_form(device: str, rows: int, reps: int = 5) -> dict:
+    """The precision configuration: `rows` rows, Int32 keys uniform over 10K
+    groups, Float32 values with log-uniform magnitudes in [1e-6, 1e6] and
+    random signs (seed 3); group_by(k).agg(sum, mean, var) accumulated in
+    FP64 (the default) and as compensated FP32 partials merged in FP64.  Per
+    arm: device-resident time per query (best of `reps`, each a full
+    dfc_groupby with its readback) and the per-group maximum errors against
+    an extended-precision (long double) oracle on the host: sums relative to
+    sum |x|, variances relative to the variance.  A Float32 column's sum is a
+    Float32 result, so the accumulated sum is read through the Float64 mean
+    (mean x count)."""
+    import torch
+    from dataframe_mojo_b200 import _native as native
+    from dataframe_mojo_b200 import provider
+    from dataframe_mojo_b200.frame import bind
+    from dataframe_mojo_b200.frame import DataFrame, Series, col
+
+    g = torch.Generator(device=device)
+    g.manual_seed(3)
+    keys = torch.randint(0, 10_000, (rows,), generator=g, device=device, dtype=torch.int32)
+    mags = torch.pow(10.0, torch.rand(rows, generator=g, device=device, dtype=torch.float64) * 12.0 - 6.0)
+    sign = torch.where(torch.rand(rows, generator=g, device=device) < 0.5, -1.0, 1.0).to(torch.float64)
+    vals = (sign * mags).to(torch.float32)
+    del mags, sign
+    torch.cuda.synchronize()
+    hs = {"k": _register(keys, native.INT32, rows), "v": _register(vals, native.FLOAT32, rows)}
+    shape = DataFrame([Series("k", np.zeros(1, np.int32)), Series("v", np.zeros(1, np.float32))])
+    plan = shape.lazy().group_by("k").agg([col("v").sum().alias("s"), col("v").mean().alias("m"),
+                                           col("v").var().alias("var")])
+    bound = bind(plan.plan)
+    cl = [hs[n] for n in bound.names]
+
+    # Extended-precision oracle on the host.
+    k_h = keys.cpu().numpy()
+    v_h = vals.cpu().numpy()
+    order = np.argsort(k_h, kind="stable")
+    ks = k_h[order]
+    starts = np.flatnonzero(np.r_[True, ks[1:] != ks[:-1]])
+    counts = np.diff(np.r_[starts, rows])
+    x = v_h[order].astype(np.longdouble)
+    del order
+    gsum = np.add.reduceat(x, starts)
+    gabs = np.add.reduceat(np.abs(x), starts)
+    d = x - np.repeat(gsum / counts, counts)
+    gvar = np.add.reduceat(d * d, starts) / (counts - 1)
+    del x, d
+    gkeys = ks[starts]
+
+    arms = {}
+    for name, flags in (("fp64", 0), ("compensated_fp32", native.Q_FLOAT32_COMPENSATED)):
+        provider.run_bound(bound, cl, flags=flags).free()  # warm-up (learned group count)
+        best, t, r = float("inf"), None, None
+        for rep in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = provider.run_bound(bound, cl, flags=flags)
+            dt = time.perf_counter() - t0
+            if dt < best:
+                best, t = dt, provider.last_timings()
+            if rep < reps - 1:
+                r.free()
+        out = r.to_frame()
+        r.free()
+        o = np.argsort(out["k"].values)
+        if not np.array_equal(out["k"].values[o], gkeys):
+            raise RuntimeError("precision form: group keys differ from the oracle")
+        s = out["m"].values[o].astype(np.longdouble) * counts
+        v = out["var"].values[o].astype(np.longdouble)
+        arms[name] = {
+            "ms": best * 1e3,
+            "rows_per_s": rows / best,
+            "scan_ms": t["scan_ns"] / 1e6,
+            "algorithmic_gbs": rows * 8 / (t["scan_ns"] / 1e9) / 1e9,
+            "cluster_ctas": t["cluster_ctas"],
+            "compensated_fields": t["compensated"],
+            "max_sum_err_over_sum_abs": float(np.max(np.abs(s - gsum) / gabs)),
+            "max_sum_rel_err": float(np.max(np.abs(s - gsum) / np.maximum(np.abs(gsum), np.finfo(np.float64).tiny))),
+            "max_var_rel_err": float(np.max(np.abs(v - gvar) / gvar)),
+        }
+    for h in hs.values():
+        native.lib().dfc_column_release(h.handle)
+    return {
+        "config": "precision: %d rows, Int32 keys uniform over 10K groups, Float32 log-uniform |x| in [1e-6, 1e6] "
+                  "with random signs; sum/mean/var; errors against a long-double oracle; 8 algorithmic bytes/row" % rows,
+        "rows": rows,
+        "groups": int(len(gkeys)),
+        **arms,
+    }
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -481,6 +583,7 @@ def main() -> int:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-queries", type=int, default=512, help="batched form: queries (0: skip)")
     ap.add_argument("--served-requests", type=int, default=400, help="served form: requests (0: skip)")
+    ap.add_argument("--precision-rows", type=int, default=100_000_000, help="precision form: rows (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("at least 3 warm-up steps")
@@ -679,7 +782,10 @@ def main() -> int:
         lib.dfc_column_release(h)
     del cols
     torch.cuda.empty_cache()
-    batched = served = None
+    batched = served = precision = None
+    if world == 1 and args.precision_rows > 0:
+        precision = precision_form(f"cuda:{local}", args.precision_rows)
+        torch.cuda.empty_cache()
     if world == 1 and args.batch_queries > 0:
         batched = batched_form(f"cuda:{local}", args.batch_queries)
         torch.cuda.empty_cache()
@@ -716,6 +822,8 @@ def main() -> int:
             "gpu_launches": launches,
             "clocks": clk,
         }
+        if precision is not None:
+            line["precision"] = precision
         if batched is not None:
             line["batched"] = batched
         if served is not None:

@@ -33,7 +33,7 @@ Q_MAINTAIN_ORDER = 1
 Q_FORCE_GLOBAL = 2
 Q_FORCE_SHARED = 4
 Q_FORCE_PARTITIONED = 16
-Q_FLOAT32_FP64 = 8
+Q_FLOAT32_COMPENSATED = 8
 
 COLUMN_HOST = 0
 COLUMN_DEVICE = 1
@@ -97,6 +97,8 @@ class Timings(C.Structure):
         ("launches", C.c_int32),
         ("partitions", C.c_int32),
         ("aggregate_ns", C.c_double),
+        ("cluster_ctas", C.c_int32),
+        ("compensated", C.c_int32),
     ]
 
 

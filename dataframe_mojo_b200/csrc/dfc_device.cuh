@@ -170,6 +170,48 @@ __device__ __forceinline__ uint64_t rec_cas_u64(void* p, uint64_t cmp, uint64_t 
 // ---------------------------------------------------------------------------
 // Values.
 // ---------------------------------------------------------------------------
+// Distributed shared memory: explicit .shared::cluster accesses on 32-bit
+// cluster addresses (mapa of a local shared address to a CTA rank).
+__device__ __forceinline__ uint32_t dsm_map(const void* local, uint32_t rank) {
+  uint32_t a;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(local)), "r"(rank));
+  return a;
+}
+__device__ __forceinline__ uint32_t dsm_ld_u32(uint32_t a) {
+  uint32_t v;
+  asm volatile("ld.relaxed.cluster.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
+  return v;
+}
+__device__ __forceinline__ uint64_t dsm_ld_u64(uint32_t a) {
+  uint64_t v;
+  asm volatile("ld.relaxed.cluster.shared::cluster.u64 %0, [%1];" : "=l"(v) : "r"(a) : "memory");
+  return v;
+}
+__device__ __forceinline__ uint32_t dsm_add_u32(uint32_t a, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.shared::cluster.add.u32 %0, [%1], %2;" : "=r"(old) : "r"(a), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ void dsm_max_u32(uint32_t a, uint32_t v) {
+  asm volatile("red.shared::cluster.max.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
+__device__ __forceinline__ void dsm_or_b32(uint32_t a, uint32_t v) {
+  asm volatile("red.shared::cluster.or.b32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t dsm_add_u64(uint32_t a, uint64_t v) {
+  uint64_t old;
+  asm volatile("atom.shared::cluster.add.u64 %0, [%1], %2;" : "=l"(old) : "r"(a), "l"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ void dsm_add_f64(uint32_t a, double v) {
+  asm volatile("red.shared::cluster.add.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t dsm_cas_u64(uint32_t a, uint64_t cmp, uint64_t val) {
+  uint64_t old;
+  asm volatile("atom.shared::cluster.cas.b64 %0, [%1], %2, %3;" : "=l"(old) : "r"(a), "l"(cmp), "l"(val) : "memory");
+  return old;
+}
+
 __device__ __forceinline__ bool dt_float(int dt) { return dt == DFC_FLOAT32 || dt == DFC_FLOAT64; }
 __device__ __forceinline__ bool dt_unsigned(int dt) {
   return dt == DFC_UINT8 || dt == DFC_UINT16 || dt == DFC_UINT32 || dt == DFC_UINT64;

@@ -39,6 +39,7 @@ enum StatusBits : uint32_t {
   ST_OVERFLOW = 4u,    // a checked integer sum does not fit
   ST_FAULT = 8u,       // ill-conditioned moments: the CPU adjudicates
   ST_ZERO_FAULT = 16u, // a zero extremum seen with both signs: the CPU adjudicates
+  ST_F32_RANGE = 32u,  // a compensated FP32 partial left the FP32 range: rerun in FP64
 };
 
 enum KeyMode : int32_t { KEY_PACKED = 0, KEY_TICKET = 1 };
@@ -128,15 +129,21 @@ struct ScanParams {
   int32_t rec_stride;
   ValField vals[kMaxVals];
   // Shared-memory regime: CTA key table (smem_slots, power of two; 0 = off)
-  // and records at these byte offsets of the dynamic shared memory.
+  // and records at these byte offsets of the dynamic shared memory.  With
+  // smem_cluster > 1 the tables of a cluster's CTAs form one table of
+  // smem_cluster * smem_slots entries (a key lives in one CTA's share, reached
+  // through distributed shared memory).
   uint32_t smem_slots;
   uint32_t smem_keys_off;
   uint32_t smem_recs_off;
-  uint32_t pad2;
+  uint32_t smem_cluster;  // CTAs sharing one table; 0 or 1: each CTA its own
   int32_t track_first;  // maintain_order: first row lowered by atomic min
   int32_t off_len;      // u32 rows of the group, -1 absent
   int32_t rec_words;    // stride / 8
-  int32_t pad1;
+  // Value fields (bit v) whose sum and shifted square sum accumulate in the
+  // shared-memory tables as compensated FP32 pairs {s, c} (Float32 columns),
+  // merged into the FP64 global records; rows on the global path add in FP64.
+  uint32_t comp_mask;
   // Tables.
   KeyEntry* table;
   uint64_t table_mask;

@@ -131,6 +131,7 @@ struct DeviceState {
   bool ready = false;
   int sms = 0;
   size_t smem_optin = 0;       // scan_kernel's dynamic shared memory limit
+  size_t smem_half = 0;        // scan_kernel's dynamic shared memory at two CTAs per SM
   size_t part_smem_optin = 0;  // partition_kernel's
   int scan_occupancy = 1;
 };
@@ -165,8 +166,11 @@ dfc_status device_ready(int dev, DeviceState** out) {
     cudaFuncAttributes fa;
     CK(cudaFuncGetAttributes(&fa, scan_kernel), "cudaFuncGetAttributes");
     d.smem_optin = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;
+    d.smem_half = (prop.sharedMemPerMultiprocessor - 2 * prop.reservedSharedMemPerBlock) / 2 - fa.sharedSizeBytes;
     CK(cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin),
        "cudaFuncSetAttribute");
+    // Cluster tables pool the shared memory of up to 16 CTAs.
+    CK(cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1), "cudaFuncSetAttribute");
     CK(cudaFuncGetAttributes(&fa, partition_kernel), "cudaFuncGetAttributes");
     d.part_smem_optin = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;
     CK(cudaFuncSetAttribute(partition_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.part_smem_optin),
@@ -276,6 +280,39 @@ struct Plan {
   std::vector<uint64_t> key_sig;  // registration numbers of the key columns
   std::vector<uint64_t> shape_sig;  // key_sig, then the filter program (columns by registration number)
 };
+
+// The stage ring for tiles of `tile` rows (a power of two >= 128, so every
+// values block (tile * size) and validity block (tile / 8) is a multiple of
+// 16 bytes, as bulk copies require): per column its values then validity
+// words, the key and filter columns first; 4 stages.  Sets the tile fields
+// of P.sp and P.smem (the ring and its mbarriers); returns one stage's bytes.
+size_t layout_ring(Plan& P, int tile) {
+  ScanParams& sp = P.sp;
+  size_t b = 0, stage_tx_count = 0;
+  for (int c = 0; c < sp.n_stage; ++c) {
+    if (c == sp.n_stage_count) stage_tx_count = b;
+    sp.stage_off[c] = (int)b;
+    b += (size_t)tile * sp.cols[c].size;
+    if (sp.cols[c].validity) {
+      sp.stage_voff[c] = (int)b;
+      b += (size_t)tile / 8;
+    } else {
+      sp.stage_voff[c] = -1;
+    }
+  }
+  if (sp.n_stage_count == sp.n_stage) stage_tx_count = b;
+  sp.stage_tx = (int)b;
+  sp.stage_tx_count = (int)stage_tx_count;
+  b = (b + 127) & ~(size_t)127;
+  sp.stage_bytes = (int)b;
+  sp.tile_rows = tile;
+  sp.stages = 4;
+  sp.tiles = (P.rows + tile - 1) / tile;
+  sp.full_tiles = P.rows / tile;
+  P.tile_rows = tile;
+  P.smem = (size_t)sp.stages * b + 2 * sp.stages * sizeof(uint64_t);
+  return b;
+}
 
 dfc_status plan_query(const dfc_query* q, Plan& P) {
   if (!q) return fail(DFC_INVALID, "null query");
@@ -473,6 +510,10 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
   }
   sp.rec_stride = (off + 15) & ~15;
   if (sp.rec_stride > kMaxRecWords * 8) return fail(DFC_UNSUPPORTED, "group record too wide");
+  sp.comp_mask = 0;
+  if (q->flags & DFC_Q_FLOAT32_COMPENSATED)
+    for (int j = 0; j < sp.n_vals; ++j)
+      if (sp.vals[j].dtype == DFC_FLOAT32 && sp.vals[j].off_sum >= 0) sp.comp_mask |= 1u << j;
   sp.rec_words = sp.rec_stride / 8;
   sp.track_first = (q->flags & DFC_Q_MAINTAIN_ORDER) ? 1 : 0;
 
@@ -508,47 +549,17 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
   fp.n_out = n_out;
   P.n_out = n_out;
 
-  // Stage layout: the largest tile whose ring of >= 3 stages fits.
+  // Stage layout: the largest tile whose 4-stage ring fits in 96 KB.
   sp.n_stage = n_slots;
   sp.n_cols = n_slots;
   sp.rows = P.rows;
   bool aligned = true;
   for (int c = 0; c < n_slots; ++c)
     if (((uintptr_t)sp.cols[c].values & 15u) != 0) aligned = false;
-  int tile = 1024;
-  size_t stage_bytes = 0, stage_tx = 0, stage_tx_count = 0;
-  for (; tile >= 128; tile >>= 1) {
-    // tile >= 128: every values block (tile * size) and validity block
-    // (tile / 8) is a multiple of 16 bytes, as bulk copies require.
-    size_t b = 0;
-    for (int c = 0; c < n_slots; ++c) {
-      if (c == sp.n_stage_count) stage_tx_count = b;
-      sp.stage_off[c] = (int)b;
-      b += (size_t)tile * sp.cols[c].size;
-      if (sp.cols[c].validity) {
-        sp.stage_voff[c] = (int)b;
-        b += (size_t)tile / 8;
-      } else {
-        sp.stage_voff[c] = -1;
-      }
-    }
-    stage_tx = b;
-    if (sp.n_stage_count == n_slots) stage_tx_count = b;
-    b = (b + 127) & ~(size_t)127;
-    stage_bytes = b;
-    if (b * 4 <= 96 * 1024) break;
-  }
-  if (tile < 128) return fail(DFC_UNSUPPORTED, "too many input columns for the stage ring");
-  sp.tile_rows = tile;
-  sp.stage_bytes = (int)stage_bytes;
-  sp.stage_tx = (int)stage_tx;
-  sp.stage_tx_count = (int)stage_tx_count;
-  sp.stages = 4;
   sp.use_tma = aligned ? 1 : 0;
-  sp.tiles = (P.rows + tile - 1) / tile;
-  sp.full_tiles = P.rows / tile;
-  P.tile_rows = tile;
-  P.smem = (size_t)sp.stages * stage_bytes + 2 * sp.stages * sizeof(uint64_t);
+  int tile = 1024;
+  while (tile >= 128 && layout_ring(P, tile) * 4 > 96 * 1024) tile >>= 1;
+  if (tile < 128) return fail(DFC_UNSUPPORTED, "too many input columns for the stage ring");
   return DFC_OK;
 }
 
@@ -682,6 +693,154 @@ void learn_groups(const Plan& P, uint64_t groups) {
   g_learned[P.shape_sig] = groups;
 }
 
+// Co-resident clusters of `ranks` scan CTAs with `smem` dynamic bytes each.
+int scan_clusters(uint32_t ranks, size_t smem) {
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = ranks;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(ranks);
+  cfg.blockDim = dim3(kScanThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, (void*)scan_kernel, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+// Shared-memory tables for an estimate of `est` groups at the current ring.
+// `own`: each CTA keeps its own table at load <= 1/2 (up to 4096 groups).
+// Otherwise the CTAs of a thread-block cluster (2..16) pool their shared
+// memory into one table (up to 32K groups), each share at average load
+// <= 0.7: the smallest cluster whose shares fit at two CTAs per SM, else the
+// smallest at one.  Cluster tables are chosen only where on-chip partials are
+// required (compensated FP32 fields) or asked for (DFC_Q_FORCE_SHARED,
+// DFC_SMEM_CLUSTER=<2..16>, which also picks the size): on B200, 100M rows
+// over 10K uniform keys took 31 ms in a cluster table against 4.6 ms in the
+// global table in L2.  Sets P.sp's shared-memory fields and P.smem; false:
+// none fits.
+constexpr uint64_t kOwnTableGroups = 4096;
+constexpr uint64_t kClusterTableGroups = 32768;
+bool plan_shared_at(Plan& P, DeviceState* ds, uint64_t est, uint32_t flags, bool own) {
+  ScanParams& sp = P.sp;
+  const bool force = (flags & DFC_Q_FORCE_SHARED) != 0;
+  const size_t ring = P.smem;
+  const size_t keys_off = (ring + 15) & ~(size_t)15;
+  auto recs_at = [&](uint64_t sslots) { return (keys_off + sslots * 8 + 15) & ~(size_t)15; };
+  auto total_for = [&](uint64_t sslots) { return recs_at(sslots) + sslots * (size_t)sp.rec_stride; };
+  auto take = [&](uint64_t sslots, uint32_t ranks) {
+    sp.smem_slots = (uint32_t)sslots;
+    sp.smem_cluster = ranks;
+    sp.smem_keys_off = (uint32_t)keys_off;
+    sp.smem_recs_off = (uint32_t)recs_at(sslots);
+    P.smem = total_for(sslots);
+    return true;
+  };
+  uint32_t want = 0;
+  if (const char* env = getenv("DFC_SMEM_CLUSTER")) want = (uint32_t)atoi(env);
+  if (own) {
+    // DFC_HOT_SLOTS=<n>: an own table of n slots whatever the estimate (a
+    // per-CTA cache for the keys that come first, hot keys; tuning).
+    uint64_t hot = 0;
+    if (const char* env = getenv("DFC_HOT_SLOTS")) hot = next_pow2(std::max<uint64_t>(64, (uint64_t)atoll(env)));
+    if (want >= 2 || (!force && !hot && est > kOwnTableGroups)) return false;
+    const uint64_t sslots =
+        hot ? hot : next_pow2(std::max<uint64_t>(64, std::min<uint64_t>(est, kOwnTableGroups) * 2));
+    // smem_optin already excludes the kernel's static shared memory.
+    return total_for(sslots) <= ds->smem_optin && take(sslots, 1);
+  }
+  auto share = [&](uint32_t ranks) {
+    return next_pow2(std::max<uint64_t>(64, (uint64_t)std::ceil((double)std::max<uint64_t>(est, 1) * 1.4 / ranks)));
+  };
+  if (want >= 2) {
+    if (want > 16 || (want & (want - 1))) return false;
+    const uint64_t sslots = share(want);
+    if (total_for(sslots) > ds->smem_optin || scan_clusters(want, total_for(sslots)) < 1) return false;
+    return take(sslots, want);
+  }
+  if (!force && (est > kClusterTableGroups || sp.comp_mask == 0)) return false;
+  for (size_t budget : {ds->smem_half, ds->smem_optin}) {
+    for (uint32_t ranks = 2; ranks <= 16; ranks *= 2) {
+      const uint64_t sslots = share(ranks);
+      const size_t total = total_for(sslots);
+      if (total > budget || scan_clusters(ranks, total) < 1) continue;
+      return take(sslots, ranks);
+    }
+  }
+  return false;
+}
+
+// Own tables, then cluster tables, each with the query's ring or else with
+// smaller tiles (down to 256 rows) that leave the tables more room; the ring
+// is restored when nothing fits.  Packed keys only; false: the global table
+// alone.
+bool plan_shared(Plan& P, DeviceState* ds, uint64_t est, uint32_t flags) {
+  ScanParams& sp = P.sp;
+  sp.smem_slots = 0;
+  sp.smem_cluster = 1;
+  if ((flags & DFC_Q_FORCE_GLOBAL) || sp.key_mode != KEY_PACKED) return false;
+  const int tile0 = sp.tile_rows;
+  for (bool own : {true, false}) {
+    for (int tile = tile0; tile >= std::min(tile0, 256); tile >>= 1) {
+      if (tile != sp.tile_rows) layout_ring(P, tile);
+      if (plan_shared_at(P, ds, est, flags, own)) return true;
+    }
+  }
+  if (sp.tile_rows != tile0) layout_ring(P, tile0);
+  return false;
+}
+
+// CTAs of the scan per SM at P.smem (cluster launches: co-resident CTAs in
+// whole clusters).
+uint64_t scan_capacity(const Plan& P, DeviceState* ds) {
+  if (P.sp.smem_cluster > 1)
+    return (uint64_t)std::max(1, scan_clusters(P.sp.smem_cluster, P.smem)) * P.sp.smem_cluster;
+  int occ = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_kernel, kScanThreads, P.smem) != cudaSuccess) {
+    cudaGetLastError();
+    occ = 1;
+  }
+  return (uint64_t)ds->sms * std::max(1, occ);
+}
+
+// The scan's persistent grid: every co-resident CTA, at most one per tile
+// (cluster launches: whole clusters).
+uint64_t scan_grid(const Plan& P, DeviceState* ds) {
+  const uint64_t tiles = std::max<uint64_t>(1, P.sp.tiles);
+  const uint64_t cap = scan_capacity(P, ds);
+  if (P.sp.smem_cluster > 1) {
+    const uint64_t r = P.sp.smem_cluster;
+    return std::min<uint64_t>(cap / r, (tiles + r - 1) / r) * r;
+  }
+  return std::max<uint64_t>(1, std::min<uint64_t>(cap, tiles));
+}
+
+cudaError_t launch_scan(const ScanParams& sp, uint64_t ncta, size_t smem, cudaStream_t stream) {
+  if (sp.smem_cluster <= 1) {
+    scan_kernel<<<(unsigned)ncta, kScanThreads, smem, stream>>>(sp);
+    return cudaGetLastError();
+  }
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = sp.smem_cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3((unsigned)ncta);
+  cfg.blockDim = dim3(kScanThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, scan_kernel, sp);
+}
+
 struct Scratch {
   cudaStream_t stream = nullptr;
   std::vector<void*> ptrs;
@@ -799,17 +958,14 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   Scratch S;
   S.stream = stream;
 
-  int occ = 1;
+  uint64_t ncta;
   if (pp) {
-    // The counting pass and pass A must see the same tiles per CTA: one grid.
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, partition_kernel, kPartThreads, pp->smem), "occupancy");
-    occ = 1;
+    // The counting pass and pass A must see the same tiles per CTA: one grid
+    // of one CTA per SM.
+    ncta = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ds->sms, std::max<uint64_t>(1, sp.tiles)));
   } else {
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_kernel, kScanThreads, P.smem), "occupancy");
+    ncta = scan_grid(P, ds);
   }
-  occ = std::max(1, occ);
-  uint64_t ncta = (uint64_t)ds->sms * (uint64_t)occ;
-  ncta = std::max<uint64_t>(1, std::min<uint64_t>(ncta, std::max<uint64_t>(1, sp.tiles)));
   uint64_t chunk = 64, recs;
   if (pp) {
     // Pass B appends every group exactly once: no holes, no chunks.
@@ -950,7 +1106,13 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
     t_timings.launches += 4;
   } else {
     if (P.rows > 0) {
-      scan_kernel<<<(unsigned)ncta, kScanThreads, P.smem, stream>>>(sp);
+      e = launch_scan(sp, ncta, P.smem, stream);
+      if (e != cudaSuccess) {
+        free_outputs();
+        S.release();
+        for (auto& x : ev) cudaEventDestroy(x);
+        return cuda_fail(e, "scan launch");
+      }
       t_timings.launches += 1;
     }
     cudaEventRecord(ev[3], stream);
@@ -1011,11 +1173,12 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   t_timings.partitions = pp ? (int32_t)nparts : 0;
   if (getenv("DFC_TRACE")) {
     fprintf(stderr,
-            "dfc attempt: rows=%llu regime=%s slots=%llu recs=%llu smem_slots=%u ctas=%llu parts=%llu agg_slots=%u "
+            "dfc attempt: rows=%llu regime=%s slots=%llu recs=%llu smem_slots=%u x%u tile=%d ctas=%llu parts=%llu agg_slots=%u "
             "clusters=%d flush=%u | status=%#x cap=%#x check=%#x alloc=%u groups=%u ms scan=%.3f (count=%.3f offsets=%.3f) "
             "agg=%.3f fin=%.3f\n",
             (unsigned long long)P.rows, pp ? "partitioned" : "table", (unsigned long long)slots,
-            (unsigned long long)recs, sp.smem_slots, (unsigned long long)ncta, (unsigned long long)nparts,
+            (unsigned long long)recs, sp.smem_slots, std::max(1u, sp.smem_cluster), sp.tile_rows, (unsigned long long)ncta,
+            (unsigned long long)nparts,
             pp ? pp->agg_slots : 0u, pp ? pp->clusters : 0, pp ? pp->flush : 0u, host_ctl->status[0],
             host_ctl->status[1], host_ctl->status[2], host_ctl->alloc, host_ctl->groups, ms_scan, ms_count, ms_offsets,
             ms_agg, ms_finish);
@@ -1032,7 +1195,9 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
     free_outputs();
     return fail(DFC_TIMEOUT, "a bounded device wait gave up");
   }
-  if (status & ST_CAPACITY) {
+  if (status & (ST_CAPACITY | ST_F32_RANGE)) {
+    // Out of capacity, or a compensated FP32 partial out of range (the caller
+    // reruns in FP64).
     free_outputs();
     *grow = true;
     return DFC_CAPACITY;
@@ -1238,20 +1403,7 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
   bool partitioned = false;
   if ((query->flags & DFC_Q_FORCE_PARTITIONED) && !(query->flags & (DFC_Q_FORCE_GLOBAL | DFC_Q_FORCE_SHARED)))
     partitioned = plan_partitions(P, ds, est, pp);
-  if (!partitioned && !(query->flags & DFC_Q_FORCE_GLOBAL) && P.sp.key_mode == KEY_PACKED &&
-      ((query->flags & DFC_Q_FORCE_SHARED) || est <= 4096)) {
-    const uint64_t sslots = next_pow2(std::max<uint64_t>(64, std::min<uint64_t>(est, 4096) * 2));
-    const size_t keys_off = (P.smem + 15) & ~(size_t)15;
-    const size_t recs_off = (keys_off + sslots * 8 + 15) & ~(size_t)15;
-    const size_t total = recs_off + sslots * (size_t)P.sp.rec_stride;
-    // smem_optin already excludes the kernel's static shared memory.
-    if (total <= ds->smem_optin) {
-      P.sp.smem_slots = (uint32_t)sslots;
-      P.sp.smem_keys_off = (uint32_t)keys_off;
-      P.sp.smem_recs_off = (uint32_t)recs_off;
-      P.smem = total;
-    }
-  }
+  if (!partitioned) plan_shared(P, ds, est, query->flags);
   uint64_t slots = next_pow2(std::max<uint64_t>(1024, est * 8));
   const uint64_t max_slots = next_pow2(std::max<uint64_t>(1024, P.rows * 8));
   slots = std::min(slots, max_slots);
@@ -1260,6 +1412,11 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
     st = run_attempt(query, P, ds, stream, slots, partitioned ? &pp : nullptr, out, &grow, host_ctl);
     if (!grow) break;
     t_timings.retries += 1;
+    if (host_ctl->status[0] & ST_F32_RANGE) {
+      // A compensated FP32 partial left the FP32 range: FP64 throughout.
+      P.sp.comp_mask = 0;
+      if (!(host_ctl->status[0] & ST_CAPACITY)) continue;
+    }
     if (partitioned) {
       // Re-plan from the column statistics (a learned count may come from a
       // query with another filter), at least 8x the last estimate and twice
@@ -1287,6 +1444,8 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
   learn_groups(P, (*out)->rows);
   t_timings.groups = (*out)->rows;
   t_timings.regime = partitioned ? 2 : (P.sp.smem_slots ? 1 : 0);
+  t_timings.cluster_ctas = P.sp.smem_slots ? (int32_t)std::max(1u, P.sp.smem_cluster) : 0;
+  t_timings.compensated = P.sp.smem_slots ? (int32_t)P.sp.comp_mask : 0;
   t_timings.total_ns = std::chrono::duration<double, std::nano>(std::chrono::steady_clock::now() - t0).count();
   return DFC_OK;
 }
@@ -1709,24 +1868,10 @@ size_t arena_take(size_t& used, size_t bytes) {
 dfc_status size_item(const dfc_query* q, BatchItem& it, DeviceState* ds, cudaStream_t stream, size_t& used) {
   Plan& P = it.P;
   const uint64_t est = estimate_groups(q, P, ds, stream);
-  P.sp.smem_slots = 0;
-  if (!(q->flags & DFC_Q_FORCE_GLOBAL) && P.sp.key_mode == KEY_PACKED && ((q->flags & DFC_Q_FORCE_SHARED) || est <= 4096)) {
-    const uint64_t sslots = next_pow2(std::max<uint64_t>(64, std::min<uint64_t>(est, 4096) * 2));
-    const size_t keys_off = (P.smem + 15) & ~(size_t)15;
-    const size_t recs_off = (keys_off + sslots * 8 + 15) & ~(size_t)15;
-    const size_t total = recs_off + sslots * (size_t)P.sp.rec_stride;
-    if (total <= ds->smem_optin) {
-      P.sp.smem_slots = (uint32_t)sslots;
-      P.sp.smem_keys_off = (uint32_t)keys_off;
-      P.sp.smem_recs_off = (uint32_t)recs_off;
-      P.smem = total;
-    }
-  }
+  plan_shared(P, ds, est, q->flags);
   it.slots = std::min(next_pow2(std::max<uint64_t>(1024, est * 8)), next_pow2(std::max<uint64_t>(1024, P.rows * 8)));
-  int occ = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_kernel, kScanThreads, P.smem);
-  it.ncta = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ds->sms * std::max(1, occ), std::max<uint64_t>(1, P.sp.tiles)));
-  it.full_grid = it.ncta >= (uint64_t)ds->sms * std::max(1, occ);
+  it.ncta = scan_grid(P, ds);
+  it.full_grid = it.ncta >= scan_capacity(P, ds);
   const uint64_t groups_cap = std::min<uint64_t>(P.rows, it.slots / 8);
   it.chunk = 64;
   while (it.chunk < 1024 && it.chunk * it.ncta * 8 < groups_cap) it.chunk <<= 1;
@@ -1770,7 +1915,7 @@ dfc_status finish_item(const dfc_query* q, BatchItem& it, const Control& c, int 
     return fail(DFC_DEVICE, msg);
   }
   if (status & ST_TIMEOUT) return fail(DFC_TIMEOUT, "a bounded device wait gave up");
-  if (status & ST_CAPACITY) return DFC_CAPACITY;
+  if (status & (ST_CAPACITY | ST_F32_RANGE)) return DFC_CAPACITY;  // rerun alone
   if (status & ST_OVERFLOW) {
     const uint32_t a = c.overflow_agg;
     const int idt = (a < (uint32_t)q->n_aggs) ? it.P.out_agg_input_dtype[a] : DFC_INT64;
@@ -1810,7 +1955,7 @@ void launch_item(BatchItem& it, DeviceState* ds, unsigned char* base, Control* d
   sp.alloc = &dctl->alloc;
   sp.status = dctl->status;
   sp.part_bits = 0;
-  if (it.P.rows > 0) scan_kernel<<<(unsigned)it.ncta, kScanThreads, it.P.smem, stream>>>(sp);
+  if (it.P.rows > 0) launch_scan(sp, it.ncta, it.P.smem, stream);
   fp.scan = sp;
   fp.order_bits = reinterpret_cast<uint32_t*>(base + it.off_bits);
   fp.word_prefix = reinterpret_cast<uint32_t*>(base + it.off_prefix);

@@ -13,9 +13,10 @@
 //      hashed (ticket mode);
 //   4. groups: with few groups a CTA-local shared-memory table, duplicate keys
 //      of a warp collapsed with __match_any_sync into one leader update;
-//      otherwise the global open-addressing table, probed two entries per
-//      round in warp-synchronous rounds, new groups claimed by a 128-bit CAS
-//      that publishes key and group id together;
+//      with up to 32K groups the CTAs of a cluster pool their shared memory
+//      into one table; otherwise the global open-addressing table, probed
+//      two entries per round in warp-synchronous rounds, a new group claimed
+//      by a CAS of its key word, then its record published in the entry;
 //   5. states: each aggregated column's read-set (first row, K, min, max) for
 //      all rows, then fire-and-forget atomics (counts, sums, the shifted
 //      square sum; first row / min / max only when the row improves them).
@@ -321,8 +322,9 @@ __device__ __forceinline__ uint64_t slot_of(const ScanParams& p, uint64_t kw) {
 // ---------------------------------------------------------------------------
 // Record numbers are handed out by CTA tickets: ticket t falls in the CTA's
 // chunk k = t / chunk, whose base the holder of the chunk's first ticket draws
-// from the global counter and publishes (tagged with k) in a small ring.  A
-// reserved record that loses its claim race stays all-zero: a hole.
+// from the global counter and publishes (tagged with k) in a small ring.
+// Records stay all-zero until used; one reserved and never used (a lost
+// race of the per-lane claims below) is a hole the finish skips.
 constexpr int kChunkRing = 64;
 
 struct ClaimState {
@@ -430,11 +432,9 @@ __device__ __forceinline__ void resolve_packed(const ScanParams& p, const uint32
   uint64_t slot[kR];
   ulonglong2 e0[kR], e1[kR];
   bool pend[kR];
-  uint32_t res[kR];
 #pragma unroll
   for (int j = 0; j < kR; ++j) {
     gid[j] = kNoGid;
-    res[j] = kNoGid;
     pend[j] = sel[j];
     slot[j] = 0;
     if (pend[j] && kw[j] == kEmpty) {
@@ -470,30 +470,28 @@ __device__ __forceinline__ void resolve_packed(const ScanParams& p, const uint32
             gid[j] = (uint32_t)e.y;
             pend[j] = false;
           }
-          break;  // a torn read of a fresh claim: look at this entry again
+          break;  // claimed, not yet published: look at this entry again
         }
         if (e.x == kEmpty) {
-          // A record reserved for a claim that lost its race is kept for this
-          // row's next attempt; one never used stays all-zero (a hole).
-          if (res[j] == kNoGid) res[j] = reserve_record(p, cs);
-          if (res[j] == kNoGid) {
+          // Two steps: a CAS of the key word claims the entry, then the
+          // winner reserves a record and publishes it in the meta word.  Only
+          // winners reserve, so no record is left unused.  Rows that find the
+          // key unpublished read the entry again next round (no waiting here).
+          KeyEntry* en = p.table + s;
+          const unsigned long long prev = atomicCAS(&en->key, kEmpty, kw[j]);
+          if (prev == kEmpty) {
+            const uint32_t g = reserve_record(p, cs);
+            if (g != kNoGid) {
+              claimed(p, g, kw[j], rows[j]);
+              atomicExch(&en->meta, (unsigned long long)g | ((unsigned long long)rows[j] << 32));
+              gid[j] = g;
+            }
             pend[j] = false;
             break;
           }
-          uint64_t ok, om;
-          cas128(p.table + s, kEmpty, kEmpty, kw[j], (uint64_t)res[j] | ((uint64_t)rows[j] << 32), ok, om);
-          if (ok == kEmpty && om == kEmpty) {
-            claimed(p, res[j], kw[j], rows[j]);
-            gid[j] = res[j];
-            pend[j] = false;
-          } else if (ok == kw[j]) {
-            gid[j] = (uint32_t)om;
-            pend[j] = false;
-          } else {
-            step = h + 1;  // taken by another key: go on past it
-            continue;
-          }
-          break;
+          if (prev == kw[j]) break;  // another row's claim of this key: read it again
+          step = h + 1;              // taken by another key: go on past it
+          continue;
         }
         step = h + 1;
       }
@@ -508,39 +506,213 @@ __device__ __forceinline__ void resolve_packed(const ScanParams& p, const uint32
   for (int j = 0; j < kR; ++j) sel[j] = sel[j] && gid[j] != kNoGid;
 }
 
+// Thread-block cluster helpers.
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_ranks() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_index() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+  return r;
+}
+// Every thread of every CTA of the cluster; release/acquire at cluster scope
+// orders the CTAs' global-memory work on the shared table across phases.
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ uint32_t ld_cluster_u32(const void* local, uint32_t rank) {
+  uint32_t a, v;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(local)), "r"(rank));
+  asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
+  return v;
+}
+
 // ---------------------------------------------------------------------------
 // 4'. Shared-memory regime (few groups): each CTA keeps its own key table and
-// all-zero group records in shared memory; duplicate keys inside a warp are
-// collapsed with __match_any_sync so one leader lane applies the combined
-// update; the CTA's records are merged into the global table when it exits.
-// Rows whose key finds no room in the CTA table take the global path.
+// all-zero group records in shared memory -- or, with smem_cluster > 1, the
+// CTAs of a thread-block cluster pool their tables into one, each key living
+// in one CTA's share and reached through distributed shared memory; duplicate
+// keys inside a warp are collapsed with __match_any_sync so one leader lane
+// applies the combined update; each CTA merges its share into the global
+// table when the cluster is done.  Rows whose key finds no room take the
+// global path.
 // ---------------------------------------------------------------------------
 struct SmemTable {
   unsigned long long* keys;  // smem_slots, kEmpty = free
   unsigned char* recs;       // smem_slots records of rec_stride bytes
   uint32_t* used;            // claimed slots
+  uint32_t ranks;            // CTAs sharing the table (power of two)
 };
 
-__device__ __forceinline__ int smem_probe(const ScanParams& p, const SmemTable& st, uint64_t kw) {
-  if (kw == kEmpty) return -1;
+// A group record of a shared-memory table as group_update sees it: in this
+// CTA's own table (generic address, native atomics) or in a cluster table
+// (the owner CTA's record as a .shared::cluster address, explicit-space
+// atomics).  On B200 a native 64-bit atomic maximum through a generic address
+// into another CTA's shared memory lost updates in this library's tests, so
+// cluster records raise 64-bit maxima by compare-and-swap.
+struct OwnRec {
+  unsigned char* p;
+  __device__ __forceinline__ void max_u32(int off, uint32_t v) const { atomicMax(reinterpret_cast<uint32_t*>(p + off), v); }
+  __device__ __forceinline__ void add_u32(int off, uint32_t v) const { atomicAdd(reinterpret_cast<uint32_t*>(p + off), v); }
+  __device__ __forceinline__ void or_u32(int off, uint32_t v) const { atomicOr(reinterpret_cast<uint32_t*>(p + off), v); }
+  __device__ __forceinline__ uint64_t add_u64(int off, uint64_t v) const {
+    return atomicAdd(reinterpret_cast<unsigned long long*>(p + off), (unsigned long long)v);
+  }
+  __device__ __forceinline__ void add_f64(int off, double v) const { atomicAdd(reinterpret_cast<double*>(p + off), v); }
+  __device__ __forceinline__ uint64_t ld_u64(int off) const {
+    return *reinterpret_cast<const volatile unsigned long long*>(p + off);
+  }
+  __device__ __forceinline__ uint64_t cas_u64(int off, uint64_t cmp, uint64_t val) const {
+    return atomicCAS(reinterpret_cast<unsigned long long*>(p + off), (unsigned long long)cmp, (unsigned long long)val);
+  }
+  __device__ __forceinline__ bool max_u64(int off, uint64_t v) const {
+    atomicMax(reinterpret_cast<unsigned long long*>(p + off), (unsigned long long)v);
+    return true;
+  }
+};
+
+struct ClusterRec {
+  uint32_t a;
+  __device__ __forceinline__ void max_u32(int off, uint32_t v) const { dsm_max_u32(a + off, v); }
+  __device__ __forceinline__ void add_u32(int off, uint32_t v) const { dsm_add_u32(a + off, v); }
+  __device__ __forceinline__ void or_u32(int off, uint32_t v) const { dsm_or_b32(a + off, v); }
+  __device__ __forceinline__ uint64_t add_u64(int off, uint64_t v) const { return dsm_add_u64(a + off, v); }
+  __device__ __forceinline__ void add_f64(int off, double v) const { dsm_add_f64(a + off, v); }
+  __device__ __forceinline__ uint64_t ld_u64(int off) const { return dsm_ld_u64(a + off); }
+  __device__ __forceinline__ uint64_t cas_u64(int off, uint64_t cmp, uint64_t val) const {
+    return dsm_cas_u64(a + off, cmp, val);
+  }
+  // False when the retries ran out.
+  __device__ __forceinline__ bool max_u64(int off, uint64_t v) const {
+    uint64_t old = dsm_ld_u64(a + off);
+    for (uint32_t i = 0; i < kSpinLimit; ++i) {
+      if (old >= v) return true;
+      const uint64_t seen = dsm_cas_u64(a + off, old, v);
+      if (seen == old) return true;
+      old = seen;
+    }
+    return false;
+  }
+};
+
+// The record of key word `kw` in this CTA's own table (claimed if new);
+// false when the key is absent and the table is three-quarters full.
+__device__ __forceinline__ bool smem_probe(const ScanParams& p, const SmemTable& st, uint64_t kw, OwnRec& rec) {
+  if (kw == kEmpty) return false;
   const uint32_t mask = p.smem_slots - 1;
   uint32_t s = (uint32_t)mix64(kw ^ 0x9FB21C651E98DF25ull) & mask;
   for (int probe = 0; probe < 32; ++probe) {
-    const unsigned long long k = st.keys[s];
-    if (k == kw) return (int)s;
-    if (k == kEmpty) {
+    const unsigned long long k = *reinterpret_cast<volatile unsigned long long*>(&st.keys[s]);
+    bool hit = k == kw;
+    if (!hit && k == kEmpty) {
       // At most three-quarters full, so probes stay short.
-      if (*(volatile uint32_t*)st.used >= p.smem_slots - p.smem_slots / 4) return -1;
+      if (*reinterpret_cast<volatile uint32_t*>(st.used) >= p.smem_slots - p.smem_slots / 4) return false;
       const unsigned long long prev = atomicCAS(&st.keys[s], kEmpty, kw);
-      if (prev == kEmpty) {
-        atomicAdd(st.used, 1u);
-        return (int)s;
-      }
-      if (prev == kw) return (int)s;
+      if (prev == kEmpty) atomicAdd(st.used, 1u);
+      hit = prev == kEmpty || prev == kw;
+    }
+    if (hit) {
+      rec.p = st.recs + (size_t)s * p.rec_stride;
+      return true;
     }
     s = (s + 1) & mask;
   }
-  return -1;
+  return false;
+}
+
+// The same in a cluster table: the hash's high bits pick the owner CTA, its
+// low bits the first slot of the owner's share; probes stay inside the share
+// and the fill limit is the owner's.
+__device__ __forceinline__ bool smem_probe(const ScanParams& p, const SmemTable& st, uint64_t kw, ClusterRec& rec) {
+  if (kw == kEmpty) return false;
+  const uint64_t h = mix64(kw ^ 0x9FB21C651E98DF25ull);
+  const uint32_t r = (uint32_t)(h >> 40) & (st.ranks - 1);
+  const uint32_t keys = dsm_map(st.keys, r), recs = dsm_map(st.recs, r), used = dsm_map(st.used, r);
+  const uint32_t mask = p.smem_slots - 1;
+  uint32_t s = (uint32_t)h & mask;
+  for (int probe = 0; probe < 32; ++probe) {
+    const uint64_t k = dsm_ld_u64(keys + s * 8u);
+    bool hit = k == kw;
+    if (!hit && k == kEmpty) {
+      if (dsm_ld_u32(used) >= p.smem_slots - p.smem_slots / 4) return false;
+      const uint64_t prev = dsm_cas_u64(keys + s * 8u, kEmpty, kw);
+      if (prev == kEmpty) dsm_add_u32(used, 1u);
+      hit = prev == kEmpty || prev == kw;
+    }
+    if (hit) {
+      rec.a = recs + s * (uint32_t)p.rec_stride;
+      return true;
+    }
+    s = (s + 1) & mask;
+  }
+  return false;
+}
+
+// Compensated FP32 pairs {s, c} (Neumaier's variant of Kahan summation; the
+// value is s + c): `x` with its low part `xc` added to the pair.  A sum that
+// leaves the FP32 range from finite operands sets `range` (the host reruns
+// the query in FP64); non-finite sums keep the compensation unchanged, so
+// +-inf and NaN propagate through s alone.
+__device__ __forceinline__ void pair_add(float& s, float& c, float x, float xc, bool& range) {
+  const float t = s + x;
+  if (isfinite(t)) {
+    const float e = fabsf(s) >= fabsf(x) ? (s - t) + x : (x - t) + s;
+    c += e + xc;
+  } else if (isfinite(s) && isfinite(x)) {
+    range = true;
+  }
+  s = t;
+}
+
+// The pair sum of each lane's group (members in lane order), as group_reduce.
+__device__ __forceinline__ void group_pair(uint32_t grp, int maxpop, float ms, float mc, bool take, float& s, float& c,
+                                           bool& range) {
+  s = 0.f;
+  c = 0.f;
+  uint32_t left = grp;
+  const int lane = threadIdx.x & 31;
+  for (int i = 0; i < maxpop; ++i) {
+    const int src = left ? __ffs(left) - 1 : lane;
+    const float vs = __shfl_sync(0xffffffffu, take ? ms : 0.f, src);
+    const float vc = __shfl_sync(0xffffffffu, take ? mc : 0.f, src);
+    if (left) {
+      pair_add(s, c, vs, vc, range);
+      left &= left - 1;
+    }
+  }
+}
+
+// Adds {x, xc} to the pair at byte `off` of a record by compare-and-swap;
+// false when the retries ran out.
+template <typename Rec>
+__device__ __forceinline__ bool pair_cas_add(const Rec& rec, int off, float x, float xc, bool& range) {
+  uint64_t old = rec.ld_u64(off);
+  for (uint32_t i = 0; i < kSpinLimit; ++i) {
+    float s = __uint_as_float((uint32_t)old), c = __uint_as_float((uint32_t)(old >> 32));
+    bool r = false;
+    pair_add(s, c, x, xc, r);
+    const uint64_t nw = ((uint64_t)__float_as_uint(c) << 32) | __float_as_uint(s);
+    const uint64_t seen = rec.cas_u64(off, old, nw);
+    if (seen == old) {
+      range = range || r;
+      return true;
+    }
+    old = seen;
+  }
+  return false;
+}
+
+// The FP64 value of a pair (s alone when it is not finite).
+__device__ __forceinline__ double pair_value(const unsigned char* at) {
+  const float s = *reinterpret_cast<const float*>(at), c = *reinterpret_cast<const float*>(at + 4);
+  return isfinite(s) ? (double)s + (double)c : (double)s;
 }
 
 // The lane holding the i-th member of `grp` (lanes outside return their own).
@@ -570,10 +742,10 @@ __device__ __forceinline__ V group_reduce(uint32_t grp, int maxpop, V mine, V id
 // reduced across lanes: `grp` the lanes sharing this lane's record `rec` (0
 // for a lane outside), `maxpop` the largest group in the warp.  The group's
 // lowest lane (the leader) applies one atomic per field.  `get(v, ok, b)`
-// gives the lane's validity and raw bits of value column v.  Works on shared
-// or global records (generic addresses).
-template <typename Get>
-__device__ __forceinline__ void group_update(const ScanParams& p, unsigned char* rec, uint32_t grp, int maxpop, bool loc,
+// gives the lane's validity and raw bits of value column v.  `Rec`: OwnRec or
+// ClusterRec.
+template <typename Rec, typename Get>
+__device__ __forceinline__ void group_update(const ScanParams& p, const Rec& rec, uint32_t grp, int maxpop, bool loc,
                                              uint32_t row, Get&& get) {
   const int lane = threadIdx.x & 31;
   {
@@ -583,8 +755,8 @@ __device__ __forceinline__ void group_update(const ScanParams& p, unsigned char*
     const uint32_t first =
         group_reduce<uint32_t>(grp, maxpop, row, 0xFFFFFFFFu, loc, [](uint32_t a, uint32_t b2) { return a < b2 ? a : b2; });
     if (leader) {
-      atomicMax(reinterpret_cast<uint32_t*>(rec + kRecFirst), ~first);
-      if (p.off_len >= 0) atomicAdd(reinterpret_cast<uint32_t*>(rec + p.off_len), (uint32_t)__popc(grp));
+      rec.max_u32(kRecFirst, ~first);
+      if (p.off_len >= 0) rec.add_u32(p.off_len, (uint32_t)__popc(grp));
     }
     for (int v = 0; v < p.n_vals; ++v) {
       const ValField& f = p.vals[v];
@@ -600,11 +772,17 @@ __device__ __forceinline__ void group_update(const ScanParams& p, unsigned char*
       const uint32_t nanmask = grp & __ballot_sync(0xffffffffu, nan);
       const uint32_t pz = grp & __ballot_sync(0xffffffffu, ok && isf && xd == 0.0 && __double_as_longlong(xd) >= 0);
       const uint32_t nz = grp & __ballot_sync(0xffffffffu, ok && isf && xd == 0.0 && __double_as_longlong(xd) < 0);
-      if (leader && vmask) atomicAdd(reinterpret_cast<uint32_t*>(rec + f.off_count), (uint32_t)__popc(vmask));
+      if (leader && vmask) rec.add_u32(f.off_count, (uint32_t)__popc(vmask));
+      const bool comp = (p.comp_mask >> v) & 1u;
+      bool range = false, stuck = false;
       if (f.off_sum >= 0) {
-        if (f.sum_kind == SUM_F64) {
+        if (comp) {
+          float ps, pc;
+          group_pair(grp, maxpop, (float)xd, 0.f, ok, ps, pc, range);
+          if (leader && vmask) stuck = !pair_cas_add(rec, f.off_sum, ps, pc, range);
+        } else if (f.sum_kind == SUM_F64) {
           const double sm = group_reduce<double>(grp, maxpop, xd, 0.0, ok, [](double a, double b2) { return a + b2; });
-          if (leader && vmask) atomicAdd(reinterpret_cast<double*>(rec + f.off_sum), sm);
+          if (leader && vmask) rec.add_f64(f.off_sum, sm);
         } else {
           // The group's partial sum, exact in 128 bits.
           const bool uns = dt == DFC_UINT64;
@@ -623,12 +801,12 @@ __device__ __forceinline__ void group_update(const ScanParams& p, unsigned char*
           }
           if (leader && vmask) {
             if (f.sum_kind == SUM_I64) {
-              atomicAdd(reinterpret_cast<unsigned long long*>(rec + f.off_sum), (unsigned long long)(long long)exact);
+              rec.add_u64(f.off_sum, (uint64_t)(int64_t)exact);
             } else {
               const uint64_t add_lo = (uint64_t)exact, add_hi = (uint64_t)(exact >> 64);
-              const uint64_t old = atomicAdd(reinterpret_cast<unsigned long long*>(rec + f.off_sum), add_lo);
+              const uint64_t old = rec.add_u64(f.off_sum, add_lo);
               const uint64_t hi_add = add_hi + ((old + add_lo) < old ? 1ull : 0ull);
-              if (hi_add) atomicAdd(reinterpret_cast<unsigned long long*>(rec + f.off_sum + 8), hi_add);
+              if (hi_add) rec.add_u64(f.off_sum + 8, hi_add);
             }
           }
         }
@@ -639,19 +817,19 @@ __device__ __forceinline__ void group_update(const ScanParams& p, unsigned char*
         if (f.off_min >= 0) {
           const unsigned long long m = group_reduce<unsigned long long>(
               grp, maxpop, ~e, 0ull, ordinary, [](unsigned long long a, unsigned long long b2) { return a > b2 ? a : b2; });
-          if (leader && m) atomicMax(reinterpret_cast<unsigned long long*>(rec + f.off_min), m);
+          if (leader && m && !rec.max_u64(f.off_min, m)) stuck = true;
         }
         if (f.off_max >= 0) {
           const unsigned long long m = group_reduce<unsigned long long>(
               grp, maxpop, e, 0ull, ordinary, [](unsigned long long a, unsigned long long b2) { return a > b2 ? a : b2; });
-          if (leader && m) atomicMax(reinterpret_cast<unsigned long long*>(rec + f.off_max), m);
+          if (leader && m && !rec.max_u64(f.off_max, m)) stuck = true;
         }
         if (leader) {
           uint32_t bits = 0;
           if (nanmask) bits |= 1u << (3 * v);
           if (pz) bits |= 1u << (3 * v + 1);
           if (nz) bits |= 1u << (3 * v + 2);
-          if (bits) atomicOr(reinterpret_cast<uint32_t*>(rec + kRecFlags), bits);
+          if (bits) rec.or_u32(kRecFlags, bits);
         }
       }
       if (f.off_m2 >= 0) {
@@ -660,33 +838,51 @@ __device__ __forceinline__ void group_update(const ScanParams& p, unsigned char*
         const uint64_t cand = __shfl_sync(0xffffffffu, xbits, vmask ? __ffs(vmask) - 1 : lane);
         uint64_t ks = 0;
         if (leader && vmask) {
-          ks = *reinterpret_cast<volatile unsigned long long*>(rec + f.off_shift);
+          ks = rec.ld_u64(f.off_shift);
           if (ks == 0) {
-            const uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long*>(rec + f.off_shift), 0ull, cand ^ kShiftTag);
+            const uint64_t prev = rec.cas_u64(f.off_shift, 0ull, cand ^ kShiftTag);
             ks = prev == 0 ? (cand ^ kShiftTag) : prev;
           }
         }
         ks = __shfl_sync(0xffffffffu, ks, grp ? __ffs(grp) - 1 : lane);
-        const double d = xd - __longlong_as_double((long long)(ks ^ kShiftTag));
-        const double s2 = group_reduce<double>(grp, maxpop, d * d, 0.0, ok, [](double a, double b2) { return a + b2; });
-        if (leader && vmask) atomicAdd(reinterpret_cast<double*>(rec + f.off_m2), s2);
+        const double kd = __longlong_as_double((long long)(ks ^ kShiftTag));
+        if (comp) {
+          // d = x - K exactly as dh + dl (Knuth's TwoSum; K is a Float32 value),
+          // d^2 as dh^2 (rounded) + its FMA residue + 2 dh dl.
+          const float xf = (float)xd, kf = (float)kd;
+          const float dh = xf - kf;
+          const float bb = dh - xf;
+          const float dl = (xf - (dh - bb)) + (-kf - bb);
+          const float sq = dh * dh;
+          const float sq_lo = fmaf(2.f * dh, dl, fmaf(dh, dh, -sq));
+          if (ok && isfinite(xf) && isfinite(kf) && !isfinite(sq)) range = true;
+          float ps, pc;
+          group_pair(grp, maxpop, sq, isfinite(sq) ? sq_lo : 0.f, ok, ps, pc, range);
+          if (leader && vmask && !stuck) stuck = !pair_cas_add(rec, f.off_m2, ps, pc, range);
+        } else {
+          const double d = xd - kd;
+          const double s2 = group_reduce<double>(grp, maxpop, d * d, 0.0, ok, [](double a, double b2) { return a + b2; });
+          if (leader && vmask) rec.add_f64(f.off_m2, s2);
+        }
       }
+      if (range) atomicOr(p.status, ST_F32_RANGE);
+      if (stuck) atomicOr(p.status, ST_TIMEOUT);
     }
   }
 }
 
-__device__ __forceinline__ void smem_rows(const ScanParams& p, const Step& s, const SmemTable& st,
-                                          const RowRef (&x)[kR], const uint32_t (&rows)[kR], bool (&sel)[kR],
-                                          const uint64_t (&kw)[kR]) {
+template <typename Rec>
+__device__ __forceinline__ void smem_rows_in(const ScanParams& p, const Step& s, const SmemTable& st,
+                                             const RowRef (&x)[kR], const uint32_t (&rows)[kR], bool (&sel)[kR],
+                                             const uint64_t (&kw)[kR]) {
 #pragma unroll
   for (int j = 0; j < kR; ++j) {
-    const int ls = sel[j] ? smem_probe(p, st, kw[j]) : -1;
-    const bool loc = ls >= 0;
+    Rec rec{};
+    const bool loc = sel[j] && smem_probe(p, st, kw[j], rec);
     uint32_t grp = __match_any_sync(0xffffffffu, kw[j]) & __ballot_sync(0xffffffffu, loc);
     if (!loc) grp = 0;
     const int maxpop = __reduce_max_sync(0xffffffffu, (unsigned)__popc(grp));
     if (maxpop == 0) continue;
-    unsigned char* rec = loc ? st.recs + (size_t)ls * p.rec_stride : nullptr;
     group_update(p, rec, grp, maxpop, loc, rows[j], [&](int v, bool& ok, uint64_t& b) {
       const int c = p.vals[v].input;
       const ColRef cr = col_ref(p, s, c);
@@ -695,6 +891,13 @@ __device__ __forceinline__ void smem_rows(const ScanParams& p, const Step& s, co
     });
     sel[j] = sel[j] && !loc;  // the rest take the global path
   }
+}
+
+__device__ __forceinline__ void smem_rows(const ScanParams& p, const Step& s, const SmemTable& st,
+                                          const RowRef (&x)[kR], const uint32_t (&rows)[kR], bool (&sel)[kR],
+                                          const uint64_t (&kw)[kR]) {
+  if (st.ranks > 1) smem_rows_in<ClusterRec>(p, s, st, x, rows, sel, kw);
+  else smem_rows_in<OwnRec>(p, s, st, x, rows, sel, kw);
 }
 
 // Full-warp butterfly reductions (every lane gets the result).
@@ -931,7 +1134,7 @@ __device__ __forceinline__ void update_column(const ScanParams& p, const ValFiel
   update_rows<T>(p, f, v, recs, ok, vb);
 }
 
-__device__ void merge_record(const ScanParams& p, const unsigned char* src, uint64_t kw, ClaimState* cs);
+__device__ void merge_into(const ScanParams& p, const unsigned char* src, uint32_t gid);
 
 // One pass over up to kPassRows compacted rows of a step.
 __device__ __forceinline__ void consume_rows(const ScanParams& p, const Step& s, const uint16_t* idx, uint32_t nsel,
@@ -1088,7 +1291,7 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
     s_nsel[0] = s_nsel[1] = s_nsel[2] = 0;
   }
   if (threadIdx.x < kChunkRing) s_claim.ring[threadIdx.x] = ~0ull;
-  SmemTable st{nullptr, nullptr, &s_used};
+  SmemTable st{nullptr, nullptr, &s_used, p.smem_cluster > 1 ? p.smem_cluster : 1u};
   if (p.smem_slots) {
     st.keys = reinterpret_cast<unsigned long long*>(smem + p.smem_keys_off);
     st.recs = smem + p.smem_recs_off;
@@ -1098,6 +1301,8 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
     for (uint32_t i = threadIdx.x; i < n16; i += blockDim.x) recs[i] = make_uint4(0, 0, 0, 0);
   }
   __syncthreads();
+  // A cluster table: every share is initialised before any CTA probes it.
+  if (st.ranks > 1) cluster_sync_all();
 
   const uint64_t T = (uint64_t)p.tile_rows;
   if (warp == 0) {
@@ -1165,19 +1370,45 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
     }
   }
   __syncthreads();
+  // A cluster table: no CTA touches another's share after this barrier, so
+  // each merges its own share and may exit.
+  if (st.ranks > 1) cluster_sync_all();
   if (p.smem_slots && !s_abort) {
-    for (uint32_t s = threadIdx.x; s < p.smem_slots; s += blockDim.x)
-      if (st.keys[s] != kEmpty) merge_record(p, st.recs + (size_t)s * p.rec_stride, st.keys[s], &s_claim);
+    // The share's records find their global records through the same
+    // warp-synchronous claim rounds as the rows (packed keys only; no thread
+    // waits on another's claim).  Every thread runs the same passes, kR slots
+    // each; CTAs start at different slots (every table hashes a key to the
+    // same slot), so fewer of them meet on one global record at a time.
+    const uint32_t mask = p.smem_slots - 1;
+    const uint32_t rot = (uint32_t)mix64(blockIdx.x + 0x51ull) & mask;
+    const uint32_t per = blockDim.x * (uint32_t)kR;
+    for (uint32_t base = 0; base < p.smem_slots; base += per) {
+      uint32_t rows[kR], gid[kR], slot[kR];
+      uint64_t kw[kR];
+      bool sel[kR];
+#pragma unroll
+      for (int j = 0; j < kR; ++j) {
+        const uint32_t i = base + threadIdx.x + (uint32_t)j * blockDim.x;
+        slot[j] = (i + rot) & mask;
+        kw[j] = i < p.smem_slots ? st.keys[slot[j]] : kEmpty;
+        const uint32_t first_enc =
+            kw[j] != kEmpty ? *reinterpret_cast<const uint32_t*>(st.recs + (size_t)slot[j] * p.rec_stride + kRecFirst) : 0u;
+        sel[j] = first_enc != 0;
+        rows[j] = ~first_enc;
+      }
+      resolve_packed(p, rows, sel, kw, gid, &s_claim);
+#pragma unroll
+      for (int j = 0; j < kR; ++j)
+        if (sel[j]) merge_into(p, st.recs + (size_t)slot[j] * p.rec_stride, gid[j]);
+    }
   }
 }
 
-// Merges one CTA-table record into the global table (function.mojo:1559-1779
-// `combine`; the shifted square sums are re-centred on the global record's K).
-__device__ void merge_record(const ScanParams& p, const unsigned char* src, uint64_t kw, ClaimState* cs) {
+// Merges one shared-memory record into global record `gid` (function.mojo:
+// 1559-1779 `combine`; the shifted square sums are re-centred on the global
+// record's K; compensated FP32 pairs enter as FP64 values).
+__device__ void merge_into(const ScanParams& p, const unsigned char* src, uint32_t gid) {
   const uint32_t first_enc = *reinterpret_cast<const uint32_t*>(src + kRecFirst);
-  if (first_enc == 0) return;
-  const uint32_t gid = find_or_claim(p, kw, ~first_enc, cs);
-  if (gid == kNoGid) return;
   unsigned char* dst = record_at(p, gid);
   if (p.track_first) atomicMax(reinterpret_cast<uint32_t*>(dst + kRecFirst), first_enc);
   if (p.off_len >= 0) red_add_u32(dst + p.off_len, *reinterpret_cast<const uint32_t*>(src + p.off_len));
@@ -1196,8 +1427,11 @@ __device__ void merge_record(const ScanParams& p, const unsigned char* src, uint
     }
     if (n == 0) continue;
     red_add_u32(dst + f.off_count, n);
+    const bool comp = (p.comp_mask >> v) & 1u;
     if (f.off_sum >= 0) {
-      if (f.sum_kind == SUM_F64) {
+      if (comp) {
+        red_add_f64(dst + f.off_sum, pair_value(src + f.off_sum));
+      } else if (f.sum_kind == SUM_F64) {
         red_add_f64(dst + f.off_sum, *reinterpret_cast<const double*>(src + f.off_sum));
       } else if (f.sum_kind == SUM_I64) {
         red_add_u64(dst + f.off_sum, *reinterpret_cast<const uint64_t*>(src + f.off_sum));
@@ -1222,7 +1456,7 @@ __device__ void merge_record(const ScanParams& p, const unsigned char* src, uint
       const double dn = (double)n;
       double s1;
       if (dt_float(f.dtype)) {
-        s1 = *reinterpret_cast<const double*>(src + f.off_sum) - dn * kl;
+        s1 = (comp ? pair_value(src + f.off_sum) : *reinterpret_cast<const double*>(src + f.off_sum)) - dn * kl;
       } else {
         __int128 isum;
         if (f.sum_kind == SUM_I64) isum = (__int128)*reinterpret_cast<const long long*>(src + f.off_sum);
@@ -1231,7 +1465,7 @@ __device__ void merge_record(const ScanParams& p, const unsigned char* src, uint
         s1 = (double)(isum - (__int128)n * (__int128)kl);
       }
       const double d = kl - kg;
-      const double s2 = *reinterpret_cast<const double*>(src + f.off_m2);
+      const double s2 = comp ? pair_value(src + f.off_m2) : *reinterpret_cast<const double*>(src + f.off_m2);
       red_add_f64(dst + f.off_m2, d == 0.0 ? s2 : s2 + 2.0 * d * s1 + dn * d * d);
     }
   }
@@ -1283,33 +1517,6 @@ __device__ __forceinline__ uint32_t partition_of(const ScanParams& p, uint64_t k
 __device__ __forceinline__ void raise_capacity(const ScanParams& p, uint32_t what) {
   atomicOr(p.status, ST_CAPACITY);
   atomicOr(p.status + 1, what);
-}
-
-__device__ __forceinline__ uint32_t cluster_rank() {
-  uint32_t r;
-  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ uint32_t cluster_ranks() {
-  uint32_t r;
-  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ uint32_t cluster_index() {
-  uint32_t r;
-  asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
-  return r;
-}
-// Every thread of every CTA of the cluster; release/acquire at cluster scope
-// orders the CTAs' global-memory work on the shared table across phases.
-__device__ __forceinline__ void cluster_sync_all() {
-  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-__device__ __forceinline__ uint32_t ld_cluster_u32(const void* local, uint32_t rank) {
-  uint32_t a, v;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(local)), "r"(rank));
-  asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
-  return v;
 }
 
 // Exclusive prefix of one value per consumer thread (512 threads) and the

@@ -96,13 +96,22 @@ _REGIMES = {"": 0, "auto": 0, "global": N.Q_FORCE_GLOBAL, "shared": N.Q_FORCE_SH
             "partitioned": N.Q_FORCE_PARTITIONED}
 
 
+_FLOAT32 = {"": 0, "fp64": 0, "compensated": N.Q_FLOAT32_COMPENSATED}
+
+
 def _regime_flags() -> int:
     """DATAFRAME_ACCEL_REGIME: auto (default; chosen from the estimated group
-    count), global, shared or partitioned.  A bad value raises."""
+    count), global, shared or partitioned.  DATAFRAME_ACCEL_FLOAT32: fp64
+    (default; Float32 sums and variances accumulate in FP64) or compensated
+    (compensated FP32 partials in the shared-memory tables, merged in FP64).
+    A bad value raises."""
     raw = os.environ.get("DATAFRAME_ACCEL_REGIME", "").strip().lower()
     if raw not in _REGIMES:
         raise ValueError(f"DATAFRAME_ACCEL_REGIME={raw!r} is not one of auto, global, shared, partitioned")
-    return _REGIMES[raw]
+    f32 = os.environ.get("DATAFRAME_ACCEL_FLOAT32", "").strip().lower()
+    if f32 not in _FLOAT32:
+        raise ValueError(f"DATAFRAME_ACCEL_FLOAT32={f32!r} is not one of fp64, compensated")
+    return _REGIMES[raw] | _FLOAT32[f32]
 
 
 # ---------------------------------------------------------------------------
@@ -353,6 +362,8 @@ def last_timings() -> dict:
         "launches": int(t.launches),
         "partitions": int(t.partitions),
         "aggregate_ns": t.aggregate_ns,
+        "cluster_ctas": int(t.cluster_ctas),
+        "compensated": int(t.compensated),
     }
 
 

@@ -203,7 +203,8 @@ typedef struct dfc_agg {
 #define DFC_Q_MAINTAIN_ORDER 1u    /* groups in first-occurrence order of the rows the filter kept */
 #define DFC_Q_FORCE_GLOBAL 2u      /* skip the shared-memory table regime */
 #define DFC_Q_FORCE_SHARED 4u      /* use the shared-memory table regime regardless of estimates */
-#define DFC_Q_FLOAT32_FP64 8u      /* Float32 values: plain FP64 accumulation instead of compensated FP32 */
+#define DFC_Q_FLOAT32_COMPENSATED 8u /* Float32 sums and variances: compensated FP32 partials in the shared-memory
+                                        tables, merged in FP64 (default: FP64 accumulation throughout) */
 #define DFC_Q_FORCE_PARTITIONED 16u /* use the radix-partitioned regime regardless of estimates (keys <= 64 bits) */
 
 typedef struct dfc_query {
@@ -384,6 +385,8 @@ typedef struct dfc_timings {
   int32_t launches; /* kernels this library launched for the query */
   int32_t partitions;  /* radix-partitioned regime: partitions (else 0) */
   double aggregate_ns; /* radix-partitioned regime: the per-partition aggregation pass (scan_ns: the partition pass) */
+  int32_t cluster_ctas; /* shared-memory regime: CTAs pooling one table (1: each CTA its own) */
+  int32_t compensated;  /* value fields accumulated as compensated FP32 partials (bit per field) */
 } dfc_timings;
 DFC_API dfc_status dfc_last_timings(dfc_timings* out);
 

@@ -98,6 +98,12 @@ def test_regime_setting(monkeypatch):
     monkeypatch.setenv("DATAFRAME_ACCEL_REGIME", "radix")
     with pytest.raises(ValueError):
         provider._regime_flags()
+    monkeypatch.setenv("DATAFRAME_ACCEL_REGIME", "shared")
+    monkeypatch.setenv("DATAFRAME_ACCEL_FLOAT32", "compensated")
+    assert provider._regime_flags() == N.Q_FORCE_SHARED | N.Q_FLOAT32_COMPENSATED
+    monkeypatch.setenv("DATAFRAME_ACCEL_FLOAT32", "fp32")
+    with pytest.raises(ValueError):
+        provider._regime_flags()
 
 
 def test_cpu_engine_is_not_part_of_the_provider():

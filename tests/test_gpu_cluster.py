@@ -1,0 +1,230 @@
+"""Shared-memory tables pooled over a thread-block cluster, and compensated
+FP32 partials, against the CPU oracle through the C ABI.
+
+A cluster table spreads one key table over the shared memory of 2..16 CTAs
+(distributed shared memory), so queries with up to 32K groups keep their
+groups on chip.  Integers, keys, nulls and group order are bit-exact, as in
+the other parity tests.  Float tolerances:
+  * FP64 accumulation (the default): the reference's budgets, SUM_RTOL of
+    the summands' magnitude and VAR_RTOL (test_gpu_parity);
+  * compensated FP32 partials (Neumaier's summation in FP32 pairs {s, c},
+    merged in FP64): the pair's error is O(n u^2) sum |x| with u = 2^-24,
+    written here as COMP_SUM_RTOL = 1e-9 of sum |x| for sums and means and
+    COMP_VAR_RTOL = 1e-8 relative for variances.
+"""
+import numpy as np
+import pytest
+
+import test_gpu_parity
+from dataframe_mojo_b200 import provider
+from dataframe_mojo_b200.frame import DataFrame, Series, col
+from test_gpu_parity import DTYPES, compare_with_oracle, magnitude, random_frame, run_device
+
+pytestmark = pytest.mark.gpu
+
+COMP_SUM_RTOL = 1e-9
+COMP_VAR_RTOL = 1e-8
+
+
+def wide_frame(rng, rows, groups, null_rate=0.05):
+    """Int32 keys over `groups` values (a few null), Float32 values with
+    log-uniform magnitudes in [1e-6, 1e6] and random signs, Int64 values."""
+    keys = rng.integers(0, groups, rows).astype(np.int32)
+    mags = 10.0 ** rng.uniform(-6, 6, rows)
+    f = (np.where(rng.random(rows) < 0.5, -1.0, 1.0) * mags).astype(np.float32)
+    i = rng.integers(-10**6, 10**6, rows, dtype=np.int64)
+    return DataFrame([
+        Series("k", keys, rng.random(rows) >= 0.001),
+        Series("f", f, rng.random(rows) >= null_rate),
+        Series("i", i, rng.random(rows) >= null_rate),
+        Series("p", rng.integers(0, 100, rows, dtype=np.int32)),
+    ])
+
+
+def wide_plan(frame, maintain_order=True):
+    f, i = col("f"), col("i")
+    return frame.lazy().filter(col("p") < 90).group_by("k", maintain_order=maintain_order).agg([
+        f.sum().alias("fs"), f.mean().alias("fm"), f.var().alias("fv"), f.std(ddof=0).alias("fsd"),
+        f.min().alias("flo"), f.max().alias("fhi"), f.count().alias("fn"),
+        i.sum().alias("is"), i.mean().alias("im"), i.var().alias("iv"), i.min().alias("ilo"), i.max().alias("ihi"),
+        i.count().alias("in"), i.len().alias("len"), i.null_count().alias("inul"),
+    ])
+
+
+def wide_scales(ref):
+    fs, fm = magnitude(ref, "fn", "flo", "fhi")
+    _, im = magnitude(ref, "in", "ilo", "ihi")
+    return {"fs": fs, "fm": fm, "im": im}
+
+
+def check_wide(frame, label, maintain_order=True):
+    return compare_with_oracle(wide_plan(frame, maintain_order), label, float_cols=("fs", "fm", "im"),
+                               var_cols=("fv", "fsd", "iv"), scales=wide_scales)
+
+
+def test_cluster_table_for_ten_thousand_groups(monkeypatch):
+    monkeypatch.setenv("DATAFRAME_ACCEL_REGIME", "shared")
+    rng = np.random.default_rng(31)
+    frame = wide_frame(rng, 400_000, 10_000)
+    dev, _ = check_wide(frame, "cluster-shared")
+    t = provider.last_timings()
+    assert t["regime"] == 1 and t["cluster_ctas"] > 1, t
+    assert t["retries"] == 0, t
+    assert dev.height > 9_000
+
+
+def test_ten_thousand_groups_take_the_global_table_in_fp64():
+    rng = np.random.default_rng(32)
+    frame = wide_frame(rng, 400_000, 10_000)
+    check_wide(frame, "fp64-auto")
+    t = provider.last_timings()
+    assert t["regime"] == 0 and t["retries"] == 0, t
+
+
+@pytest.mark.parametrize("ranks", [2, 4, 8, 16])
+def test_cluster_sizes(ranks, monkeypatch):
+    monkeypatch.setenv("DFC_SMEM_CLUSTER", str(ranks))
+    rng = np.random.default_rng(40 + ranks)
+    frame = wide_frame(rng, 200_000, 1_000)  # a two-CTA table of 128-byte records holds this many
+    check_wide(frame, f"cluster-{ranks}")
+    t = provider.last_timings()
+    assert t["regime"] == 1 and t["cluster_ctas"] == ranks, t
+
+
+def test_cluster_table_hot_keys(monkeypatch):
+    """Zipf keys: a few groups take most rows (warp collapse and shared
+    records under contention across the cluster)."""
+    monkeypatch.setenv("DFC_SMEM_CLUSTER", "16")
+    rng = np.random.default_rng(33)
+    rows = 300_000
+    keys = np.minimum(rng.zipf(1.2, rows), 8_000).astype(np.int32)
+    frame = wide_frame(rng, rows, 8_000)
+    frame = DataFrame([Series("k", keys)] + [frame[c] for c in ("f", "i", "p")])
+    check_wide(frame, "cluster-zipf")
+    assert provider.last_timings()["cluster_ctas"] == 16
+
+
+def test_cluster_table_overflow_takes_global_path(monkeypatch):
+    """A cluster table far too small for the groups: rows whose share is full
+    take the global table; results unchanged."""
+    monkeypatch.setenv("DFC_SMEM_CLUSTER", "2")
+    monkeypatch.setenv("DFC_GROUPS_ESTIMATE", "500")
+    rng = np.random.default_rng(34)
+    frame = wide_frame(rng, 200_000, 20_000)
+    check_wide(frame, "cluster-overflow")
+    assert provider.last_timings()["cluster_ctas"] == 2
+
+
+@pytest.fixture
+def compensated(monkeypatch):
+    monkeypatch.setenv("DATAFRAME_ACCEL_FLOAT32", "compensated")
+    monkeypatch.setattr(test_gpu_parity, "SUM_RTOL", COMP_SUM_RTOL)
+    monkeypatch.setattr(test_gpu_parity, "VAR_RTOL", COMP_VAR_RTOL)
+
+
+def test_compensated_cluster_against_oracle(compensated):
+    rng = np.random.default_rng(35)
+    frame = wide_frame(rng, 400_000, 10_000)
+    check_wide(frame, "compensated-cluster")
+    t = provider.last_timings()
+    assert t["cluster_ctas"] > 1 and t["compensated"] != 0, t
+
+
+def test_compensated_own_tables_against_oracle(compensated):
+    rng = np.random.default_rng(36)
+    frame = wide_frame(rng, 300_000, 300)
+    check_wide(frame, "compensated-own")
+    t = provider.last_timings()
+    assert t["cluster_ctas"] == 1 and t["compensated"] != 0, t
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_compensated_random_dtypes(seed, compensated, monkeypatch):
+    monkeypatch.setenv("DATAFRAME_ACCEL_REGIME", "shared")
+    rng = np.random.default_rng(2000 + seed)
+    nk = 1 + seed % 2
+    key_dtypes = [DTYPES[(seed * 3 + i) % 8] for i in range(nk)]  # integer keys
+    val_dtypes = [np.float32, DTYPES[(seed * 5) % len(DTYPES)]]
+    rows = int(rng.integers(1, 80_000))
+    frame = random_frame(rng, rows, key_dtypes, val_dtypes, null_rate=0.1 if seed % 2 else 0.0)
+    aggs, floats, vars_ = [], [], []
+    for i, dt in enumerate(val_dtypes):
+        v = col(f"v{i}")
+        aggs += [v.sum().alias(f"s{i}"), v.count().alias(f"n{i}"), v.min().alias(f"lo{i}"), v.max().alias(f"hi{i}"),
+                 v.mean().alias(f"m{i}"), v.var().alias(f"var{i}"), v.std(ddof=0).alias(f"sd{i}")]
+        floats.append(f"m{i}")
+        vars_ += [f"var{i}", f"sd{i}"]
+        if np.dtype(dt).kind == "f":
+            floats.append(f"s{i}")
+    plan = frame.lazy().filter(col("p") >= 5).group_by([f"k{i}" for i in range(nk)], maintain_order=True).agg(aggs)
+
+    def scales(ref):
+        out = {}
+        for i in range(len(val_dtypes)):
+            out[f"s{i}"], out[f"m{i}"] = magnitude(ref, f"n{i}", f"lo{i}", f"hi{i}")
+        return out
+
+    try:
+        compare_with_oracle(plan, f"compensated-random{seed}", float_cols=floats, var_cols=vars_, scales=scales)
+    except provider.DataFaultError:
+        pytest.skip("moments adjudicated by the CPU (data fault)")
+
+
+def test_compensated_out_of_range_reruns_in_fp64(compensated):
+    """Float32 values near the top of the FP32 range: their partial sums leave
+    it, the kernel flags the query and the host reruns it in FP64."""
+    rows = 4096
+    keys = (np.arange(rows) % 4).astype(np.int32)
+    vals = np.full(rows, 3.0e38, np.float32)
+    frame = DataFrame([Series("k", keys), Series("v", vals)])
+    out = run_device(frame.lazy().group_by("k", maintain_order=True).agg(
+        [col("v").sum().alias("s"), col("v").var().alias("var")]))
+    assert np.allclose(out["s"].values, 1024 * float(np.float32(3.0e38)), rtol=1e-12)
+    assert np.all(out["var"].values == 0.0)
+    t = provider.last_timings()
+    assert t["retries"] >= 1 and t["compensated"] == 0, t
+
+
+def exact_groups(keys, vals):
+    """Per-group keys, sums, variances (ddof 1), sums of |x| and counts in
+    extended precision (np.longdouble)."""
+    order = np.argsort(keys, kind="stable")
+    k, x = keys[order], vals[order].astype(np.longdouble)
+    starts = np.flatnonzero(np.r_[True, k[1:] != k[:-1]])
+    counts = np.diff(np.r_[starts, len(k)])
+    s = np.add.reduceat(x, starts)
+    d = x - np.repeat(s / counts, counts)
+    var = np.add.reduceat(d * d, starts) / (counts - 1)
+    return k[starts], s, var, np.add.reduceat(np.abs(x), starts), counts
+
+
+@pytest.mark.parametrize("mode", ["fp64", "compensated"])
+def test_precision_against_extended_oracle(mode, monkeypatch):
+    """The precision configuration's data at 2M rows (10K uniform Int32 keys,
+    Float32 log-uniform magnitudes, random signs): each accumulation against
+    a long-double oracle, within its stated bound.  A Float32 column's sum is
+    a Float32 result, so the accumulated sum is read through the Float64
+    mean (mean x count)."""
+    monkeypatch.setenv("DATAFRAME_ACCEL_FLOAT32", mode)
+    rng = np.random.default_rng(3)
+    rows = 2_000_000
+    keys = rng.integers(0, 10_000, rows).astype(np.int32)
+    vals = (np.where(rng.random(rows) < 0.5, -1.0, 1.0) * 10.0 ** rng.uniform(-6, 6, rows)).astype(np.float32)
+    frame = DataFrame([Series("k", keys), Series("v", vals)])
+    out = run_device(frame.lazy().group_by("k").agg([col("v").mean().alias("m"), col("v").var().alias("var")]))
+    t = provider.last_timings()
+    if mode == "fp64":
+        assert t["regime"] == 0, t  # the global table in L2
+    else:
+        assert t["cluster_ctas"] > 1 and t["compensated"] != 0, t
+    gk, gs, gv, gabs, gn = exact_groups(keys, vals)
+    order = np.argsort(out["k"].values)
+    assert np.array_equal(out["k"].values[order], gk)
+    s = out["m"].values[order].astype(np.longdouble) * gn
+    v = out["var"].values[order].astype(np.longdouble)
+    sum_err = float(np.max(np.abs(s - gs) / gabs))
+    var_err = float(np.max(np.abs(v - gv) / gv))
+    bound_sum, bound_var = ((test_gpu_parity.SUM_RTOL, test_gpu_parity.VAR_RTOL) if mode == "fp64"
+                            else (COMP_SUM_RTOL, COMP_VAR_RTOL))
+    assert sum_err <= bound_sum, (mode, sum_err)
+    assert var_err <= bound_var, (mode, var_err)

@@ -391,7 +391,7 @@ def batched_form(device: str, nq: int) -> dict:
     }
 
 
-def served_form(device: str, nreq: int, rate: float = 2000.0) -> dict:
+def served_form(device: str, nreq: int, rate: float = 2000.0, inflight: int = 32) -> dict:
     """The served configuration: 8 resident tables of 10M-200M rows (the
     100M-row workload's schema, seeds 5 + table id), nreq requests arriving
     as a Poisson process at `rate` per second, each a group-by with a random
@@ -446,7 +446,7 @@ def served_form(device: str, nreq: int, rate: float = 2000.0) -> dict:
         return np.array(lat), time.perf_counter() - t0
 
     def served():
-        server = provider.Server(max_inflight=32)
+        server = provider.Server(max_inflight=inflight)
         lat = {}
         t0 = time.perf_counter()
         i = 0
@@ -583,6 +583,7 @@ def main() -> int:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-queries", type=int, default=512, help="batched form: queries (0: skip)")
     ap.add_argument("--served-requests", type=int, default=400, help="served form: requests (0: skip)")
+    ap.add_argument("--served-inflight", type=int, default=32, help="served form: requests in flight at most")
     ap.add_argument("--precision-rows", type=int, default=100_000_000, help="precision form: rows (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -790,7 +791,7 @@ def main() -> int:
         batched = batched_form(f"cuda:{local}", args.batch_queries)
         torch.cuda.empty_cache()
     if world == 1 and args.served_requests > 0:
-        served = served_form(f"cuda:{local}", args.served_requests)
+        served = served_form(f"cuda:{local}", args.served_requests, inflight=args.served_inflight)
         torch.cuda.empty_cache()
     if world > 1:
         dist.barrier()

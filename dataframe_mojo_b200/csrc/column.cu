@@ -84,27 +84,33 @@ __global__ void column_hll(DevColumn c, uint64_t rows, uint32_t* regs) {
 // key word (keys <= 64 bits) or the 64-bit key hash, both as the scan forms
 // them.  The group count of a multi-key query is estimated from these
 // directly instead of from the product of the columns' distinct counts.
+// The query's key word of row i (packed keys) or its 64-bit key hash (ticket
+// keys), as the scan forms them.
+__device__ __forceinline__ uint64_t query_key_word(const ScanParams& p, uint64_t i) {
+  const bool packed = p.key_mode == KEY_PACKED;
+  uint64_t kw = packed ? 0ull : 0x243F6A8885A308D3ull;
+  for (int k = 0; k < p.n_keys; ++k) {
+    const KeyField& f = p.keys[k];
+    const DevColumn& c = p.cols[f.input];
+    const bool ok = !c.validity || bit_valid(c.validity, i);
+    const uint64_t cell = ok ? key_cell(load_bits(c.values, c.size, i), f.dtype) : 0ull;
+    if (packed) {
+      if (!ok) kw |= 1ull << f.null_bit;
+      else kw |= (f.bits == 64) ? cell : (cell << f.shift);
+    } else {
+      const uint64_t v = ok ? cell + 1 : 0x9E3779B97F4A7C15ull;
+      kw = mix64(kw ^ (v * 0x9E3779B97F4A7C15ull + (uint64_t)k));
+    }
+  }
+  return kw;
+}
+
 __global__ void keys_hll(const __grid_constant__ ScanParams p, uint32_t* regs) {
   __shared__ uint32_t local[1u << kHllBits];
   for (uint32_t i = threadIdx.x; i < (1u << kHllBits); i += blockDim.x) local[i] = 0;
   __syncthreads();
-  const bool packed = p.key_mode == KEY_PACKED;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < p.rows; i += (uint64_t)gridDim.x * blockDim.x) {
-    uint64_t kw = packed ? 0ull : 0x243F6A8885A308D3ull;
-    for (int k = 0; k < p.n_keys; ++k) {
-      const KeyField& f = p.keys[k];
-      const DevColumn& c = p.cols[f.input];
-      const bool ok = !c.validity || bit_valid(c.validity, i);
-      const uint64_t cell = ok ? key_cell(load_bits(c.values, c.size, i), f.dtype) : 0ull;
-      if (packed) {
-        if (!ok) kw |= 1ull << f.null_bit;
-        else kw |= (f.bits == 64) ? cell : (cell << f.shift);
-      } else {
-        const uint64_t v = ok ? cell + 1 : 0x9E3779B97F4A7C15ull;
-        kw = mix64(kw ^ (v * 0x9E3779B97F4A7C15ull + (uint64_t)k));
-      }
-    }
-    const uint64_t h = mix64(kw ^ 0xD6E8FEB86659FD93ull);
+    const uint64_t h = mix64(query_key_word(p, i) ^ 0xD6E8FEB86659FD93ull);
     const uint32_t reg = (uint32_t)(h >> (64 - kHllBits));
     const uint64_t rest = h << kHllBits;
     const uint32_t rho = rest == 0 ? (65 - kHllBits) : (uint32_t)__clzll(rest) + 1;
@@ -113,6 +119,13 @@ __global__ void keys_hll(const __grid_constant__ ScanParams p, uint32_t* regs) {
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < (1u << kHllBits); i += blockDim.x)
     if (local[i]) atomicMax(&regs[i], local[i]);
+}
+
+// Key words of the rows i * stride, i < n (a sample for the planner's skew
+// estimate); the caller keeps (n - 1) * stride below the row count.
+__global__ void keys_sample(const __grid_constant__ ScanParams p, unsigned long long* out, uint32_t n, uint64_t stride) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = query_key_word(p, (uint64_t)i * stride);
 }
 
 }  // namespace dfc

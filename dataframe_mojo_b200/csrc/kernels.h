@@ -42,4 +42,5 @@ __global__ void column_minmax(DevColumn c, uint64_t rows, unsigned long long* ou
 constexpr int kHllBits = 12;
 __global__ void column_hll(DevColumn c, uint64_t rows, uint32_t* regs);
 __global__ void keys_hll(const __grid_constant__ ScanParams p, uint32_t* regs);
+__global__ void keys_sample(const __grid_constant__ ScanParams p, unsigned long long* out, uint32_t n, uint64_t stride);
 }  // namespace dfc

@@ -15,6 +15,7 @@
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <functional>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -145,6 +146,8 @@ std::map<int, DeviceState> g_dev;
 std::mutex g_learn_mu;
 std::map<std::vector<uint64_t>, uint64_t> g_learned;
 std::map<std::vector<uint64_t>, double> g_joint;
+// Key skew per key-column set: {top-1 share, top-kHotSlots share} of a sample.
+std::map<std::vector<uint64_t>, std::pair<double, double>> g_skew;
 std::atomic<uint64_t> g_column_serial{0};
 
 dfc_status device_ready(int dev, DeviceState** out) {
@@ -279,6 +282,9 @@ struct Plan {
   uint64_t est_groups = 0;
   std::vector<uint64_t> key_sig;  // registration numbers of the key columns
   std::vector<uint64_t> shape_sig;  // key_sig, then the filter program (columns by registration number)
+  // Key skew from a 64K-row sample of the key words (-1: not measured): the
+  // most frequent key's share and the share of the kHotSlots most frequent.
+  double top1 = -1, top_hot = -1;
 };
 
 // The stage ring for tiles of `tile` rows (a power of two >= 128, so every
@@ -688,6 +694,59 @@ uint64_t estimate_groups(const dfc_query* q, const Plan& P, DeviceState* ds, cud
   return (uint64_t)std::max(1.0, est);
 }
 
+// Per-CTA hot-key tables: slots, and the sampled share of rows their keys
+// must cover to be used when the groups do not fit a CTA.
+constexpr uint64_t kHotSlots = 512;
+constexpr double kHotCoverage = 0.6;
+constexpr uint64_t kOwnAlwaysGroups = 256;  // own tables whatever the skew
+constexpr double kSkewedTop1 = 0.01;        // own tables up to 4096 groups
+
+// The key skew of the query's key columns over all rows (the filter is not
+// applied), from the key words of 64K evenly spaced rows; cached per key set.
+void measure_skew(Plan& P, DeviceState* ds, cudaStream_t stream) {
+  {
+    std::lock_guard<std::mutex> lk(g_learn_mu);
+    auto it = g_skew.find(P.key_sig);
+    if (it != g_skew.end()) {
+      P.top1 = it->second.first;
+      P.top_hot = it->second.second;
+      return;
+    }
+  }
+  if (P.rows == 0) return;
+  const uint32_t n = (uint32_t)std::min<uint64_t>(P.rows, 65536);
+  const uint64_t stride = P.rows / n;
+  unsigned long long* d = nullptr;
+  std::vector<unsigned long long> h(n);
+  cudaError_t e = cudaMallocAsync((void**)&d, (size_t)n * 8, stream);
+  if (e == cudaSuccess) {
+    keys_sample<<<std::max(1u, std::min((n + 255) / 256, (uint32_t)ds->sms * 4)), 256, 0, stream>>>(P.sp, d, n, stride);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), d, (size_t)n * 8, cudaMemcpyDeviceToHost, stream);
+  if (d) cudaFreeAsync(d, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  std::sort(h.begin(), h.end());
+  std::vector<uint32_t> runs;
+  for (uint32_t i = 0; i < n;) {
+    uint32_t j = i + 1;
+    while (j < n && h[j] == h[i]) ++j;
+    runs.push_back(j - i);
+    i = j;
+  }
+  std::sort(runs.begin(), runs.end(), std::greater<uint32_t>());
+  uint64_t hot = 0;
+  for (size_t i = 0; i < runs.size() && i < kHotSlots; ++i) hot += runs[i];
+  P.top1 = (double)runs[0] / n;
+  P.top_hot = (double)hot / n;
+  std::lock_guard<std::mutex> lk(g_learn_mu);
+  g_skew[P.key_sig] = {P.top1, P.top_hot};
+}
+
 void learn_groups(const Plan& P, uint64_t groups) {
   std::lock_guard<std::mutex> lk(g_learn_mu);
   g_learned[P.shape_sig] = groups;
@@ -745,11 +804,25 @@ bool plan_shared_at(Plan& P, DeviceState* ds, uint64_t est, uint32_t flags, bool
   uint32_t want = 0;
   if (const char* env = getenv("DFC_SMEM_CLUSTER")) want = (uint32_t)atoi(env);
   if (own) {
-    // DFC_HOT_SLOTS=<n>: an own table of n slots whatever the estimate (a
-    // per-CTA cache for the keys that come first, hot keys; tuning).
+    // Own tables: always for a few groups; up to 4096 groups when the keys
+    // are skewed (a hot key's updates stay in each CTA instead of meeting on
+    // one global record); beyond that a kHotSlots table that caches the keys
+    // that come first (the hot ones) when those cover enough of the rows.
+    // Measured on B200 (512 queries of 1K-20M rows): uniform keys over 300 to
+    // 4K groups ran 1.5-2.5x faster in the global table, skewed ones up to
+    // 1.4x faster in own tables, and Zipf keys over 8K-300K groups about 1.7x
+    // faster with a 512-slot hot table; the 100M-row query over 7.4M (Int32
+    // Zipf, code) pairs, whose 512 most frequent keys cover 31% of the rows,
+    // ran 3x slower with one (misses probe a full table).  DFC_HOT_SLOTS=<n>
+    // forces an n-slot hot table (tuning).
     uint64_t hot = 0;
-    if (const char* env = getenv("DFC_HOT_SLOTS")) hot = next_pow2(std::max<uint64_t>(64, (uint64_t)atoll(env)));
-    if (want >= 2 || (!force && !hot && est > kOwnTableGroups)) return false;
+    if (const char* env = getenv("DFC_HOT_SLOTS"))
+      if (atoll(env) > 0) hot = next_pow2(std::max<uint64_t>(64, (uint64_t)atoll(env)));
+    const bool skewed = P.top1 >= kSkewedTop1;
+    // Compensated FP32 fields need on-chip partials: own tables whenever they fit.
+    const bool sized = est <= kOwnAlwaysGroups || ((skewed || sp.comp_mask) && est <= kOwnTableGroups);
+    if (!force && !hot && !sized && est > kOwnTableGroups && P.top_hot >= kHotCoverage) hot = kHotSlots;
+    if (want >= 2 || (!force && !hot && !sized)) return false;
     const uint64_t sslots =
         hot ? hot : next_pow2(std::max<uint64_t>(64, std::min<uint64_t>(est, kOwnTableGroups) * 2));
     // smem_optin already excludes the kernel's static shared memory.
@@ -1173,11 +1246,12 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   t_timings.partitions = pp ? (int32_t)nparts : 0;
   if (getenv("DFC_TRACE")) {
     fprintf(stderr,
-            "dfc attempt: rows=%llu regime=%s slots=%llu recs=%llu smem_slots=%u x%u tile=%d ctas=%llu parts=%llu agg_slots=%u "
+            "dfc attempt: rows=%llu regime=%s slots=%llu recs=%llu smem_slots=%u x%u tile=%d top1=%.4f hot=%.3f ctas=%llu parts=%llu agg_slots=%u "
             "clusters=%d flush=%u | status=%#x cap=%#x check=%#x alloc=%u groups=%u ms scan=%.3f (count=%.3f offsets=%.3f) "
             "agg=%.3f fin=%.3f\n",
             (unsigned long long)P.rows, pp ? "partitioned" : "table", (unsigned long long)slots,
-            (unsigned long long)recs, sp.smem_slots, std::max(1u, sp.smem_cluster), sp.tile_rows, (unsigned long long)ncta,
+            (unsigned long long)recs, sp.smem_slots, std::max(1u, sp.smem_cluster), sp.tile_rows, P.top1, P.top_hot,
+            (unsigned long long)ncta,
             (unsigned long long)nparts,
             pp ? pp->agg_slots : 0u, pp ? pp->clusters : 0, pp ? pp->flush : 0u, host_ctl->status[0],
             host_ctl->status[1], host_ctl->status[2], host_ctl->alloc, host_ctl->groups, ms_scan, ms_count, ms_offsets,
@@ -1403,7 +1477,11 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
   bool partitioned = false;
   if ((query->flags & DFC_Q_FORCE_PARTITIONED) && !(query->flags & (DFC_Q_FORCE_GLOBAL | DFC_Q_FORCE_SHARED)))
     partitioned = plan_partitions(P, ds, est, pp);
-  if (!partitioned) plan_shared(P, ds, est, query->flags);
+  if (!partitioned) {
+    if (P.sp.key_mode == KEY_PACKED && est > kOwnAlwaysGroups && !(query->flags & DFC_Q_FORCE_GLOBAL))
+      measure_skew(P, ds, stream);
+    plan_shared(P, ds, est, query->flags);
+  }
   uint64_t slots = next_pow2(std::max<uint64_t>(1024, est * 8));
   const uint64_t max_slots = next_pow2(std::max<uint64_t>(1024, P.rows * 8));
   slots = std::min(slots, max_slots);
@@ -1826,6 +1904,7 @@ DFC_API dfc_status dfc_groupby_noalloc(const dfc_query* query, int32_t device, u
 namespace {
 
 constexpr int kBatchStreams = 8;
+constexpr int kFullGridAhead = 2;  // served form: full-grid requests in flight at most
 thread_local std::vector<std::string> t_batch_errors;
 
 // The batch's streams on `dev`, created once per thread.
@@ -1868,6 +1947,8 @@ size_t arena_take(size_t& used, size_t bytes) {
 dfc_status size_item(const dfc_query* q, BatchItem& it, DeviceState* ds, cudaStream_t stream, size_t& used) {
   Plan& P = it.P;
   const uint64_t est = estimate_groups(q, P, ds, stream);
+  if (P.sp.key_mode == KEY_PACKED && est > kOwnAlwaysGroups && !(q->flags & DFC_Q_FORCE_GLOBAL))
+    measure_skew(P, ds, stream);
   plan_shared(P, ds, est, q->flags);
   it.slots = std::min(next_pow2(std::max<uint64_t>(1024, est * 8)), next_pow2(std::max<uint64_t>(1024, P.rows * 8)));
   it.ncta = scan_grid(P, ds);
@@ -2028,6 +2109,7 @@ DFC_API dfc_status dfc_groupby_batch(const dfc_query* const* queries, int32_t n,
   const auto& streams = batch_streams(device);
 
   // Plans: regime and capacities per query, working memory in one arena.
+  const auto t_plan = std::chrono::steady_clock::now();
   size_t used = 0;
   for (int i = 0; i < n; ++i) {
     BatchItem& it = items[i];
@@ -2035,6 +2117,7 @@ DFC_API dfc_status dfc_groupby_batch(const dfc_query* const* queries, int32_t n,
     const dfc_status st = size_item(queries[i], it, ds, main, used);
     if (st) reject(i, st);
   }
+  const auto t_alloc = std::chrono::steady_clock::now();
   unsigned char* arena = nullptr;
   Control* dctl = nullptr;
   cudaError_t e = cudaMallocAsync((void**)&arena, std::max<size_t>(used, 256), main);
@@ -2070,11 +2153,23 @@ DFC_API dfc_status dfc_groupby_batch(const dfc_query* const* queries, int32_t n,
     cudaStreamWaitEvent(streams[s], fork, 0);
     cudaEventCreateWithFlags(&joins[s], cudaEventDisableTiming);
   }
+  const auto t_launch = std::chrono::steady_clock::now();
+  // Two phases: the smaller queries side by side on streams 1-7, then the
+  // full-grid ones one after another on stream 0.  A persistent scan sized to
+  // every SM runs late on the SMs other kernels still hold, so it never runs
+  // beside the small ones.
   int k = 0;
-  for (int i = 0; i < n; ++i) {
-    if (items[i].st) continue;
-    launch_item(items[i], ds, arena, dctl + i, streams[item_stream(items[i], k)]);
-    bt.launches += items[i].P.rows > 0 ? 7 : 6;
+  for (int phase = 0; phase < 2; ++phase) {
+    for (int i = 0; i < n; ++i) {
+      if (items[i].st || items[i].full_grid != (phase == 1)) continue;
+      launch_item(items[i], ds, arena, dctl + i, streams[item_stream(items[i], k)]);
+      bt.launches += items[i].P.rows > 0 ? 7 : 6;
+    }
+    if (phase == 0)
+      for (size_t s = 1; s < streams.size(); ++s) {
+        cudaEventRecord(joins[s], streams[s]);
+        cudaStreamWaitEvent(streams[0], joins[s], 0);
+      }
   }
   for (size_t s = 0; s < streams.size(); ++s) {
     cudaEventRecord(joins[s], streams[s]);
@@ -2091,7 +2186,9 @@ DFC_API dfc_status dfc_groupby_batch(const dfc_query* const* queries, int32_t n,
   }
   e = cudaGetLastError();
   if (e == cudaSuccess && pinned) e = cudaMemcpyAsync(pinned, dctl, (size_t)n * sizeof(Control), cudaMemcpyDeviceToHost, main);
+  const auto t_wait = std::chrono::steady_clock::now();
   dfc_status st = e == cudaSuccess ? wait_bounded(main) : cuda_fail(e, "batch launch");
+  const auto t_done = std::chrono::steady_clock::now();
   if (st == DFC_OK && !pinned) st = fail(DFC_OOM, "pinned batch control blocks");
   cudaEventDestroy(fork);
   for (auto& j : joins) cudaEventDestroy(j);
@@ -2124,6 +2221,12 @@ DFC_API dfc_status dfc_groupby_batch(const dfc_query* const* queries, int32_t n,
     if (qs) t_batch_errors[i] = t_error;
   }
   bt.total_ns = std::chrono::duration<double, std::nano>(std::chrono::steady_clock::now() - t0).count();
+  if (getenv("DFC_TRACE")) {
+    auto ms = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+    fprintf(stderr, "dfc batch: n=%d arena=%zu MB plan=%.2f alloc=%.2f launch=%.2f wait=%.2f results=%.2f ms retries=%d\n",
+            n, used >> 20, ms(t_plan, t_alloc), ms(t_alloc, t_launch), ms(t_launch, t_wait), ms(t_wait, t_done),
+            ms(t_done, std::chrono::steady_clock::now()), bt.retries);
+  }
   t_timings = bt;
   return DFC_OK;
 }
@@ -2167,6 +2270,7 @@ struct Request {
   unsigned char* arena = nullptr;
   Control* dctl = nullptr;
   int slot = -1;     // pinned control slot
+  bool full = false; // its scan fills every SM
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
 };
@@ -2179,6 +2283,8 @@ struct dfc_server {
   int max_inflight = 64;
   int64_t budget = 0;       // device bytes in flight at most
   int64_t held = 0;
+  int full_inflight = 0;  // admitted requests whose scan fills every SM
+  int full_ahead = kFullGridAhead;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<Request*> pending;
@@ -2214,6 +2320,7 @@ void server_complete(dfc_server* sv, Request* r, dfc_status st, dfc_result* res,
 // Plans, sizes and launches one request; false when it must wait for memory
 // (nothing done) or failed (completed with its error).
 bool server_launch(dfc_server* sv, Request* r, int& k) {
+  const auto t_start = Clock::now();
   r->item = BatchItem{};  // a request that waited for memory is planned afresh
   BatchItem& it = r->item;
   dfc_status st = plan_query(&r->oq.q, it.P);
@@ -2233,10 +2340,16 @@ bool server_launch(dfc_server* sv, Request* r, int& k) {
   size_t out_bytes = 0;
   for (int c = 0; c < it.P.n_out; ++c) out_bytes += it.out_rows * 8 + ((it.out_rows + 31) / 32) * 4 + 512;
   r->bytes = used + out_bytes + sizeof(Control);
+  r->full = it.full_grid;
   {
     std::lock_guard<std::mutex> lk(sv->mu);
     if (sv->held > 0 && sv->held + (int64_t)r->bytes > sv->budget) return false;  // wait for memory
+    // A scan that fills every SM runs after the ones queued before it: with
+    // kFullGridAhead of them in flight the device stays busy, and admitting
+    // more would only hold their memory early.
+    if (r->full && sv->full_inflight >= sv->full_ahead) return false;
     sv->held += (int64_t)r->bytes;
+    sv->full_inflight += r->full ? 1 : 0;
   }
   r->admitted = Clock::now();
   r->stream = stream;
@@ -2254,6 +2367,7 @@ bool server_launch(dfc_server* sv, Request* r, int& k) {
     {
       std::lock_guard<std::mutex> lk(sv->mu);
       sv->held -= (int64_t)r->bytes;
+      sv->full_inflight -= r->full ? 1 : 0;
     }
     server_complete(sv, r, DFC_OOM, nullptr, "device memory for the request");
     delete r;
@@ -2266,11 +2380,17 @@ bool server_launch(dfc_server* sv, Request* r, int& k) {
   cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming);
   cudaEventRecord(r->done, stream);
   sv->inflight.push_back(r);
+  if (getenv("DFC_TRACE"))
+    fprintf(stderr, "dfc serve launch tag=%llu full=%d slots=%llu recs=%llu bytes=%zu smem=%u plan+launch_us=%.1f queued_us=%.1f\n",
+            (unsigned long long)r->tag, (int)r->full, (unsigned long long)it.slots, (unsigned long long)it.recs, r->bytes,
+            it.P.sp.smem_slots, std::chrono::duration<double, std::micro>(Clock::now() - t_start).count(),
+            std::chrono::duration<double, std::micro>(r->admitted - r->submitted).count());
   return true;
 }
 
 // Finishes a request whose work is done on the device.
 void server_finish(dfc_server* sv, Request* r) {
+  const auto t_start = Clock::now();
   dfc_result* res = nullptr;
   const Control c = sv->pinned[r->slot];
   sv->free_slots.push_back(r->slot);
@@ -2292,7 +2412,13 @@ void server_finish(dfc_server* sv, Request* r) {
   {
     std::lock_guard<std::mutex> lk(sv->mu);
     sv->held -= (int64_t)r->bytes;
+    sv->full_inflight -= r->full ? 1 : 0;
   }
+  if (getenv("DFC_TRACE"))
+    fprintf(stderr, "dfc serve finish tag=%llu st=%d groups=%u status=%#x run_us=%.1f finish_us=%.1f\n",
+            (unsigned long long)r->tag, (int)st, c.groups, c.status[0],
+            std::chrono::duration<double, std::micro>(t_start - r->admitted).count(),
+            std::chrono::duration<double, std::micro>(Clock::now() - t_start).count());
   server_complete(sv, r, st, res, msg);
   delete r;
 }
@@ -2342,6 +2468,7 @@ void server_loop(dfc_server* sv) {
         {
           std::lock_guard<std::mutex> lk(sv->mu);
           sv->held -= (int64_t)r->bytes;
+          sv->full_inflight -= r->full ? 1 : 0;
         }
         server_complete(sv, r, cuda_fail(q, "request execution"), nullptr, t_error);
         delete r;
@@ -2375,6 +2502,9 @@ DFC_API dfc_status dfc_server_create(int32_t device, int32_t max_inflight, int64
     memory_budget = (int64_t)(free_b * 0.8);
   }
   sv->budget = memory_budget;
+  // DFC_SERVER_FULL_AHEAD=<n>: full-grid requests in flight at most (tuning).
+  if (const char* env = getenv("DFC_SERVER_FULL_AHEAD"))
+    if (atoi(env) > 0) sv->full_ahead = atoi(env);
   sv->streams.resize(kBatchStreams);
   for (auto& s : sv->streams) cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
   cudaStreamCreateWithFlags(&sv->plan_stream, cudaStreamNonBlocking);

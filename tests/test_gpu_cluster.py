@@ -115,6 +115,22 @@ def test_cluster_table_overflow_takes_global_path(monkeypatch):
     assert provider.last_timings()["cluster_ctas"] == 2
 
 
+def test_regime_follows_key_skew():
+    """300 groups: uniform keys take the global table, Zipf keys (one key
+    with about a fifth of the rows) per-CTA tables; a handful of groups always
+    take per-CTA tables.  Results match the oracle in every case."""
+    rng = np.random.default_rng(37)
+    rows = 300_000
+    base = wide_frame(rng, rows, 300)
+    zipf = np.minimum(rng.zipf(1.2, rows), 300).astype(np.int32)
+    few = rng.integers(0, 40, rows).astype(np.int32)
+    for keys, label, regime in ((base["k"], "uniform", 0), (Series("k", zipf), "zipf", 1), (Series("k", few), "few", 1)):
+        frame = DataFrame([keys] + [base[c] for c in ("f", "i", "p")])
+        check_wide(frame, f"skew-{label}")
+        t = provider.last_timings()
+        assert t["regime"] == regime, (label, t)
+
+
 @pytest.fixture
 def compensated(monkeypatch):
     monkeypatch.setenv("DATAFRAME_ACCEL_FLOAT32", "compensated")

@@ -673,7 +673,17 @@ __device__ __forceinline__ void pair_add(float& s, float& c, float x, float xc, 
 
 // The pair sum of each lane's group (members in lane order), as group_reduce.
 __device__ __forceinline__ void group_pair(uint32_t grp, int maxpop, float ms, float mc, bool take, float& s, float& c,
-                                           bool& range) {
+                                           bool& range, bool one = false) {
+  if (one) {
+    s = take ? ms : 0.f;
+    c = take ? mc : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const float os = __shfl_xor_sync(0xffffffffu, s, o), oc = __shfl_xor_sync(0xffffffffu, c, o);
+      pair_add(s, c, os, oc, range);
+    }
+    return;
+  }
   s = 0.f;
   c = 0.f;
   uint32_t left = grp;
@@ -721,10 +731,44 @@ __device__ __forceinline__ int nth_lane(uint32_t grp, int i) {
   return grp ? __ffs(grp) - 1 : (int)(threadIdx.x & 31);
 }
 
+// Full-warp butterfly reductions (every lane gets the result).
+__device__ __forceinline__ double warp_sum_f64(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ uint64_t warp_max_u64(uint64_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const uint64_t w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = w > v ? w : v;
+  }
+  return v;
+}
+__device__ __forceinline__ __int128 warp_sum_i128(__int128 v) {
+  uint64_t lo = (uint64_t)v, hi = (uint64_t)((unsigned __int128)v >> 64);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const uint64_t olo = __shfl_xor_sync(0xffffffffu, lo, o), ohi = __shfl_xor_sync(0xffffffffu, hi, o);
+    const uint64_t nlo = lo + olo;
+    hi = hi + ohi + (nlo < lo ? 1ull : 0ull);
+    lo = nlo;
+  }
+  return (__int128)(((unsigned __int128)hi << 64) | lo);
+}
+
 // Reduction over each lane's group, members in lane order; shuffles run on
-// the full warp, one per member of the largest group.
+// the full warp, one per member of the largest group.  `one`: every lane in
+// a group is in the same one, reduced by a five-step butterfly instead.
 template <typename V, typename Op>
-__device__ __forceinline__ V group_reduce(uint32_t grp, int maxpop, V mine, V identity, bool take, Op op) {
+__device__ __forceinline__ V group_reduce(uint32_t grp, int maxpop, V mine, V identity, bool take, Op op,
+                                          bool one = false) {
+  if (one) {
+    V acc = take ? mine : identity;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc = op(acc, __shfl_xor_sync(0xffffffffu, acc, o));
+    return acc;
+  }
   V acc = identity;
   uint32_t left = grp;
   const int lane = threadIdx.x & 31;
@@ -750,10 +794,13 @@ __device__ __forceinline__ void group_update(const ScanParams& p, const Rec& rec
   const int lane = threadIdx.x & 31;
   {
     const bool leader = loc && lane == __ffs(grp) - 1;
+    // All rows of the warp in one group (a hot key): butterfly reductions.
+    const bool one = maxpop > 4 && maxpop == __popc(__ballot_sync(0xffffffffu, loc));
     // The group's earliest row.  A CTA record always keeps its first row:
     // it is the claim row when the record is merged into the global table.
     const uint32_t first =
-        group_reduce<uint32_t>(grp, maxpop, row, 0xFFFFFFFFu, loc, [](uint32_t a, uint32_t b2) { return a < b2 ? a : b2; });
+        group_reduce<uint32_t>(grp, maxpop, row, 0xFFFFFFFFu, loc, [](uint32_t a, uint32_t b2) { return a < b2 ? a : b2; },
+                               one);
     if (leader) {
       rec.max_u32(kRecFirst, ~first);
       if (p.off_len >= 0) rec.add_u32(p.off_len, (uint32_t)__popc(grp));
@@ -778,10 +825,10 @@ __device__ __forceinline__ void group_update(const ScanParams& p, const Rec& rec
       if (f.off_sum >= 0) {
         if (comp) {
           float ps, pc;
-          group_pair(grp, maxpop, (float)xd, 0.f, ok, ps, pc, range);
+          group_pair(grp, maxpop, (float)xd, 0.f, ok, ps, pc, range, one);
           if (leader && vmask) stuck = !pair_cas_add(rec, f.off_sum, ps, pc, range);
         } else if (f.sum_kind == SUM_F64) {
-          const double sm = group_reduce<double>(grp, maxpop, xd, 0.0, ok, [](double a, double b2) { return a + b2; });
+          const double sm = group_reduce<double>(grp, maxpop, xd, 0.0, ok, [](double a, double b2) { return a + b2; }, one);
           if (leader && vmask) rec.add_f64(f.off_sum, sm);
         } else {
           // The group's partial sum, exact in 128 bits.
@@ -789,8 +836,9 @@ __device__ __forceinline__ void group_update(const ScanParams& p, const Rec& rec
           const uint64_t xv = ok ? (uns ? b : (uint64_t)bits_to_i64(b, dt)) : 0ull;
           const uint64_t xhi = (!uns && (int64_t)xv < 0) ? ~0ull : 0ull;
           __int128 exact = 0;
-          uint32_t left = grp;
-          for (int i = 0; i < maxpop; ++i) {
+          uint32_t left = one ? 0u : grp;
+          if (one) exact = warp_sum_i128(ok ? (__int128)(((unsigned __int128)xhi << 64) | xv) : (__int128)0);
+          for (int i = 0; i < (one ? 0 : maxpop); ++i) {
             const int src = left ? __ffs(left) - 1 : lane;
             const uint64_t vlo = __shfl_sync(0xffffffffu, xv, src);
             const uint64_t vhi = __shfl_sync(0xffffffffu, xhi, src);
@@ -816,12 +864,14 @@ __device__ __forceinline__ void group_update(const ScanParams& p, const Rec& rec
         const uint64_t e = ordinary ? order_encode(b, dt) : 0ull;
         if (f.off_min >= 0) {
           const unsigned long long m = group_reduce<unsigned long long>(
-              grp, maxpop, ~e, 0ull, ordinary, [](unsigned long long a, unsigned long long b2) { return a > b2 ? a : b2; });
+              grp, maxpop, ~e, 0ull, ordinary, [](unsigned long long a, unsigned long long b2) { return a > b2 ? a : b2; },
+              one);
           if (leader && m && !rec.max_u64(f.off_min, m)) stuck = true;
         }
         if (f.off_max >= 0) {
           const unsigned long long m = group_reduce<unsigned long long>(
-              grp, maxpop, e, 0ull, ordinary, [](unsigned long long a, unsigned long long b2) { return a > b2 ? a : b2; });
+              grp, maxpop, e, 0ull, ordinary, [](unsigned long long a, unsigned long long b2) { return a > b2 ? a : b2; },
+              one);
           if (leader && m && !rec.max_u64(f.off_max, m)) stuck = true;
         }
         if (leader) {
@@ -857,11 +907,11 @@ __device__ __forceinline__ void group_update(const ScanParams& p, const Rec& rec
           const float sq_lo = fmaf(2.f * dh, dl, fmaf(dh, dh, -sq));
           if (ok && isfinite(xf) && isfinite(kf) && !isfinite(sq)) range = true;
           float ps, pc;
-          group_pair(grp, maxpop, sq, isfinite(sq) ? sq_lo : 0.f, ok, ps, pc, range);
+          group_pair(grp, maxpop, sq, isfinite(sq) ? sq_lo : 0.f, ok, ps, pc, range, one);
           if (leader && vmask && !stuck) stuck = !pair_cas_add(rec, f.off_m2, ps, pc, range);
         } else {
           const double d = xd - kd;
-          const double s2 = group_reduce<double>(grp, maxpop, d * d, 0.0, ok, [](double a, double b2) { return a + b2; });
+          const double s2 = group_reduce<double>(grp, maxpop, d * d, 0.0, ok, [](double a, double b2) { return a + b2; }, one);
           if (leader && vmask) rec.add_f64(f.off_m2, s2);
         }
       }
@@ -898,32 +948,6 @@ __device__ __forceinline__ void smem_rows(const ScanParams& p, const Step& s, co
                                           const uint64_t (&kw)[kR]) {
   if (st.ranks > 1) smem_rows_in<ClusterRec>(p, s, st, x, rows, sel, kw);
   else smem_rows_in<OwnRec>(p, s, st, x, rows, sel, kw);
-}
-
-// Full-warp butterfly reductions (every lane gets the result).
-__device__ __forceinline__ double warp_sum_f64(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-__device__ __forceinline__ uint64_t warp_max_u64(uint64_t v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const uint64_t w = __shfl_xor_sync(0xffffffffu, v, o);
-    v = w > v ? w : v;
-  }
-  return v;
-}
-__device__ __forceinline__ __int128 warp_sum_i128(__int128 v) {
-  uint64_t lo = (uint64_t)v, hi = (uint64_t)((unsigned __int128)v >> 64);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const uint64_t olo = __shfl_xor_sync(0xffffffffu, lo, o), ohi = __shfl_xor_sync(0xffffffffu, hi, o);
-    const uint64_t nlo = lo + olo;
-    hi = hi + ohi + (nlo < lo ? 1ull : 0ull);
-    lo = nlo;
-  }
-  return (__int128)(((unsigned __int128)hi << 64) | lo);
 }
 
 // Folds the lanes of the warp's largest group -- `grp` is each lane's group

@@ -131,6 +131,20 @@ def test_regime_follows_key_skew():
         assert t["regime"] == regime, (label, t)
 
 
+@pytest.mark.parametrize("keys", ["one", "hot"])
+def test_warp_wide_groups(keys):
+    """Warps whose rows all share one group (one key, or one key with 97% of
+    the rows) fold their rows by butterfly reductions; every aggregation
+    against the oracle."""
+    rng = np.random.default_rng(38)
+    rows = 500_000
+    base = wide_frame(rng, rows, 10)
+    k = np.zeros(rows, np.int32) if keys == "one" else np.where(rng.random(rows) < 0.97, 7, rng.integers(0, 50, rows)).astype(np.int32)
+    frame = DataFrame([Series("k", k)] + [base[c] for c in ("f", "i", "p")])
+    check_wide(frame, f"warp-wide-{keys}")
+    assert provider.last_timings()["regime"] == 1
+
+
 @pytest.fixture
 def compensated(monkeypatch):
     monkeypatch.setenv("DATAFRAME_ACCEL_FLOAT32", "compensated")
@@ -184,6 +198,14 @@ def test_compensated_random_dtypes(seed, compensated, monkeypatch):
         compare_with_oracle(plan, f"compensated-random{seed}", float_cols=floats, var_cols=vars_, scales=scales)
     except provider.DataFaultError:
         pytest.skip("moments adjudicated by the CPU (data fault)")
+
+
+def test_compensated_one_group(compensated):
+    rng = np.random.default_rng(39)
+    base = wide_frame(rng, 300_000, 10)
+    frame = DataFrame([Series("k", np.zeros(300_000, np.int32))] + [base[c] for c in ("f", "i", "p")])
+    check_wide(frame, "compensated-one-group")
+    assert provider.last_timings()["compensated"] != 0
 
 
 def test_compensated_out_of_range_reruns_in_fp64(compensated):

@@ -816,9 +816,13 @@ __device__ __forceinline__ void group_update(const ScanParams& p, const Rec& rec
       const double xd = isf ? bits_to_f64(b, dt) : bits_as_double(b, dt);
       const bool nan = ok && isf && xd != xd;
       const uint32_t vmask = grp & __ballot_sync(0xffffffffu, ok);
-      const uint32_t nanmask = grp & __ballot_sync(0xffffffffu, nan);
-      const uint32_t pz = grp & __ballot_sync(0xffffffffu, ok && isf && xd == 0.0 && __double_as_longlong(xd) >= 0);
-      const uint32_t nz = grp & __ballot_sync(0xffffffffu, ok && isf && xd == 0.0 && __double_as_longlong(xd) < 0);
+      // NaN and signed-zero flags: float columns only (isf is warp-uniform).
+      uint32_t nanmask = 0, pz = 0, nz = 0;
+      if (isf) {
+        nanmask = grp & __ballot_sync(0xffffffffu, nan);
+        pz = grp & __ballot_sync(0xffffffffu, ok && xd == 0.0 && __double_as_longlong(xd) >= 0);
+        nz = grp & __ballot_sync(0xffffffffu, ok && xd == 0.0 && __double_as_longlong(xd) < 0);
+      }
       if (leader && vmask) rec.add_u32(f.off_count, (uint32_t)__popc(vmask));
       const bool comp = (p.comp_mask >> v) & 1u;
       bool range = false, stuck = false;
@@ -1179,7 +1183,15 @@ __device__ __forceinline__ void consume_rows(const ScanParams& p, const Step& s,
   }
   uint64_t kw[kR];
   key_words(p, s, x, kw);
-  if (st) smem_rows(p, s, *st, x, rows, sel, kw);
+  if (st) {
+    smem_rows(p, s, *st, x, rows, sel, kw);
+    // Every row found its shared-memory record: nothing is left for the
+    // global table (a warp-uniform exit).
+    bool left = false;
+#pragma unroll
+    for (int j = 0; j < kR; ++j) left |= sel[j];
+    if (!__any_sync(0xffffffffu, left)) return;
+  }
 
   uint32_t gid[kR];
   if (p.key_mode == KEY_PACKED) {

@@ -11,6 +11,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -914,20 +915,48 @@ cudaError_t launch_scan(const ScanParams& sp, uint64_t ncta, size_t smem, cudaSt
   return cudaLaunchKernelEx(&cfg, scan_kernel, sp);
 }
 
+// A query's working buffers carved from one stream-ordered allocation:
+// alloc() records each request (256-byte aligned), commit() allocates the
+// block and sets every recorded pointer.
 struct Scratch {
   cudaStream_t stream = nullptr;
-  std::vector<void*> ptrs;
-  dfc_status alloc(void** p, size_t bytes, const char* what) {
-    cudaError_t e = cudaMallocAsync(p, std::max<size_t>(bytes, 256), stream);
-    if (e != cudaSuccess) return cuda_fail(e, what);
-    ptrs.push_back(*p);
+  void* block = nullptr;
+  std::vector<std::pair<void**, size_t>> wants;
+  size_t total = 0;
+  dfc_status alloc(void** p, size_t bytes, const char*) {
+    wants.push_back({p, total});
+    total += (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255;
+    *p = nullptr;
+    return DFC_OK;
+  }
+  dfc_status commit(const char* what) {
+    cudaError_t e = cudaMallocAsync(&block, std::max<size_t>(total, 256), stream);
+    if (e != cudaSuccess) {
+      block = nullptr;
+      return cuda_fail(e, what);
+    }
+    for (auto& w : wants) *w.first = static_cast<unsigned char*>(block) + w.second;
     return DFC_OK;
   }
   void release() {
-    for (void* p : ptrs) cudaFreeAsync(p, stream);
-    ptrs.clear();
+    if (block) cudaFreeAsync(block, stream);
+    block = nullptr;
+    wants.clear();
+    total = 0;
   }
 };
+
+// The attempt's timing events, created once per thread and device.
+cudaEvent_t* attempt_events(int device) {
+  thread_local std::map<int, std::array<cudaEvent_t, 6>> events;
+  auto it = events.find(device);
+  if (it == events.end()) {
+    std::array<cudaEvent_t, 6> ev{};
+    for (auto& x : ev) cudaEventCreate(&x);
+    it = events.emplace(device, ev).first;
+  }
+  return it->second.data();
+}
 
 // Control block copied back after every attempt.
 struct Control {
@@ -1078,6 +1107,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   if ((st = S.alloc(&bsums, chunks * 4, "prefix chunks"))) return S.release(), st;
   if ((st = S.alloc(&perm, recs * 4, "group permutation"))) return S.release(), st;
   if ((st = S.alloc(&firsts, recs * 4, "first rows"))) return S.release(), st;
+  if ((st = S.commit("query working memory"))) return S.release(), st;
   // Output columns sized for the group capacity (the group count is known
   // only on the device; the host reads it once, at the end).
   const uint64_t out_rows = std::min<uint64_t>(P.rows, recs);
@@ -1146,8 +1176,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
     sp.part_next = &dctl->part_next;
   }
 
-  cudaEvent_t ev[6];
-  for (auto& x : ev) cudaEventCreate(&x);
+  cudaEvent_t* ev = attempt_events(P.device);
   cudaEventRecord(ev[0], stream);
   if (pp) {
     partition_count<<<(unsigned)ncta, kPartThreads, pp->count_smem, stream>>>(sp);
@@ -1173,8 +1202,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
     if (e != cudaSuccess) {
       free_outputs();
       S.release();
-      for (auto& x : ev) cudaEventDestroy(x);
-      return cuda_fail(e, "partition aggregation launch");
+        return cuda_fail(e, "partition aggregation launch");
     }
     t_timings.launches += 4;
   } else {
@@ -1183,7 +1211,6 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
       if (e != cudaSuccess) {
         free_outputs();
         S.release();
-        for (auto& x : ev) cudaEventDestroy(x);
         return cuda_fail(e, "scan launch");
       }
       t_timings.launches += 1;
@@ -1221,12 +1248,10 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   S.release();
   if (e != cudaSuccess) {
     free_outputs();
-    for (auto& x : ev) cudaEventDestroy(x);
     return cuda_fail(e, "kernel launch");
   }
   st = wait_bounded(stream);
   if (st) {
-    for (auto& x : ev) cudaEventDestroy(x);
     free_outputs();
     return st;
   }
@@ -1238,7 +1263,6 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   }
   cudaEventElapsedTime(&ms_agg, ev[3], ev[1]);
   cudaEventElapsedTime(&ms_finish, ev[1], ev[2]);
-  for (auto& x : ev) cudaEventDestroy(x);
   t_timings.scan_ns += ms_scan * 1e6;
   t_timings.aggregate_ns += ms_agg * 1e6;
   t_timings.finish_ns += ms_finish * 1e6;

@@ -718,7 +718,7 @@ def main() -> int:
     achieved = algo_bytes / scan_s / 1e9
     roofline = {
         "bound": "hbm",
-        "kernel": "scan_kernel",
+        "kernel": "scan_kernel_global",
         "achieved": achieved,
         "peak": peak,
         "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",

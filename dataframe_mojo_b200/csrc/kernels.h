@@ -12,7 +12,13 @@ constexpr int kScanThreads = kScanConsumerThreads + 32;  // + one producer warp
 constexpr int kFinishThreads = 256;
 constexpr int kFinishChunk = 4096;  // bitmap words per prefix-scan block
 
-__global__ void scan_kernel(const __grid_constant__ ScanParams p);
+// The scan, one kernel per table regime: the global table only, per-CTA
+// shared-memory tables, shared-memory tables pooled over a thread-block
+// cluster (launched with a cluster dimension of ScanParams::smem_cluster).
+enum ScanRegime : int { kScanGlobal = 0, kScanOwn = 1, kScanCluster = 2 };
+__global__ void scan_kernel_global(const __grid_constant__ ScanParams p);
+__global__ void scan_kernel_own(const __grid_constant__ ScanParams p);
+__global__ void scan_kernel_cluster(const __grid_constant__ ScanParams p);
 // Radix-partitioned regime: pass A (filter, keys, partition) and pass B
 // (per-partition aggregation by clusters of kAggCluster CTAs).
 constexpr int kAggCluster = 8;

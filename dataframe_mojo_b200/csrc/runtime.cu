@@ -129,6 +129,15 @@ std::string overflow_message(int input_dtype) {
   return std::string(dtype_name(sum_dtype(input_dtype))) + " expression sum overflow";
 }
 
+// The scan kernels (one per table regime) share this signature.
+using ScanFn = void (*)(ScanParams);
+
+// The scan kernel for a planned query's table regime.
+ScanFn scan_fn(const ScanParams& sp) {
+  if (!sp.smem_slots) return scan_kernel_global;
+  return sp.smem_cluster > 1 ? scan_kernel_cluster : scan_kernel_own;
+}
+
 struct DeviceState {
   bool ready = false;
   int sms = 0;
@@ -168,13 +177,19 @@ dfc_status device_ready(int dev, DeviceState** out) {
     CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold), "cudaMemPoolSetAttribute");
     // Dynamic shared memory may use what the kernel's static buffers leave.
     cudaFuncAttributes fa;
-    CK(cudaFuncGetAttributes(&fa, scan_kernel), "cudaFuncGetAttributes");
-    d.smem_optin = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;
-    d.smem_half = (prop.sharedMemPerMultiprocessor - 2 * prop.reservedSharedMemPerBlock) / 2 - fa.sharedSizeBytes;
-    CK(cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin),
-       "cudaFuncSetAttribute");
+    size_t scan_static = 0;
+    for (ScanFn f : {scan_kernel_global, scan_kernel_own, scan_kernel_cluster}) {
+      CK(cudaFuncGetAttributes(&fa, f), "cudaFuncGetAttributes");
+      scan_static = std::max(scan_static, fa.sharedSizeBytes);
+    }
+    d.smem_optin = prop.sharedMemPerBlockOptin - scan_static;
+    d.smem_half = (prop.sharedMemPerMultiprocessor - 2 * prop.reservedSharedMemPerBlock) / 2 - scan_static;
+    for (ScanFn f : {scan_kernel_global, scan_kernel_own, scan_kernel_cluster})
+      CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin),
+         "cudaFuncSetAttribute");
     // Cluster tables pool the shared memory of up to 16 CTAs.
-    CK(cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1), "cudaFuncSetAttribute");
+    CK(cudaFuncSetAttribute(scan_kernel_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
+       "cudaFuncSetAttribute");
     CK(cudaFuncGetAttributes(&fa, partition_kernel), "cudaFuncGetAttributes");
     d.part_smem_optin = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;
     CK(cudaFuncSetAttribute(partition_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.part_smem_optin),
@@ -769,7 +784,7 @@ int scan_clusters(uint32_t ranks, size_t smem) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   int n = 0;
-  if (cudaOccupancyMaxActiveClusters(&n, (void*)scan_kernel, &cfg) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveClusters(&n, (void*)scan_kernel_cluster, &cfg) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
@@ -878,7 +893,7 @@ uint64_t scan_capacity(const Plan& P, DeviceState* ds) {
   if (P.sp.smem_cluster > 1)
     return (uint64_t)std::max(1, scan_clusters(P.sp.smem_cluster, P.smem)) * P.sp.smem_cluster;
   int occ = 1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_kernel, kScanThreads, P.smem) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_fn(P.sp), kScanThreads, P.smem) != cudaSuccess) {
     cudaGetLastError();
     occ = 1;
   }
@@ -898,8 +913,9 @@ uint64_t scan_grid(const Plan& P, DeviceState* ds) {
 }
 
 cudaError_t launch_scan(const ScanParams& sp, uint64_t ncta, size_t smem, cudaStream_t stream) {
-  if (sp.smem_cluster <= 1) {
-    scan_kernel<<<(unsigned)ncta, kScanThreads, smem, stream>>>(sp);
+  const ScanFn fn = scan_fn(sp);
+  if (fn != scan_kernel_cluster) {
+    fn<<<(unsigned)ncta, kScanThreads, smem, stream>>>(sp);
     return cudaGetLastError();
   }
   cudaLaunchConfig_t cfg = {};
@@ -914,7 +930,7 @@ cudaError_t launch_scan(const ScanParams& sp, uint64_t ncta, size_t smem, cudaSt
   cfg.stream = stream;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, scan_kernel, sp);
+  return cudaLaunchKernelEx(&cfg, scan_kernel_cluster, sp);
 }
 
 // A query's working buffers carved from one stream-ordered allocation:
@@ -1777,7 +1793,7 @@ DFC_API dfc_status dfc_groupby_noalloc(const dfc_query* query, int32_t device, u
   const uint64_t slots = std::min(next_pow2(std::max<uint64_t>(1024, est * 2)),
                                   next_pow2(std::max<uint64_t>(1024, P.rows * 2)));
   int occ = 1;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_kernel, kScanThreads, P.smem), "occupancy");
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_fn(P.sp), kScanThreads, P.smem), "occupancy");
   occ = std::max(1, occ);
   uint64_t ncta = (uint64_t)ds->sms * (uint64_t)occ;
   ncta = std::max<uint64_t>(1, std::min<uint64_t>(ncta, std::max<uint64_t>(1, sp.tiles)));
@@ -1840,7 +1856,7 @@ DFC_API dfc_status dfc_groupby_noalloc(const dfc_query* query, int32_t device, u
   sp.alloc = &dctl->alloc;
   sp.status = dctl->status;
   if (P.rows > 0) {
-    scan_kernel<<<(unsigned)ncta, kScanThreads, P.smem, stream>>>(sp);
+    scan_fn(sp)<<<(unsigned)ncta, kScanThreads, P.smem, stream>>>(sp);
     t_timings.launches += 1;
   }
   fp.scan = sp;

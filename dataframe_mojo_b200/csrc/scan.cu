@@ -947,12 +947,6 @@ __device__ __forceinline__ void smem_rows_in(const ScanParams& p, const Step& s,
   }
 }
 
-__device__ __forceinline__ void smem_rows(const ScanParams& p, const Step& s, const SmemTable& st,
-                                          const RowRef (&x)[kR], const uint32_t (&rows)[kR], bool (&sel)[kR],
-                                          const uint64_t (&kw)[kR]) {
-  if (st.ranks > 1) smem_rows_in<ClusterRec>(p, s, st, x, rows, sel, kw);
-  else smem_rows_in<OwnRec>(p, s, st, x, rows, sel, kw);
-}
 
 // Folds the lanes of the warp's largest group -- `grp` is each lane's group
 // mask (0 outside), `maxpop` its size -- into the group's record (`rec`, the
@@ -1165,6 +1159,7 @@ __device__ __forceinline__ void update_column(const ScanParams& p, const ValFiel
 __device__ void merge_into(const ScanParams& p, const unsigned char* src, uint32_t gid);
 
 // One pass over up to kPassRows compacted rows of a step.
+template <int R>
 __device__ __forceinline__ void consume_rows(const ScanParams& p, const Step& s, const uint16_t* idx, uint32_t nsel,
                                              uint32_t base, uint32_t shift, ClaimState* cs, const SmemTable* st) {
   const uint32_t ct = threadIdx.x - 32;
@@ -1183,8 +1178,9 @@ __device__ __forceinline__ void consume_rows(const ScanParams& p, const Step& s,
   }
   uint64_t kw[kR];
   key_words(p, s, x, kw);
-  if (st) {
-    smem_rows(p, s, *st, x, rows, sel, kw);
+  if (R != kScanGlobal && st) {
+    if constexpr (R == kScanCluster) smem_rows_in<ClusterRec>(p, s, *st, x, rows, sel, kw);
+    else if constexpr (R == kScanOwn) smem_rows_in<OwnRec>(p, s, *st, x, rows, sel, kw);
     // Every row found its shared-memory record: nothing is left for the
     // global table (a warp-uniform exit).
     bool left = false;
@@ -1302,7 +1298,11 @@ __device__ void produce_tiles(const ScanParams& p, unsigned char* smem, uint64_t
   }
 }
 
-__global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_constant__ ScanParams p) {
+// The scan body, specialised by table regime R (kScan*): each regime's
+// kernel carries only its own table code, which keeps the instruction
+// footprint of the hot loop small.
+template <int R>
+__device__ __forceinline__ void scan_body(const ScanParams& p) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int S = p.stages;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)S * p.stage_bytes);
@@ -1327,8 +1327,8 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
     s_nsel[0] = s_nsel[1] = s_nsel[2] = 0;
   }
   if (threadIdx.x < kChunkRing) s_claim.ring[threadIdx.x] = ~0ull;
-  SmemTable st{nullptr, nullptr, &s_used, p.smem_cluster > 1 ? p.smem_cluster : 1u};
-  if (p.smem_slots) {
+  SmemTable st{nullptr, nullptr, &s_used, R == kScanCluster ? p.smem_cluster : 1u};
+  if (R != kScanGlobal && p.smem_slots) {
     st.keys = reinterpret_cast<unsigned long long*>(smem + p.smem_keys_off);
     st.recs = smem + p.smem_recs_off;
     for (uint32_t s = threadIdx.x; s < p.smem_slots; s += blockDim.x) st.keys[s] = kEmpty;
@@ -1338,7 +1338,7 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
   }
   __syncthreads();
   // A cluster table: every share is initialised before any CTA probes it.
-  if (st.ranks > 1) cluster_sync_all();
+  if (R == kScanCluster) cluster_sync_all();
 
   const uint64_t T = (uint64_t)p.tile_rows;
   if (warp == 0) {
@@ -1398,7 +1398,7 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
       }
       // 3 - 5 over the compacted rows.
       for (uint32_t base = 0; base < nsel; base += kPassRows)
-        consume_rows(p, s, s_idx[b], nsel, base, shift, &s_claim, p.smem_slots ? &st : nullptr);
+        consume_rows<R>(p, s, s_idx[b], nsel, base, shift, &s_claim, p.smem_slots ? &st : nullptr);
       __syncwarp();
       for (int k = 0; k < nt; ++k)
         if (lane == 0) mbar_arrive(&empty[(it + k) % S]);
@@ -1408,8 +1408,8 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
   __syncthreads();
   // A cluster table: no CTA touches another's share after this barrier, so
   // each merges its own share and may exit.
-  if (st.ranks > 1) cluster_sync_all();
-  if (p.smem_slots && !s_abort) {
+  if (R == kScanCluster) cluster_sync_all();
+  if (R != kScanGlobal && p.smem_slots && !s_abort) {
     // The share's records find their global records through the same
     // warp-synchronous claim rounds as the rows (packed keys only; no thread
     // waits on another's claim).  Every thread runs the same passes, kR slots
@@ -1438,6 +1438,16 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
         if (sel[j]) merge_into(p, st.recs + (size_t)slot[j] * p.rec_stride, gid[j]);
     }
   }
+}
+
+__global__ void __launch_bounds__(kScanThreads, 2) scan_kernel_global(const __grid_constant__ ScanParams p) {
+  scan_body<kScanGlobal>(p);
+}
+__global__ void __launch_bounds__(kScanThreads, 2) scan_kernel_own(const __grid_constant__ ScanParams p) {
+  scan_body<kScanOwn>(p);
+}
+__global__ void __launch_bounds__(kScanThreads, 2) scan_kernel_cluster(const __grid_constant__ ScanParams p) {
+  scan_body<kScanCluster>(p);
 }
 
 // Merges one shared-memory record into global record `gid` (function.mojo:

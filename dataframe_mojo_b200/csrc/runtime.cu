@@ -25,6 +25,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -243,30 +244,27 @@ double wait_limit_seconds() {
 
 // Host-side bounded wait on the stream's work (cudaEventQuery polling).
 dfc_status wait_bounded(cudaStream_t stream) {
-  cudaEvent_t ev;
-  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+  // One completion event per thread and device, created on first use.
+  thread_local std::map<int, cudaEvent_t> events;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaEvent_t& ev = events[dev];
+  if (!ev) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
   cudaError_t e = cudaEventRecord(ev, stream);
-  if (e != cudaSuccess) {
-    cudaEventDestroy(ev);
-    return cuda_fail(e, "cudaEventRecord");
-  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
   const auto t0 = std::chrono::steady_clock::now();
   const double limit = wait_limit_seconds();
-  int spins = 0;
   while (true) {
     e = cudaEventQuery(ev);
     if (e == cudaSuccess) break;
-    if (e != cudaErrorNotReady) {
-      cudaEventDestroy(ev);
-      return cuda_fail(e, "query execution");
-    }
-    if (++spins > 64) std::this_thread::sleep_for(std::chrono::microseconds(20));
-    if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > limit) {
-      cudaEventDestroy(ev);
-      return fail(DFC_TIMEOUT, "device work did not finish within the wait limit");
-    }
+    if (e != cudaErrorNotReady) return cuda_fail(e, "query execution");
+    // Poll without sleeping for the first 2 ms (most queries end sooner, and
+    // a sleep overshoots by tens of microseconds), then every 20 us.
+    const double waited = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (waited > limit) return fail(DFC_TIMEOUT, "device work did not finish within the wait limit");
+    if (waited > 2e-3) std::this_thread::sleep_for(std::chrono::microseconds(20));
+    else std::this_thread::yield();
   }
-  cudaEventDestroy(ev);
   return DFC_OK;
 }
 
@@ -770,8 +768,29 @@ void learn_groups(const Plan& P, uint64_t groups) {
   g_learned[P.shape_sig] = groups;
 }
 
+// Occupancy answers per (kernel, cluster size, shared memory), cached: the
+// queries ask the same few shapes again and again.
+std::mutex g_occ_mu;
+std::map<std::tuple<const void*, uint32_t, size_t>, int> g_occ;
+
 // Co-resident clusters of `ranks` scan CTAs with `smem` dynamic bytes each.
+int scan_clusters_uncached(uint32_t ranks, size_t smem);
 int scan_clusters(uint32_t ranks, size_t smem) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple((const void*)scan_kernel_cluster, ranks + 64u * (uint32_t)dev, smem);
+  {
+    std::lock_guard<std::mutex> lk(g_occ_mu);
+    auto it = g_occ.find(key);
+    if (it != g_occ.end()) return it->second;
+  }
+  const int n = scan_clusters_uncached(ranks, smem);
+  std::lock_guard<std::mutex> lk(g_occ_mu);
+  g_occ[key] = n;
+  return n;
+}
+
+int scan_clusters_uncached(uint32_t ranks, size_t smem) {
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -892,10 +911,22 @@ bool plan_shared(Plan& P, DeviceState* ds, uint64_t est, uint32_t flags) {
 uint64_t scan_capacity(const Plan& P, DeviceState* ds) {
   if (P.sp.smem_cluster > 1)
     return (uint64_t)std::max(1, scan_clusters(P.sp.smem_cluster, P.smem)) * P.sp.smem_cluster;
-  int occ = 1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_fn(P.sp), kScanThreads, P.smem) != cudaSuccess) {
-    cudaGetLastError();
-    occ = 1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple((const void*)scan_fn(P.sp), 64u * (uint32_t)dev, P.smem);
+  int occ = -1;
+  {
+    std::lock_guard<std::mutex> lk(g_occ_mu);
+    auto it = g_occ.find(key);
+    if (it != g_occ.end()) occ = it->second;
+  }
+  if (occ < 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_fn(P.sp), kScanThreads, P.smem) != cudaSuccess) {
+      cudaGetLastError();
+      occ = 1;
+    }
+    std::lock_guard<std::mutex> lk(g_occ_mu);
+    g_occ[key] = occ;
   }
   return (uint64_t)ds->sms * std::max(1, occ);
 }
@@ -1974,7 +2005,8 @@ struct BatchItem {
 // stream 0, one after another (two such scans side by side only interleave
 // and share L2 between their tables); smaller queries spread over the rest.
 int item_stream(const BatchItem& it, int& k) {
-  if (it.full_grid) return 0;
+  static const bool serial = getenv("DFC_BATCH_SERIAL") != nullptr;  // tuning: every query on stream 0
+  if (it.full_grid || serial) return 0;
   return 1 + (k++ % (kBatchStreams - 1));
 }
 

@@ -2005,8 +2005,7 @@ struct BatchItem {
 // stream 0, one after another (two such scans side by side only interleave
 // and share L2 between their tables); smaller queries spread over the rest.
 int item_stream(const BatchItem& it, int& k) {
-  static const bool serial = getenv("DFC_BATCH_SERIAL") != nullptr;  // tuning: every query on stream 0
-  if (it.full_grid || serial) return 0;
+  if (it.full_grid) return 0;
   return 1 + (k++ % (kBatchStreams - 1));
 }
 

@@ -438,4 +438,5 @@ def pack_validity(valid: np.ndarray | None) -> np.ndarray | None:
 
 
 def unpack_validity(bits: np.ndarray, rows: int) -> np.ndarray:
-    return np.unpackbits(bits, bitorder="little")[:rows].astype(bool)
+    # unpackbits yields 0/1 bytes, which are valid booleans: a view, no copy.
+    return np.unpackbits(bits, bitorder="little")[:rows].view(bool)

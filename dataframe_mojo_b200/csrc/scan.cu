@@ -376,7 +376,9 @@ __device__ __forceinline__ uint64_t entry_meta(const ScanParams& p, const KeyEnt
 }
 
 // The group of key word kw at row `row`, claiming a new record if the key is
-// new: the per-lane path for ticket keys, the all-ones key word and merges.
+// new: the per-lane path for ticket keys and the all-ones key word (one-step
+// claims: a 128-bit CAS of key and reserved record; a lost race leaves the
+// reserved record unused).
 // Visits slots in the same order as the lock-step rounds.  kNoGid when
 // records or table slots ran out (ST_CAPACITY set).
 __device__ __noinline__ uint32_t find_or_claim(const ScanParams& p, uint64_t kw, uint32_t row, ClaimState* cs) {

@@ -77,3 +77,37 @@ def test_memory_admission_one_at_a_time():
     for cols in keep:
         for c in cols:
             c.release()
+
+
+def test_full_grid_requests_two_in_flight():
+    """Requests whose scans fill every SM (2M rows each): the server keeps at
+    most two of them in flight, reuses finished requests' working memory, and
+    every result matches the query run alone."""
+    rng = np.random.default_rng(17)
+    jobs, keep = [], []
+    from dataframe_mojo_b200.frame import bind, col
+    from test_gpu_parity import random_frame
+
+    frames = [random_frame(rng, 2_000_000, [np.int32], [np.int64, np.float64], null_rate=0.02) for _ in range(2)]
+    for i in range(12):
+        frame = frames[i % 2]
+        plan = frame.lazy().filter(col("p") >= int(rng.integers(0, 60))).group_by("k0", maintain_order=True).agg(
+            [col("v0").sum().alias("s0"), col("v0").min().alias("lo0"), col("v0").max().alias("hi0"),
+             col("v0").count().alias("n0"), col("v1").mean().alias("m1"), col("v1").var().alias("var1"),
+             col("v1").min().alias("lo1"), col("v1").max().alias("hi1"), col("v1").count().alias("n1")])
+        bound = bind(plan.plan)
+        cols = [provider.DeviceColumn(s) for s in bound.series]
+        keep.append(cols)
+        jobs.append((bound, cols))
+    server = provider.Server(max_inflight=16)
+    try:
+        got = serve_all(server, jobs)
+        stats = server.stats()
+        assert stats["completed"] == len(jobs)
+        assert stats["max_inflight_seen"] <= 2, stats
+    finally:
+        server.close()
+    check_against_alone(jobs, got)
+    for cols in keep:
+        for c in cols:
+            c.release()

@@ -62,6 +62,7 @@ struct dfc_result {
   int32_t device = 0;
   uint64_t rows = 0;
   std::vector<ResultCol> cols;
+  void* slab = nullptr;  // every column's buffers, carved from one allocation
   std::atomic<int> refs{1};
 };
 
@@ -964,6 +965,43 @@ cudaError_t launch_scan(const ScanParams& sp, uint64_t ncta, size_t smem, cudaSt
   return cudaLaunchKernelEx(&cfg, scan_kernel_cluster, sp);
 }
 
+// A query's output columns, sized for out_rows groups, carved from one
+// stream-ordered allocation (256-byte aligned pieces: each column's values,
+// then its validity words).  One allocation instead of two per column.
+cudaError_t alloc_result_cols(const Plan& P, uint64_t out_rows, std::vector<ResultCol>& rc, void** slab,
+                              cudaStream_t stream) {
+  rc.assign(P.n_out, ResultCol{});
+  auto piece = [](uint64_t bytes) { return (std::max<uint64_t>(bytes, 256) + 255) & ~(uint64_t)255; };
+  std::vector<uint64_t> off(2 * (size_t)P.n_out);
+  uint64_t total = 0;
+  for (int c = 0; c < P.n_out; ++c) {
+    off[2 * c] = total;
+    total += piece(out_rows * dtype_size(P.out_dtype[c]));
+    off[2 * c + 1] = total;
+    total += piece(((out_rows + 31) / 32) * 4);
+  }
+  cudaError_t e = cudaMallocAsync(slab, std::max<uint64_t>(total, 256), stream);
+  if (e != cudaSuccess) {
+    *slab = nullptr;
+    cudaGetLastError();
+    return e;
+  }
+  unsigned char* base = static_cast<unsigned char*>(*slab);
+  for (int c = 0; c < P.n_out; ++c) {
+    rc[c].dtype = (dfc_dtype)P.out_dtype[c];
+    rc[c].values = base + off[2 * c];
+    rc[c].validity = reinterpret_cast<uint32_t*>(base + off[2 * c + 1]);
+  }
+  return cudaSuccess;
+}
+
+// Releases output columns that did not become a result.
+void release_result_cols(std::vector<ResultCol>& rc, void*& slab, cudaStream_t stream) {
+  if (slab) cudaFreeAsync(slab, stream);
+  slab = nullptr;
+  for (auto& r : rc) r.values = nullptr, r.validity = nullptr;
+}
+
 // A query's working buffers carved from one stream-ordered allocation:
 // alloc() records each request (256-byte aligned), commit() allocates the
 // block and sets every recorded pointer.
@@ -1160,27 +1198,16 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   // Output columns sized for the group capacity (the group count is known
   // only on the device; the host reads it once, at the end).
   const uint64_t out_rows = std::min<uint64_t>(P.rows, recs);
-  std::vector<ResultCol> rc(P.n_out);
-  for (int c = 0; c < P.n_out; ++c) {
-    rc[c].dtype = (dfc_dtype)P.out_dtype[c];
-    cudaError_t e = cudaMallocAsync(&rc[c].values, std::max<uint64_t>(256, out_rows * dtype_size(P.out_dtype[c])), stream);
-    if (e == cudaSuccess)
-      e = cudaMallocAsync((void**)&rc[c].validity, std::max<uint64_t>(256, ((out_rows + 31) / 32) * 4), stream);
+  std::vector<ResultCol> rc;
+  void* out_slab = nullptr;
+  {
+    const cudaError_t e = alloc_result_cols(P, out_rows, rc, &out_slab, stream);
     if (e != cudaSuccess) {
-      for (auto& r : rc) {
-        if (r.values) cudaFreeAsync(r.values, stream);
-        if (r.validity) cudaFreeAsync(r.validity, stream);
-      }
       S.release();
       return cuda_fail(e, "output columns");
     }
   }
-  auto free_outputs = [&]() {
-    for (auto& r : rc) {
-      if (r.values) cudaFreeAsync(r.values, stream);
-      if (r.validity) cudaFreeAsync(r.validity, stream);
-    }
-  };
+  auto free_outputs = [&]() { release_result_cols(rc, out_slab, stream); };
 
   Control* dctl = static_cast<Control*>(ctl);
   cudaError_t e;
@@ -1369,6 +1396,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   r->rows = host_ctl->groups;
   for (int c = 0; c < P.n_out; ++c) rc[c].has_nulls = host_ctl->has_nulls[c] != 0;
   r->cols = std::move(rc);
+  r->slab = out_slab;
   *out = r;
   return DFC_OK;
 }
@@ -1634,9 +1662,13 @@ DFC_API void dfc_result_free(dfc_result* result) {
   if (result->refs.fetch_sub(1) != 1) return;
   DeviceGuard guard(result->device);
   cudaStream_t stream = thread_stream(result->device);
-  for (auto& c : result->cols) {
-    if (c.values) cudaFreeAsync(c.values, stream);
-    if (c.validity) cudaFreeAsync(c.validity, stream);
+  if (result->slab) {
+    cudaFreeAsync(result->slab, stream);
+  } else {
+    for (auto& c : result->cols) {
+      if (c.values) cudaFreeAsync(c.values, stream);
+      if (c.validity) cudaFreeAsync(c.validity, stream);
+    }
   }
   delete result;
 }
@@ -1999,6 +2031,7 @@ struct BatchItem {
   bool full_grid = false;  // the scan's grid fills every SM
   size_t off_table = 0, off_records = 0, off_bits = 0, off_prefix = 0, off_bsums = 0, off_perm = 0, off_firsts = 0;
   std::vector<ResultCol> rc;
+  void* slab = nullptr;  // rc's buffers
 };
 
 // The stream of a sized query: a scan whose grid fills every SM runs on
@@ -2044,19 +2077,10 @@ dfc_status size_item(const dfc_query* q, BatchItem& it, DeviceState* ds, cudaStr
   return DFC_OK;
 }
 
-// Output columns of a sized query (stream-ordered allocations).
+// Output columns of a sized query (one stream-ordered allocation).
 dfc_status alloc_outputs(BatchItem& it, cudaStream_t stream) {
-  it.rc.resize(it.P.n_out);
-  for (int c = 0; c < it.P.n_out; ++c) {
-    it.rc[c].dtype = (dfc_dtype)it.P.out_dtype[c];
-    cudaError_t e = cudaMallocAsync(&it.rc[c].values, std::max<uint64_t>(256, it.out_rows * dtype_size(it.P.out_dtype[c])), stream);
-    if (e == cudaSuccess)
-      e = cudaMallocAsync((void**)&it.rc[c].validity, std::max<uint64_t>(256, ((it.out_rows + 31) / 32) * 4), stream);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      return fail(DFC_OOM, "output columns");
-    }
-  }
+  if (alloc_result_cols(it.P, it.out_rows, it.rc, &it.slab, stream) != cudaSuccess)
+    return fail(DFC_OOM, "output columns");
   return DFC_OK;
 }
 
@@ -2084,6 +2108,8 @@ dfc_status finish_item(const dfc_query* q, BatchItem& it, const Control& c, int 
   r->rows = c.groups;
   for (int col = 0; col < it.P.n_out; ++col) it.rc[col].has_nulls = c.has_nulls[col] != 0;
   r->cols = std::move(it.rc);
+  r->slab = it.slab;
+  it.slab = nullptr;
   *out = r;
   learn_groups(it.P, c.groups);
   return DFC_OK;
@@ -2199,14 +2225,7 @@ DFC_API dfc_status dfc_groupby_batch(const dfc_query* const* queries, int32_t n,
     if (arena) cudaFreeAsync(arena, main);
     return cuda_fail(e, "batch working memory");
   }
-  auto free_outputs = [&](BatchItem& it) {
-    for (auto& r : it.rc) {
-      if (r.values) cudaFreeAsync(r.values, main);
-      if (r.validity) cudaFreeAsync(r.validity, main);
-      r.values = nullptr;
-      r.validity = nullptr;
-    }
-  };
+  auto free_outputs = [&](BatchItem& it) { release_result_cols(it.rc, it.slab, main); };
   for (int i = 0; i < n; ++i) {
     BatchItem& it = items[i];
     if (it.st) continue;
@@ -2469,10 +2488,7 @@ bool server_launch(dfc_server* sv, Request* r, int& k) {
   if (e == cudaSuccess && alloc_outputs(it, stream)) e = cudaErrorMemoryAllocation;
   if (e != cudaSuccess) {
     cudaGetLastError();
-    for (auto& c : it.rc) {
-      if (c.values) cudaFreeAsync(c.values, stream);
-      if (c.validity) cudaFreeAsync(c.validity, stream);
-    }
+    release_result_cols(it.rc, it.slab, stream);
     if (r->arena) arena_put(sv, r);
     if (r->dctl) cudaFreeAsync(r->dctl, stream);
     {
@@ -2510,12 +2526,7 @@ void server_finish(dfc_server* sv, Request* r) {
   cudaFreeAsync(r->dctl, r->stream);
   dfc_status st = finish_item(&r->oq.q, r->item, c, sv->device, &res);
   std::string msg = st ? t_error : std::string();
-  if (st) {
-    for (auto& col : r->item.rc) {
-      if (col.values) cudaFreeAsync(col.values, r->stream);
-      if (col.validity) cudaFreeAsync(col.validity, r->stream);
-    }
-  }
+  if (st) release_result_cols(r->item.rc, r->item.slab, r->stream);
   if (st == DFC_CAPACITY) {  // alone, with regrowth
     st = dfc_groupby(&r->oq.q, &res);
     msg = st ? t_error : std::string();

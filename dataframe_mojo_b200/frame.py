@@ -47,7 +47,12 @@ def np_dtype(code: int) -> np.dtype:
 
 
 class Series:
-    """A named column: values plus an optional validity mask (True = valid)."""
+    """A named column: values plus an optional validity mask (True = valid).
+
+    A column made by `from_bits` keeps its validity as the packed bitmap it
+    came with (bit i of byte i // 8 set = row i valid, the layout the
+    reference's columns and the provider use) and unpacks it to the bool
+    mask only when `valid` is first read."""
 
     def __init__(self, name: str, values, valid=None, dtype=None):
         arr = np.asarray(values, dtype=dtype)
@@ -56,13 +61,50 @@ class Series:
         dfc_dtype(arr.dtype)
         self.name = name
         self.values = np.ascontiguousarray(arr)
+        self._bits = None
+        self.valid = valid
+
+    @classmethod
+    def from_bits(cls, name: str, values, bits: np.ndarray | None) -> "Series":
+        """A column over `values` whose validity is the packed bitmap `bits`
+        (None = every row valid).  The bitmap is kept, not copied."""
+        s = cls(name, values)
+        n = len(s.values)
+        if bits is not None:
+            bits = np.asarray(bits, dtype=np.uint8)
+            if len(bits) < (n + 7) // 8:
+                raise ValueError("validity bitmap shorter than the values")
+            if not bits_all_set(bits, n):
+                s._bits = bits[: (n + 7) // 8]
+        return s
+
+    @property
+    def valid(self) -> np.ndarray | None:
+        if self._bits is not None:
+            self._valid = unpack_validity(self._bits, len(self.values))
+            self._bits = None
+        return self._valid
+
+    @valid.setter
+    def valid(self, valid) -> None:
         if valid is not None:
             valid = np.asarray(valid, dtype=bool)
             if valid.shape != self.values.shape:
                 raise ValueError("validity length differs from values")
             if valid.all():
                 valid = None
-        self.valid = valid
+        self._bits = None
+        self._valid = valid
+
+    @property
+    def has_nulls(self) -> bool:
+        return self._bits is not None or self._valid is not None
+
+    def validity_bits(self) -> np.ndarray | None:
+        """The validity as a packed little-endian bitmap (None = all valid)."""
+        if self._bits is not None:
+            return self._bits
+        return pack_validity(self._valid)
 
     def __len__(self) -> int:
         return len(self.values)
@@ -435,6 +477,18 @@ def pack_validity(valid: np.ndarray | None) -> np.ndarray | None:
     if valid is None:
         return None
     return np.packbits(valid.astype(np.uint8), bitorder="little")
+
+
+def bits_all_set(bits: np.ndarray, rows: int) -> bool:
+    """Whether the first `rows` bits of a little-endian bitmap are all set."""
+    full = rows // 8
+    head = full - full % 8
+    if head and not np.all(bits[:head].view(np.uint64) == np.uint64(0xFFFFFFFFFFFFFFFF)):
+        return False
+    if full > head and not np.all(bits[head:full] == 0xFF):
+        return False
+    rem = rows % 8
+    return not rem or (int(bits[full]) & ((1 << rem) - 1)) == (1 << rem) - 1
 
 
 def unpack_validity(bits: np.ndarray, rows: int) -> np.ndarray:

@@ -28,7 +28,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _native as N
-from .frame import Bound, DataFrame, LazyFrame, Plan, Series, bind, dfc_dtype, np_dtype, pack_validity, unpack_validity
+from .frame import Bound, DataFrame, LazyFrame, Plan, Series, bind, dfc_dtype, np_dtype
 
 BACKEND = "cuda"
 MEMORY_DISCRETE = 1
@@ -126,7 +126,7 @@ class DeviceColumn:
         self.dtype = series.dtype
         self.rows = len(series)
         self.device = device
-        bits = pack_validity(series.valid)
+        bits = series.validity_bits()
         handle = C.c_void_p()
         if device_pointer is None:
             values = series.values
@@ -224,8 +224,7 @@ class DeviceResult:
                     bits.ctypes.data if bits is not None and self.rows else None,
                 )
             )
-            valid = unpack_validity(bits, self.rows) if bits is not None else None
-            cols.append(Series(name, values, valid))
+            cols.append(Series.from_bits(name, values, bits))
         return DataFrame(cols)
 
     def free(self) -> None:

@@ -110,3 +110,38 @@ def test_cpu_engine_is_not_part_of_the_provider():
     plan = config1_plan(config1(rows=10))
     with pytest.raises(ValueError):
         plan.collect(engine="cpu")
+
+
+@pytest.mark.parametrize("rows", [0, 1, 7, 8, 9, 63, 64, 65, 1000, 4099])
+def test_packed_validity_series(rows):
+    """Result columns keep the packed bitmap they were copied into and unpack
+    it on first use; an all-set bitmap means no nulls."""
+    from dataframe_mojo_b200.frame import bits_all_set, pack_validity
+
+    rng = np.random.default_rng(rows)
+    values = rng.integers(0, 100, rows).astype(np.int64)
+    all_set = np.full((rows + 7) // 8 + 3, 0xFF, np.uint8)  # longer than needed, tail bytes ignored
+    s = Series.from_bits("x", values, all_set)
+    assert not s.has_nulls and s.valid is None and s.validity_bits() is None
+    assert bits_all_set(all_set, rows)
+
+    valid = rng.random(rows) < 0.7
+    if rows:
+        valid[-1] = False  # a null in the last (possibly partial) byte
+    bits = pack_validity(valid)
+    padded = np.concatenate([bits, np.zeros(2, np.uint8)]) if rows else bits
+    s = Series.from_bits("x", values, padded)
+    assert s.has_nulls == (rows > 0)
+    if rows:
+        assert not bits_all_set(bits, rows)
+        assert np.array_equal(s.validity_bits(), bits)  # kept packed, not repacked
+        assert np.array_equal(s.valid, valid)
+        assert s.equals(Series("x", values, valid))
+        assert s.to_list() == [int(v) if ok else None for v, ok in zip(values, valid)]
+    # Bits beyond `rows` in the last byte do not count.
+    if rows % 8:
+        tail = pack_validity(np.ones(rows, bool))
+        tail[-1] &= (1 << (rows % 8)) - 1
+        assert bits_all_set(tail, rows)
+    with pytest.raises(ValueError):
+        Series.from_bits("x", np.zeros(64, np.int64), np.zeros(7, np.uint8))

@@ -32,21 +32,51 @@ __global__ void normalize_validity(const uint8_t* src, uint64_t nbytes, uint64_t
   if ((threadIdx.x & 31) == 0 && local) atomicAdd(valid_rows, local);
 }
 
-// Order-encoded minimum and maximum of the valid values of a column
-// (out[0] = min, out[1] = max; NaN skipped).  Bounds a key's domain when the
-// planner sizes the group table.
-__global__ void column_minmax(DevColumn c, uint64_t rows, unsigned long long* out) {
+// One HyperLogLog update: register = the hash's top kHllBits bits, value =
+// the position of the first set bit of the rest.
+__device__ __forceinline__ void hll_add(uint32_t* local, uint64_t h) {
+  const uint32_t reg = (uint32_t)(h >> (64 - kHllBits));
+  const uint64_t rest = h << kHllBits;
+  const uint32_t rho = rest == 0 ? (65 - kHllBits) : (uint32_t)__clzll(rest) + 1;
+  if (rho > local[reg]) atomicMax(&local[reg], rho);
+}
+
+// Statistics of a column in one pass: the order-encoded minimum and maximum
+// of its valid values (mm[0] = min, mm[1] = max; NaN skipped), which bound a
+// key's domain when the planner sizes the group table, and the HyperLogLog
+// sketch (2^kHllBits registers) of its distinct valid values under group
+// equality (floats canonical).  Each thread loads kStatsUnroll rows, a grid
+// stride apart, before it uses any of them, so that enough loads are in
+// flight to stream the column at HBM rate; each block keeps its registers in
+// shared memory and merges them into `regs` with atomicMax.
+__global__ void column_stats(DevColumn c, uint64_t rows, unsigned long long* mm, uint32_t* regs) {
+  __shared__ uint32_t local[1u << kHllBits];
+  for (uint32_t i = threadIdx.x; i < (1u << kHllBits); i += blockDim.x) local[i] = 0;
+  __syncthreads();
   unsigned long long lo = ~0ull, hi = 0ull;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < rows; i += (uint64_t)gridDim.x * blockDim.x) {
-    if (c.validity && !bit_valid(c.validity, i)) continue;
-    const uint64_t b = load_bits(c.values, c.size, i);
-    if (dt_float(c.dtype)) {
-      const double d = bits_to_f64(b, c.dtype);
-      if (d != d) continue;
+  const bool is_f = dt_float(c.dtype);
+  const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; base < rows; base += step * kStatsUnroll) {
+    uint64_t b[kStatsUnroll];
+    bool ok[kStatsUnroll];
+#pragma unroll
+    for (int j = 0; j < kStatsUnroll; ++j) {
+      const uint64_t i = base + j * step;
+      ok[j] = i < rows && (!c.validity || bit_valid(c.validity, i));
+      b[j] = ok[j] ? load_bits(c.values, c.size, i) : 0ull;
     }
-    const uint64_t e = order_encode(b, c.dtype);
-    lo = e < lo ? e : lo;
-    hi = e > hi ? e : hi;
+#pragma unroll
+    for (int j = 0; j < kStatsUnroll; ++j) {
+      if (!ok[j]) continue;
+      hll_add(local, mix64(key_cell(b[j], c.dtype) ^ 0xD6E8FEB86659FD93ull));
+      if (is_f) {
+        const double d = bits_to_f64(b[j], c.dtype);
+        if (d != d) continue;
+      }
+      const uint64_t e = order_encode(b[j], c.dtype);
+      lo = e < lo ? e : lo;
+      hi = e > hi ? e : hi;
+    }
   }
   for (int o = 16; o > 0; o >>= 1) {
     const unsigned long long a = __shfl_xor_sync(0xffffffffu, lo, o);
@@ -55,25 +85,8 @@ __global__ void column_minmax(DevColumn c, uint64_t rows, unsigned long long* ou
     hi = b > hi ? b : hi;
   }
   if ((threadIdx.x & 31) == 0) {
-    atomicMin(&out[0], lo);
-    atomicMax(&out[1], hi);
-  }
-}
-
-// HyperLogLog sketch (2^kHllBits registers) of a column's distinct valid
-// values under group equality (floats canonical).  Each block keeps its
-// registers in shared memory and merges them into `regs` with atomicMax.
-__global__ void column_hll(DevColumn c, uint64_t rows, uint32_t* regs) {
-  __shared__ uint32_t local[1u << kHllBits];
-  for (uint32_t i = threadIdx.x; i < (1u << kHllBits); i += blockDim.x) local[i] = 0;
-  __syncthreads();
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < rows; i += (uint64_t)gridDim.x * blockDim.x) {
-    if (c.validity && !bit_valid(c.validity, i)) continue;
-    const uint64_t h = mix64(key_cell(load_bits(c.values, c.size, i), c.dtype) ^ 0xD6E8FEB86659FD93ull);
-    const uint32_t reg = (uint32_t)(h >> (64 - kHllBits));
-    const uint64_t rest = h << kHllBits;
-    const uint32_t rho = rest == 0 ? (65 - kHllBits) : (uint32_t)__clzll(rest) + 1;
-    if (rho > local[reg]) atomicMax(&local[reg], rho);
+    atomicMin(&mm[0], lo);
+    atomicMax(&mm[1], hi);
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < (1u << kHllBits); i += blockDim.x)
@@ -105,16 +118,23 @@ __device__ __forceinline__ uint64_t query_key_word(const ScanParams& p, uint64_t
   return kw;
 }
 
+// Rows are loaded kKeysUnroll at a time per thread (all key columns of
+// each) before any register update, as in column_stats.
 __global__ void keys_hll(const __grid_constant__ ScanParams p, uint32_t* regs) {
   __shared__ uint32_t local[1u << kHllBits];
   for (uint32_t i = threadIdx.x; i < (1u << kHllBits); i += blockDim.x) local[i] = 0;
   __syncthreads();
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < p.rows; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t h = mix64(query_key_word(p, i) ^ 0xD6E8FEB86659FD93ull);
-    const uint32_t reg = (uint32_t)(h >> (64 - kHllBits));
-    const uint64_t rest = h << kHllBits;
-    const uint32_t rho = rest == 0 ? (65 - kHllBits) : (uint32_t)__clzll(rest) + 1;
-    if (rho > local[reg]) atomicMax(&local[reg], rho);
+  const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; base < p.rows; base += step * kKeysUnroll) {
+    uint64_t kw[kKeysUnroll];
+#pragma unroll
+    for (int j = 0; j < kKeysUnroll; ++j) {
+      const uint64_t i = base + j * step;
+      kw[j] = i < p.rows ? query_key_word(p, i) : 0ull;
+    }
+#pragma unroll
+    for (int j = 0; j < kKeysUnroll; ++j)
+      if (base + j * step < p.rows) hll_add(local, mix64(kw[j] ^ 0xD6E8FEB86659FD93ull));
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < (1u << kHllBits); i += blockDim.x)

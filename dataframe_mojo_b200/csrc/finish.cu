@@ -297,8 +297,14 @@ __device__ uint64_t output_cell(const FinishParams& f, const OutCol& oc, const u
   return 0;
 }
 
+// Output columns with any null are noted per block in shared memory and
+// reported with one global atomicOr per block and column (a per-warp atomic
+// on the same word serialises in L2 when most warps hold a null group).
 __global__ void finish_output(const __grid_constant__ FinishParams f) {
   const ScanParams& p = f.scan;
+  __shared__ uint32_t block_nulls[kMaxOut];
+  for (int c = threadIdx.x; c < kMaxOut; c += blockDim.x) block_nulls[c] = 0;
+  __syncthreads();
   const uint32_t G = f.groups[0];
   const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const uint64_t gwarp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
@@ -322,10 +328,13 @@ __global__ void finish_output(const __grid_constant__ FinishParams f) {
       if (lane == 0) {
         oc.validity[wbase >> 5] = bits;
         const uint32_t want = (G - wbase >= 32) ? 0xffffffffu : ((1u << (G - wbase)) - 1u);
-        if (bits != want) atomicOr(&f.has_nulls[c], 1u);
+        if (bits != want) block_nulls[c] = 1u;
       }
     }
   }
+  __syncthreads();
+  for (int c = threadIdx.x; c < f.n_out; c += blockDim.x)
+    if (block_nulls[c]) atomicOr(&f.has_nulls[c], 1u);
 }
 
 }  // namespace dfc

@@ -44,9 +44,10 @@ __global__ void finish_output(const __grid_constant__ FinishParams f);
 namespace dfc {
 __global__ void normalize_validity(const uint8_t* src, uint64_t nbytes, uint64_t off, uint64_t rows, uint32_t* dst,
                                    unsigned long long* valid_rows);
-__global__ void column_minmax(DevColumn c, uint64_t rows, unsigned long long* out);
 constexpr int kHllBits = 12;
-__global__ void column_hll(DevColumn c, uint64_t rows, uint32_t* regs);
+constexpr int kStatsUnroll = 8;  // rows in flight per thread in column_stats
+constexpr int kKeysUnroll = 4;   // and in keys_hll (each row loads every key column)
+__global__ void column_stats(DevColumn c, uint64_t rows, unsigned long long* mm, uint32_t* regs);
 __global__ void keys_hll(const __grid_constant__ ScanParams p, uint32_t* regs);
 __global__ void keys_sample(const __grid_constant__ ScanParams p, unsigned long long* out, uint32_t n, uint64_t stride);
 }  // namespace dfc

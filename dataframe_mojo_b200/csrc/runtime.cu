@@ -604,6 +604,23 @@ double hll_estimate(const std::vector<uint32_t>& regs) {
   return est;
 }
 
+// Resident 256-thread blocks per SM of a statistics kernel (cached): its
+// grid-stride loop then runs in one wave.
+unsigned stats_blocks_per_sm(const void* fn) {
+  static std::mutex mu;
+  static std::map<const void*, int> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(fn);
+  if (it != cache.end()) return (unsigned)it->second;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 256, 0) != cudaSuccess || n < 1) {
+    cudaGetLastError();
+    n = 4;
+  }
+  cache[fn] = n;
+  return (unsigned)n;
+}
+
 // Distinct key words of the query over all rows (HyperLogLog; 0 on failure).
 double joint_key_estimate(const Plan& P, DeviceState* ds, cudaStream_t stream) {
   const uint32_t nreg = 1u << kHllBits;
@@ -612,7 +629,7 @@ double joint_key_estimate(const Plan& P, DeviceState* ds, cudaStream_t stream) {
   cudaError_t e = cudaMallocAsync((void**)&d_regs, nreg * 4, stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_regs, 0, nreg * 4, stream);
   if (e == cudaSuccess) {
-    const unsigned blocks = (unsigned)std::min<uint64_t>((P.rows + 255) / 256, (uint64_t)ds->sms * 4);
+    const unsigned blocks = (unsigned)std::min<uint64_t>((P.rows + 255) / 256, (uint64_t)ds->sms * stats_blocks_per_sm((const void*)keys_hll));
     keys_hll<<<std::max(1u, blocks), 256, 0, stream>>>(P.sp, d_regs);
     e = cudaGetLastError();
   }
@@ -640,9 +657,8 @@ dfc_status ensure_stats(dfc_column* c, DeviceState* ds, cudaStream_t stream) {
   if (e == cudaSuccess) e = cudaMemsetAsync(d_regs, 0, nreg * 4, stream);
   if (e == cudaSuccess) {
     DevColumn dc{c->values, c->validity, c->dtype, dtype_size(c->dtype)};
-    const unsigned blocks = (unsigned)std::min<uint64_t>((c->rows + 255) / 256, (uint64_t)ds->sms * 4);
-    column_minmax<<<std::max(1u, blocks), 256, 0, stream>>>(dc, c->rows, d_mm);
-    column_hll<<<std::max(1u, blocks), 256, 0, stream>>>(dc, c->rows, d_regs);
+    const unsigned blocks = (unsigned)std::min<uint64_t>((c->rows + 255) / 256, (uint64_t)ds->sms * stats_blocks_per_sm((const void*)column_stats));
+    column_stats<<<std::max(1u, blocks), 256, 0, stream>>>(dc, c->rows, d_mm, d_regs);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(h_mm, d_mm, 16, cudaMemcpyDeviceToHost, stream);
@@ -747,18 +763,31 @@ void measure_skew(Plan& P, DeviceState* ds, cudaStream_t stream) {
     cudaGetLastError();
     return;
   }
-  std::sort(h.begin(), h.end());
-  std::vector<uint32_t> runs;
-  for (uint32_t i = 0; i < n;) {
-    uint32_t j = i + 1;
-    while (j < n && h[j] == h[i]) ++j;
-    runs.push_back(j - i);
-    i = j;
+  // Rows per distinct key word (open addressing over at least 2n slots),
+  // then a histogram of those counts: the largest count, and the rows the
+  // kHotSlots most frequent keys cover, without sorting the sample.
+  const uint32_t cap = (uint32_t)next_pow2(2ull * n);
+  std::vector<unsigned long long> keys(cap);
+  std::vector<uint32_t> count(cap, 0);
+  const int shift = 64 - __builtin_ctzll(cap);
+  for (uint32_t i = 0; i < n; ++i) {
+    uint32_t slot = shift >= 64 ? 0 : (uint32_t)((h[i] * 0x9E3779B97F4A7C15ull) >> shift);
+    while (count[slot] && keys[slot] != h[i]) slot = (slot + 1) & (cap - 1);
+    keys[slot] = h[i];
+    count[slot] += 1;
   }
-  std::sort(runs.begin(), runs.end(), std::greater<uint32_t>());
-  uint64_t hot = 0;
-  for (size_t i = 0; i < runs.size() && i < kHotSlots; ++i) hot += runs[i];
-  P.top1 = (double)runs[0] / n;
+  std::vector<uint32_t> keys_with(n + 1, 0);
+  for (uint32_t c : count)
+    if (c) keys_with[c] += 1;
+  uint32_t top = n;
+  while (top > 1 && keys_with[top] == 0) --top;
+  uint64_t hot = 0, taken = 0;
+  for (uint32_t c = top; c >= 1 && taken < kHotSlots; --c) {
+    const uint64_t k = std::min<uint64_t>(keys_with[c], kHotSlots - taken);
+    hot += k * c;
+    taken += k;
+  }
+  P.top1 = (double)top / n;
   P.top_hot = (double)hot / n;
   std::lock_guard<std::mutex> lk(g_learn_mu);
   g_skew[P.key_sig] = {P.top1, P.top_hot};

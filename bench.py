@@ -14,7 +14,8 @@ timed with CUDA events on the query's stream, max over ranks.  Inputs are
 `e2e` = the same query through the C ABI with host buffers: every step
 registers the inputs from pinned host memory (host->device copies), runs the
 query and copies every result column back (device->host), timed by CUDA
-events on the library's stream.
+events on the library's stream; `e2e.phases_ms` splits one further, untimed
+step by the host clock into upload, query, download and release.
 
 `--impl reference` times the CPU restatement of the reference's parallel
 aggregate table (oracle/, all host threads) on a bounded sample of the same
@@ -749,18 +750,30 @@ def main() -> int:
         for n, t in out_types.items()
     }
 
-    def e2e_step():
+    def e2e_step(marks=None):
+        # `marks`: host clock readings after each phase (upload, query,
+        # download, release), each after a device synchronisation.
+        def mark():
+            if marks is not None:
+                torch.cuda.synchronize()
+                marks.append(time.perf_counter())
+
+        mark()
         dcols = {}
         for n in ("k1", "k2", "v", "p"):
             dcols[n] = provider.DeviceColumn.from_host_pointer(
                 n, dtypes[n], rows, host[n].data_ptr(), host_bits.data_ptr() if n == "v" else None, 0, device
             )
+        mark()
         res = provider.run_bound(bound, [dcols[n] for n in bound.names])
+        mark()
         frame = res.to_frame(into=pinned_out)
         out_bytes = sum(frame.column(c).values.nbytes + (len(frame.column(c)) + 7) // 8 for c in frame.columns)
+        mark()
         res.free()
         for c in dcols.values():
             c.release()
+        mark()
         return out_bytes
 
     for _ in range(1):
@@ -776,6 +789,11 @@ def main() -> int:
         d2h = e2e_step()
     e1.record(e2e_stream)
     torch.cuda.synchronize()
+    # One more step, after the timed ones and not part of them, read by the
+    # host clock phase by phase: what an end-to-end step is made of.
+    marks = []
+    e2e_step(marks)
+    phases = {k: (b - a) * 1e3 for k, a, b in zip(("upload", "query", "download", "release"), marks, marks[1:])}
     provider.set_thread_stream(device, None)
     e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
     et = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
@@ -788,6 +806,7 @@ def main() -> int:
         "d2h_bytes_per_step": int(d2h),
         "steps": args.e2e_steps,
         "ms_per_step": float(et.item()),
+        "phases_ms": {k: round(v, 3) for k, v in phases.items()},
     }
 
     cpu = None

@@ -275,6 +275,18 @@ uint64_t next_pow2(uint64_t x) {
   return p;
 }
 
+// Global-table slots per estimated group (a power of two, 2 to 16; default
+// 8, DFC_TABLE_FACTOR=<n> sets it): the table's load stays at most 1/factor
+// of the estimate.  Record capacity follows the estimate, not the table.
+uint64_t table_factor() {
+  static const uint64_t f = [] {
+    const char* env = getenv("DFC_TABLE_FACTOR");
+    const long v = env && *env ? atol(env) : 8;
+    return (v == 2 || v == 4 || v == 8 || v == 16) ? (uint64_t)v : 8ull;
+  }();
+  return f;
+}
+
 // Host decoding of the order encoding (kernels' order_encode) for integer ranges.
 __int128 order_value(uint64_t e, int dt) {
   if (is_unsigned(dt)) return (__int128)e;
@@ -1189,10 +1201,10 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
     // Pass B appends every group exactly once: no holes, no chunks.
     recs = std::max<uint64_t>(1, pp->recs);
   } else {
-    // Records: the groups the table may hold (load factor <= 1/8: the lock-step
-    // probe rounds run as long as a warp's longest chain) plus every CTA's
-    // partly used last chunk.
-    const uint64_t groups_cap = std::min<uint64_t>(P.rows, slots / 8);
+    // Records: the groups the table may hold (load factor <= 1/table_factor:
+    // the lock-step probe rounds run as long as a warp's longest chain) plus
+    // every CTA's partly used last chunk.
+    const uint64_t groups_cap = std::min<uint64_t>(P.rows, slots / table_factor());
     while (chunk < 1024 && chunk * ncta * 8 < groups_cap) chunk <<= 1;
     // Slack for holes: records reserved by claims that lost a race.
     recs = groups_cap + groups_cap / 8 + chunk * ncta;
@@ -1612,8 +1624,8 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
       measure_skew(P, ds, stream);
     plan_shared(P, ds, est, query->flags);
   }
-  uint64_t slots = next_pow2(std::max<uint64_t>(1024, est * 8));
-  const uint64_t max_slots = next_pow2(std::max<uint64_t>(1024, P.rows * 8));
+  uint64_t slots = next_pow2(std::max<uint64_t>(1024, est * table_factor()));
+  const uint64_t max_slots = next_pow2(std::max<uint64_t>(1024, P.rows * table_factor()));
   slots = std::min(slots, max_slots);
   for (int attempt = 0; attempt < 6; ++attempt) {
     bool grow = false;
@@ -1641,7 +1653,7 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
         if (pp.bits != last.bits || pp.recs != last.recs || pp.agg_slots != last.agg_slots) continue;
       }
       partitioned = false;
-      slots = std::min(next_pow2(std::max<uint64_t>(1024, est * 8)), max_slots);
+      slots = std::min(next_pow2(std::max<uint64_t>(1024, est * table_factor())), max_slots);
       continue;
     }
     if (slots >= max_slots) return fail(DFC_CAPACITY, "group table could not grow further");
@@ -2085,10 +2097,11 @@ dfc_status size_item(const dfc_query* q, BatchItem& it, DeviceState* ds, cudaStr
   if (P.sp.key_mode == KEY_PACKED && est > kOwnAlwaysGroups && !(q->flags & DFC_Q_FORCE_GLOBAL))
     measure_skew(P, ds, stream);
   plan_shared(P, ds, est, q->flags);
-  it.slots = std::min(next_pow2(std::max<uint64_t>(1024, est * 8)), next_pow2(std::max<uint64_t>(1024, P.rows * 8)));
+  it.slots = std::min(next_pow2(std::max<uint64_t>(1024, est * table_factor())),
+                      next_pow2(std::max<uint64_t>(1024, P.rows * table_factor())));
   it.ncta = scan_grid(P, ds);
   it.full_grid = it.ncta >= scan_capacity(P, ds);
-  const uint64_t groups_cap = std::min<uint64_t>(P.rows, it.slots / 8);
+  const uint64_t groups_cap = std::min<uint64_t>(P.rows, it.slots / table_factor());
   it.chunk = 64;
   while (it.chunk < 1024 && it.chunk * it.ncta * 8 < groups_cap) it.chunk <<= 1;
   it.recs = groups_cap + groups_cap / 8 + it.chunk * it.ncta;

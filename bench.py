@@ -588,7 +588,7 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dfcuda")
     ap.add_argument("--rows", type=int, default=ROWS)
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--sample-rows", type=int, default=10_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-queries", type=int, default=512, help="batched form: queries (0: skip)")

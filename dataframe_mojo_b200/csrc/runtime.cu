@@ -275,16 +275,26 @@ uint64_t next_pow2(uint64_t x) {
   return p;
 }
 
-// Global-table slots per estimated group (a power of two, 2 to 16; default
-// 8, DFC_TABLE_FACTOR=<n> sets it): the table's load stays at most 1/factor
-// of the estimate.  Record capacity follows the estimate, not the table.
-uint64_t table_factor() {
+// Global-table slots per estimated group: the table's load stays at most
+// 1/factor of the estimate, and record capacity follows the estimate, not the
+// table.  DFC_TABLE_FACTOR=<2,4,8,16> sets it; by default 16 while such a
+// table stays within kRoomyTableBytes, else 8.  On the 100M-row, 7.4M-group
+// workload the scan took 7.17 ms at 16, 7.48 at 8, 8.10 at 4 and 9.35 at 2:
+// shorter probe chains outweigh the table's size.
+constexpr uint64_t kRoomyTableBytes = 4ull << 30;
+
+uint64_t table_factor_setting() {
   static const uint64_t f = [] {
     const char* env = getenv("DFC_TABLE_FACTOR");
-    const long v = env && *env ? atol(env) : 8;
-    return (v == 2 || v == 4 || v == 8 || v == 16) ? (uint64_t)v : 8ull;
+    const long v = env && *env ? atol(env) : 0;
+    return (v == 2 || v == 4 || v == 8 || v == 16) ? (uint64_t)v : 0ull;
   }();
   return f;
+}
+
+uint64_t table_factor_for(uint64_t est) {
+  if (const uint64_t f = table_factor_setting()) return f;
+  return next_pow2(std::max<uint64_t>(1024, est * 16)) * sizeof(KeyEntry) <= kRoomyTableBytes ? 16 : 8;
 }
 
 // Host decoding of the order encoding (kernels' order_encode) for integer ranges.
@@ -1181,7 +1191,7 @@ bool plan_partitions(const Plan& P, const DeviceState* ds, uint64_t est, PartPla
 // regrows it (host_ctl->status[1] says which in the partitioned regime) and
 // retries.
 dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_t stream, uint64_t slots,
-                       const PartPlan* pp, dfc_result** out, bool* grow, Control* host_ctl) {
+                       uint64_t factor, const PartPlan* pp, dfc_result** out, bool* grow, Control* host_ctl) {
   *grow = false;
   ScanParams& sp = P.sp;
   FinishParams& fp = P.fp;
@@ -1204,7 +1214,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
     // Records: the groups the table may hold (load factor <= 1/table_factor:
     // the lock-step probe rounds run as long as a warp's longest chain) plus
     // every CTA's partly used last chunk.
-    const uint64_t groups_cap = std::min<uint64_t>(P.rows, slots / table_factor());
+    const uint64_t groups_cap = std::min<uint64_t>(P.rows, slots / factor);
     while (chunk < 1024 && chunk * ncta * 8 < groups_cap) chunk <<= 1;
     // Slack for holes: records reserved by claims that lost a race.
     recs = groups_cap + groups_cap / 8 + chunk * ncta;
@@ -1624,12 +1634,14 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
       measure_skew(P, ds, stream);
     plan_shared(P, ds, est, query->flags);
   }
-  uint64_t slots = next_pow2(std::max<uint64_t>(1024, est * table_factor()));
-  const uint64_t max_slots = next_pow2(std::max<uint64_t>(1024, P.rows * table_factor()));
+  // The query keeps its table factor through regrowth.
+  const uint64_t factor = table_factor_for(est);
+  uint64_t slots = next_pow2(std::max<uint64_t>(1024, est * factor));
+  const uint64_t max_slots = next_pow2(std::max<uint64_t>(1024, P.rows * factor));
   slots = std::min(slots, max_slots);
   for (int attempt = 0; attempt < 6; ++attempt) {
     bool grow = false;
-    st = run_attempt(query, P, ds, stream, slots, partitioned ? &pp : nullptr, out, &grow, host_ctl);
+    st = run_attempt(query, P, ds, stream, slots, factor, partitioned ? &pp : nullptr, out, &grow, host_ctl);
     if (!grow) break;
     t_timings.retries += 1;
     if (host_ctl->status[0] & ST_F32_RANGE) {
@@ -1653,7 +1665,7 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
         if (pp.bits != last.bits || pp.recs != last.recs || pp.agg_slots != last.agg_slots) continue;
       }
       partitioned = false;
-      slots = std::min(next_pow2(std::max<uint64_t>(1024, est * table_factor())), max_slots);
+      slots = std::min(next_pow2(std::max<uint64_t>(1024, est * factor)), max_slots);
       continue;
     }
     if (slots >= max_slots) return fail(DFC_CAPACITY, "group table could not grow further");
@@ -2097,11 +2109,12 @@ dfc_status size_item(const dfc_query* q, BatchItem& it, DeviceState* ds, cudaStr
   if (P.sp.key_mode == KEY_PACKED && est > kOwnAlwaysGroups && !(q->flags & DFC_Q_FORCE_GLOBAL))
     measure_skew(P, ds, stream);
   plan_shared(P, ds, est, q->flags);
-  it.slots = std::min(next_pow2(std::max<uint64_t>(1024, est * table_factor())),
-                      next_pow2(std::max<uint64_t>(1024, P.rows * table_factor())));
+  const uint64_t factor = table_factor_for(est);
+  it.slots = std::min(next_pow2(std::max<uint64_t>(1024, est * factor)),
+                      next_pow2(std::max<uint64_t>(1024, P.rows * factor)));
   it.ncta = scan_grid(P, ds);
   it.full_grid = it.ncta >= scan_capacity(P, ds);
-  const uint64_t groups_cap = std::min<uint64_t>(P.rows, it.slots / table_factor());
+  const uint64_t groups_cap = std::min<uint64_t>(P.rows, it.slots / factor);
   it.chunk = 64;
   while (it.chunk < 1024 && it.chunk * it.ncta * 8 < groups_cap) it.chunk <<= 1;
   it.recs = groups_cap + groups_cap / 8 + it.chunk * it.ncta;

@@ -1616,7 +1616,9 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
   cudaStream_t stream = query->stream ? static_cast<cudaStream_t>(query->stream) : thread_stream(P.device);
   thread_local Control* host_ctl = nullptr;
   if (!host_ctl) CK(cudaMallocHost((void**)&host_ctl, sizeof(Control)), "pinned control block");
+  const auto t_est = std::chrono::steady_clock::now();
   uint64_t est = estimate_groups(query, P, ds, stream);
+  const auto t_skew = std::chrono::steady_clock::now();
   // Regime: per-CTA shared-memory tables when the estimated groups fit in
   // shared memory at load <= 1/2 (two CTAs per SM if possible, else one);
   // otherwise the global table alone.  Rows whose key finds no room in a CTA
@@ -1633,6 +1635,12 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
     if (P.sp.key_mode == KEY_PACKED && est > kOwnAlwaysGroups && !(query->flags & DFC_Q_FORCE_GLOBAL))
       measure_skew(P, ds, stream);
     plan_shared(P, ds, est, query->flags);
+  }
+  const auto t_plan = std::chrono::steady_clock::now();
+  if (getenv("DFC_TRACE")) {
+    auto us = [](auto a, auto b) { return std::chrono::duration<double, std::micro>(b - a).count(); };
+    fprintf(stderr, "dfc plan: est=%llu prepare_us=%.1f estimate_us=%.1f skew+regime_us=%.1f\n", (unsigned long long)est,
+            us(t0, t_est), us(t_est, t_skew), us(t_skew, t_plan));
   }
   // The query keeps its table factor through regrowth.
   const uint64_t factor = table_factor_for(est);

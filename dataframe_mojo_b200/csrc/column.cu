@@ -41,6 +41,38 @@ __device__ __forceinline__ void hll_add(uint32_t* local, uint64_t h) {
   if (rho > local[reg]) atomicMax(&local[reg], rho);
 }
 
+// The rows of column_stats for one column type: DT is the dtype, U the
+// unsigned integer of its size, so that every per-row dtype test folds away.
+template <int DT, typename U>
+__device__ __forceinline__ void stats_rows(const DevColumn& c, uint64_t rows, uint32_t* local, unsigned long long& lo,
+                                           unsigned long long& hi) {
+  constexpr bool kFloat = DT == DFC_FLOAT32 || DT == DFC_FLOAT64;
+  const U* vals = static_cast<const U*>(c.values);
+  const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; base < rows; base += step * kStatsUnroll) {
+    uint64_t b[kStatsUnroll];
+    bool ok[kStatsUnroll];
+#pragma unroll
+    for (int j = 0; j < kStatsUnroll; ++j) {
+      const uint64_t i = base + j * step;
+      ok[j] = i < rows && (!c.validity || bit_valid(c.validity, i));
+      b[j] = ok[j] ? (uint64_t)vals[i] : 0ull;
+    }
+#pragma unroll
+    for (int j = 0; j < kStatsUnroll; ++j) {
+      if (!ok[j]) continue;
+      hll_add(local, mix64(key_cell(b[j], DT) ^ 0xD6E8FEB86659FD93ull));
+      if (kFloat) {
+        const double d = bits_to_f64(b[j], DT);
+        if (d != d) continue;
+      }
+      const uint64_t e = order_encode(b[j], DT);
+      lo = e < lo ? e : lo;
+      hi = e > hi ? e : hi;
+    }
+  }
+}
+
 // Statistics of a column in one pass: the order-encoded minimum and maximum
 // of its valid values (mm[0] = min, mm[1] = max; NaN skipped), which bound a
 // key's domain when the planner sizes the group table, and the HyperLogLog
@@ -54,29 +86,18 @@ __global__ void column_stats(DevColumn c, uint64_t rows, unsigned long long* mm,
   for (uint32_t i = threadIdx.x; i < (1u << kHllBits); i += blockDim.x) local[i] = 0;
   __syncthreads();
   unsigned long long lo = ~0ull, hi = 0ull;
-  const bool is_f = dt_float(c.dtype);
-  const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; base < rows; base += step * kStatsUnroll) {
-    uint64_t b[kStatsUnroll];
-    bool ok[kStatsUnroll];
-#pragma unroll
-    for (int j = 0; j < kStatsUnroll; ++j) {
-      const uint64_t i = base + j * step;
-      ok[j] = i < rows && (!c.validity || bit_valid(c.validity, i));
-      b[j] = ok[j] ? load_bits(c.values, c.size, i) : 0ull;
-    }
-#pragma unroll
-    for (int j = 0; j < kStatsUnroll; ++j) {
-      if (!ok[j]) continue;
-      hll_add(local, mix64(key_cell(b[j], c.dtype) ^ 0xD6E8FEB86659FD93ull));
-      if (is_f) {
-        const double d = bits_to_f64(b[j], c.dtype);
-        if (d != d) continue;
-      }
-      const uint64_t e = order_encode(b[j], c.dtype);
-      lo = e < lo ? e : lo;
-      hi = e > hi ? e : hi;
-    }
+  switch (c.dtype) {
+    case DFC_INT8: stats_rows<DFC_INT8, uint8_t>(c, rows, local, lo, hi); break;
+    case DFC_INT16: stats_rows<DFC_INT16, uint16_t>(c, rows, local, lo, hi); break;
+    case DFC_INT32: stats_rows<DFC_INT32, uint32_t>(c, rows, local, lo, hi); break;
+    case DFC_INT64: stats_rows<DFC_INT64, uint64_t>(c, rows, local, lo, hi); break;
+    case DFC_UINT8: stats_rows<DFC_UINT8, uint8_t>(c, rows, local, lo, hi); break;
+    case DFC_UINT16: stats_rows<DFC_UINT16, uint16_t>(c, rows, local, lo, hi); break;
+    case DFC_UINT32: stats_rows<DFC_UINT32, uint32_t>(c, rows, local, lo, hi); break;
+    case DFC_UINT64: stats_rows<DFC_UINT64, uint64_t>(c, rows, local, lo, hi); break;
+    case DFC_FLOAT32: stats_rows<DFC_FLOAT32, uint32_t>(c, rows, local, lo, hi); break;
+    case DFC_FLOAT64: stats_rows<DFC_FLOAT64, uint64_t>(c, rows, local, lo, hi); break;
+    default: break;  // the host registers only the types above
   }
   for (int o = 16; o > 0; o >>= 1) {
     const unsigned long long a = __shfl_xor_sync(0xffffffffu, lo, o);

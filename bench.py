@@ -31,6 +31,7 @@ import math
 import os
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -122,7 +123,7 @@ class Clocks:
     """nvidia-smi clock and throttle samples during the timed region."""
 
     def __init__(self, index: int):
-        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+        self.path = Path(tempfile.gettempdir()) / f"dfc_clocks_{os.getpid()}.csv"
         self.proc = None
         try:
             self.path.parent.mkdir(exist_ok=True)

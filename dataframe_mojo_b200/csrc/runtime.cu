@@ -1898,11 +1898,18 @@ DFC_API dfc_status dfc_groupby_noalloc(const dfc_query* query, int32_t device, u
   ScanParams& sp = P.sp;
   FinishParams& fp = P.fp;
 
-  // Regime and table size from the caller's capacity (no statistics pass).
+  // Regime and table size from the caller's capacity (no statistics pass,
+  // so no skew sample): per-CTA shared-memory tables up to the group count
+  // dfc_groupby takes them for whatever the skew (kOwnAlwaysGroups), up to
+  // kOwnTableGroups for compensated FP32 fields (they need on-chip partials)
+  // or on DFC_Q_FORCE_SHARED; the global table otherwise.  The
+  // radix-partitioned regime is never used here (DFC_Q_FORCE_PARTITIONED is
+  // ignored): its partition buffers would not fit the array.
   const uint64_t est = std::min<uint64_t>(capacity, P.rows);
   sp.smem_slots = 0;
-  if (!(query->flags & DFC_Q_FORCE_GLOBAL) && sp.key_mode == KEY_PACKED &&
-      ((query->flags & DFC_Q_FORCE_SHARED) || est <= 4096)) {
+  const bool own_tables = (query->flags & DFC_Q_FORCE_SHARED) || est <= kOwnAlwaysGroups ||
+                          (sp.comp_mask != 0 && est <= kOwnTableGroups);
+  if (!(query->flags & DFC_Q_FORCE_GLOBAL) && sp.key_mode == KEY_PACKED && own_tables) {
     const uint64_t sslots = next_pow2(std::max<uint64_t>(64, std::min<uint64_t>(est, 4096) * 2));
     const size_t keys_off = (P.smem + 15) & ~(size_t)15;
     const size_t recs_off = (keys_off + sslots * 8 + 15) & ~(size_t)15;
@@ -1965,53 +1972,66 @@ DFC_API dfc_status dfc_groupby_noalloc(const dfc_query* query, int32_t device, u
   void* firsts = cv.take(recs * 4);
 
   // The array keeps the previous call's contents: clear what starts known.
-  cudaError_t e = cudaMemsetAsync(table, 0xFF, (slots + 1) * sizeof(KeyEntry), stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(records, 0, recs * sp.rec_stride, stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(dctl, 0, sizeof(Control), stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(&dctl->overflow_agg, 0xFF, 4, stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(bits, 0, words * 4 + 16, stream);
-  if (e != cudaSuccess) return cuda_fail(e, "scratch initialisation");
-
-  sp.table = static_cast<KeyEntry*>(table);
-  sp.table_mask = slots - 1;
-  sp.records = static_cast<unsigned char*>(records);
-  sp.recs_total = (uint32_t)recs;
-  sp.chunk = (uint32_t)chunk;
-  sp.alloc = &dctl->alloc;
-  sp.status = dctl->status;
-  if (P.rows > 0) {
-    scan_fn(sp)<<<(unsigned)ncta, kScanThreads, P.smem, stream>>>(sp);
-    t_timings.launches += 1;
-  }
-  fp.scan = sp;
-  fp.order_bits = static_cast<uint32_t*>(bits);
-  fp.word_prefix = static_cast<uint32_t*>(prefix);
-  fp.block_sums = static_cast<uint32_t*>(bsums);
-  fp.perm = static_cast<uint32_t*>(perm);
-  fp.firsts = static_cast<uint32_t*>(firsts);
-  fp.groups = &dctl->groups;
-  fp.has_nulls = dctl->has_nulls;
-  fp.overflow_agg = &dctl->overflow_agg;
-  fp.words = words;
-  for (int c = 0; c < P.n_out; ++c) {
-    fp.out[c].values = out_vals[c];
-    fp.out[c].validity = out_valid[c];
-  }
-  const unsigned rec_blocks = (unsigned)std::min<uint64_t>((recs + kFinishThreads - 1) / kFinishThreads, (uint64_t)ds->sms * 16);
-  finish_mark<<<std::max(1u, rec_blocks), kFinishThreads, 0, stream>>>(fp);
-  finish_chunk_sums<<<(unsigned)chunks, kFinishThreads, 0, stream>>>(fp);
-  finish_scan_chunks<<<1, 1024, 0, stream>>>(fp, (uint32_t)chunks);
-  finish_word_prefix<<<(unsigned)chunks, 1024, 0, stream>>>(fp);
-  finish_rank<<<std::max(1u, rec_blocks), kFinishThreads, 0, stream>>>(fp);
-  const unsigned out_blocks = (unsigned)std::min<uint64_t>((out_rows + kFinishThreads - 1) / kFinishThreads, (uint64_t)ds->sms * 16);
-  finish_output<<<std::max(1u, out_blocks), kFinishThreads, 0, stream>>>(fp);
-  t_timings.launches += 6;
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
-  if ((st = noalloc_wait(stream))) return st;
+  // A compensated FP32 partial that leaves the FP32 range (ST_F32_RANGE)
+  // makes dfc_groupby rerun the query in FP64; here the rerun happens in the
+  // same array, once, after the first attempt has finished on the GPU.
   Control hc;
-  CK(cudaMemcpyAsync(&hc, dctl, sizeof(Control), cudaMemcpyDeviceToHost, stream), "control block");
-  if ((st = noalloc_wait(stream))) return st;
+  for (int attempt = 0;; ++attempt) {
+    cudaError_t e = cudaMemsetAsync(table, 0xFF, (slots + 1) * sizeof(KeyEntry), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(records, 0, recs * sp.rec_stride, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dctl, 0, sizeof(Control), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(&dctl->overflow_agg, 0xFF, 4, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bits, 0, words * 4 + 16, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "scratch initialisation");
+
+    sp.table = static_cast<KeyEntry*>(table);
+    sp.table_mask = slots - 1;
+    sp.records = static_cast<unsigned char*>(records);
+    sp.recs_total = (uint32_t)recs;
+    sp.chunk = (uint32_t)chunk;
+    sp.alloc = &dctl->alloc;
+    sp.status = dctl->status;
+    if (P.rows > 0) {
+      scan_fn(sp)<<<(unsigned)ncta, kScanThreads, P.smem, stream>>>(sp);
+      t_timings.launches += 1;
+    }
+    fp.scan = sp;
+    fp.order_bits = static_cast<uint32_t*>(bits);
+    fp.word_prefix = static_cast<uint32_t*>(prefix);
+    fp.block_sums = static_cast<uint32_t*>(bsums);
+    fp.perm = static_cast<uint32_t*>(perm);
+    fp.firsts = static_cast<uint32_t*>(firsts);
+    fp.groups = &dctl->groups;
+    fp.has_nulls = dctl->has_nulls;
+    fp.overflow_agg = &dctl->overflow_agg;
+    fp.words = words;
+    for (int c = 0; c < P.n_out; ++c) {
+      fp.out[c].values = out_vals[c];
+      fp.out[c].validity = out_valid[c];
+    }
+    const unsigned rec_blocks =
+        (unsigned)std::min<uint64_t>((recs + kFinishThreads - 1) / kFinishThreads, (uint64_t)ds->sms * 16);
+    finish_mark<<<std::max(1u, rec_blocks), kFinishThreads, 0, stream>>>(fp);
+    finish_chunk_sums<<<(unsigned)chunks, kFinishThreads, 0, stream>>>(fp);
+    finish_scan_chunks<<<1, 1024, 0, stream>>>(fp, (uint32_t)chunks);
+    finish_word_prefix<<<(unsigned)chunks, 1024, 0, stream>>>(fp);
+    finish_rank<<<std::max(1u, rec_blocks), kFinishThreads, 0, stream>>>(fp);
+    const unsigned out_blocks =
+        (unsigned)std::min<uint64_t>((out_rows + kFinishThreads - 1) / kFinishThreads, (uint64_t)ds->sms * 16);
+    finish_output<<<std::max(1u, out_blocks), kFinishThreads, 0, stream>>>(fp);
+    t_timings.launches += 6;
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+    if ((st = noalloc_wait(stream))) return st;
+    CK(cudaMemcpyAsync(&hc, dctl, sizeof(Control), cudaMemcpyDeviceToHost, stream), "control block");
+    if ((st = noalloc_wait(stream))) return st;
+    if (attempt == 0 && (hc.status[0] & ST_F32_RANGE) && !(hc.status[0] & ST_TIMEOUT) && !hc.status[2]) {
+      sp.comp_mask = 0;
+      t_timings.retries += 1;
+      continue;
+    }
+    break;
+  }
 
   const uint32_t status = hc.status[0];
   if (hc.status[2]) {
@@ -2049,7 +2069,7 @@ DFC_API dfc_status dfc_groupby_noalloc(const dfc_query* query, int32_t device, u
     outputs[c].dtype = P.out_dtype[c];
     outputs[c].has_nulls = hc.has_nulls[c] != 0 ? 1 : 0;
     if (G == 0) continue;
-    e = cudaMemcpyAsync(outputs[c].values, out_vals[c], G * dtype_size(P.out_dtype[c]), cudaMemcpyDeviceToDevice, stream);
+    cudaError_t e = cudaMemcpyAsync(outputs[c].values, out_vals[c], G * dtype_size(P.out_dtype[c]), cudaMemcpyDeviceToDevice, stream);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(outputs[c].validity, out_valid[c], ((G + 31) / 32) * 4, cudaMemcpyDeviceToDevice, stream);
     if (e != cudaSuccess) return cuda_fail(e, "output copy");
@@ -2059,6 +2079,7 @@ DFC_API dfc_status dfc_groupby_noalloc(const dfc_query* query, int32_t device, u
   t_timings.groups = G;
   t_timings.table_slots = slots;
   t_timings.regime = sp.smem_slots ? 1 : 0;
+  t_timings.compensated = sp.smem_slots ? (int32_t)sp.comp_mask : 0;
   return DFC_OK;
 }
 

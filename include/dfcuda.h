@@ -319,7 +319,15 @@ DFC_API void dfc_server_destroy(dfc_server* server);
 /*   with it and corrupts both: calls must not overlap on the GPU.          */
 /* - Results are the same as dfc_groupby's.  Groups come back in the same   */
 /*   order; floating sums and moments may differ in the last bits, as      */
-/*   between two dfc_groupby calls.  No timings are recorded.               */
+/*   between two dfc_groupby calls.  A compensated FP32 partial that leaves */
+/*   the FP32 range reruns the query in FP64 in the same array, as          */
+/*   dfc_groupby reruns it.                                                 */
+/* - The table regime comes from `capacity` alone (no statistics pass):     */
+/*   per-CTA shared-memory tables up to 256 groups (4096 with               */
+/*   DFC_Q_FLOAT32_COMPENSATED, any count with DFC_Q_FORCE_SHARED), the    */
+/*   global table otherwise; DFC_Q_FORCE_PARTITIONED is ignored.            */
+/* - dfc_last_timings reports this call's groups, table slots, regime,      */
+/*   launches, retries and compensated fields; no phase times.              */
 /* ------------------------------------------------------------------------ */
 #define DFC_NOALLOC_SCRATCH_BYTES (64ull << 20)
 

@@ -67,12 +67,15 @@ def device_columns(frame: DataFrame, names: list[str]):
     return descs, keep
 
 
-def run_noalloc(plan, capacity: int) -> DataFrame:
+def run_noalloc(plan, capacity: int, flags: int = 0, stream=None) -> DataFrame:
+    """The plan through dfc_groupby_noalloc; `stream` (a torch stream) is
+    passed as the query's stream when given."""
     torch = _torch()
     bound = bind(plan.plan if hasattr(plan, "plan") else plan)
     frame = DataFrame(bound.series)
     descs, keep = device_columns(frame, [s.name for s in bound.series])
-    q = provider._query_struct(bound, [C.c_void_p(None)] * len(bound.names), None, 0)
+    q = provider._query_struct(bound, [C.c_void_p(None)] * len(bound.names),
+                               stream.cuda_stream if stream is not None else None, flags)
     n_out = len(bound.out_names)
     outs = (N.DeviceOutput * n_out)()
     bufs = []
@@ -86,6 +89,8 @@ def run_noalloc(plan, capacity: int) -> DataFrame:
     st = N.lib().dfc_groupby_noalloc(C.byref(q), 0, len(bound.series[0]), descs, capacity, outs, C.byref(groups))
     if st != N.OK:
         raise provider.ProviderError(st, N.last_error())
+    if stream is not None:
+        stream.synchronize()
     g = groups.value
     cols = []
     for i, name in enumerate(bound.out_names):
@@ -175,3 +180,95 @@ def test_noalloc_reports_more_groups_than_capacity():
     # The next call is unaffected.
     out = run_noalloc(plan, capacity=5000)
     assert out.height == 5000 and int(out["v"].values.sum()) == 5000
+
+
+def test_noalloc_compensated_out_of_range_reruns_in_fp64():
+    """Float32 partials that leave the FP32 range: the entry point reruns the
+    query in FP64 inside its own array, as dfc_groupby does, and the second
+    call in a row (same array) agrees again."""
+    rows = 4096
+    keys = (np.arange(rows) % 4).astype(np.int32)
+    frame = DataFrame([Series("k", keys), Series("v", np.full(rows, 3.0e38, np.float32))])
+    plan = frame.lazy().group_by("k", maintain_order=True).agg([col("v").sum().alias("s"), col("v").var().alias("var")])
+    for call in range(2):
+        out = run_noalloc(plan, capacity=64, flags=N.Q_FLOAT32_COMPENSATED)
+        assert np.allclose(out["s"].values, 1024 * float(np.float32(3.0e38)), rtol=1e-12), call
+        assert np.all(out["var"].values == 0.0), call
+        t = provider.last_timings()
+        assert t["retries"] == 1 and t["compensated"] == 0, t
+
+
+def test_noalloc_compensated_in_range_matches_groupby():
+    rng = np.random.default_rng(71)
+    rows = 200_000
+    frame = DataFrame([
+        Series("k", rng.integers(0, 300, rows).astype(np.int32)),
+        Series("v", (rng.standard_normal(rows) * 1e3).astype(np.float32)),
+    ])
+    plan = frame.lazy().group_by("k", maintain_order=True).agg(
+        [col("v").sum().alias("s"), col("v").mean().alias("m"), col("v").var().alias("var")])
+    ref, _ = provider.execute(plan)
+    out = run_noalloc(plan, capacity=1024, flags=N.Q_FLOAT32_COMPENSATED)
+    assert provider.last_timings()["compensated"] != 0
+    # Compensated FP32 partials against dfc_groupby's FP64 accumulation:
+    # 1e-9 of the summands' magnitude (sum |x| per group), the bound the
+    # compensated tests hold against the oracle; variances 1e-8 relative.
+    order = {int(k): i for i, k in enumerate(ref["k"].values)}
+    idx = np.array([order[int(k)] for k in frame["k"].values])
+    mags = {"s": np.bincount(idx, weights=np.abs(frame["v"].values.astype(np.float64)), minlength=ref.height)}
+    mags["m"] = mags["s"] / np.bincount(idx, minlength=ref.height)
+    assert out.columns == ref.columns and out.height == ref.height
+    assert np.array_equal(out["k"].values, ref["k"].values)
+    for c in ("s", "m"):
+        assert np.all(np.abs(out[c].values - ref[c].values) <= 1e-9 * mags[c]), c
+    assert np.all(np.abs(out["var"].values - ref["var"].values) <= 1e-8 * (1 + np.abs(ref["var"].values)))
+
+
+def ticket_frame(rows: int, seed: int) -> DataFrame:
+    """Three nullable Int64 keys (wider than one 64-bit key word together, so
+    keys are hashed and checked at the claiming row) and a nullable value."""
+    rng = np.random.default_rng(seed)
+    cols = []
+    for i in range(3):
+        cols.append(Series(f"k{i}", rng.integers(-3, 3, rows).astype(np.int64) * (1 << 40),
+                           rng.random(rows) > 0.1))
+    cols.append(Series("v", rng.integers(-1000, 1000, rows).astype(np.int64), rng.random(rows) > 0.05))
+    cols.append(Series("p", rng.integers(0, 10, rows).astype(np.int32)))
+    return DataFrame(cols)
+
+
+def ticket_plan(frame: DataFrame):
+    return (frame.lazy().filter(col("p") >= 2).group_by(["k0", "k1", "k2"], maintain_order=True)
+            .agg([col("v").sum().alias("s"), col("v").min().alias("lo"), col("v").max().alias("hi"),
+                  col("v").count().alias("n"), col("v").null_count().alias("nulls"), col("v").len().alias("len")]))
+
+
+def test_noalloc_ticket_keys_with_nulls_against_oracle():
+    """A 3-key nullable Int64 query (ticket keys) against the CPU oracle
+    directly, bit for bit: every output here is an integer."""
+    from oracle import binding
+
+    plan = ticket_plan(ticket_frame(300_000, 72))
+    ref, _ = binding.run(plan)
+    assert ref.height > 200
+    for call in range(2):
+        out = run_noalloc(plan, capacity=4096)
+        assert_same(out, ref, f"ticket call {call}")
+
+
+def test_noalloc_empty_input():
+    frame = DataFrame([Series("k", np.zeros(0, np.int64)), Series("v", np.zeros(0, np.float64))])
+    plan = frame.lazy().group_by("k", maintain_order=True).agg([col("v").sum().alias("s"), col("v").count().alias("n")])
+    ref, _ = provider.execute(plan)
+    out = run_noalloc(plan, capacity=16)
+    assert out.height == 0 == ref.height
+    assert out.columns == ref.columns
+
+
+def test_noalloc_on_a_caller_stream():
+    torch = _torch()
+    plan = ticket_plan(ticket_frame(100_000, 73))
+    ref, _ = provider.execute(plan)
+    s = torch.cuda.Stream()
+    out = run_noalloc(plan, capacity=4096, stream=s)
+    assert_same(out, ref, "caller stream")

@@ -99,6 +99,8 @@ class Timings(C.Structure):
         ("aggregate_ns", C.c_double),
         ("cluster_ctas", C.c_int32),
         ("compensated", C.c_int32),
+        ("count_ns", C.c_double),
+        ("place_ns", C.c_double),
     ]
 
 

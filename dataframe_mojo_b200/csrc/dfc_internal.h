@@ -152,29 +152,26 @@ struct ScanParams {
   uint32_t chunk;        // records a CTA draws from `alloc` at a time (power of two)
   uint32_t* alloc;       // [0] records handed out (may exceed recs_total)
   uint32_t* status;      // [0] status bits, [1] CapacityBits, [2] partition-pass checks
-  // Radix-partitioned regime.  A counting pass (the key and filter columns
-  // only: the first n_stage_count staged columns) counts each CTA's selected
-  // rows per partition; their prefixes give every (CTA, partition) an exact
-  // range of part_buf.  Pass A stages each selected row as part_words 8-byte
-  // words {key word, row | value validity << 32, values...} and appends it to
-  // its range; partition q occupies rows [part_start[q], + part_totals[q]).
-  // Pass B aggregates a partition at a time per cluster in an L2-resident
-  // table of agg_slots records (+1 for the all-ones key word), then appends
-  // its groups densely to `records`.
+  // Radix-partitioned regime (partition = the top part_bits bits of a hash
+  // of the key word).  A counting pass stages only the key and filter columns
+  // (the first n_stage_count staged columns, stage_tx_count bytes a full
+  // tile) and counts the selected rows per partition into part_totals; their
+  // exclusive prefix (part_start) gives every partition its range of
+  // part_buf.  Pass A stages every column and places each selected row at
+  // part_start[q] + the partition's cursor, raised by one atomic per warp and
+  // partition, as part_words 8-byte words {key word, row | value validity
+  // << 32, values...}.  Pass B folds one partition at a time per CTA into a
+  // shared-memory table of agg_slots records and appends its live records to
+  // `records` in chunks drawn from `alloc`.
   int32_t n_stage_count;   // staged columns the counting pass needs
   int32_t stage_tx_count;  // bytes of one full tile of those columns
   uint32_t part_bits;      // log2 partitions, 0 = regime off
   uint32_t part_words;
   unsigned long long* part_buf;
-  uint64_t part_cap;       // rows part_buf holds
-  uint32_t* part_counts;   // [CTA][partition]: rows, then the CTA's exclusive prefix
-  uint32_t* part_totals;   // [partition] rows
-  uint32_t* part_start;    // [partition] first row in part_buf
-  uint32_t part_flush;     // staged rows the shared-memory staging area holds
-  uint32_t part_stage_off; // dynamic shared-memory offset of the staging area
-  uint32_t agg_slots;      // power of two
-  uint32_t agg_tables_n;   // cluster tables allocated
-  unsigned char* agg_tables;
+  uint32_t* part_totals;   // [partition] selected rows
+  uint32_t* part_start;    // [partition] first row of the partition in part_buf
+  uint32_t* part_cursor;   // [partition] rows pass A placed (zeroed before pass A)
+  uint32_t agg_slots;      // pass B table slots
   uint32_t* part_next;     // pass B work counter
 };
 
@@ -184,12 +181,9 @@ enum CapacityBits : uint32_t { CAP_RECORDS = 1u, CAP_AGG_TABLE = 2u };
 // Index and consistency checks (status word 2).  A failed check skips the
 // access it guards; the host fails the query with the code.
 enum CheckBits : uint32_t {
-  CHK_STAGE = 1u,     // a staged row beyond the staging area
-  CHK_ORDER = 2u,     // a flush position beyond the staged rows
   CHK_PART = 4u,      // a partition number out of range
-  CHK_RANGE = 8u,     // a CTA's rows of a partition disagree with the count
+  CHK_RANGE = 8u,     // pass A placed a row beyond its partition's count
   CHK_SLOT = 16u,     // a table slot out of range
-  CHK_CLUSTER = 32u,  // a cluster without a table
   CHK_FIRST = 128u,   // a record's first row beyond the rows
   CHK_DUP = 256u,     // two records with the same first row
   CHK_PERM = 512u,    // a rank naming no record

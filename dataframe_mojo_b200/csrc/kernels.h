@@ -19,17 +19,18 @@ enum ScanRegime : int { kScanGlobal = 0, kScanOwn = 1, kScanCluster = 2 };
 __global__ void scan_kernel_global(const __grid_constant__ ScanParams p);
 __global__ void scan_kernel_own(const __grid_constant__ ScanParams p);
 __global__ void scan_kernel_cluster(const __grid_constant__ ScanParams p);
-// Radix-partitioned regime: pass A (filter, keys, partition) and pass B
-// (per-partition aggregation by clusters of kAggCluster CTAs).
-constexpr int kAggCluster = 8;
+// Radix-partitioned regime: the counting pass, the partition starts, pass A
+// (filter, keys, placement into partitions) and pass B (per-partition
+// aggregation in a shared-memory table, kAggThreads threads per CTA).
 constexpr int kAggThreads = 512;
-constexpr int kPartMax = 1024;  // partitions at most
+constexpr int kPartMaxBits = 15;  // partitions at most: 2^15
 // The partition passes: one producer warp and kPartWarps consumer warps.
 constexpr int kPartWarps = 16;
 constexpr int kPartConsumerThreads = kPartWarps * 32;
 constexpr int kPartThreads = kPartConsumerThreads + 32;
+constexpr uint32_t kRecChunk = 4096;  // records pass B draws from `alloc` at a time
 __global__ void partition_count(const __grid_constant__ ScanParams p);
-__global__ void partition_offsets(const __grid_constant__ ScanParams p, uint32_t ctas);
+__global__ void partition_offsets(const __grid_constant__ ScanParams p);
 __global__ void partition_kernel(const __grid_constant__ ScanParams p);
 __global__ void partition_aggregate(const __grid_constant__ ScanParams p);
 __global__ void finish_mark(const __grid_constant__ FinishParams f);

@@ -146,6 +146,9 @@ struct DeviceState {
   size_t smem_optin = 0;       // scan_kernel's dynamic shared memory limit
   size_t smem_half = 0;        // scan_kernel's dynamic shared memory at two CTAs per SM
   size_t part_smem_optin = 0;  // partition_kernel's
+  size_t count_smem_optin = 0; // partition_count's
+  size_t agg_smem_optin = 0;   // partition_aggregate's, one CTA per SM
+  size_t agg_smem_half = 0;    // partition_aggregate's at two CTAs per SM
   int scan_occupancy = 1;
 };
 std::mutex g_dev_mu;
@@ -162,21 +165,53 @@ std::map<std::vector<uint64_t>, double> g_joint;
 std::map<std::vector<uint64_t>, std::pair<double, double>> g_skew;
 std::atomic<uint64_t> g_column_serial{0};
 
+// The library's own stream-ordered memory pool per device.  Freed query
+// memory stays cached in it (queries reuse it without returning to the
+// driver); the device's default pool, which other code in the process may
+// use, keeps its own release threshold.
+constexpr int kMaxDevices = 64;
+cudaMemPool_t g_pools[kMaxDevices] = {};
+
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t stream) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaMemPool_t pool = dev >= 0 && dev < kMaxDevices ? g_pools[dev] : nullptr;
+  if (!pool) return cudaMallocAsync(p, bytes, stream);
+  return cudaMallocFromPoolAsync(p, bytes, pool, stream);
+}
+
 dfc_status device_ready(int dev, DeviceState** out) {
   std::lock_guard<std::mutex> lk(g_dev_mu);
+  if (dev < 0 || dev >= kMaxDevices) return fail(DFC_INVALID, "device ordinal out of range");
   DeviceState& d = g_dev[dev];
   if (!d.ready) {
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
     if (prop.major < 10) return fail(DFC_NO_DEVICE, "device is not sm_100 class");
+    // Function attributes apply to the current device: set it for the
+    // set-up and give the caller's back afterwards.
+    int prev = -1;
+    cudaGetDevice(&prev);
     CK(cudaSetDevice(dev), "cudaSetDevice");
+    struct Restore {
+      int prev;
+      ~Restore() {
+        if (prev >= 0) cudaSetDevice(prev);
+      }
+    } restore{prev};
     d.sms = prop.multiProcessorCount;
     d.smem_optin = prop.sharedMemPerBlockOptin;
-    // Keep freed pool memory cached: queries reuse it without returning to the OS.
-    cudaMemPool_t pool;
-    CK(cudaDeviceGetDefaultMemPool(&pool, dev), "cudaDeviceGetDefaultMemPool");
-    uint64_t threshold = UINT64_MAX;
-    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold), "cudaMemPoolSetAttribute");
+    if (!g_pools[dev]) {
+      cudaMemPoolProps props = {};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      cudaMemPool_t pool;
+      CK(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
+      uint64_t threshold = UINT64_MAX;
+      CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold), "cudaMemPoolSetAttribute");
+      g_pools[dev] = pool;
+    }
     // Dynamic shared memory may use what the kernel's static buffers leave.
     cudaFuncAttributes fa;
     size_t scan_static = 0;
@@ -192,14 +227,20 @@ dfc_status device_ready(int dev, DeviceState** out) {
     // Cluster tables pool the shared memory of up to 16 CTAs.
     CK(cudaFuncSetAttribute(scan_kernel_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
        "cudaFuncSetAttribute");
+    // The partition passes: the counting pass and pass A at one CTA per SM,
+    // pass B at two when its table fits half an SM.
     CK(cudaFuncGetAttributes(&fa, partition_kernel), "cudaFuncGetAttributes");
     d.part_smem_optin = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;
     CK(cudaFuncSetAttribute(partition_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.part_smem_optin),
        "cudaFuncSetAttribute");
-    // The counting pass uses the scan's ring (smaller static shared memory).
     CK(cudaFuncGetAttributes(&fa, partition_count), "cudaFuncGetAttributes");
-    CK(cudaFuncSetAttribute(partition_count, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)(prop.sharedMemPerBlockOptin - fa.sharedSizeBytes)),
+    d.count_smem_optin = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;
+    CK(cudaFuncSetAttribute(partition_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.count_smem_optin),
+       "cudaFuncSetAttribute");
+    CK(cudaFuncGetAttributes(&fa, partition_aggregate), "cudaFuncGetAttributes");
+    d.agg_smem_optin = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;
+    d.agg_smem_half = (prop.sharedMemPerMultiprocessor - 2 * prop.reservedSharedMemPerBlock) / 2 - fa.sharedSizeBytes;
+    CK(cudaFuncSetAttribute(partition_aggregate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.agg_smem_optin),
        "cudaFuncSetAttribute");
     d.ready = true;
   }
@@ -648,7 +689,7 @@ double joint_key_estimate(const Plan& P, DeviceState* ds, cudaStream_t stream) {
   const uint32_t nreg = 1u << kHllBits;
   uint32_t* d_regs = nullptr;
   std::vector<uint32_t> regs(nreg);
-  cudaError_t e = cudaMallocAsync((void**)&d_regs, nreg * 4, stream);
+  cudaError_t e = pool_alloc((void**)&d_regs, nreg * 4, stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_regs, 0, nreg * 4, stream);
   if (e == cudaSuccess) {
     const unsigned blocks = (unsigned)std::min<uint64_t>((P.rows + 255) / 256, (uint64_t)ds->sms * stats_blocks_per_sm((const void*)keys_hll));
@@ -673,8 +714,8 @@ dfc_status ensure_stats(dfc_column* c, DeviceState* ds, cudaStream_t stream) {
   uint32_t* d_regs = nullptr;
   unsigned long long h_mm[2] = {~0ull, 0ull};
   std::vector<uint32_t> regs(nreg);
-  cudaError_t e = cudaMallocAsync((void**)&d_mm, 16, stream);
-  if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_regs, nreg * 4, stream);
+  cudaError_t e = pool_alloc((void**)&d_mm, 16, stream);
+  if (e == cudaSuccess) e = pool_alloc((void**)&d_regs, nreg * 4, stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_mm, h_mm, 16, cudaMemcpyHostToDevice, stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_regs, 0, nreg * 4, stream);
   if (e == cudaSuccess) {
@@ -773,7 +814,7 @@ void measure_skew(Plan& P, DeviceState* ds, cudaStream_t stream) {
   const uint64_t stride = P.rows / n;
   unsigned long long* d = nullptr;
   std::vector<unsigned long long> h(n);
-  cudaError_t e = cudaMallocAsync((void**)&d, (size_t)n * 8, stream);
+  cudaError_t e = pool_alloc((void**)&d, (size_t)n * 8, stream);
   if (e == cudaSuccess) {
     keys_sample<<<std::max(1u, std::min((n + 255) / 256, (uint32_t)ds->sms * 4)), 256, 0, stream>>>(P.sp, d, n, stride);
     e = cudaGetLastError();
@@ -1031,7 +1072,7 @@ cudaError_t alloc_result_cols(const Plan& P, uint64_t out_rows, std::vector<Resu
     off[2 * c + 1] = total;
     total += piece(((out_rows + 31) / 32) * 4);
   }
-  cudaError_t e = cudaMallocAsync(slab, std::max<uint64_t>(total, 256), stream);
+  cudaError_t e = pool_alloc(slab, std::max<uint64_t>(total, 256), stream);
   if (e != cudaSuccess) {
     *slab = nullptr;
     cudaGetLastError();
@@ -1068,7 +1109,7 @@ struct Scratch {
     return DFC_OK;
   }
   dfc_status commit(const char* what) {
-    cudaError_t e = cudaMallocAsync(&block, std::max<size_t>(total, 256), stream);
+    cudaError_t e = pool_alloc(&block, std::max<size_t>(total, 256), stream);
     if (e != cudaSuccess) {
       block = nullptr;
       return cuda_fail(e, what);
@@ -1111,78 +1152,85 @@ struct Control {
 struct PartPlan {
   uint32_t bits = 0;
   uint32_t words = 0;
-  uint32_t flush = 0;
-  uint32_t stage_off = 0;
   uint32_t agg_slots = 0;
   uint64_t recs = 0;
-  size_t smem = 0;        // pass A dynamic shared memory
-  size_t count_smem = 0;  // counting pass dynamic shared memory
-  int clusters = 0;       // pass B clusters resident at once
+  int count_stages = 0;       // counting pass ring stages
+  int count_stage_bytes = 0;  // and their stride (the key and filter columns only)
+  int stages = 0;             // pass A ring stages (every staged column)
+  size_t count_smem = 0;      // counting pass dynamic shared memory
+  size_t smem = 0;            // pass A
+  size_t agg_smem = 0;        // pass B
+  uint64_t ctas = 0;          // counting pass and pass A grid: one CTA per SM
+  uint64_t agg_ctas = 0;      // pass B grid: every resident CTA
 };
 
-// Clusters of kAggCluster CTAs resident at once with `smem` bytes of
-// dynamic shared memory each (0: no cluster launch possible).
-int agg_clusters(size_t smem) {
-  cudaLaunchConfig_t cfg = {};
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = kAggCluster;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.gridDim = dim3(kAggCluster * 64);
-  cfg.blockDim = dim3(kAggThreads);
-  cfg.dynamicSmemBytes = smem;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  int clusters = 0;
-  if (cudaOccupancyMaxActiveClusters(&clusters, partition_aggregate, &cfg) != cudaSuccess) {
-    cudaGetLastError();
-    return 0;
-  }
-  return clusters;
-}
+// A pass B table holds a partition's groups at load <= kAggLoad on average
+// (partitions take groups by a hash, so their sizes vary by a few percent).
+constexpr double kAggLoad = 0.6;
+constexpr uint32_t kPartMinBits = 10;  // at least 1024 partitions: pass B balances over them
 
-// L2 bytes the clusters' pass B tables may take together: the rest serves
-// the streamed partition rows and the records being written.
-constexpr double kAggL2Budget = 40.0 * 1024 * 1024;
-
-// Sizes the regime for `est` groups; false when it does not apply (keys
-// wider than 64 bits, too little shared memory, no cluster launch).
-bool plan_partitions(const Plan& P, const DeviceState* ds, uint64_t est, PartPlan& pp) {
+// Sizes the regime for `est` groups with at least 2^min_bits partitions;
+// false when it does not apply (keys wider than 64 bits, records too wide
+// for a shared-memory table, more groups than 2^15 tables hold).
+bool plan_partitions(const Plan& P, const DeviceState* ds, uint64_t est, PartPlan& pp, uint32_t min_bits = 0) {
   const ScanParams& sp = P.sp;
   if (sp.key_mode != KEY_PACKED || P.rows == 0 || P.rows >= 0xFFFFFFFFull) return false;
   pp.words = 2 + (uint32_t)sp.n_vals;
-  pp.clusters = agg_clusters(0);
-  if (pp.clusters < 1) return false;
-  // Staging area: what the ring leaves, a power of two of rows, split into
-  // one region per consumer warp of at least one step's share (a warp stages
-  // up to 128 rows a two-tile step); at most 2^15 rows (flush positions are
-  // 16-bit).
-  const size_t ring = (size_t)sp.stages * sp.stage_bytes + 2 * sp.stages * sizeof(uint64_t);
-  pp.count_smem = ring;
-  pp.stage_off = (uint32_t)((ring + 15) & ~(size_t)15);
-  if (ds->part_smem_optin <= pp.stage_off) return false;
-  const size_t per_row = (size_t)pp.words * 8 + 4;
-  size_t rows_fit = (ds->part_smem_optin - pp.stage_off) / per_row;
-  rows_fit = std::min<size_t>(rows_fit, 32768);
-  uint32_t flush = 1;
-  while ((size_t)flush * 2 <= rows_fit) flush <<= 1;
-  if (flush < (uint32_t)kPartWarps * 128u) return false;
-  pp.flush = flush;
-  pp.smem = pp.stage_off + (size_t)flush * per_row;
-  // Partitions: the fewest (>= 16) whose tables, at load <= 1/2, fit the L2
-  // budget together.
-  const uint64_t groups = std::max<uint64_t>(est, 1);
-  uint32_t bits = 4;
-  uint64_t slots = 0;
-  for (;; ++bits) {
-    slots = next_pow2(std::max<uint64_t>(256, 2 * ((groups >> bits) + 1)));
-    if (bits >= 10 || (double)pp.clusters * (double)(slots + 1) * sp.rec_stride <= kAggL2Budget) break;
+  const size_t rs = (size_t)sp.rec_stride;
+  const double groups = (double)std::max<uint64_t>(est, 1);
+  // Slots of a table in `bytes` (any count, a multiple of 32), besides the
+  // record of the all-ones key word.
+  auto slots_in = [&](size_t bytes) { return bytes / rs > 0 ? (uint64_t)(bytes / rs - 1) & ~(uint64_t)31 : 0ull; };
+  auto bits_for = [&](uint64_t slots) {
+    uint32_t b = std::max(kPartMinBits, min_bits);
+    while (b < (uint32_t)kPartMaxBits && groups / (double)(1ull << b) > (double)slots * kAggLoad) ++b;
+    return b;
+  };
+  // Two pass B CTAs per SM when their tables hold the groups, else one CTA
+  // per SM with twice the table.
+  uint64_t slots = slots_in(ds->agg_smem_half);
+  uint32_t bits = bits_for(slots);
+  const bool two = slots >= 256 && groups / (double)(1ull << bits) <= (double)slots * kAggLoad;
+  if (!two) {
+    slots = slots_in(ds->agg_smem_optin);
+    bits = bits_for(slots);
   }
+  if (slots < 64 || bits > (uint32_t)kPartMaxBits || groups / (double)(1ull << bits) > (double)slots * kAggLoad)
+    return false;
   pp.bits = bits;
   pp.agg_slots = (uint32_t)slots;
-  pp.recs = std::min<uint64_t>(P.rows, groups + groups / 4 + 4096);
+  pp.agg_smem = (slots + 1) * rs;
+  pp.agg_ctas = (uint64_t)ds->sms * (two ? 2 : 1);
+  // Counting pass: a ring of the key and filter columns only (they hold the
+  // first bytes of every stage), then one counter per partition.
+  const size_t mbar = 2 * sizeof(uint64_t);
+  pp.count_stage_bytes = (int)(((size_t)sp.stage_tx_count + 127) & ~(size_t)127);
+  const size_t counters = (size_t)4 << bits;
+  if (ds->count_smem_optin <= counters) return false;
+  pp.count_stages = (int)std::min<size_t>(16, (ds->count_smem_optin - counters) / (pp.count_stage_bytes + mbar));
+  if (pp.count_stages < 4) return false;
+  pp.count_smem = (size_t)pp.count_stages * (pp.count_stage_bytes + mbar) + counters;
+  // Pass A: a ring of every staged column.
+  pp.stages = (int)std::min<size_t>(8, ds->part_smem_optin / ((size_t)sp.stage_bytes + mbar));
+  if (pp.stages < 4) return false;
+  pp.smem = (size_t)pp.stages * ((size_t)sp.stage_bytes + mbar);
+  pp.ctas = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ds->sms, sp.tiles));
+  // Every group once, plus the unused tail of each pass B CTA's last chunk.
+  pp.recs = std::min<uint64_t>(0xFFFFFFDFull, (uint64_t)(groups * 1.25) + 4096 + pp.agg_ctas * kRecChunk);
   return true;
+}
+
+// The automatic choice of the radix-partitioned regime: the estimated
+// groups' records take more than kPartitionRecordBytes (half the L2) and
+// the sampled hottest key holds under kPartitionTop1 of the rows.
+// DFC_PARTITION_MIN_GROUPS=<n> replaces the record test by est >= n (tuning).
+constexpr double kPartitionRecordBytes = 64.0 * 1024 * 1024;
+constexpr double kPartitionTop1 = 0.01;
+bool partition_by_default(const Plan& P, uint64_t est) {
+  if (P.sp.key_mode != KEY_PACKED || P.top1 < 0 || P.top1 >= kPartitionTop1) return false;
+  if (const char* env = getenv("DFC_PARTITION_MIN_GROUPS"))
+    if (atoll(env) > 0) return est >= (uint64_t)atoll(env);
+  return (double)est * P.sp.rec_stride > kPartitionRecordBytes;
 }
 
 // One attempt of the query at the given capacities: the global or
@@ -1198,17 +1246,10 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   Scratch S;
   S.stream = stream;
 
-  uint64_t ncta;
-  if (pp) {
-    // The counting pass and pass A must see the same tiles per CTA: one grid
-    // of one CTA per SM.
-    ncta = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ds->sms, std::max<uint64_t>(1, sp.tiles)));
-  } else {
-    ncta = scan_grid(P, ds);
-  }
+  const uint64_t ncta = pp ? pp->ctas : scan_grid(P, ds);
   uint64_t chunk = 64, recs;
   if (pp) {
-    // Pass B appends every group exactly once: no holes, no chunks.
+    // Pass B appends every group once, in chunks of kRecChunk per CTA.
     recs = std::max<uint64_t>(1, pp->recs);
   } else {
     // Records: the groups the table may hold (load factor <= 1/table_factor:
@@ -1222,7 +1263,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   if (recs >= 0xFFFFFFE0ull) return fail(DFC_CAPACITY, "group capacity exceeds 2^32 - 32 records");
 
   void *table = nullptr, *records, *ctl, *bits, *prefix, *bsums, *perm, *firsts;
-  void *part_buf = nullptr, *part_counts = nullptr, *part_totals = nullptr, *part_start = nullptr, *agg_tables = nullptr;
+  void *part_buf = nullptr, *part_totals = nullptr, *part_start = nullptr, *part_cursor = nullptr;
   const uint64_t words = (P.rows + 31) / 32;
   const uint64_t chunks = std::max<uint64_t>(1, (words + kFinishChunk - 1) / kFinishChunk);
   const uint64_t nparts = pp ? (1ull << pp->bits) : 0;
@@ -1230,11 +1271,9 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   if (pp) {
     // Every row may pass the filter: part_buf holds all of them.
     if ((st = S.alloc(&part_buf, P.rows * pp->words * 8, "partition rows"))) return S.release(), st;
-    if ((st = S.alloc(&part_counts, ncta * nparts * 4, "partition counts"))) return S.release(), st;
     if ((st = S.alloc(&part_totals, nparts * 4, "partition totals"))) return S.release(), st;
     if ((st = S.alloc(&part_start, nparts * 4, "partition starts"))) return S.release(), st;
-    if ((st = S.alloc(&agg_tables, (uint64_t)pp->clusters * (pp->agg_slots + 1ull) * sp.rec_stride, "partition tables")))
-      return S.release(), st;
+    if ((st = S.alloc(&part_cursor, nparts * 4, "partition cursors"))) return S.release(), st;
   } else {
     if ((st = S.alloc(&table, (slots + 1) * sizeof(KeyEntry), "key table"))) return S.release(), st;
   }
@@ -1263,9 +1302,10 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   Control* dctl = static_cast<Control*>(ctl);
   cudaError_t e;
   if (pp) {
-    // The partition kernels write everything they read; pass B writes every
-    // record it hands out.
-    e = cudaSuccess;
+    // Pass B writes every record it hands out (holes included); the counting
+    // pass and pass A add into zeroed counters.
+    e = cudaMemsetAsync(part_totals, 0, nparts * 4, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(part_cursor, 0, nparts * 4, stream);
   } else {
     e = cudaMemsetAsync(table, 0xFF, (slots + 1) * sizeof(KeyEntry), stream);
     // Group records start all-zero: every field's identity (dfc_internal.h).
@@ -1291,45 +1331,35 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   if (pp) {
     sp.part_words = pp->words;
     sp.part_buf = static_cast<unsigned long long*>(part_buf);
-    sp.part_cap = P.rows;
-    sp.part_counts = static_cast<uint32_t*>(part_counts);
     sp.part_totals = static_cast<uint32_t*>(part_totals);
     sp.part_start = static_cast<uint32_t*>(part_start);
-    sp.part_flush = pp->flush;
-    sp.part_stage_off = pp->stage_off;
+    sp.part_cursor = static_cast<uint32_t*>(part_cursor);
     sp.agg_slots = pp->agg_slots;
-    sp.agg_tables_n = (uint32_t)pp->clusters;
-    sp.agg_tables = static_cast<unsigned char*>(agg_tables);
     sp.part_next = &dctl->part_next;
   }
 
   cudaEvent_t* ev = attempt_events(P.device);
   cudaEventRecord(ev[0], stream);
   if (pp) {
-    partition_count<<<(unsigned)ncta, kPartThreads, pp->count_smem, stream>>>(sp);
+    // The counting pass streams the key and filter columns through a deeper
+    // ring of narrower stages (their bytes lead every stage).
+    ScanParams spc = sp;
+    spc.stages = pp->count_stages;
+    spc.stage_bytes = pp->count_stage_bytes;
+    partition_count<<<(unsigned)ncta, kPartThreads, pp->count_smem, stream>>>(spc);
     cudaEventRecord(ev[4], stream);
-    partition_offsets<<<(unsigned)((nparts + 255) / 256), 256, 0, stream>>>(sp, (uint32_t)ncta);
+    partition_offsets<<<1, 1024, 0, stream>>>(sp);
     cudaEventRecord(ev[5], stream);
-    partition_kernel<<<(unsigned)ncta, kPartThreads, pp->smem, stream>>>(sp);
+    ScanParams spa = sp;
+    spa.stages = pp->stages;
+    partition_kernel<<<(unsigned)ncta, kPartThreads, pp->smem, stream>>>(spa);
     cudaEventRecord(ev[3], stream);
-    cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = kAggCluster;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    const uint64_t clusters = std::min<uint64_t>((uint64_t)pp->clusters, nparts);
-    cfg.gridDim = dim3((unsigned)(clusters * kAggCluster));
-    cfg.blockDim = dim3(kAggThreads);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = stream;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    e = cudaLaunchKernelEx(&cfg, partition_aggregate, sp);
+    partition_aggregate<<<(unsigned)std::min<uint64_t>(pp->agg_ctas, nparts), kAggThreads, pp->agg_smem, stream>>>(sp);
+    e = cudaGetLastError();
     if (e != cudaSuccess) {
       free_outputs();
       S.release();
-        return cuda_fail(e, "partition aggregation launch");
+      return cuda_fail(e, "partition pass launch");
     }
     t_timings.launches += 4;
   } else {
@@ -1395,18 +1425,21 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   t_timings.finish_ns += ms_finish * 1e6;
   t_timings.table_slots = pp ? (uint64_t)pp->agg_slots : slots;
   t_timings.partitions = pp ? (int32_t)nparts : 0;
+  if (pp) {
+    t_timings.count_ns += ms_count * 1e6;
+    t_timings.place_ns += (ms_scan - ms_count - ms_offsets) * 1e6;
+  }
   if (getenv("DFC_TRACE")) {
     fprintf(stderr,
-            "dfc attempt: rows=%llu regime=%s slots=%llu recs=%llu smem_slots=%u x%u tile=%d top1=%.4f hot=%.3f ctas=%llu parts=%llu agg_slots=%u "
-            "clusters=%d flush=%u | status=%#x cap=%#x check=%#x alloc=%u groups=%u ms scan=%.3f (count=%.3f offsets=%.3f) "
-            "agg=%.3f fin=%.3f\n",
+            "dfc attempt: rows=%llu regime=%s slots=%llu recs=%llu smem_slots=%u x%u tile=%d top1=%.4f hot=%.3f ctas=%llu "
+            "parts=%llu agg_slots=%u agg_ctas=%llu stages=%d/%d | status=%#x cap=%#x check=%#x alloc=%u groups=%u ms "
+            "scan=%.3f (count=%.3f offsets=%.3f) agg=%.3f fin=%.3f\n",
             (unsigned long long)P.rows, pp ? "partitioned" : "table", (unsigned long long)slots,
             (unsigned long long)recs, sp.smem_slots, std::max(1u, sp.smem_cluster), sp.tile_rows, P.top1, P.top_hot,
-            (unsigned long long)ncta,
-            (unsigned long long)nparts,
-            pp ? pp->agg_slots : 0u, pp ? pp->clusters : 0, pp ? pp->flush : 0u, host_ctl->status[0],
-            host_ctl->status[1], host_ctl->status[2], host_ctl->alloc, host_ctl->groups, ms_scan, ms_count, ms_offsets,
-            ms_agg, ms_finish);
+            (unsigned long long)ncta, (unsigned long long)nparts, pp ? pp->agg_slots : 0u,
+            (unsigned long long)(pp ? pp->agg_ctas : 0), pp ? pp->count_stages : 0, pp ? pp->stages : 0,
+            host_ctl->status[0], host_ctl->status[1], host_ctl->status[2], host_ctl->alloc, host_ctl->groups, ms_scan,
+            ms_count, ms_offsets, ms_agg, ms_finish);
   }
   if (host_ctl->status[2] && !(host_ctl->status[0] & ST_TIMEOUT)) {
     free_outputs();
@@ -1535,7 +1568,7 @@ DFC_API dfc_status dfc_column_register(int32_t device, dfc_dtype dtype, uint64_t
     return s;
   };
   if (flags == DFC_COLUMN_HOST) {
-    cudaError_t e = cudaMallocAsync(&c->values, std::max<size_t>(256, (bytes + 255) & ~(size_t)255), stream);
+    cudaError_t e = pool_alloc(&c->values, std::max<size_t>(256, (bytes + 255) & ~(size_t)255), stream);
     if (e != cudaSuccess) return bail(cuda_fail(e, "column values"));
     c->owns_values = true;
     if (bytes) {
@@ -1548,15 +1581,15 @@ DFC_API dfc_status dfc_column_register(int32_t device, dfc_dtype dtype, uint64_t
   if (validity && rows > 0) {
     const uint64_t nbytes = (validity_bit_offset + rows + 7) / 8;
     const uint64_t words = (rows + 31) / 32;
-    cudaError_t e = cudaMallocAsync((void**)&c->validity, ((words * 4 + 255) & ~(uint64_t)255), stream);
+    cudaError_t e = pool_alloc((void**)&c->validity, ((words * 4 + 255) & ~(uint64_t)255), stream);
     if (e != cudaSuccess) return bail(cuda_fail(e, "validity bitmap"));
     const uint8_t* src = validity;
     void* staging = nullptr;
     unsigned long long* d_count = nullptr;
-    e = cudaMallocAsync((void**)&d_count, 8, stream);
+    e = pool_alloc((void**)&d_count, 8, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_count, 0, 8, stream);
     if (e == cudaSuccess && flags == DFC_COLUMN_HOST) {
-      e = cudaMallocAsync(&staging, nbytes, stream);
+      e = pool_alloc(&staging, nbytes, stream);
       if (e == cudaSuccess) e = cudaMemcpyAsync(staging, validity, nbytes, cudaMemcpyHostToDevice, stream);
       src = static_cast<const uint8_t*>(staging);
     }
@@ -1624,18 +1657,18 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
   // otherwise the global table alone.  Rows whose key finds no room in a CTA
   // table take the global path, so a low estimate costs speed, not results.
   P.sp.smem_slots = 0;
-  // The radix-partitioned regime on request.  Measured on B200 it does not
-  // yet beat the global table at load <= 1/8 (100M rows, 7.4M groups:
-  // about 14 ms against 8.7), so the automatic choice keeps the global table.
+  // The radix-partitioned regime: on request, or when the estimated groups'
+  // records outgrow the L2-sized budget (the global table's probes and
+  // atomics would then miss L2) and no key is hot enough to leave one pass B
+  // CTA with much more than its share of the rows.
   PartPlan pp;
   bool partitioned = false;
-  if ((query->flags & DFC_Q_FORCE_PARTITIONED) && !(query->flags & (DFC_Q_FORCE_GLOBAL | DFC_Q_FORCE_SHARED)))
+  const bool forced_off = (query->flags & (DFC_Q_FORCE_GLOBAL | DFC_Q_FORCE_SHARED)) != 0;
+  if (P.sp.key_mode == KEY_PACKED && est > kOwnAlwaysGroups && !(query->flags & DFC_Q_FORCE_GLOBAL))
+    measure_skew(P, ds, stream);
+  if (!forced_off && ((query->flags & DFC_Q_FORCE_PARTITIONED) || partition_by_default(P, est)))
     partitioned = plan_partitions(P, ds, est, pp);
-  if (!partitioned) {
-    if (P.sp.key_mode == KEY_PACKED && est > kOwnAlwaysGroups && !(query->flags & DFC_Q_FORCE_GLOBAL))
-      measure_skew(P, ds, stream);
-    plan_shared(P, ds, est, query->flags);
-  }
+  if (!partitioned) plan_shared(P, ds, est, query->flags);
   const auto t_plan = std::chrono::steady_clock::now();
   if (getenv("DFC_TRACE")) {
     auto us = [](auto a, auto b) { return std::chrono::duration<double, std::micro>(b - a).count(); };
@@ -1658,21 +1691,26 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
       if (!(host_ctl->status[0] & ST_CAPACITY)) continue;
     }
     if (partitioned) {
-      // Re-plan from the column statistics (a learned count may come from a
-      // query with another filter), at least 8x the last estimate and twice
-      // the groups already seen; the table and records at least double.
-      // A full table asks for more partitions or slots; when the plan cannot
-      // grow, the global regime takes the query.
+      // A partition's groups did not fit its table (the estimate was low):
+      // more partitions, sized from the column statistics, twice the last
+      // estimate and twice the records already handed out.  Records ran out:
+      // twice the records.  When the plan cannot grow, the global regime
+      // takes the query.
       const uint32_t why = host_ctl->status[1];
       const PartPlan last = pp;
-      const uint64_t stats = estimate_groups(query, P, ds, stream, false);
-      est = std::min<uint64_t>(P.rows, std::max<uint64_t>({stats, est * 8, (uint64_t)host_ctl->alloc * 2}));
-      if (plan_partitions(P, ds, est, pp)) {
-        if ((why & CAP_AGG_TABLE) && pp.agg_slots <= last.agg_slots) pp.agg_slots = std::min(last.agg_slots * 2, 1u << 28);
-        if (why & CAP_RECORDS) pp.recs = std::max<uint64_t>(pp.recs, std::min<uint64_t>(P.rows, last.recs * 2));
-        if (pp.bits != last.bits || pp.recs != last.recs || pp.agg_slots != last.agg_slots) continue;
+      if (why & CAP_AGG_TABLE) {
+        const uint64_t stats = estimate_groups(query, P, ds, stream, false);
+        est = std::min<uint64_t>(P.rows, std::max<uint64_t>({stats, est * 2, (uint64_t)host_ctl->alloc * 2}));
+        if (last.bits < (uint32_t)kPartMaxBits && plan_partitions(P, ds, est, pp, last.bits + 1)) {
+          pp.recs = std::max(pp.recs, last.recs);
+          continue;
+        }
+      } else if (why & CAP_RECORDS) {
+        pp.recs = std::min<uint64_t>(0xFFFFFFDFull, last.recs * 2);
+        if (pp.recs > last.recs) continue;
       }
       partitioned = false;
+      plan_shared(P, ds, est, query->flags);
       slots = std::min(next_pow2(std::max<uint64_t>(1024, est * factor)), max_slots);
       continue;
     }
@@ -2303,8 +2341,8 @@ DFC_API dfc_status dfc_groupby_batch(const dfc_query* const* queries, int32_t n,
   const auto t_alloc = std::chrono::steady_clock::now();
   unsigned char* arena = nullptr;
   Control* dctl = nullptr;
-  cudaError_t e = cudaMallocAsync((void**)&arena, std::max<size_t>(used, 256), main);
-  if (e == cudaSuccess) e = cudaMallocAsync((void**)&dctl, (size_t)n * sizeof(Control), main);
+  cudaError_t e = pool_alloc((void**)&arena, std::max<size_t>(used, 256), main);
+  if (e == cudaSuccess) e = pool_alloc((void**)&dctl, (size_t)n * sizeof(Control), main);
   if (e != cudaSuccess) {
     if (arena) cudaFreeAsync(arena, main);
     return cuda_fail(e, "batch working memory");
@@ -2514,7 +2552,7 @@ cudaError_t arena_get(dfc_server* sv, size_t need, cudaStream_t stream, Request*
   }
   const size_t size = (need + (64u << 20) - 1) & ~(size_t)((64u << 20) - 1);
   r->arena_size = size;
-  return cudaMallocAsync((void**)&r->arena, size, stream);
+  return pool_alloc((void**)&r->arena, size, stream);
 }
 
 // Keeps a finished request's arena (at most a quarter of the budget in all,
@@ -2568,7 +2606,7 @@ bool server_launch(dfc_server* sv, Request* r, int& k) {
   r->admitted = Clock::now();
   r->stream = stream;
   cudaError_t e = arena_get(sv, std::max<size_t>(used, 256), stream, r);
-  if (e == cudaSuccess) e = cudaMallocAsync((void**)&r->dctl, sizeof(Control), stream);
+  if (e == cudaSuccess) e = pool_alloc((void**)&r->dctl, sizeof(Control), stream);
   if (e == cudaSuccess && alloc_outputs(it, stream)) e = cudaErrorMemoryAllocation;
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -2742,7 +2780,7 @@ DFC_API dfc_status dfc_server_create(int32_t device, int32_t max_inflight, int64
   // side by side do not pay for mapping new memory (up to 0.6 s for 8 GB).
   {
     void* warm = nullptr;
-    if (cudaMallocAsync(&warm, (size_t)(sv->budget / 4), sv->streams[0]) == cudaSuccess) {
+    if (pool_alloc(&warm, (size_t)(sv->budget / 4), sv->streams[0]) == cudaSuccess) {
       cudaFreeAsync(warm, sv->streams[0]);
       cudaStreamSynchronize(sv->streams[0]);
     }

@@ -1063,15 +1063,15 @@ __device__ __forceinline__ T from_bits(uint64_t b) {
 // The rows' updates of one aggregated column: `recs` the rows' group records,
 // `ok` whether the row holds a valid value, `vb` the value's raw bits.
 // kShared: the records are in shared memory (generic loads, not .cg).
-template <typename T, bool kShared = false>
-__device__ __forceinline__ void update_rows(const ScanParams& p, const ValField& f, int v, unsigned char* const (&recs)[kR],
-                                            const bool (&ok)[kR], const uint64_t (&vb)[kR]) {
+template <typename T, bool kShared = false, int R = kR>
+__device__ __forceinline__ void update_rows(const ScanParams& p, const ValField& f, int v, unsigned char* const (&recs)[R],
+                                            const bool (&ok)[R], const uint64_t (&vb)[R]) {
   constexpr bool kFloat = std::is_floating_point<T>::value;
-  T val[kR];
-  uint64_t lo[kR], hi[kR], ks[kR];
+  T val[R];
+  uint64_t lo[R], hi[R], ks[R];
   // Values and the read-set of every row, loads in flight together.
 #pragma unroll
-  for (int j = 0; j < kR; ++j) {
+  for (int j = 0; j < R; ++j) {
     val[j] = ok[j] ? from_bits<T>(vb[j]) : T(0);
     lo[j] = hi[j] = ks[j] = 0;
     if (!ok[j]) continue;
@@ -1085,7 +1085,7 @@ __device__ __forceinline__ void update_rows(const ScanParams& p, const ValField&
     if (f.off_m2 >= 0) ks[j] = ld(f.off_shift);
   }
 #pragma unroll
-  for (int j = 0; j < kR; ++j) {
+  for (int j = 0; j < R; ++j) {
     if (!ok[j]) continue;
     unsigned char* rec = recs[j];
     rec_add_u32<kShared>(rec + f.off_count, 1u);
@@ -1523,43 +1523,40 @@ __device__ void merge_into(const ScanParams& p, const unsigned char* src, uint32
 // Radix-partitioned regime (many groups).
 //
 // With millions of groups the global table and records outgrow L2, and every
-// probe, read-set load and atomic becomes an HBM round trip: HBM serves about
-// 50 G random 16-byte loads and 25 G random atomics a second, L2 about 284 G
-// and 187 G.  So the scan only partitions, in three streaming kernels:
-//   count    the key and filter columns only: each CTA's selected rows per
-//            partition (shared-memory counters);
-//   offsets  per partition, the CTAs' exclusive prefix and the total;
-//   pass A   every staged column; each selected row is staged in shared
-//            memory and, partition-sorted, appended to its CTA's exact range
-//            of part_buf with coalesced writes -- no global atomics, so a
-//            flush costs shared-memory work and the writes only.
-// Pass B then hands each partition to a cluster of CTAs whose table
-// (agg_slots records, a few MB) stays L2-resident while the cluster folds the
-// partition into it; the live records are appended densely to `records`.
-// Both kernels see the same tiles per CTA (t = blockIdx.x + k * gridDim.x),
-// so pass A's rows of a partition fill exactly the range the count gave;
-// pass A checks that, and failed checks record a code in status word 2.
+// probe, read-set load and atomic of the global regime is an HBM round trip
+// (HBM serves about 50 G random 16-byte loads and 25 G random atomics a
+// second).  This regime turns the group-by into streaming passes and on-chip
+// work:
+//   count    the key and filter columns only: the selected rows per
+//            partition (shared-memory counters, one global add per CTA and
+//            partition at the end);
+//   offsets  the partitions' exclusive prefix: each partition's range of
+//            part_buf;
+//   pass A   every column: each selected row is written to the next place of
+//            its partition's range; a warp's rows of one partition reserve
+//            their places with one atomic on the partition's cursor.  The
+//            cursors of all partitions are a few tens of KB, so they and the
+//            partitions' write frontiers stay in L2, which merges the rows
+//            into whole lines before they reach HBM;
+//   pass B   one partition at a time per CTA: its rows (read once, streaming)
+//            fold into a shared-memory table sized so a partition's groups
+//            fit it; the live records are then appended to `records`.
+// Partitions are sized from the group estimate; a partition whose groups do
+// not fit the table raises CAP_AGG_TABLE and the host reruns with more.
 // ===========================================================================
-constexpr int kPartPerThread = kPartMax / kPartConsumerThreads;
-
-// Barrier of the partition kernels' consumer warps (named barrier 1).
-__device__ __forceinline__ bool part_sync_or(bool flag) {
-  uint32_t out;
-  asm volatile(
-      "{\n\t.reg .pred p, q;\n\t"
-      "setp.ne.u32 p, %1, 0;\n\t"
-      "bar.red.or.pred q, 1, %2, p;\n\t"
-      "selp.u32 %0, 1, 0, q;\n\t}"
-      : "=r"(out)
-      : "r"((uint32_t)flag), "n"(kPartConsumerThreads)
-      : "memory");
-  return out != 0;
-}
 
 __device__ __forceinline__ void part_check(const ScanParams& p, uint32_t code) { atomicOr(p.status + 2, code); }
 
+// The key word folded to 32 bits (its high half multiplied in), shared by the
+// partition hash and pass B's slot hash.
+__device__ __forceinline__ uint32_t fold_key(uint64_t kw) {
+  return (uint32_t)kw ^ ((uint32_t)(kw >> 32) * 0x9E3779B1u);
+}
+
+// Partition: the top part_bits bits of a multiplicative hash of the folded
+// key word (one multiply per row in the streaming passes).
 __device__ __forceinline__ uint32_t partition_of(const ScanParams& p, uint64_t kw) {
-  return (uint32_t)(mix64(kw ^ 0xA0761D6478BD642Full) >> (64 - p.part_bits));
+  return (fold_key(kw) * 0x85EBCA77u) >> (32 - p.part_bits);
 }
 
 __device__ __forceinline__ void raise_capacity(const ScanParams& p, uint32_t what) {
@@ -1567,33 +1564,10 @@ __device__ __forceinline__ void raise_capacity(const ScanParams& p, uint32_t wha
   atomicOr(p.status + 1, what);
 }
 
-// Exclusive prefix of one value per consumer thread (512 threads) and the
-// total; consumer warps only.
-__device__ __forceinline__ uint32_t consumer_exclusive_scan(uint32_t v, uint32_t* warp_tot, uint32_t* total) {
-  const int lane = threadIdx.x & 31, cw = (threadIdx.x >> 5) - 1;
-  uint32_t x = v;
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) warp_tot[cw] = x;
-  part_sync_or(false);
-  uint32_t before = 0, all = 0;
-  for (int w = 0; w < kPartWarps; ++w) {
-    const uint32_t t = warp_tot[w];
-    if (w < cw) before += t;
-    all += t;
-  }
-  *total = all;
-  part_sync_or(false);
-  return before + x - v;
-}
-
-// The partition kernels need no compaction: consumer warp w owns words
+// The partition passes need no compaction: consumer warp w owns words
 // w, w + 16, ... of every tile (kPR of them at most), and each lane handles
 // its own row of each word.  Selection is a ballot per word; unselected rows
-// are masked off.  Between flushes the warps pass no CTA barrier, so their
-// latencies overlap freely.
+// are masked off.  The warps pass no CTA barrier while streaming.
 constexpr int kPR = kMaxTileRows / 32 / kPartWarps;  // rows a lane holds per tile
 static_assert(kPR >= 1, "a consumer warp owns whole words");
 
@@ -1666,13 +1640,16 @@ __device__ __forceinline__ void ring_init(int S, uint64_t* full, uint64_t* empty
   __syncthreads();
 }
 
+// Counting pass.  Dynamic shared memory: the ring (p.stages stages of
+// p.stage_bytes, only the key and filter columns staged), its mbarriers,
+// then one counter per partition.
 __global__ void __launch_bounds__(kPartThreads, 1) partition_count(const __grid_constant__ ScanParams p) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int S = p.stages;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)S * p.stage_bytes);
   uint64_t* empty = full + S;
+  uint32_t* s_count = reinterpret_cast<uint32_t*>(empty + S);
   __shared__ volatile uint32_t s_abort;
-  __shared__ uint32_t s_count[kPartMax];
   const uint32_t nparts = 1u << p.part_bits;
   for (uint32_t q = threadIdx.x; q < nparts; q += blockDim.x) s_count[q] = 0;
   ring_init(S, full, empty, &s_abort);
@@ -1697,220 +1674,127 @@ __global__ void __launch_bounds__(kPartThreads, 1) partition_count(const __grid_
     }
   }
   __syncthreads();
-  for (uint32_t q = threadIdx.x; q < nparts; q += blockDim.x) p.part_counts[(size_t)blockIdx.x * nparts + q] = s_count[q];
+  for (uint32_t q = threadIdx.x; q < nparts; q += blockDim.x) {
+    const uint32_t c = s_count[q];
+    if (c) atomicAdd(&p.part_totals[q], c);
+  }
 }
 
-// Per partition (one thread each): the CTAs' counts become their exclusive
-// prefix; the total goes to part_totals.
-__global__ void partition_offsets(const __grid_constant__ ScanParams p, uint32_t ctas) {
+// The partitions' exclusive prefix (one CTA of 1024 threads).
+__global__ void __launch_bounds__(1024) partition_offsets(const __grid_constant__ ScanParams p) {
+  __shared__ uint32_t s_warp[32];
   const uint32_t nparts = 1u << p.part_bits;
-  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nparts) return;
-  uint32_t run = 0;
-  for (uint32_t c = 0; c < ctas; ++c) {
-    uint32_t* e = p.part_counts + (size_t)c * nparts + q;
-    const uint32_t v = *e;
-    *e = run;
-    run += v;
+  const uint32_t per = (nparts + blockDim.x - 1) / blockDim.x;
+  const uint32_t q0 = threadIdx.x * per;
+  uint32_t sum = 0;
+  for (uint32_t k = 0; k < per; ++k)
+    if (q0 + k < nparts) sum += p.part_totals[q0 + k];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = sum;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
   }
-  p.part_totals[q] = run;
-}
-
-struct PartSmem {
-  uint32_t cur[kPartMax];   // counts, then scatter cursors
-  uint32_t off[kPartMax];   // first sorted position of each partition in the flush
-  uint32_t base[kPartMax];  // part_buf row of that position (all ones: not stored)
-  uint32_t next[kPartMax];  // this CTA's next part_buf row of each partition
-  uint32_t end[kPartMax];   // the end of this CTA's range of each partition
-  uint32_t wfill[kPartWarps];  // rows each warp's staging region holds
-  uint32_t warp_tot[kPartWarps];
-};
-
-// Pass A's flush: the staged rows of every warp region (region rows each,
-// ps.wfill[w] used) sorted by partition through shared-memory counters and
-// appended to this CTA's ranges, consecutive threads writing consecutive
-// rows.  Every consumer thread calls it.
-__device__ void flush_staged(const ScanParams& p, const unsigned long long* staged, uint16_t* order,
-                             const uint16_t* rpart, uint32_t region_shift, PartSmem& ps) {
-  const uint32_t ct = threadIdx.x - 32;
-  const uint32_t nparts = 1u << p.part_bits;
-  const uint32_t cap = (uint32_t)kPartWarps << region_shift;
-  const uint32_t rmask = (1u << region_shift) - 1u;
-  for (uint32_t q = ct; q < nparts; q += kPartConsumerThreads) ps.cur[q] = 0;
-  part_sync_or(false);
-  uint32_t rows = 0;
-  for (int w = 0; w < kPartWarps; ++w) rows += ps.wfill[w];
-  for (uint32_t u = ct; u < cap; u += kPartConsumerThreads)
-    if ((u & rmask) < ps.wfill[u >> region_shift]) atomicAdd(&ps.cur[rpart[u]], 1u);
-  part_sync_or(false);
-  uint32_t h[kPartPerThread], sum = 0;
-#pragma unroll
-  for (int k = 0; k < kPartPerThread; ++k) {
-    const uint32_t q = ct * kPartPerThread + k;
-    h[k] = q < nparts ? ps.cur[q] : 0u;
-    sum += h[k];
-  }
-  uint32_t total;
-  uint32_t off = consumer_exclusive_scan(sum, ps.warp_tot, &total);
-#pragma unroll
-  for (int k = 0; k < kPartPerThread; ++k) {
-    const uint32_t q = ct * kPartPerThread + k;
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  uint32_t before = 0;
+  for (int w = 0; w < warp; ++w) before += s_warp[w];
+  uint32_t run = before + x - sum;
+  for (uint32_t k = 0; k < per; ++k) {
+    const uint32_t q = q0 + k;
     if (q < nparts) {
-      ps.off[q] = off;
-      ps.cur[q] = off;
-      const uint32_t at = ps.next[q];
-      if (h[k] && (at > ps.end[q] || ps.end[q] - at < h[k])) {
-        part_check(p, CHK_RANGE);
-        ps.base[q] = ~0u;
-      } else {
-        ps.base[q] = at;
-        ps.next[q] = at + h[k];
-      }
+      p.part_start[q] = run;
+      run += p.part_totals[q];
     }
-    off += h[k];
   }
-  part_sync_or(false);
-  for (uint32_t u = ct; u < cap; u += kPartConsumerThreads)
-    if ((u & rmask) < ps.wfill[u >> region_shift]) order[atomicAdd(&ps.cur[rpart[u]], 1u)] = (uint16_t)u;
-  part_sync_or(false);
-  const uint32_t W = p.part_words;
-  for (uint32_t s = ct; s < rows; s += kPartConsumerThreads) {
-    const uint32_t u = order[s];
-    const uint32_t q = rpart[u];
-    const uint32_t base = ps.base[q];
-    if (base == ~0u) continue;
-    const uint64_t x = (uint64_t)base + (s - ps.off[q]);
-    if (x >= p.part_cap) {
-      part_check(p, CHK_RANGE);
-      continue;
-    }
-    const unsigned long long* src = staged + (size_t)u * W;
-    unsigned long long* dst = p.part_buf + x * W;
-    for (uint32_t j = 0; j < W; ++j) dst[j] = src[j];
-  }
-  part_sync_or(false);
 }
 
+// Pass A.  Dynamic shared memory: the ring of every staged column and its
+// mbarriers.  Each selected row goes to part_start[q] + a place reserved on
+// q's cursor: the lanes of a warp with the same partition reserve together
+// (__match_any_sync), the lowest of them adds their count to the cursor, and
+// the reservations of all of a step's row slots are in flight at once.
 __global__ void __launch_bounds__(kPartThreads, 1) partition_kernel(const __grid_constant__ ScanParams p) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int S = p.stages;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)S * p.stage_bytes);
   uint64_t* empty = full + S;
-  unsigned long long* staged = reinterpret_cast<unsigned long long*>(smem + p.part_stage_off);
-  uint16_t* order = reinterpret_cast<uint16_t*>(staged + (size_t)p.part_flush * p.part_words);
-  uint16_t* rpart = order + p.part_flush;
   __shared__ volatile uint32_t s_abort;
-  __shared__ PartSmem s_part;
   ring_init(S, full, empty, &s_abort);
   if ((threadIdx.x >> 5) == 0) {
     if ((threadIdx.x & 31) == 0) produce_tiles(p, smem, full, empty, &s_abort, p.n_stage, (uint32_t)p.stage_tx);
     return;
   }
-  const uint32_t ct = threadIdx.x - 32;
-  const int cw = (threadIdx.x >> 5) - 1, lane = threadIdx.x & 31;
-  const uint32_t nparts = 1u << p.part_bits;
+  const int lane = threadIdx.x & 31;
   const uint32_t W = p.part_words;
-  // Staging: one region per consumer warp; a warp stages at most kSR * 32
-  // rows a step, so flushing every `every` steps never overflows a region.
-  uint32_t region_shift = 0;
-  while ((kPartWarps << (region_shift + 1)) <= p.part_flush) ++region_shift;
-  const uint32_t every = (1u << region_shift) / (kSR * 32);
-  // This CTA's range of each partition: the partition's start (prefix of the
-  // totals) plus the CTA's prefix among the CTAs.
-  {
-    uint32_t tot[kPartPerThread], sum = 0;
-#pragma unroll
-    for (int k = 0; k < kPartPerThread; ++k) {
-      const uint32_t q = ct * kPartPerThread + k;
-      tot[k] = q < nparts ? p.part_totals[q] : 0u;
-      sum += tot[k];
-    }
-    uint32_t all;
-    uint32_t start = consumer_exclusive_scan(sum, s_part.warp_tot, &all);
-#pragma unroll
-    for (int k = 0; k < kPartPerThread; ++k) {
-      const uint32_t q = ct * kPartPerThread + k;
-      if (q < nparts) {
-        const uint32_t mine = p.part_counts[(size_t)blockIdx.x * nparts + q];
-        const uint32_t upto = blockIdx.x + 1 < gridDim.x ? p.part_counts[(size_t)(blockIdx.x + 1) * nparts + q] : tot[k];
-        s_part.next[q] = start + mine;
-        s_part.end[q] = start + upto;
-        if (blockIdx.x == 0) p.part_start[q] = start;
-      }
-      start += tot[k];
-    }
-  }
-  const uint32_t rbase = (uint32_t)cw << region_shift;
-  uint32_t wfill = 0;  // this warp's staged rows (the same in all its lanes)
-  bool aborted = false;
-  uint32_t it = 0, step = 0;
-  for (uint64_t t = blockIdx.x; t < p.tiles; t += (uint64_t)kTilesPerStep * gridDim.x, ++step) {
+  const uint32_t nparts = 1u << p.part_bits;
+  uint32_t it = 0;
+  for (uint64_t t = blockIdx.x; t < p.tiles; t += (uint64_t)kTilesPerStep * gridDim.x) {
     Step s;
     int nt = 0;
-    if (!aborted && !step_wait(p, smem, full, t, it, &s_abort, s, nt)) aborted = true;
-    if (!aborted) {
-      RowRef x[kSR];
-      uint32_t bits[kSR];
-      uint64_t kw[kSR];
-      step_rows(p, s, nt, x, bits);
-      key_words<kSR>(p, s, x, kw);
-      // Positions in this warp's region: words in order, lanes in order.
-      uint32_t at[kSR];
-      uint32_t run = wfill;
+    if (!step_wait(p, smem, full, t, it, &s_abort, s, nt)) break;
+    RowRef x[kSR];
+    uint32_t bits[kSR];
+    uint64_t kw[kSR];
+    step_rows(p, s, nt, x, bits);
+    key_words<kSR>(p, s, x, kw);
+    uint32_t q[kSR], grp[kSR], base[kSR];
+    int lead[kSR];
 #pragma unroll
-      for (int j = 0; j < kSR; ++j) {
-        at[j] = rbase + run + __popc(bits[j] & ((1u << lane) - 1u));
-        run += __popc(bits[j]);
-      }
-      uint32_t vflags[kSR] = {};
-      for (int v = 0; v < p.n_vals; ++v) {
-        const int c = p.vals[v].input;
-        const ColRef cr = col_ref(p, s, c);
-        const int size = p.cols[c].size;
-#pragma unroll
-        for (int j = 0; j < kSR; ++j) {
-          if (!x[j].on) continue;
-          const bool ok = rvalid(cr, x[j]);
-          vflags[j] |= (uint32_t)ok << v;
-          staged[(size_t)at[j] * W + 2 + v] = ok ? load_bits(rv(cr, x[j]), size, x[j].r) : 0ull;
-        }
-      }
-      step_release(p, empty, it, nt);
-      it += nt;
-#pragma unroll
-      for (int j = 0; j < kSR; ++j) {
-        if (!x[j].on) continue;
-        staged[(size_t)at[j] * W] = kw[j];
-        staged[(size_t)at[j] * W + 1] = (uint64_t)(uint32_t)(s.start[x[j].tile] + x[j].r) | ((uint64_t)vflags[j] << 32);
-        rpart[at[j]] = (uint16_t)partition_of(p, kw[j]);
-      }
-      wfill = run;
+    for (int j = 0; j < kSR; ++j) {
+      q[j] = x[j].on ? partition_of(p, kw[j]) : 0u;
+      grp[j] = __match_any_sync(0xffffffffu, x[j].on ? q[j] : (0x80000000u | (uint32_t)lane));
+      lead[j] = __ffs(grp[j]) - 1;
     }
-    if ((step + 1) % every == 0) {
-      if (lane == 0) s_part.wfill[cw] = wfill;
-      if (part_sync_or(aborted)) {
-        aborted = true;
-        break;
+#pragma unroll
+    for (int j = 0; j < kSR; ++j) {
+      base[j] = 0;
+      if (x[j].on && lane == lead[j]) base[j] = atomicAdd(&p.part_cursor[q[j]], (uint32_t)__popc(grp[j]));
+    }
+    unsigned long long* dst[kSR];
+#pragma unroll
+    for (int j = 0; j < kSR; ++j) {
+      base[j] = __shfl_sync(0xffffffffu, base[j], lead[j]);
+      dst[j] = nullptr;
+      if (!x[j].on) continue;
+      const uint32_t at = base[j] + (uint32_t)__popc(grp[j] & ((1u << lane) - 1u));
+      if (q[j] >= nparts || at >= __ldg(p.part_totals + q[j])) {
+        part_check(p, CHK_RANGE);
+        continue;
       }
-      flush_staged(p, staged, order, rpart, region_shift, s_part);
-      wfill = 0;
+      dst[j] = p.part_buf + ((uint64_t)__ldg(p.part_start + q[j]) + at) * W;
+    }
+    uint32_t vflags[kSR] = {};
+    for (int v = 0; v < p.n_vals; ++v) {
+      const int c = p.vals[v].input;
+      const ColRef cr = col_ref(p, s, c);
+      const int size = p.cols[c].size;
+#pragma unroll
+      for (int j = 0; j < kSR; ++j) {
+        if (!dst[j]) continue;
+        const bool ok = rvalid(cr, x[j]);
+        vflags[j] |= (uint32_t)ok << v;
+        dst[j][2 + v] = ok ? load_bits(rv(cr, x[j]), size, x[j].r) : 0ull;
+      }
+    }
+    step_release(p, empty, it, nt);
+    it += nt;
+#pragma unroll
+    for (int j = 0; j < kSR; ++j) {
+      if (!dst[j]) continue;
+      dst[j][0] = kw[j];
+      dst[j][1] = (uint64_t)(uint32_t)(s.start[x[j].tile] + x[j].r) | ((uint64_t)vflags[j] << 32);
     }
   }
-  if (lane == 0) s_part.wfill[cw] = wfill;
-  if (part_sync_or(aborted)) return;
-  flush_staged(p, staged, order, rpart, region_shift, s_part);
-  // Every range filled exactly as counted.
-  for (uint32_t q = ct; q < nparts; q += kPartConsumerThreads)
-    if (s_part.next[q] != s_part.end[q]) part_check(p, CHK_RANGE);
 }
 
-
 // ---------------------------------------------------------------------------
-// Pass B.  A cluster's table is initialised once (key words all ones, fields
-// zero: every field's identity); then per partition taken from p.part_next
-// its CTAs fold the partition's rows into it with lock-step probe rounds and
-// the read-set/atomic updates of the global regime, all L2 hits, and append
-// the live records densely to `records`, resetting each slot as it is read.
+// Pass B.  The table: agg_slots records (any count) of rec_stride bytes in
+// dynamic shared memory, the key word at kRecKey (all ones = free), every
+// other field at its identity (zero), and one more record for the all-ones
+// key word.  A row finds its record by linear probing from a hash of its key
+// word (independent of the partition hash).  A record is live once a row set
+// its first row.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void reset_record(unsigned char* rec, size_t rs) {
   uint4* r = reinterpret_cast<uint4*>(rec);
@@ -1918,101 +1802,95 @@ __device__ __forceinline__ void reset_record(unsigned char* rec, size_t rs) {
   for (size_t q = 1; q < rs / 16; ++q) r[q] = make_uint4(0u, 0u, 0u, 0u);
 }
 
-__device__ __forceinline__ void fold_rows(const ScanParams& p, unsigned char* table, const unsigned long long* rows,
-                                          uint32_t n, uint64_t first, uint64_t stride) {
-  const uint32_t W = p.part_words;
-  const uint64_t mask = p.agg_slots - 1;
+// The shared-memory record of key word `kw` (claimed if new); false when the
+// table is seven-eighths full and the key is not in it.  Below that fill a
+// free slot always exists, so the probe ends within agg_slots steps.
+__device__ __forceinline__ bool agg_probe(const ScanParams& p, unsigned char* table, uint32_t* used, uint64_t kw,
+                                          unsigned char*& rec) {
+  const uint32_t S = p.agg_slots;
   const size_t rs = (size_t)p.rec_stride;
-  const int lane = threadIdx.x & 31;
-  bool on[kR], pend[kR];
-  uint64_t kw[kR], slot[kR], ek[kR];
-  uint32_t row[kR], vf[kR], ef[kR];
-  const unsigned long long* src[kR];
+  if (kw == kEmpty) {
+    rec = table + (size_t)S * rs;
+    return true;
+  }
+  uint32_t h = fold_key(kw) ^ 0x632BE59Bu;
+  h ^= h >> 16;
+  h *= 0x7FEB352Du;
+  h ^= h >> 15;
+  h *= 0x846CA68Bu;
+  h ^= h >> 16;
+  // First slot: the hash scaled to [0, S) (S need not be a power of two).
+  uint32_t s = (uint32_t)(((uint64_t)h * S) >> 32);
+  for (uint32_t probe = 0; probe < S; ++probe) {
+    unsigned long long* key = reinterpret_cast<unsigned long long*>(table + (size_t)s * rs + kRecKey);
+    const unsigned long long k = *reinterpret_cast<volatile unsigned long long*>(key);
+    bool hit = k == kw;
+    if (!hit && k == kEmpty) {
+      if (*reinterpret_cast<volatile uint32_t*>(used) >= S - S / 8) return false;
+      const unsigned long long prev = atomicCAS(key, kEmpty, kw);
+      if (prev == kEmpty) atomicAdd(used, 1u);
+      hit = prev == kEmpty || prev == kw;
+    }
+    if (hit) {
+      rec = table + (size_t)s * rs;
+      return true;
+    }
+    s = s + 1 == S ? 0u : s + 1;
+  }
+  return false;
+}
+
+constexpr int kBR = 2;  // rows a pass B thread holds in flight
+
+// kBR rows of a partition per thread: rows first + j * stride (< n).  Each
+// row updates its shared-memory record with per-lane atomics (the global
+// regime's update_rows on shared records); a warp's largest group of rows on
+// one record (a hot key) is first folded by butterflies (collapse_largest),
+// one atomic per field.
+__device__ __forceinline__ void fold_rows(const ScanParams& p, unsigned char* table, uint32_t* used,
+                                          const unsigned long long* rows, uint32_t n, uint32_t first, uint32_t stride) {
+  const uint32_t W = p.part_words;
+  bool on[kBR];
+  uint64_t kw[kBR], v0[kBR];
+  uint32_t row[kBR], vf[kBR];
+  const unsigned long long* src[kBR];
 #pragma unroll
-  for (int j = 0; j < kR; ++j) {
-    const uint64_t i = first + (uint64_t)j * stride;
+  for (int j = 0; j < kBR; ++j) {
+    const uint32_t i = first + (uint32_t)j * stride;
     on[j] = i < n;
-    src[j] = rows + (on[j] ? i : 0) * W;
-    kw[j] = slot[j] = 0;
+    src[j] = rows + (uint64_t)(on[j] ? i : 0) * W;
+    kw[j] = v0[j] = 0;
     row[j] = vf[j] = 0;
     if (!on[j]) continue;
     kw[j] = __ldcs(src[j]);
     const uint64_t w1 = __ldcs(src[j] + 1);
+    if (p.n_vals > 0) v0[j] = __ldcs(src[j] + 2);  // the first value column, loaded with the rest
     row[j] = (uint32_t)w1;
     vf[j] = (uint32_t)(w1 >> 32);
-    slot[j] = kw[j] == kEmpty ? (uint64_t)p.agg_slots : (mix64(kw[j] ^ 0x632BE59BD9B4E019ull) & mask);
   }
-  // Probe rounds; the first 16 bytes of a record are {key word, ~first row, flags}.
+  unsigned char* recs[kBR];
+  bool lost = false;
 #pragma unroll
-  for (int j = 0; j < kR; ++j) {
-    pend[j] = on[j] && kw[j] != kEmpty;
-    ek[j] = 0;
-    ef[j] = 0;
-    if (on[j]) {
-      const ulonglong2 e = __ldcg(reinterpret_cast<const ulonglong2*>(table + slot[j] * rs));
-      ek[j] = e.x;
-      ef[j] = (uint32_t)e.y;
-    }
+  for (int j = 0; j < kBR; ++j) {
+    recs[j] = table;
+    const bool hit = on[j] && agg_probe(p, table, used, kw[j], recs[j]);
+    lost |= on[j] && !hit;
+    on[j] = hit;
   }
-  const uint32_t limit = (uint32_t)(mask < 1024 ? mask + 1 : 1024);
-  for (uint32_t round = 0;; ++round) {
-    bool any = false;
+  if (lost) raise_capacity(p, CAP_AGG_TABLE);
+  // Hot keys: the warp's largest group per row slot folds by butterflies.
 #pragma unroll
-    for (int j = 0; j < kR; ++j) any |= pend[j];
-    if (!__any_sync(0xffffffffu, any)) break;
-    if (round > limit) {  // a full table: the host grows it
-#pragma unroll
-      for (int j = 0; j < kR; ++j) {
-        if (pend[j]) on[j] = false;
-        pend[j] = false;
-      }
-      if (any) raise_capacity(p, CAP_AGG_TABLE);
-      break;
-    }
-#pragma unroll
-    for (int j = 0; j < kR; ++j) {
-      if (!pend[j]) continue;
-      if (ek[j] == kw[j]) {
-        pend[j] = false;
-        continue;
-      }
-      if (ek[j] == kEmpty) {
-        const unsigned long long prev =
-            atomicCAS(reinterpret_cast<unsigned long long*>(table + slot[j] * rs), kEmpty, kw[j]);
-        if (prev == kEmpty || prev == kw[j]) {
-          pend[j] = false;
-          continue;
-        }
-      }
-      slot[j] = (slot[j] + 1) & mask;
-      const ulonglong2 e = __ldcg(reinterpret_cast<const ulonglong2*>(table + slot[j] * rs));
-      ek[j] = e.x;
-      ef[j] = (uint32_t)e.y;
-    }
-  }
-#pragma unroll
-  for (int j = 0; j < kR; ++j) {
-    if (on[j] && slot[j] > p.agg_slots) {
-      part_check(p, CHK_SLOT);
-      on[j] = false;
-    }
-    if (!on[j]) slot[j] = 0;
-  }
-  // Large groups of one record within the warp (hot keys) are folded by a
-  // butterfly first (up to two per row set): one atomic per field and group.
-#pragma unroll
-  for (int j = 0; j < kR; ++j) {
-    const uint64_t tag = on[j] ? slot[j] : (0x8000000000000000ull | (uint64_t)lane);
-    uint32_t grp = __match_any_sync(0xffffffffu, tag) & __ballot_sync(0xffffffffu, on[j]);
+  for (int j = 0; j < kBR; ++j) {
+    uint32_t grp = __match_any_sync(0xffffffffu, kw[j]) & __ballot_sync(0xffffffffu, on[j]);
     if (!on[j]) grp = 0;
     int maxpop = __reduce_max_sync(0xffffffffu, (unsigned)__popc(grp));
     for (int round = 0; round < 2 && maxpop >= kCollapseMin; ++round) {
-      unsigned char* rec = table + slot[j] * rs;
       const unsigned long long* sp = src[j];
       const uint32_t flags = vf[j];
-      if (collapse_largest(p, rec, grp, maxpop, on[j], row[j], [&](int v, bool& ok, uint64_t& b) {
+      const uint64_t first_val = v0[j];
+      if (collapse_largest(p, recs[j], grp, maxpop, on[j], row[j], [&](int v, bool& ok, uint64_t& b) {
             ok = (flags >> v) & 1u;
-            b = ok ? __ldcs(sp + 2 + v) : 0ull;
+            b = ok ? (v == 0 ? first_val : __ldcs(sp + 2 + v)) : 0ull;
           })) {
         on[j] = false;
         grp = 0;
@@ -2020,76 +1898,68 @@ __device__ __forceinline__ void fold_rows(const ScanParams& p, unsigned char* ta
       maxpop = __reduce_max_sync(0xffffffffu, (unsigned)__popc(grp));
     }
   }
-  unsigned char* recs[kR];
 #pragma unroll
-  for (int j = 0; j < kR; ++j) {
-    recs[j] = table + slot[j] * rs;
-    if (on[j] && ~row[j] > ef[j]) atomicMax(reinterpret_cast<uint32_t*>(recs[j] + kRecFirst), ~row[j]);
-    if (on[j] && p.off_len >= 0) red_add_u32(recs[j] + p.off_len, 1u);
+  for (int j = 0; j < kBR; ++j) {
+    if (!on[j]) continue;
+    rec_max_u32<true>(recs[j] + kRecFirst, ~row[j]);
+    if (p.off_len >= 0) rec_add_u32<true>(recs[j] + p.off_len, 1u);
   }
   for (int v = 0; v < p.n_vals; ++v) {
-    bool ok[kR];
-    uint64_t vb[kR];
+    bool ok[kBR];
+    uint64_t vb[kBR];
 #pragma unroll
-    for (int j = 0; j < kR; ++j) {
+    for (int j = 0; j < kBR; ++j) {
       ok[j] = on[j] && ((vf[j] >> v) & 1u);
-      vb[j] = ok[j] ? __ldcs(src[j] + 2 + v) : 0ull;
+      vb[j] = ok[j] ? (v == 0 ? v0[j] : __ldcs(src[j] + 2 + v)) : 0ull;
     }
     const ValField& f = p.vals[v];
     switch (f.dtype) {
-      case DFC_INT8: update_rows<int8_t>(p, f, v, recs, ok, vb); break;
-      case DFC_INT16: update_rows<int16_t>(p, f, v, recs, ok, vb); break;
-      case DFC_INT32: update_rows<int32_t>(p, f, v, recs, ok, vb); break;
-      case DFC_INT64: update_rows<int64_t>(p, f, v, recs, ok, vb); break;
-      case DFC_UINT8: update_rows<uint8_t>(p, f, v, recs, ok, vb); break;
-      case DFC_UINT16: update_rows<uint16_t>(p, f, v, recs, ok, vb); break;
-      case DFC_UINT32: update_rows<uint32_t>(p, f, v, recs, ok, vb); break;
-      case DFC_UINT64: update_rows<uint64_t>(p, f, v, recs, ok, vb); break;
-      case DFC_FLOAT32: update_rows<float>(p, f, v, recs, ok, vb); break;
-      default: update_rows<double>(p, f, v, recs, ok, vb); break;
+      case DFC_INT8: update_rows<int8_t, true, kBR>(p, f, v, recs, ok, vb); break;
+      case DFC_INT16: update_rows<int16_t, true, kBR>(p, f, v, recs, ok, vb); break;
+      case DFC_INT32: update_rows<int32_t, true, kBR>(p, f, v, recs, ok, vb); break;
+      case DFC_INT64: update_rows<int64_t, true, kBR>(p, f, v, recs, ok, vb); break;
+      case DFC_UINT8: update_rows<uint8_t, true, kBR>(p, f, v, recs, ok, vb); break;
+      case DFC_UINT16: update_rows<uint16_t, true, kBR>(p, f, v, recs, ok, vb); break;
+      case DFC_UINT32: update_rows<uint32_t, true, kBR>(p, f, v, recs, ok, vb); break;
+      case DFC_UINT64: update_rows<uint64_t, true, kBR>(p, f, v, recs, ok, vb); break;
+      case DFC_FLOAT32: update_rows<float, true, kBR>(p, f, v, recs, ok, vb); break;
+      default: update_rows<double, true, kBR>(p, f, v, recs, ok, vb); break;
     }
   }
 }
 
-__global__ void __launch_bounds__(kAggThreads, 1) partition_aggregate(const __grid_constant__ ScanParams p) {
-  __shared__ uint32_t s_part;
+__global__ void __launch_bounds__(kAggThreads, 2) partition_aggregate(const __grid_constant__ ScanParams p) {
+  extern __shared__ __align__(16) unsigned char table[];
+  __shared__ uint32_t s_next, s_used, s_base, s_hole_lo, s_hole_hi, s_chunk_next, s_chunk_end;
   __shared__ uint32_t s_warp[kAggThreads / 32];
-  __shared__ uint32_t s_base;
-  const uint32_t crank = cluster_rank(), csize = cluster_ranks();
-  const uint32_t cid = cluster_index();
-  if (cid >= p.agg_tables_n) {  // uniform over the cluster
-    if (threadIdx.x == 0) part_check(p, CHK_CLUSTER);
-    return;
-  }
-  const uint64_t slots = p.agg_slots;
-  const size_t rs = (size_t)p.rec_stride;
-  unsigned char* table = p.agg_tables + (size_t)cid * (slots + 1) * rs;
   const uint32_t nparts = 1u << p.part_bits;
-  const uint64_t lt = (uint64_t)crank * blockDim.x + threadIdx.x, lstride = (uint64_t)csize * blockDim.x;
+  const uint32_t S = p.agg_slots;
+  const size_t rs = (size_t)p.rec_stride;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // This CTA's share of the slots (initialisation, extraction and reset).
-  const uint64_t per = (slots + 1 + csize - 1) / csize;
-  const uint64_t lo = (uint64_t)crank * per < slots + 1 ? (uint64_t)crank * per : slots + 1;
-  const uint64_t hi = lo + per < slots + 1 ? lo + per : slots + 1;
-  for (uint64_t s = lo + threadIdx.x; s < hi; s += blockDim.x) reset_record(table + s * rs, rs);
+  for (uint32_t s = threadIdx.x; s <= S; s += blockDim.x) reset_record(table + (size_t)s * rs, rs);
+  if (threadIdx.x == 0) {
+    s_next = atomicAdd(p.part_next, 1u);
+    s_used = 0;
+    s_chunk_next = s_chunk_end = 0;
+  }
+  __syncthreads();
   for (;;) {
-    if (crank == 0 && threadIdx.x == 0) s_part = atomicAdd(p.part_next, 1u);
-    cluster_sync_all();
-    const uint32_t part = ld_cluster_u32(&s_part, 0);
-    if (part >= nparts) {
-      cluster_sync_all();  // rank 0's shared memory outlives every read of it
-      break;
-    }
-    // Fold the partition's rows.
-    const uint64_t start = p.part_start[part];
-    const uint64_t total = p.part_totals[part];
-    const uint32_t n = (uint32_t)(start >= p.part_cap ? 0 : (total < p.part_cap - start ? total : p.part_cap - start));
-    const unsigned long long* rows = p.part_buf + start * p.part_words;
-    for (uint64_t base = 0; base < n; base += lstride * kR) fold_rows(p, table, rows, n, base + lt, lstride);
-    cluster_sync_all();
-    // Append the live records (first row set), one counter reservation per CTA.
+    const uint32_t part = s_next;
+    if (part >= nparts) break;
+    __syncthreads();  // every thread read s_next
+    // The next partition is fetched while this one folds.
+    if (threadIdx.x == 0) s_next = atomicAdd(p.part_next, 1u);
+    const uint32_t n = p.part_totals[part];
+    if (threadIdx.x == 0 && p.part_cursor[part] != n) part_check(p, CHK_RANGE);
+    const unsigned long long* rows = p.part_buf + (uint64_t)p.part_start[part] * p.part_words;
+    const uint32_t per = blockDim.x * (uint32_t)kBR;
+    for (uint32_t base = 0; base < n; base += per) fold_rows(p, table, &s_used, rows, n, base + threadIdx.x, blockDim.x);
+    __syncthreads();
+    // Live records: count, reserve (chunks of kRecChunk from p.alloc), copy
+    // out and reset.
     uint32_t mine = 0;
-    for (uint64_t s = lo + threadIdx.x; s < hi; s += blockDim.x) mine += ld_cg_u32(table + s * rs + kRecFirst) != 0;
+    for (uint32_t s = threadIdx.x; s <= S; s += blockDim.x)
+      mine += *reinterpret_cast<const uint32_t*>(table + (size_t)s * rs + kRecFirst) != 0u;
     uint32_t x = mine;
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
@@ -2104,23 +1974,40 @@ __global__ void __launch_bounds__(kAggThreads, 1) partition_aggregate(const __gr
         s_warp[w] = tot;
         tot += t;
       }
-      s_base = tot ? atomicAdd(p.alloc, tot) : 0u;
-      if (tot && (uint64_t)s_base + tot > p.recs_total) raise_capacity(p, CAP_RECORDS);
+      s_hole_lo = s_hole_hi = 0;
+      if (tot > s_chunk_end - s_chunk_next) {
+        // The rest of the current chunk stays unused: holes for the finish.
+        s_hole_lo = s_chunk_next;
+        s_hole_hi = s_chunk_end;
+        const uint32_t grab = tot > kRecChunk ? tot : kRecChunk;
+        s_chunk_next = atomicAdd(p.alloc, grab);
+        s_chunk_end = s_chunk_next + grab;
+        if ((uint64_t)s_chunk_next + grab > p.recs_total) raise_capacity(p, CAP_RECORDS);
+      }
+      s_base = s_chunk_next;
+      s_chunk_next += tot;
+      s_used = 0;
     }
     __syncthreads();
+    for (uint32_t r = s_hole_lo + threadIdx.x; r < s_hole_hi; r += blockDim.x)
+      if (r < p.recs_total) *reinterpret_cast<uint32_t*>(record_at(p, r) + kRecFirst) = 0u;
     uint32_t dst = s_base + s_warp[warp] + x - mine;
-    for (uint64_t s = lo + threadIdx.x; s < hi; s += blockDim.x) {
-      unsigned char* rec = table + s * rs;
-      if (ld_cg_u32(rec + kRecFirst) == 0) continue;
+    for (uint32_t s = threadIdx.x; s <= S; s += blockDim.x) {
+      unsigned char* rec = table + (size_t)s * rs;
+      if (*reinterpret_cast<const uint32_t*>(rec + kRecFirst) == 0u) continue;
       if (dst < p.recs_total) {
         uint4* out = reinterpret_cast<uint4*>(record_at(p, dst));
-        for (size_t q = 0; q < rs / 16; ++q) out[q] = __ldcg(reinterpret_cast<const uint4*>(rec) + q);
+        const uint4* in = reinterpret_cast<const uint4*>(rec);
+        for (size_t q = 0; q < rs / 16; ++q) out[q] = in[q];
       }
       reset_record(rec, rs);
       ++dst;
     }
-    __syncthreads();  // s_warp and s_base are rewritten for the next partition
+    __syncthreads();  // s_warp, s_base and the table are reused for the next partition
   }
+  // The unused rest of the last chunk: holes.
+  for (uint32_t r = s_chunk_next + threadIdx.x; r < s_chunk_end; r += blockDim.x)
+    if (r < p.recs_total) *reinterpret_cast<uint32_t*>(record_at(p, r) + kRecFirst) = 0u;
 }
 
 }  // namespace dfc

@@ -363,6 +363,8 @@ def last_timings() -> dict:
         "aggregate_ns": t.aggregate_ns,
         "cluster_ctas": int(t.cluster_ctas),
         "compensated": int(t.compensated),
+        "count_ns": t.count_ns,
+        "place_ns": t.place_ns,
     }
 
 

@@ -395,6 +395,8 @@ typedef struct dfc_timings {
   double aggregate_ns; /* radix-partitioned regime: the per-partition aggregation pass (scan_ns: the partition pass) */
   int32_t cluster_ctas; /* shared-memory regime: CTAs pooling one table (1: each CTA its own) */
   int32_t compensated;  /* value fields accumulated as compensated FP32 partials (bit per field) */
+  double count_ns;      /* radix-partitioned regime: the counting pass (part of scan_ns) */
+  double place_ns;      /* radix-partitioned regime: the pass placing rows into partitions (part of scan_ns) */
 } dfc_timings;
 DFC_API dfc_status dfc_last_timings(dfc_timings* out);
 

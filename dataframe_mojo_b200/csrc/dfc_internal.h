@@ -173,7 +173,23 @@ struct ScanParams {
   uint32_t* part_cursor;   // [partition] rows pass A placed (zeroed before pass A)
   uint32_t agg_slots;      // pass B table slots
   uint32_t* part_next;     // pass B work counter
+  // The quad row path of the counting pass and pass A (fast_rows = 1): every
+  // lane takes four consecutive rows of a 1024-row tile with vector loads.
+  // It needs integer key columns and no filter or one comparison, held in
+  // range form: a row is selected when its filter value x (valid, read as
+  // fast_kind) satisfies (fast_lo <= x <= fast_hi) != fast_neg.
+  int32_t fast_rows;
+  int32_t fast_col;   // the compared column's slot, -1: no filter
+  int32_t fast_kind;  // FAST_SIGNED (sign-extended int64), FAST_UNSIGNED (zero-extended uint64) or FAST_FLOAT (double)
+  int32_t fast_neg;
+  union {
+    int64_t i;
+    uint64_t u;
+    double f;
+  } fast_lo, fast_hi;
 };
+
+enum FastKind : int32_t { FAST_SIGNED = 0, FAST_UNSIGNED = 1, FAST_FLOAT = 2 };
 
 // Which capacity ran out (status word 1), so the host grows only that.
 enum CapacityBits : uint32_t { CAP_RECORDS = 1u, CAP_AGG_TABLE = 2u };

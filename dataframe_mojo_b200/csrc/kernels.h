@@ -30,8 +30,10 @@ constexpr int kPartConsumerThreads = kPartWarps * 32;
 constexpr int kPartThreads = kPartConsumerThreads + 32;
 constexpr uint32_t kRecChunk = 4096;  // records pass B draws from `alloc` at a time
 __global__ void partition_count(const __grid_constant__ ScanParams p);
+__global__ void partition_count_quad(const __grid_constant__ ScanParams p);  // the quad row path (fast_rows)
 __global__ void partition_offsets(const __grid_constant__ ScanParams p);
 __global__ void partition_kernel(const __grid_constant__ ScanParams p);
+__global__ void partition_kernel_quad(const __grid_constant__ ScanParams p);
 __global__ void partition_aggregate(const __grid_constant__ ScanParams p);
 __global__ void finish_mark(const __grid_constant__ FinishParams f);
 __global__ void finish_chunk_sums(const __grid_constant__ FinishParams f);

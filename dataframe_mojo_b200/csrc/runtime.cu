@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <string>
@@ -229,14 +230,22 @@ dfc_status device_ready(int dev, DeviceState** out) {
        "cudaFuncSetAttribute");
     // The partition passes: the counting pass and pass A at one CTA per SM,
     // pass B at two when its table fits half an SM.
-    CK(cudaFuncGetAttributes(&fa, partition_kernel), "cudaFuncGetAttributes");
-    d.part_smem_optin = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;
-    CK(cudaFuncSetAttribute(partition_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.part_smem_optin),
-       "cudaFuncSetAttribute");
-    CK(cudaFuncGetAttributes(&fa, partition_count), "cudaFuncGetAttributes");
-    d.count_smem_optin = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;
-    CK(cudaFuncSetAttribute(partition_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.count_smem_optin),
-       "cudaFuncSetAttribute");
+    d.part_smem_optin = prop.sharedMemPerBlockOptin;
+    for (auto f : {partition_kernel, partition_kernel_quad}) {
+      CK(cudaFuncGetAttributes(&fa, f), "cudaFuncGetAttributes");
+      d.part_smem_optin = std::min(d.part_smem_optin, prop.sharedMemPerBlockOptin - fa.sharedSizeBytes);
+    }
+    for (auto f : {partition_kernel, partition_kernel_quad})
+      CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.part_smem_optin),
+         "cudaFuncSetAttribute");
+    d.count_smem_optin = prop.sharedMemPerBlockOptin;
+    for (auto f : {partition_count, partition_count_quad}) {
+      CK(cudaFuncGetAttributes(&fa, f), "cudaFuncGetAttributes");
+      d.count_smem_optin = std::min(d.count_smem_optin, prop.sharedMemPerBlockOptin - fa.sharedSizeBytes);
+    }
+    for (auto f : {partition_count, partition_count_quad})
+      CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.count_smem_optin),
+         "cudaFuncSetAttribute");
     CK(cudaFuncGetAttributes(&fa, partition_aggregate), "cudaFuncGetAttributes");
     d.agg_smem_optin = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;
     d.agg_smem_half = (prop.sharedMemPerMultiprocessor - 2 * prop.reservedSharedMemPerBlock) / 2 - fa.sharedSizeBytes;
@@ -1176,7 +1185,7 @@ bool plan_partitions(const Plan& P, const DeviceState* ds, uint64_t est, PartPla
   const ScanParams& sp = P.sp;
   if (sp.key_mode != KEY_PACKED || P.rows == 0 || P.rows >= 0xFFFFFFFFull) return false;
   pp.words = 2 + (uint32_t)sp.n_vals;
-  const size_t rs = (size_t)sp.rec_stride;
+  const size_t rs = (size_t)sp.rec_stride + 8;  // the shared-memory record stride (scan.cu agg_stride)
   const double groups = (double)std::max<uint64_t>(est, 1);
   // Slots of a table in `bytes` (any count, a multiple of 32), besides the
   // record of the all-ones key word.
@@ -1217,6 +1226,97 @@ bool plan_partitions(const Plan& P, const DeviceState* ds, uint64_t est, PartPla
   pp.ctas = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ds->sms, sp.tiles));
   // Every group once, plus the unused tail of each pass B CTA's last chunk.
   pp.recs = std::min<uint64_t>(0xFFFFFFDFull, (uint64_t)(groups * 1.25) + 4096 + pp.agg_ctas * kRecChunk);
+  return true;
+}
+
+// The quad row path of the partition passes (ScanParams::fast_rows): staged
+// 1024-row tiles, integer key columns, and no filter or one comparison, put
+// in range form here: the row is selected when its valid value x satisfies
+// (lo <= x <= hi) != neg, with the comparison semantics of the kernels'
+// select_word_cmp (floats in their own type, UInt64 unsigned, other integers
+// as Int64).  False leaves the generic row path.
+bool plan_quad(ScanParams& sp) {
+  sp.fast_rows = 0;
+  sp.fast_col = -1;
+  sp.fast_neg = 0;
+  sp.fast_kind = FAST_SIGNED;
+  if (sp.tile_rows != 1024 || !sp.use_tma || sp.key_mode != KEY_PACKED) return false;
+  for (int k = 0; k < sp.n_keys; ++k)
+    if (is_float(sp.keys[k].dtype)) return false;
+  if (sp.n_pred == 0) {
+    sp.fast_rows = 1;
+    return true;
+  }
+  if (sp.n_pred != 1 || sp.pred[0].kind != DFC_PRED_CMP) return false;
+  const PredOp& op = sp.pred[0];
+  const int dt = sp.cols[op.input].dtype;
+  const int cmp = op.cmp;
+  sp.fast_col = op.input;
+  sp.fast_neg = cmp == DFC_NE ? 1 : 0;
+  if (is_float(dt)) {
+    sp.fast_kind = FAST_FLOAT;
+    const double inf = std::numeric_limits<double>::infinity();
+    double lit = op.lit.f, below, above;
+    if (dt == DFC_FLOAT32) {
+      const float lf = (float)lit;
+      lit = lf;
+      below = std::nextafter(lf, -std::numeric_limits<float>::infinity());
+      above = std::nextafter(lf, std::numeric_limits<float>::infinity());
+    } else {
+      below = std::nextafter(lit, -inf);
+      above = std::nextafter(lit, inf);
+    }
+    double lo = -inf, hi = inf;
+    switch (cmp) {
+      case DFC_LT: hi = below; if (lit == -inf) { lo = 1; hi = 0; } break;
+      case DFC_LE: hi = lit; break;
+      case DFC_GT: lo = above; if (lit == inf) { lo = 1; hi = 0; } break;
+      case DFC_GE: lo = lit; break;
+      default: lo = hi = lit; break;  // EQ, NE (a NaN literal matches nothing)
+    }
+    sp.fast_lo.f = lo;
+    sp.fast_hi.f = hi;
+  } else if (dt == DFC_UINT64) {
+    sp.fast_kind = FAST_UNSIGNED;
+    const uint64_t lit = op.lit.u;
+    uint64_t lo = 0, hi = UINT64_MAX;
+    switch (cmp) {
+      case DFC_LT: if (lit == 0) { lo = 1; hi = 0; } else hi = lit - 1; break;
+      case DFC_LE: hi = lit; break;
+      case DFC_GT: if (lit == UINT64_MAX) { lo = 1; hi = 0; } else lo = lit + 1; break;
+      case DFC_GE: lo = lit; break;
+      default: lo = hi = lit; break;
+    }
+    sp.fast_lo.u = lo;
+    sp.fast_hi.u = hi;
+  } else {
+    const int64_t lit = op.lit.i;
+    int64_t lo = INT64_MIN, hi = INT64_MAX;
+    bool empty = false;
+    switch (cmp) {
+      case DFC_LT: if (lit == INT64_MIN) empty = true; else hi = lit - 1; break;
+      case DFC_LE: hi = lit; break;
+      case DFC_GT: if (lit == INT64_MAX) empty = true; else lo = lit + 1; break;
+      case DFC_GE: lo = lit; break;
+      default: lo = hi = lit; break;
+    }
+    if (is_unsigned(dt)) {
+      // Zero-extended values up to 32 bits: the range clipped to x >= 0.
+      sp.fast_kind = FAST_UNSIGNED;
+      if (empty || hi < 0) {
+        sp.fast_lo.u = 1;
+        sp.fast_hi.u = 0;
+      } else {
+        sp.fast_lo.u = (uint64_t)std::max<int64_t>(lo, 0);
+        sp.fast_hi.u = (uint64_t)hi;
+      }
+    } else {
+      sp.fast_kind = FAST_SIGNED;
+      sp.fast_lo.i = empty ? 1 : lo;
+      sp.fast_hi.i = empty ? 0 : hi;
+    }
+  }
+  sp.fast_rows = 1;
   return true;
 }
 
@@ -1343,16 +1443,17 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   if (pp) {
     // The counting pass streams the key and filter columns through a deeper
     // ring of narrower stages (their bytes lead every stage).
+    const bool quad = plan_quad(sp) && !getenv("DFC_NO_QUAD");
     ScanParams spc = sp;
     spc.stages = pp->count_stages;
     spc.stage_bytes = pp->count_stage_bytes;
-    partition_count<<<(unsigned)ncta, kPartThreads, pp->count_smem, stream>>>(spc);
+    (quad ? partition_count_quad : partition_count)<<<(unsigned)ncta, kPartThreads, pp->count_smem, stream>>>(spc);
     cudaEventRecord(ev[4], stream);
     partition_offsets<<<1, 1024, 0, stream>>>(sp);
     cudaEventRecord(ev[5], stream);
     ScanParams spa = sp;
     spa.stages = pp->stages;
-    partition_kernel<<<(unsigned)ncta, kPartThreads, pp->smem, stream>>>(spa);
+    (quad ? partition_kernel_quad : partition_kernel)<<<(unsigned)ncta, kPartThreads, pp->smem, stream>>>(spa);
     cudaEventRecord(ev[3], stream);
     partition_aggregate<<<(unsigned)std::min<uint64_t>(pp->agg_ctas, nparts), kAggThreads, pp->agg_smem, stream>>>(sp);
     e = cudaGetLastError();

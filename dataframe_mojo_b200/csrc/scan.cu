@@ -1640,10 +1640,135 @@ __device__ __forceinline__ void ring_init(int S, uint64_t* full, uint64_t* empty
   __syncthreads();
 }
 
+// ---------------------------------------------------------------------------
+// The quad row path (ScanParams::fast_rows).  Consumer thread g of a step
+// takes rows 4 (g % 256) .. + 3 of the step's tile g / 256 (1024-row tiles),
+// reading each column's four values with one or two vector loads from the
+// stage; the filter is one range test per row and each key column is packed
+// by its size, with no per-row type dispatch.
+// ---------------------------------------------------------------------------
+static_assert(kTilesPerStep * kMaxTileRows / 4 == kPartConsumerThreads, "one quad per consumer thread and step");
+
+struct Quad {
+  int tile;                    // the step's tile, -1: none
+  uint32_t r0;                 // first row inside the tile
+  uint32_t in;                 // rows inside the tile (bits 0..3)
+  bool staged;
+  const unsigned char* stage;  // the tile's stage (staged tiles)
+  uint64_t start;              // the tile's first row
+};
+
+// The tile fields are chosen with compile-time indices (a runtime index
+// into Step would put it in local memory).
+__device__ __forceinline__ Quad quad_of(const Step& s, int nt) {
+  const uint32_t g = threadIdx.x - 32;
+  Quad q;
+  q.tile = (int)(g >> 8);
+  q.r0 = (g & 255u) * 4;
+  const bool second = q.tile != 0;
+  q.staged = second ? s.staged[1] : s.staged[0];
+  q.stage = second ? s.stage[1] : s.stage[0];
+  q.start = second ? s.start[1] : s.start[0];
+  const uint32_t n = second ? s.n[1] : s.n[0];
+  if (q.tile >= nt) {
+    q.tile = -1;
+    q.in = 0;
+    return q;
+  }
+  const uint32_t left = n > q.r0 ? n - q.r0 : 0u;
+  q.in = left >= 4 ? 0xFu : (1u << left) - 1u;
+  return q;
+}
+
+// Raw bits (zero-extended) of the quad's rows of column c.
+__device__ __forceinline__ void quad_load(const ScanParams& p, const Quad& q, int c, uint64_t (&x)[4]) {
+  const int size = p.cols[c].size;
+  if (q.staged) {
+    const unsigned char* at = q.stage + p.stage_off[c] + (size_t)q.r0 * size;
+    switch (size) {
+      case 8: {
+        const ulonglong2 a = reinterpret_cast<const ulonglong2*>(at)[0], b = reinterpret_cast<const ulonglong2*>(at)[1];
+        x[0] = a.x; x[1] = a.y; x[2] = b.x; x[3] = b.y;
+        return;
+      }
+      case 4: {
+        const uint4 a = *reinterpret_cast<const uint4*>(at);
+        x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+        return;
+      }
+      case 2: {
+        const uint2 a = *reinterpret_cast<const uint2*>(at);
+        x[0] = a.x & 0xFFFFu; x[1] = a.x >> 16; x[2] = a.y & 0xFFFFu; x[3] = a.y >> 16;
+        return;
+      }
+      default: {
+        const uint32_t a = *reinterpret_cast<const uint32_t*>(at);
+        x[0] = a & 0xFFu; x[1] = (a >> 8) & 0xFFu; x[2] = (a >> 16) & 0xFFu; x[3] = a >> 24;
+        return;
+      }
+    }
+  }
+  const unsigned char* vals = static_cast<const unsigned char*>(p.cols[c].values) + q.start * (uint64_t)size;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) x[i] = ((q.in >> i) & 1u) ? load_bits(vals, size, q.r0 + i) : 0ull;
+}
+
+// Validity bits of the quad's rows of column c (bits 0..3, rows outside the
+// tile 0).
+__device__ __forceinline__ uint32_t quad_valid(const ScanParams& p, const Quad& q, int c) {
+  const uint32_t* w;
+  if (q.staged) w = p.stage_voff[c] >= 0 ? reinterpret_cast<const uint32_t*>(q.stage + p.stage_voff[c]) : nullptr;
+  else w = p.cols[c].validity ? p.cols[c].validity + q.start / 32 : nullptr;
+  if (w == nullptr || q.in == 0) return q.in;
+  return (w[q.r0 >> 5] >> (q.r0 & 31u)) & q.in;
+}
+
+// Selected rows of the quad (bits 0..3).
+__device__ __forceinline__ uint32_t quad_select(const ScanParams& p, const Quad& q) {
+  if (p.fast_col < 0 || q.in == 0) return q.in;
+  const int c = p.fast_col;
+  uint64_t x[4];
+  quad_load(p, q, c, x);
+  const uint32_t valid = quad_valid(p, q, c);
+  const int dt = p.cols[c].dtype;
+  const int sh = 64 - 8 * p.cols[c].size;
+  uint32_t sel = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    bool v;
+    if (p.fast_kind == FAST_FLOAT) {
+      const double d = bits_to_f64(x[i], dt);
+      v = d >= p.fast_lo.f && d <= p.fast_hi.f;
+    } else if (p.fast_kind == FAST_UNSIGNED) {
+      v = x[i] >= p.fast_lo.u && x[i] <= p.fast_hi.u;
+    } else {
+      const int64_t xi = (int64_t)(x[i] << sh) >> sh;  // sign-extended from the column's size
+      v = xi >= p.fast_lo.i && xi <= p.fast_hi.i;
+    }
+    sel |= (uint32_t)(v != (p.fast_neg != 0)) << i;
+  }
+  return sel & valid;
+}
+
+// Packed key words of the quad's rows (packed key mode).
+__device__ __forceinline__ void quad_keys(const ScanParams& p, const Quad& q, uint64_t (&kw)[4]) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) kw[i] = 0;
+  for (int k = 0; k < p.n_keys; ++k) {
+    const KeyField& f = p.keys[k];
+    uint64_t x[4];
+    quad_load(p, q, f.input, x);
+    const uint32_t valid = f.null_bit >= 0 ? quad_valid(p, q, f.input) : 0xFu;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) kw[i] |= ((valid >> i) & 1u) ? (x[i] << f.shift) : (1ull << f.null_bit);
+  }
+}
+
 // Counting pass.  Dynamic shared memory: the ring (p.stages stages of
 // p.stage_bytes, only the key and filter columns staged), its mbarriers,
 // then one counter per partition.
-__global__ void __launch_bounds__(kPartThreads, 1) partition_count(const __grid_constant__ ScanParams p) {
+template <bool kQuad>
+__device__ __forceinline__ void count_body(const ScanParams& p) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int S = p.stages;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)S * p.stage_bytes);
@@ -1661,16 +1786,31 @@ __global__ void __launch_bounds__(kPartThreads, 1) partition_count(const __grid_
       Step s;
       int nt;
       if (!step_wait(p, smem, full, t, it, &s_abort, s, nt)) break;
-      RowRef x[kSR];
-      uint32_t bits[kSR];
-      uint64_t kw[kSR];
-      step_rows(p, s, nt, x, bits);
-      key_words<kSR>(p, s, x, kw);
-      step_release(p, empty, it, nt);
-      it += nt;
+      if constexpr (kQuad) {
+        const Quad q = quad_of(s, nt);
+        uint32_t sel = 0;
+        uint64_t kw[4];
+        if (q.tile >= 0) {
+          sel = quad_select(p, q);
+          quad_keys(p, q, kw);
+        }
+        step_release(p, empty, it, nt);
+        it += nt;
 #pragma unroll
-      for (int j = 0; j < kSR; ++j)
-        if (x[j].on) atomicAdd(&s_count[partition_of(p, kw[j])], 1u);
+        for (int i = 0; i < 4; ++i)
+          if ((sel >> i) & 1u) atomicAdd(&s_count[partition_of(p, kw[i])], 1u);
+      } else {
+        RowRef x[kSR];
+        uint32_t bits[kSR];
+        uint64_t kw[kSR];
+        step_rows(p, s, nt, x, bits);
+        key_words<kSR>(p, s, x, kw);
+        step_release(p, empty, it, nt);
+        it += nt;
+#pragma unroll
+        for (int j = 0; j < kSR; ++j)
+          if (x[j].on) atomicAdd(&s_count[partition_of(p, kw[j])], 1u);
+      }
     }
   }
   __syncthreads();
@@ -1678,6 +1818,13 @@ __global__ void __launch_bounds__(kPartThreads, 1) partition_count(const __grid_
     const uint32_t c = s_count[q];
     if (c) atomicAdd(&p.part_totals[q], c);
   }
+}
+
+__global__ void __launch_bounds__(kPartThreads, 1) partition_count(const __grid_constant__ ScanParams p) {
+  count_body<false>(p);
+}
+__global__ void __launch_bounds__(kPartThreads, 1) partition_count_quad(const __grid_constant__ ScanParams p) {
+  count_body<true>(p);
 }
 
 // The partitions' exclusive prefix (one CTA of 1024 threads).
@@ -1713,8 +1860,42 @@ __global__ void __launch_bounds__(1024) partition_offsets(const __grid_constant_
 // mbarriers.  Each selected row goes to part_start[q] + a place reserved on
 // q's cursor: the lanes of a warp with the same partition reserve together
 // (__match_any_sync), the lowest of them adds their count to the cursor, and
-// the reservations of all of a step's row slots are in flight at once.
-__global__ void __launch_bounds__(kPartThreads, 1) partition_kernel(const __grid_constant__ ScanParams p) {
+// the reservations of all of a lane's row slots are in flight at once.
+// RS row slots per lane: kSR rows (generic path) or a quad.
+template <int RS>
+__device__ __forceinline__ void place_rows(const ScanParams& p, const bool (&on)[RS], const uint64_t (&kw)[RS],
+                                           unsigned long long* (&dst)[RS]) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t nparts = 1u << p.part_bits;
+  uint32_t q[RS], grp[RS], base[RS];
+  int lead[RS];
+#pragma unroll
+  for (int j = 0; j < RS; ++j) {
+    q[j] = on[j] ? partition_of(p, kw[j]) : 0u;
+    grp[j] = __match_any_sync(0xffffffffu, on[j] ? q[j] : (0x80000000u | (uint32_t)lane));
+    lead[j] = __ffs(grp[j]) - 1;
+  }
+#pragma unroll
+  for (int j = 0; j < RS; ++j) {
+    base[j] = 0;
+    if (on[j] && lane == lead[j]) base[j] = atomicAdd(&p.part_cursor[q[j]], (uint32_t)__popc(grp[j]));
+  }
+#pragma unroll
+  for (int j = 0; j < RS; ++j) {
+    base[j] = __shfl_sync(0xffffffffu, base[j], lead[j]);
+    dst[j] = nullptr;
+    if (!on[j]) continue;
+    const uint32_t at = base[j] + (uint32_t)__popc(grp[j] & ((1u << lane) - 1u));
+    if (q[j] >= nparts || at >= __ldg(p.part_totals + q[j])) {
+      part_check(p, CHK_RANGE);
+      continue;
+    }
+    dst[j] = p.part_buf + ((uint64_t)__ldg(p.part_start + q[j]) + at) * p.part_words;
+  }
+}
+
+template <bool kQuad>
+__device__ __forceinline__ void place_body(const ScanParams& p) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int S = p.stages;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)S * p.stage_bytes);
@@ -1725,81 +1906,109 @@ __global__ void __launch_bounds__(kPartThreads, 1) partition_kernel(const __grid
     if ((threadIdx.x & 31) == 0) produce_tiles(p, smem, full, empty, &s_abort, p.n_stage, (uint32_t)p.stage_tx);
     return;
   }
-  const int lane = threadIdx.x & 31;
-  const uint32_t W = p.part_words;
-  const uint32_t nparts = 1u << p.part_bits;
   uint32_t it = 0;
   for (uint64_t t = blockIdx.x; t < p.tiles; t += (uint64_t)kTilesPerStep * gridDim.x) {
     Step s;
     int nt = 0;
     if (!step_wait(p, smem, full, t, it, &s_abort, s, nt)) break;
-    RowRef x[kSR];
-    uint32_t bits[kSR];
-    uint64_t kw[kSR];
-    step_rows(p, s, nt, x, bits);
-    key_words<kSR>(p, s, x, kw);
-    uint32_t q[kSR], grp[kSR], base[kSR];
-    int lead[kSR];
-#pragma unroll
-    for (int j = 0; j < kSR; ++j) {
-      q[j] = x[j].on ? partition_of(p, kw[j]) : 0u;
-      grp[j] = __match_any_sync(0xffffffffu, x[j].on ? q[j] : (0x80000000u | (uint32_t)lane));
-      lead[j] = __ffs(grp[j]) - 1;
-    }
-#pragma unroll
-    for (int j = 0; j < kSR; ++j) {
-      base[j] = 0;
-      if (x[j].on && lane == lead[j]) base[j] = atomicAdd(&p.part_cursor[q[j]], (uint32_t)__popc(grp[j]));
-    }
-    unsigned long long* dst[kSR];
-#pragma unroll
-    for (int j = 0; j < kSR; ++j) {
-      base[j] = __shfl_sync(0xffffffffu, base[j], lead[j]);
-      dst[j] = nullptr;
-      if (!x[j].on) continue;
-      const uint32_t at = base[j] + (uint32_t)__popc(grp[j] & ((1u << lane) - 1u));
-      if (q[j] >= nparts || at >= __ldg(p.part_totals + q[j])) {
-        part_check(p, CHK_RANGE);
-        continue;
+    if constexpr (kQuad) {
+      const Quad q = quad_of(s, nt);
+      uint32_t sel = 0;
+      uint64_t kw[4] = {0, 0, 0, 0};
+      if (q.tile >= 0) {
+        sel = quad_select(p, q);
+        if (sel) quad_keys(p, q, kw);
       }
-      dst[j] = p.part_buf + ((uint64_t)__ldg(p.part_start + q[j]) + at) * W;
-    }
-    uint32_t vflags[kSR] = {};
-    for (int v = 0; v < p.n_vals; ++v) {
-      const int c = p.vals[v].input;
-      const ColRef cr = col_ref(p, s, c);
-      const int size = p.cols[c].size;
+      bool on[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) on[i] = (sel >> i) & 1u;
+      unsigned long long* dst[4];
+      place_rows<4>(p, on, kw, dst);
+      uint32_t vflags[4] = {0, 0, 0, 0};
+      if (sel) {
+        for (int v = 0; v < p.n_vals; ++v) {
+          const int c = p.vals[v].input;
+          uint64_t x[4];
+          quad_load(p, q, c, x);
+          const uint32_t valid = quad_valid(p, q, c);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            if (!dst[i]) continue;
+            const bool ok = (valid >> i) & 1u;
+            vflags[i] |= (uint32_t)ok << v;
+            dst[i][2 + v] = ok ? x[i] : 0ull;
+          }
+        }
+      }
+      const uint64_t row0 = q.start + q.r0;
+      step_release(p, empty, it, nt);
+      it += nt;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        if (!dst[i]) continue;
+        dst[i][0] = kw[i];
+        dst[i][1] = (uint64_t)(uint32_t)(row0 + i) | ((uint64_t)vflags[i] << 32);
+      }
+    } else {
+      RowRef x[kSR];
+      uint32_t bits[kSR];
+      uint64_t kw[kSR];
+      step_rows(p, s, nt, x, bits);
+      key_words<kSR>(p, s, x, kw);
+      bool on[kSR];
+#pragma unroll
+      for (int j = 0; j < kSR; ++j) on[j] = x[j].on;
+      unsigned long long* dst[kSR];
+      place_rows<kSR>(p, on, kw, dst);
+      uint32_t vflags[kSR] = {};
+      for (int v = 0; v < p.n_vals; ++v) {
+        const int c = p.vals[v].input;
+        const ColRef cr = col_ref(p, s, c);
+        const int size = p.cols[c].size;
+#pragma unroll
+        for (int j = 0; j < kSR; ++j) {
+          if (!dst[j]) continue;
+          const bool ok = rvalid(cr, x[j]);
+          vflags[j] |= (uint32_t)ok << v;
+          dst[j][2 + v] = ok ? load_bits(rv(cr, x[j]), size, x[j].r) : 0ull;
+        }
+      }
+      step_release(p, empty, it, nt);
+      it += nt;
 #pragma unroll
       for (int j = 0; j < kSR; ++j) {
         if (!dst[j]) continue;
-        const bool ok = rvalid(cr, x[j]);
-        vflags[j] |= (uint32_t)ok << v;
-        dst[j][2 + v] = ok ? load_bits(rv(cr, x[j]), size, x[j].r) : 0ull;
+        dst[j][0] = kw[j];
+        dst[j][1] = (uint64_t)(uint32_t)(s.start[x[j].tile] + x[j].r) | ((uint64_t)vflags[j] << 32);
       }
-    }
-    step_release(p, empty, it, nt);
-    it += nt;
-#pragma unroll
-    for (int j = 0; j < kSR; ++j) {
-      if (!dst[j]) continue;
-      dst[j][0] = kw[j];
-      dst[j][1] = (uint64_t)(uint32_t)(s.start[x[j].tile] + x[j].r) | ((uint64_t)vflags[j] << 32);
     }
   }
 }
 
+__global__ void __launch_bounds__(kPartThreads, 1) partition_kernel(const __grid_constant__ ScanParams p) {
+  place_body<false>(p);
+}
+__global__ void __launch_bounds__(kPartThreads, 1) partition_kernel_quad(const __grid_constant__ ScanParams p) {
+  place_body<true>(p);
+}
+
 // ---------------------------------------------------------------------------
-// Pass B.  The table: agg_slots records (any count) of rec_stride bytes in
-// dynamic shared memory, the key word at kRecKey (all ones = free), every
-// other field at its identity (zero), and one more record for the all-ones
-// key word.  A row finds its record by linear probing from a hash of its key
-// word (independent of the partition hash).  A record is live once a row set
-// its first row.
+// Pass B.  The table: agg_slots records (any count) in dynamic shared memory,
+// the key word at kRecKey (all ones = free), every other field at its
+// identity (zero), and one more record for the all-ones key word.  Records
+// are rec_stride bytes, laid out agg_stride() = rec_stride + 8 bytes apart: a
+// stride of 8 mod 16 bytes spreads the same field of random slots over every
+// bank pair (a 64-byte stride put all of a warp's accesses to one field in
+// two banks).  A row finds its record by linear probing from a hash of its
+// key word (independent of the partition hash).  A record is live once a row
+// set its first row.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ size_t agg_stride(const ScanParams& p) { return (size_t)p.rec_stride + 8; }
+
 __device__ __forceinline__ void reset_record(unsigned char* rec, size_t rs) {
-  uint4* r = reinterpret_cast<uint4*>(rec);
-  r[0] = make_uint4(~0u, ~0u, 0u, 0u);
-  for (size_t q = 1; q < rs / 16; ++q) r[q] = make_uint4(0u, 0u, 0u, 0u);
+  unsigned long long* r = reinterpret_cast<unsigned long long*>(rec);
+  r[0] = kEmpty;
+  for (size_t q = 1; q < rs / 8; ++q) r[q] = 0ull;
 }
 
 // The shared-memory record of key word `kw` (claimed if new); false when the
@@ -1808,7 +2017,7 @@ __device__ __forceinline__ void reset_record(unsigned char* rec, size_t rs) {
 __device__ __forceinline__ bool agg_probe(const ScanParams& p, unsigned char* table, uint32_t* used, uint64_t kw,
                                           unsigned char*& rec) {
   const uint32_t S = p.agg_slots;
-  const size_t rs = (size_t)p.rec_stride;
+  const size_t rs = agg_stride(p);
   if (kw == kEmpty) {
     rec = table + (size_t)S * rs;
     return true;
@@ -1934,9 +2143,10 @@ __global__ void __launch_bounds__(kAggThreads, 2) partition_aggregate(const __gr
   __shared__ uint32_t s_warp[kAggThreads / 32];
   const uint32_t nparts = 1u << p.part_bits;
   const uint32_t S = p.agg_slots;
-  const size_t rs = (size_t)p.rec_stride;
+  const size_t rs = agg_stride(p);
+  const size_t rw = (size_t)p.rec_stride / 8;  // words of a record
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (uint32_t s = threadIdx.x; s <= S; s += blockDim.x) reset_record(table + (size_t)s * rs, rs);
+  for (uint32_t s = threadIdx.x; s <= S; s += blockDim.x) reset_record(table + (size_t)s * rs, p.rec_stride);
   if (threadIdx.x == 0) {
     s_next = atomicAdd(p.part_next, 1u);
     s_used = 0;
@@ -1996,11 +2206,11 @@ __global__ void __launch_bounds__(kAggThreads, 2) partition_aggregate(const __gr
       unsigned char* rec = table + (size_t)s * rs;
       if (*reinterpret_cast<const uint32_t*>(rec + kRecFirst) == 0u) continue;
       if (dst < p.recs_total) {
-        uint4* out = reinterpret_cast<uint4*>(record_at(p, dst));
-        const uint4* in = reinterpret_cast<const uint4*>(rec);
-        for (size_t q = 0; q < rs / 16; ++q) out[q] = in[q];
+        unsigned long long* out = reinterpret_cast<unsigned long long*>(record_at(p, dst));
+        const unsigned long long* in = reinterpret_cast<const unsigned long long*>(rec);
+        for (size_t q = 0; q < rw; ++q) out[q] = in[q];
       }
-      reset_record(rec, rs);
+      reset_record(rec, p.rec_stride);
       ++dst;
     }
     __syncthreads();  // s_warp, s_base and the table are reused for the next partition

@@ -134,3 +134,38 @@ def test_regimes_agree_on_integers(monkeypatch):
         monkeypatch.setenv("DATAFRAME_ACCEL_REGIME", name)
         outs[name] = run_device(plan)
     assert outs["global"].equals(outs["partitioned"])
+
+
+QUAD_FILTERS = [
+    (np.int32, "<", -5), (np.int32, ">=", 2**31 - 1), (np.int64, ">", 2**63 - 1), (np.int64, "<", -(2**63)),
+    (np.int64, "!=", 7), (np.uint32, "<", -3), (np.uint32, "!=", -3), (np.uint32, ">", 2**31),
+    (np.uint64, "<=", 2**63), (np.uint64, "<", 0), (np.int8, "==", -2), (np.uint16, ">=", 40000),
+    (np.float64, "<", float("-inf")), (np.float64, ">", float("inf")), (np.float64, "!=", float("nan")),
+    (np.float64, "==", float("nan")), (np.float64, "<=", 0.0), (np.float32, ">", 0.1), (np.float32, "<", 1e39),
+]
+
+
+@pytest.mark.parametrize("dt,op,lit", QUAD_FILTERS, ids=[f"{np.dtype(d).name}{o}{l}" for d, o, l in QUAD_FILTERS])
+def test_quad_filter_edges(dt, op, lit, partitioned):
+    """The quad row path's range form of one comparison (integer keys,
+    1024-row tiles): boundary literals, empty ranges, NaN and infinities,
+    unsigned columns against negative literals; a nullable filter column."""
+    rng = np.random.default_rng(abs(hash((np.dtype(dt).name, op))) % 2**32)
+    rows = 70_000  # several full tiles and a ragged one
+    keys = rng.integers(0, 3000, rows, dtype=np.int64)
+    if np.dtype(dt).kind == "f":
+        pool = np.array([0.0, -0.0, np.nan, np.inf, -np.inf, 0.1, -7.5, 1e300 if dt == np.float64 else 3e38], dt)
+        f = pool[rng.integers(0, len(pool), rows)]
+    else:
+        info = np.iinfo(dt)
+        pool = np.array([info.min, info.max, 0, 1, 2, 7] + list(rng.integers(info.min, info.max, 10, dtype=dt,
+                                                                               endpoint=True)), dtype=dt)
+        f = pool[rng.integers(0, len(pool), rows)]
+    frame = DataFrame([Series("k", keys), Series("f", f, rng.random(rows) > 0.05),
+                       Series("v", rng.integers(-50, 50, rows, dtype=np.int64))])
+    x = col("f")
+    pred = {"<": x.__lt__, "<=": x.__le__, ">": x.__gt__, ">=": x.__ge__, "==": x.__eq__, "!=": x.__ne__}[op](lit)
+    plan = frame.lazy().filter(pred).group_by("k", maintain_order=True).agg(
+        [col("v").sum().alias("s"), col("v").count().alias("n"), col("v").min().alias("lo")])
+    compare_with_oracle(plan, f"quad-{np.dtype(dt).name}{op}{lit}")
+    assert regime() == 2

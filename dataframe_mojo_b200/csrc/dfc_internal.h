@@ -171,6 +171,7 @@ struct ScanParams {
   uint32_t* part_totals;   // [partition] selected rows
   uint32_t* part_start;    // [partition] first row of the partition in part_buf
   uint32_t* part_cursor;   // [partition] rows pass A placed (zeroed before pass A)
+  uint32_t* part_order;    // pass B's order of the partitions: the large ones first
   uint32_t agg_slots;      // pass B table slots
   uint32_t* part_next;     // pass B work counter
   // The quad row path of the counting pass and pass A (fast_rows = 1): every

@@ -1175,7 +1175,10 @@ struct PartPlan {
 
 // A pass B table holds a partition's groups at load <= kAggLoad on average
 // (partitions take groups by a hash, so their sizes vary by a few percent).
-constexpr double kAggLoad = 0.6;
+// A warp's probe lasts as long as its longest chain, so the load is kept low:
+// on the 100M-row, 7.4M-group workload pass B took 7.8, 4.7 and 3.6 ms at
+// loads of 0.51, 0.26 and 0.13.
+constexpr double kAggLoad = 0.25;
 constexpr uint32_t kPartMinBits = 10;  // at least 1024 partitions: pass B balances over them
 
 // Sizes the regime for `est` groups with at least 2^min_bits partitions;
@@ -1190,6 +1193,9 @@ bool plan_partitions(const Plan& P, const DeviceState* ds, uint64_t est, PartPla
   // Slots of a table in `bytes` (any count, a multiple of 32), besides the
   // record of the all-ones key word.
   auto slots_in = [&](size_t bytes) { return bytes / rs > 0 ? (uint64_t)(bytes / rs - 1) & ~(uint64_t)31 : 0ull; };
+  // DFC_PART_MIN_BITS=<n> raises the least partition count (tuning).
+  if (const char* env = getenv("DFC_PART_MIN_BITS"))
+    if (atoi(env) > 0) min_bits = std::max<uint32_t>(min_bits, (uint32_t)atoi(env));
   auto bits_for = [&](uint64_t slots) {
     uint32_t b = std::max(kPartMinBits, min_bits);
     while (b < (uint32_t)kPartMaxBits && groups / (double)(1ull << b) > (double)slots * kAggLoad) ++b;
@@ -1363,7 +1369,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   if (recs >= 0xFFFFFFE0ull) return fail(DFC_CAPACITY, "group capacity exceeds 2^32 - 32 records");
 
   void *table = nullptr, *records, *ctl, *bits, *prefix, *bsums, *perm, *firsts;
-  void *part_buf = nullptr, *part_totals = nullptr, *part_start = nullptr, *part_cursor = nullptr;
+  void *part_buf = nullptr, *part_totals = nullptr, *part_start = nullptr, *part_cursor = nullptr, *part_order = nullptr;
   const uint64_t words = (P.rows + 31) / 32;
   const uint64_t chunks = std::max<uint64_t>(1, (words + kFinishChunk - 1) / kFinishChunk);
   const uint64_t nparts = pp ? (1ull << pp->bits) : 0;
@@ -1374,6 +1380,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
     if ((st = S.alloc(&part_totals, nparts * 4, "partition totals"))) return S.release(), st;
     if ((st = S.alloc(&part_start, nparts * 4, "partition starts"))) return S.release(), st;
     if ((st = S.alloc(&part_cursor, nparts * 4, "partition cursors"))) return S.release(), st;
+    if ((st = S.alloc(&part_order, nparts * 4, "partition order"))) return S.release(), st;
   } else {
     if ((st = S.alloc(&table, (slots + 1) * sizeof(KeyEntry), "key table"))) return S.release(), st;
   }
@@ -1434,6 +1441,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
     sp.part_totals = static_cast<uint32_t*>(part_totals);
     sp.part_start = static_cast<uint32_t*>(part_start);
     sp.part_cursor = static_cast<uint32_t*>(part_cursor);
+    sp.part_order = static_cast<uint32_t*>(part_order);
     sp.agg_slots = pp->agg_slots;
     sp.part_next = &dctl->part_next;
   }

@@ -1827,9 +1827,13 @@ __global__ void __launch_bounds__(kPartThreads, 1) partition_count_quad(const __
   count_body<true>(p);
 }
 
-// The partitions' exclusive prefix (one CTA of 1024 threads).
+// The partitions' exclusive prefix (one CTA of 1024 threads), and pass B's
+// order: partitions holding more than four times the average rows (hot keys)
+// first, so none of them starts late and leaves one CTA working alone at the
+// end.
 __global__ void __launch_bounds__(1024) partition_offsets(const __grid_constant__ ScanParams p) {
   __shared__ uint32_t s_warp[32];
+  __shared__ uint32_t s_total, s_big, s_small;
   const uint32_t nparts = 1u << p.part_bits;
   const uint32_t per = (nparts + blockDim.x - 1) / blockDim.x;
   const uint32_t q0 = threadIdx.x * per;
@@ -1843,9 +1847,15 @@ __global__ void __launch_bounds__(1024) partition_offsets(const __grid_constant_
     if (lane >= o) x += y;
   }
   if (lane == 31) s_warp[warp] = x;
+  if (threadIdx.x == 0) s_big = 0;
   __syncthreads();
   uint32_t before = 0;
   for (int w = 0; w < warp; ++w) before += s_warp[w];
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w) t += s_warp[w];
+    s_total = t;
+  }
   uint32_t run = before + x - sum;
   for (uint32_t k = 0; k < per; ++k) {
     const uint32_t q = q0 + k;
@@ -1853,6 +1863,25 @@ __global__ void __launch_bounds__(1024) partition_offsets(const __grid_constant_
       p.part_start[q] = run;
       run += p.part_totals[q];
     }
+  }
+  __syncthreads();
+  const uint64_t big_rows = 4ull * s_total / nparts;
+  uint32_t nbig = 0;
+  for (uint32_t k = 0; k < per; ++k)
+    if (q0 + k < nparts && p.part_totals[q0 + k] > big_rows) ++nbig;
+  if (nbig) atomicAdd(&s_big, nbig);
+  __syncthreads();
+  if (threadIdx.x == 0) s_small = s_big;
+  __syncthreads();
+  __shared__ uint32_t s_next_big;
+  if (threadIdx.x == 0) s_next_big = 0;
+  __syncthreads();
+  for (uint32_t k = 0; k < per; ++k) {
+    const uint32_t q = q0 + k;
+    if (q >= nparts) continue;
+    const uint32_t at = p.part_totals[q] > big_rows ? atomicAdd(&s_next_big, 1u) : atomicAdd(&s_small, 1u);
+    if (at < nparts) p.part_order[at] = q;
+    else part_check(p, CHK_PART);
   }
 }
 
@@ -2154,8 +2183,13 @@ __global__ void __launch_bounds__(kAggThreads, 2) partition_aggregate(const __gr
   }
   __syncthreads();
   for (;;) {
-    const uint32_t part = s_next;
-    if (part >= nparts) break;
+    const uint32_t pick = s_next;
+    if (pick >= nparts) break;
+    const uint32_t part = p.part_order[pick];
+    if (part >= nparts) {  // uniform over the CTA
+      if (threadIdx.x == 0) part_check(p, CHK_PART);
+      break;
+    }
     __syncthreads();  // every thread read s_next
     // The next partition is fetched while this one folds.
     if (threadIdx.x == 0) s_next = atomicAdd(p.part_next, 1u);

@@ -69,13 +69,7 @@ struct KeyField {
   int32_t shift;     // bit position of the value bits inside the key word
   int32_t bits;      // 8, 16, 32 or 64
   int32_t null_bit;  // bit position of the null flag, -1: the column has no nulls
-  // Compact partition rows (ScanParams::part_compact): the field's code is
-  // its order encoding minus cmin, cbits wide, at bit cshift of the row's
-  // code; a nullable column's code is shifted up one bit over a null flag.
-  int32_t cbits;
-  int32_t cshift;
   int32_t pad;
-  uint64_t cmin;
 };
 
 struct ValField {
@@ -178,10 +172,6 @@ struct ScanParams {
   uint32_t* part_start;    // [partition] first row of the partition in part_buf
   uint32_t* part_cursor;   // [partition] rows pass A placed (zeroed before pass A)
   uint32_t* part_order;    // pass B's order of the partitions: the large ones first
-  // Compact rows: part_words = 1 + n_vals, the first word
-  // {row | value validity << 32 | key code << (32 + n_vals)}, the key code
-  // made from the key columns' value ranges (KeyField cbits, cshift, cmin).
-  int32_t part_compact;
   uint32_t agg_slots;      // pass B table slots
   uint32_t* part_next;     // pass B work counter
   // The quad row path of the counting pass and pass A (fast_rows = 1): every
@@ -203,9 +193,7 @@ struct ScanParams {
 enum FastKind : int32_t { FAST_SIGNED = 0, FAST_UNSIGNED = 1, FAST_FLOAT = 2 };
 
 // Which capacity ran out (status word 1), so the host grows only that.
-// CAP_COMPACT: a key value outside the range its compact code was planned
-// for (the host reruns with full partition rows).
-enum CapacityBits : uint32_t { CAP_RECORDS = 1u, CAP_AGG_TABLE = 2u, CAP_COMPACT = 4u };
+enum CapacityBits : uint32_t { CAP_RECORDS = 1u, CAP_AGG_TABLE = 2u };
 
 // Index and consistency checks (status word 2).  A failed check skips the
 // access it guards; the host fails the query with the code.

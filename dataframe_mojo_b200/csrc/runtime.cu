@@ -1235,36 +1235,6 @@ bool plan_partitions(const Plan& P, const DeviceState* ds, uint64_t est, PartPla
   return true;
 }
 
-// Compact partition rows: when every key column is an integer column with
-// statistics and the codes of their value ranges (plus a null flag per
-// nullable column) fit beside the row index and the value validity bits in
-// one 64-bit word, pass A writes {that word, values...} instead of {key
-// word, row word, values...} (16 bytes instead of 24 for one value column,
-// in one store).  Sets the KeyField code layout, P.sp.part_compact and
-// pp.words; `allow` false: full rows.
-void plan_compact(const dfc_query* q, Plan& P, PartPlan& pp, bool allow) {
-  ScanParams& sp = P.sp;
-  sp.part_compact = 0;
-  pp.words = 2 + (uint32_t)sp.n_vals;
-  if (!allow || sp.key_mode != KEY_PACKED || sp.n_vals > 2 || getenv("DFC_NO_COMPACT")) return;
-  int at = 0;
-  for (int k = 0; k < sp.n_keys; ++k) {
-    const dfc_column* c = q->inputs[q->keys[k]];
-    KeyField& f = sp.keys[k];
-    if (is_float(c->dtype) || !c->have_stats || c->min_enc > c->max_enc) return;
-    const uint64_t span = c->max_enc - c->min_enc;
-    int bits = 0;
-    while (bits < 64 && (span >> bits) != 0) ++bits;
-    f.cbits = bits;
-    f.cmin = c->min_enc;
-    f.cshift = at;
-    at += bits + (f.null_bit >= 0 ? 1 : 0);
-  }
-  if (at > 32 - sp.n_vals) return;
-  sp.part_compact = 1;
-  pp.words = 1 + (uint32_t)sp.n_vals;
-}
-
 // The quad row path of the partition passes (ScanParams::fast_rows): staged
 // 1024-row tiles, integer key columns, and no filter or one comparison, put
 // in range form here: the row is selected when its valid value x satisfies
@@ -1805,10 +1775,8 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
   const bool forced_off = (query->flags & (DFC_Q_FORCE_GLOBAL | DFC_Q_FORCE_SHARED)) != 0;
   if (P.sp.key_mode == KEY_PACKED && est > kOwnAlwaysGroups && !(query->flags & DFC_Q_FORCE_GLOBAL))
     measure_skew(P, ds, stream);
-  bool compact = true;  // compact partition rows while no key leaves its planned range
   if (!forced_off && ((query->flags & DFC_Q_FORCE_PARTITIONED) || partition_by_default(P, est)))
     partitioned = plan_partitions(P, ds, est, pp);
-  if (partitioned) plan_compact(query, P, pp, compact);
   if (!partitioned) plan_shared(P, ds, est, query->flags);
   const auto t_plan = std::chrono::steady_clock::now();
   if (getenv("DFC_TRACE")) {
@@ -1839,19 +1807,11 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
       // takes the query.
       const uint32_t why = host_ctl->status[1];
       const PartPlan last = pp;
-      if (why & CAP_COMPACT) {
-        // A key value left the range of its column statistics (a borrowed
-        // device column changed): full partition rows.
-        compact = false;
-        plan_compact(query, P, pp, false);
-        if (!(why & (CAP_AGG_TABLE | CAP_RECORDS))) continue;
-      }
       if (why & CAP_AGG_TABLE) {
         const uint64_t stats = estimate_groups(query, P, ds, stream, false);
         est = std::min<uint64_t>(P.rows, std::max<uint64_t>({stats, est * 2, (uint64_t)host_ctl->alloc * 2}));
         if (last.bits < (uint32_t)kPartMaxBits && plan_partitions(P, ds, est, pp, last.bits + 1)) {
           pp.recs = std::max(pp.recs, last.recs);
-          plan_compact(query, P, pp, compact);
           continue;
         }
       } else if (why & CAP_RECORDS) {

@@ -1564,50 +1564,6 @@ __device__ __forceinline__ void raise_capacity(const ScanParams& p, uint32_t wha
   atomicOr(p.status + 1, what);
 }
 
-// Compact partition rows: the key code of packed key word kw (false when a
-// key value lies outside the planned range), and the key word of a code.
-__device__ __forceinline__ bool compact_code(const ScanParams& p, uint64_t kw, uint64_t& code) {
-  code = 0;
-  bool ok = true;
-  for (int k = 0; k < p.n_keys; ++k) {
-    const KeyField& f = p.keys[k];
-    const bool null = f.null_bit >= 0 && ((kw >> f.null_bit) & 1ull);
-    uint64_t c = 0;
-    if (!null) {
-      const uint64_t cell = f.bits == 64 ? kw : (kw >> f.shift) & ((1ull << f.bits) - 1ull);
-      c = order_encode(cell, f.dtype) - f.cmin;
-      ok = ok && (f.cbits >= 64 || (c >> f.cbits) == 0);
-    }
-    if (f.null_bit >= 0) c = null ? 1ull : (c << 1);
-    code |= c << f.cshift;
-  }
-  return ok;
-}
-
-__device__ __forceinline__ uint64_t expand_code(const ScanParams& p, uint64_t code) {
-  uint64_t kw = 0;
-  for (int k = 0; k < p.n_keys; ++k) {
-    const KeyField& f = p.keys[k];
-    const int width = f.cbits + (f.null_bit >= 0 ? 1 : 0);
-    uint64_t c = width >= 64 ? code >> f.cshift : (code >> f.cshift) & ((1ull << width) - 1ull);
-    if (f.null_bit >= 0) {
-      if (c & 1ull) {
-        kw |= 1ull << f.null_bit;
-        continue;
-      }
-      c >>= 1;
-    }
-    const uint64_t bits = order_decode(c + f.cmin, f.dtype);
-    kw |= f.bits == 64 ? bits : (bits & ((1ull << f.bits) - 1ull)) << f.shift;
-  }
-  return kw;
-}
-
-// The first word of a compact row.
-__device__ __forceinline__ uint64_t compact_word(const ScanParams& p, uint64_t code, uint32_t vflags, uint32_t row) {
-  return (code << (32 + p.n_vals)) | ((uint64_t)vflags << 32) | row;
-}
-
 // The partition passes need no compaction: consumer warp w owns words
 // w, w + 16, ... of every tile (kPR of them at most), and each lane handles
 // its own row of each word.  Selection is a ballot per word; unselected rows
@@ -1967,30 +1923,6 @@ __device__ __forceinline__ void place_rows(const ScanParams& p, const bool (&on)
   }
 }
 
-// The first words of a placed row (the other value columns are already
-// written): full rows {key word, row | validity << 32, first value}; compact
-// rows {row | validity << 32 | key code << (32 + n_vals), first value}, one
-// 16-byte store when that is the whole row.  A key outside its compact
-// range raises CAP_COMPACT (the host reruns with full rows).
-__device__ __forceinline__ void write_row(const ScanParams& p, unsigned long long* dst, uint64_t kw, uint32_t vflags,
-                                          uint32_t row, uint64_t val0) {
-  if (p.part_compact) {
-    uint64_t code;
-    if (!compact_code(p, kw, code)) raise_capacity(p, CAP_COMPACT);
-    const uint64_t w0 = compact_word(p, code, vflags, row);
-    if (p.n_vals == 1) {
-      *reinterpret_cast<ulonglong2*>(dst) = make_ulonglong2(w0, val0);
-    } else {
-      dst[0] = w0;
-      if (p.n_vals > 0) dst[1] = val0;
-    }
-    return;
-  }
-  dst[0] = kw;
-  dst[1] = (uint64_t)row | ((uint64_t)vflags << 32);
-  if (p.n_vals > 0) dst[2] = val0;
-}
-
 template <bool kQuad>
 __device__ __forceinline__ void place_body(const ScanParams& p) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -2022,8 +1954,6 @@ __device__ __forceinline__ void place_body(const ScanParams& p) {
       unsigned long long* dst[4];
       place_rows<4>(p, on, kw, dst);
       uint32_t vflags[4] = {0, 0, 0, 0};
-      uint64_t val0[4] = {0, 0, 0, 0};  // the first value column, written with the row's first word
-      const int vb = p.part_compact ? 1 : 2;
       if (sel) {
         for (int v = 0; v < p.n_vals; ++v) {
           const int c = p.vals[v].input;
@@ -2035,8 +1965,7 @@ __device__ __forceinline__ void place_body(const ScanParams& p) {
             if (!dst[i]) continue;
             const bool ok = (valid >> i) & 1u;
             vflags[i] |= (uint32_t)ok << v;
-            if (v == 0) val0[i] = ok ? x[i] : 0ull;
-            else dst[i][vb + v] = ok ? x[i] : 0ull;
+            dst[i][2 + v] = ok ? x[i] : 0ull;
           }
         }
       }
@@ -2044,8 +1973,11 @@ __device__ __forceinline__ void place_body(const ScanParams& p) {
       step_release(p, empty, it, nt);
       it += nt;
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
-        if (dst[i]) write_row(p, dst[i], kw[i], vflags[i], (uint32_t)(row0 + i), val0[i]);
+      for (int i = 0; i < 4; ++i) {
+        if (!dst[i]) continue;
+        dst[i][0] = kw[i];
+        dst[i][1] = (uint64_t)(uint32_t)(row0 + i) | ((uint64_t)vflags[i] << 32);
+      }
     } else {
       RowRef x[kSR];
       uint32_t bits[kSR];
@@ -2058,8 +1990,6 @@ __device__ __forceinline__ void place_body(const ScanParams& p) {
       unsigned long long* dst[kSR];
       place_rows<kSR>(p, on, kw, dst);
       uint32_t vflags[kSR] = {};
-      uint64_t val0[kSR] = {};
-      const int vb = p.part_compact ? 1 : 2;
       for (int v = 0; v < p.n_vals; ++v) {
         const int c = p.vals[v].input;
         const ColRef cr = col_ref(p, s, c);
@@ -2069,16 +1999,17 @@ __device__ __forceinline__ void place_body(const ScanParams& p) {
           if (!dst[j]) continue;
           const bool ok = rvalid(cr, x[j]);
           vflags[j] |= (uint32_t)ok << v;
-          const uint64_t b = ok ? load_bits(rv(cr, x[j]), size, x[j].r) : 0ull;
-          if (v == 0) val0[j] = b;
-          else dst[j][vb + v] = b;
+          dst[j][2 + v] = ok ? load_bits(rv(cr, x[j]), size, x[j].r) : 0ull;
         }
       }
       step_release(p, empty, it, nt);
       it += nt;
 #pragma unroll
-      for (int j = 0; j < kSR; ++j)
-        if (dst[j]) write_row(p, dst[j], kw[j], vflags[j], (uint32_t)(s.start[x[j].tile] + x[j].r), val0[j]);
+      for (int j = 0; j < kSR; ++j) {
+        if (!dst[j]) continue;
+        dst[j][0] = kw[j];
+        dst[j][1] = (uint64_t)(uint32_t)(s.start[x[j].tile] + x[j].r) | ((uint64_t)vflags[j] << 32);
+      }
     }
   }
 }
@@ -2169,28 +2100,12 @@ __device__ __forceinline__ void fold_rows(const ScanParams& p, unsigned char* ta
     kw[j] = v0[j] = 0;
     row[j] = vf[j] = 0;
     if (!on[j]) continue;
-    if (p.part_compact) {
-      uint64_t w0;
-      if (p.n_vals == 1) {
-        const ulonglong2 r = __ldcs(reinterpret_cast<const ulonglong2*>(src[j]));
-        w0 = r.x;
-        v0[j] = r.y;
-      } else {
-        w0 = __ldcs(src[j]);
-        if (p.n_vals > 0) v0[j] = __ldcs(src[j] + 1);
-      }
-      row[j] = (uint32_t)w0;
-      vf[j] = (uint32_t)(w0 >> 32) & ((1u << p.n_vals) - 1u);
-      kw[j] = expand_code(p, w0 >> (32 + p.n_vals));
-    } else {
-      kw[j] = __ldcs(src[j]);
-      const uint64_t w1 = __ldcs(src[j] + 1);
-      if (p.n_vals > 0) v0[j] = __ldcs(src[j] + 2);  // the first value column, loaded with the rest
-      row[j] = (uint32_t)w1;
-      vf[j] = (uint32_t)(w1 >> 32);
-    }
+    kw[j] = __ldcs(src[j]);
+    const uint64_t w1 = __ldcs(src[j] + 1);
+    if (p.n_vals > 0) v0[j] = __ldcs(src[j] + 2);  // the first value column, loaded with the rest
+    row[j] = (uint32_t)w1;
+    vf[j] = (uint32_t)(w1 >> 32);
   }
-  const int vb = p.part_compact ? 1 : 2;  // the first value word of a row
   unsigned char* recs[kBR];
   bool lost = false;
 #pragma unroll
@@ -2213,7 +2128,7 @@ __device__ __forceinline__ void fold_rows(const ScanParams& p, unsigned char* ta
       const uint64_t first_val = v0[j];
       if (collapse_largest(p, recs[j], grp, maxpop, on[j], row[j], [&](int v, bool& ok, uint64_t& b) {
             ok = (flags >> v) & 1u;
-            b = ok ? (v == 0 ? first_val : __ldcs(sp + vb + v)) : 0ull;
+            b = ok ? (v == 0 ? first_val : __ldcs(sp + 2 + v)) : 0ull;
           })) {
         on[j] = false;
         grp = 0;
@@ -2229,24 +2144,24 @@ __device__ __forceinline__ void fold_rows(const ScanParams& p, unsigned char* ta
   }
   for (int v = 0; v < p.n_vals; ++v) {
     bool ok[kBR];
-    uint64_t vbits[kBR];
+    uint64_t vb[kBR];
 #pragma unroll
     for (int j = 0; j < kBR; ++j) {
       ok[j] = on[j] && ((vf[j] >> v) & 1u);
-      vbits[j] = ok[j] ? (v == 0 ? v0[j] : __ldcs(src[j] + vb + v)) : 0ull;
+      vb[j] = ok[j] ? (v == 0 ? v0[j] : __ldcs(src[j] + 2 + v)) : 0ull;
     }
     const ValField& f = p.vals[v];
     switch (f.dtype) {
-      case DFC_INT8: update_rows<int8_t, true, kBR>(p, f, v, recs, ok, vbits); break;
-      case DFC_INT16: update_rows<int16_t, true, kBR>(p, f, v, recs, ok, vbits); break;
-      case DFC_INT32: update_rows<int32_t, true, kBR>(p, f, v, recs, ok, vbits); break;
-      case DFC_INT64: update_rows<int64_t, true, kBR>(p, f, v, recs, ok, vbits); break;
-      case DFC_UINT8: update_rows<uint8_t, true, kBR>(p, f, v, recs, ok, vbits); break;
-      case DFC_UINT16: update_rows<uint16_t, true, kBR>(p, f, v, recs, ok, vbits); break;
-      case DFC_UINT32: update_rows<uint32_t, true, kBR>(p, f, v, recs, ok, vbits); break;
-      case DFC_UINT64: update_rows<uint64_t, true, kBR>(p, f, v, recs, ok, vbits); break;
-      case DFC_FLOAT32: update_rows<float, true, kBR>(p, f, v, recs, ok, vbits); break;
-      default: update_rows<double, true, kBR>(p, f, v, recs, ok, vbits); break;
+      case DFC_INT8: update_rows<int8_t, true, kBR>(p, f, v, recs, ok, vb); break;
+      case DFC_INT16: update_rows<int16_t, true, kBR>(p, f, v, recs, ok, vb); break;
+      case DFC_INT32: update_rows<int32_t, true, kBR>(p, f, v, recs, ok, vb); break;
+      case DFC_INT64: update_rows<int64_t, true, kBR>(p, f, v, recs, ok, vb); break;
+      case DFC_UINT8: update_rows<uint8_t, true, kBR>(p, f, v, recs, ok, vb); break;
+      case DFC_UINT16: update_rows<uint16_t, true, kBR>(p, f, v, recs, ok, vb); break;
+      case DFC_UINT32: update_rows<uint32_t, true, kBR>(p, f, v, recs, ok, vb); break;
+      case DFC_UINT64: update_rows<uint64_t, true, kBR>(p, f, v, recs, ok, vb); break;
+      case DFC_FLOAT32: update_rows<float, true, kBR>(p, f, v, recs, ok, vb); break;
+      default: update_rows<double, true, kBR>(p, f, v, recs, ok, vb); break;
     }
   }
 }

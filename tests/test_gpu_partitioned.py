@@ -169,51 +169,3 @@ def test_quad_filter_edges(dt, op, lit, partitioned):
         [col("v").sum().alias("s"), col("v").count().alias("n"), col("v").min().alias("lo")])
     compare_with_oracle(plan, f"quad-{np.dtype(dt).name}{op}{lit}")
     assert regime() == 2
-
-
-def test_compact_rows_fall_back_when_a_key_leaves_its_range():
-    """Compact partition rows code keys from their columns' value ranges.  A
-    borrowed device column whose values change after its statistics were
-    taken must not corrupt results: the kernel flags the out-of-range key and
-    the query reruns with full rows, matching the oracle on the new data."""
-    import ctypes as C
-
-    import torch
-
-    from dataframe_mojo_b200 import _native as N
-    from dataframe_mojo_b200.frame import bind
-    from oracle import binding
-
-    rows = 200_000
-    g = torch.Generator(device="cuda")
-    g.manual_seed(77)
-    k = torch.randint(0, 1000, (rows,), generator=g, device="cuda", dtype=torch.int64)
-    v = torch.randint(-5, 5, (rows,), generator=g, device="cuda", dtype=torch.int64)
-
-    def reg(t):
-        h = C.c_void_p()
-        assert N.lib().dfc_column_register(0, N.INT64, rows, t.data_ptr(), None, 0, N.COLUMN_DEVICE, C.byref(h)) == N.OK
-        return type("H", (), {"handle": h})()
-
-    shape = DataFrame([Series("k", np.zeros(1, np.int64)), Series("v", np.zeros(1, np.int64))])
-    plan = shape.lazy().group_by("k", maintain_order=True).agg([col("v").sum().alias("s"), col("v").count().alias("n")])
-    bound = bind(plan.plan)
-    cols = {"k": reg(k), "v": reg(v)}
-    try:
-        first = provider.run_bound(bound, [cols[n] for n in bound.names], flags=N.Q_FORCE_PARTITIONED)
-        first.free()
-        assert provider.last_timings()["retries"] == 0
-        k[::7] += 10**12
-        torch.cuda.synchronize()
-        res = provider.run_bound(bound, [cols[n] for n in bound.names], flags=N.Q_FORCE_PARTITIONED)
-        t = provider.last_timings()
-        got = res.to_frame()
-        res.free()
-        assert t["regime"] == 2 and t["retries"] >= 1, t
-        host = DataFrame([Series("k", k.cpu().numpy()), Series("v", v.cpu().numpy())])
-        want, _ = binding.run(host.lazy().group_by("k", maintain_order=True).agg(
-            [col("v").sum().alias("s"), col("v").count().alias("n")]))
-        assert got.equals(want)
-    finally:
-        for h in cols.values():
-            N.lib().dfc_column_release(h.handle)

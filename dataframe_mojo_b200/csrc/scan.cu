@@ -1923,6 +1923,16 @@ __device__ __forceinline__ void place_rows(const ScanParams& p, const bool (&on)
   }
 }
 
+// The row's key word, row word and first value, stored together once the
+// row's place is known (the other value columns are already written):
+// consecutive stores to one row let L2 merge them before the line leaves.
+__device__ __forceinline__ void write_row(const ScanParams& p, unsigned long long* dst, uint64_t kw, uint32_t vflags,
+                                          uint32_t row, uint64_t val0) {
+  dst[0] = kw;
+  dst[1] = (uint64_t)row | ((uint64_t)vflags << 32);
+  if (p.n_vals > 0) dst[2] = val0;
+}
+
 template <bool kQuad>
 __device__ __forceinline__ void place_body(const ScanParams& p) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -1954,6 +1964,7 @@ __device__ __forceinline__ void place_body(const ScanParams& p) {
       unsigned long long* dst[4];
       place_rows<4>(p, on, kw, dst);
       uint32_t vflags[4] = {0, 0, 0, 0};
+      uint64_t val0[4] = {0, 0, 0, 0};  // the first value column, written with the row's first words
       if (sel) {
         for (int v = 0; v < p.n_vals; ++v) {
           const int c = p.vals[v].input;
@@ -1965,7 +1976,8 @@ __device__ __forceinline__ void place_body(const ScanParams& p) {
             if (!dst[i]) continue;
             const bool ok = (valid >> i) & 1u;
             vflags[i] |= (uint32_t)ok << v;
-            dst[i][2 + v] = ok ? x[i] : 0ull;
+            if (v == 0) val0[i] = ok ? x[i] : 0ull;
+            else dst[i][2 + v] = ok ? x[i] : 0ull;
           }
         }
       }
@@ -1973,11 +1985,8 @@ __device__ __forceinline__ void place_body(const ScanParams& p) {
       step_release(p, empty, it, nt);
       it += nt;
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        if (!dst[i]) continue;
-        dst[i][0] = kw[i];
-        dst[i][1] = (uint64_t)(uint32_t)(row0 + i) | ((uint64_t)vflags[i] << 32);
-      }
+      for (int i = 0; i < 4; ++i)
+        if (dst[i]) write_row(p, dst[i], kw[i], vflags[i], (uint32_t)(row0 + i), val0[i]);
     } else {
       RowRef x[kSR];
       uint32_t bits[kSR];
@@ -1990,6 +1999,7 @@ __device__ __forceinline__ void place_body(const ScanParams& p) {
       unsigned long long* dst[kSR];
       place_rows<kSR>(p, on, kw, dst);
       uint32_t vflags[kSR] = {};
+      uint64_t val0[kSR] = {};
       for (int v = 0; v < p.n_vals; ++v) {
         const int c = p.vals[v].input;
         const ColRef cr = col_ref(p, s, c);
@@ -1999,17 +2009,16 @@ __device__ __forceinline__ void place_body(const ScanParams& p) {
           if (!dst[j]) continue;
           const bool ok = rvalid(cr, x[j]);
           vflags[j] |= (uint32_t)ok << v;
-          dst[j][2 + v] = ok ? load_bits(rv(cr, x[j]), size, x[j].r) : 0ull;
+          const uint64_t b = ok ? load_bits(rv(cr, x[j]), size, x[j].r) : 0ull;
+          if (v == 0) val0[j] = b;
+          else dst[j][2 + v] = b;
         }
       }
       step_release(p, empty, it, nt);
       it += nt;
 #pragma unroll
-      for (int j = 0; j < kSR; ++j) {
-        if (!dst[j]) continue;
-        dst[j][0] = kw[j];
-        dst[j][1] = (uint64_t)(uint32_t)(s.start[x[j].tile] + x[j].r) | ((uint64_t)vflags[j] << 32);
-      }
+      for (int j = 0; j < kSR; ++j)
+        if (dst[j]) write_row(p, dst[j], kw[j], vflags[j], (uint32_t)(s.start[x[j].tile] + x[j].r), val0[j]);
     }
   }
 }

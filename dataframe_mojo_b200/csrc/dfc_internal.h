@@ -31,6 +31,9 @@ constexpr uint64_t kEmpty = ~0ull;
 // NaNs are stored canonical (0x7FF8...), so no value stores as zero.
 constexpr uint64_t kShiftTag = 0x7FF40000000D0FC5ull;
 constexpr uint64_t kCanonNaN = 0x7FF8000000000000ull;
+// perm entry of the identity record: the one output row of an ungrouped
+// query that kept no row (record numbers stay below 2^32 - 32).
+constexpr uint32_t kIdentityRecord = 0xFFFFFFFFu;
 
 // Status bits raised by kernels.
 enum StatusBits : uint32_t {

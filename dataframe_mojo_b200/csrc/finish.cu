@@ -109,6 +109,12 @@ __global__ void finish_scan_chunks(const __grid_constant__ FinishParams f, uint3
     if (i < chunks) f.block_sums[i] = carry + ex;
     carry += total;
   }
+  // Ungrouped reductions (no key columns) give one row even when no row was
+  // kept: the identity record (every state at zero).
+  if (threadIdx.x == 0 && f.scan.n_keys == 0 && carry == 0) {
+    carry = 1;
+    f.perm[0] = kIdentityRecord;
+  }
   if (threadIdx.x == 0) f.groups[0] = carry;
 }
 
@@ -303,7 +309,9 @@ __device__ uint64_t output_cell(const FinishParams& f, const OutCol& oc, const u
 __global__ void finish_output(const __grid_constant__ FinishParams f) {
   const ScanParams& p = f.scan;
   __shared__ uint32_t block_nulls[kMaxOut];
+  __shared__ __align__(16) unsigned char zero_record[kMaxRecWords * 8];
   for (int c = threadIdx.x; c < kMaxOut; c += blockDim.x) block_nulls[c] = 0;
+  for (int w = threadIdx.x; w < kMaxRecWords; w += blockDim.x) reinterpret_cast<uint64_t*>(zero_record)[w] = 0;
   __syncthreads();
   const uint32_t G = f.groups[0];
   const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -313,11 +321,12 @@ __global__ void finish_output(const __grid_constant__ FinishParams f) {
     const uint64_t i = wbase + lane;
     bool active = i < G;
     const uint32_t gid = active ? f.perm[i] : 0u;
-    if (active && gid >= records_handed_out(p)) {
+    const bool identity = active && gid == kIdentityRecord && p.n_keys == 0;
+    if (active && !identity && gid >= records_handed_out(p)) {
       atomicOr(p.status + 2, CHK_PERM);
       active = false;
     }
-    const unsigned char* rec = active ? record_at(p, gid) : nullptr;
+    const unsigned char* rec = identity ? zero_record : active ? record_at(p, gid) : nullptr;
     for (int c = 0; c < f.n_out; ++c) {
       const OutCol& oc = f.out[c];
       bool ok = false;

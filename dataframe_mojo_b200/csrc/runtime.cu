@@ -412,7 +412,8 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
   if (q->abi_version != DFC_ABI_VERSION) return fail(DFC_INVALID, "ABI version mismatch");
   if (q->n_inputs < 1 || q->n_inputs > kMaxInputs || !q->inputs)
     return fail(DFC_UNSUPPORTED, "between 1 and 16 input columns are supported");
-  if (q->n_keys < 1 || q->n_keys > kMaxKeys || !q->keys) return fail(DFC_UNSUPPORTED, "between 1 and 4 keys are supported");
+  if (q->n_keys < 0 || q->n_keys > kMaxKeys || (q->n_keys > 0 && !q->keys))
+    return fail(DFC_UNSUPPORTED, "at most 4 keys are supported");
   if (q->n_aggs < 0 || q->n_aggs > kMaxAggs || (q->n_aggs > 0 && !q->aggs))
     return fail(DFC_UNSUPPORTED, "at most 32 aggregations are supported");
   if (q->n_pred < 0 || q->n_pred > kMaxPred || (q->n_pred > 0 && !q->pred))
@@ -1394,7 +1395,8 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   if ((st = S.commit("query working memory"))) return S.release(), st;
   // Output columns sized for the group capacity (the group count is known
   // only on the device; the host reads it once, at the end).
-  const uint64_t out_rows = std::min<uint64_t>(P.rows, recs);
+  // Ungrouped reductions always give one row.
+  const uint64_t out_rows = std::max<uint64_t>(P.sp.n_keys == 0 ? 1 : 0, std::min<uint64_t>(P.rows, recs));
   std::vector<ResultCol> rc;
   void* out_slab = nullptr;
   {
@@ -2081,7 +2083,7 @@ DFC_API dfc_status dfc_groupby_noalloc(const dfc_query* query, int32_t device, u
   const uint64_t words = (P.rows + 31) / 32;
   const uint64_t chunks = std::max<uint64_t>(1, (words + kFinishChunk - 1) / kFinishChunk);
   // Every group holds a table entry, so the table bounds the group count.
-  const uint64_t out_rows = std::min<uint64_t>(P.rows, slots + 1);
+  const uint64_t out_rows = std::max<uint64_t>(P.sp.n_keys == 0 ? 1 : 0, std::min<uint64_t>(P.rows, slots + 1));
 
   // Working memory, carved from the array: the fixed parts, then as many
   // group records as the rest holds.  Besides the groups, records go to
@@ -2297,7 +2299,7 @@ dfc_status size_item(const dfc_query* q, BatchItem& it, DeviceState* ds, cudaStr
   if (it.recs >= 0xFFFFFFE0ull) return fail(DFC_CAPACITY, "group capacity exceeds 2^32 - 32 records");
   it.words = (P.rows + 31) / 32;
   it.chunks = std::max<uint64_t>(1, (it.words + kFinishChunk - 1) / kFinishChunk);
-  it.out_rows = std::min<uint64_t>(P.rows, it.recs);
+  it.out_rows = std::max<uint64_t>(P.sp.n_keys == 0 ? 1 : 0, std::min<uint64_t>(P.rows, it.recs));
   it.off_table = arena_take(used, (it.slots + 1) * sizeof(KeyEntry));
   it.off_records = arena_take(used, it.recs * P.sp.rec_stride);
   it.off_bits = arena_take(used, it.words * 4 + 16);

@@ -316,7 +316,9 @@ class Plan:
     def describe(self) -> str:
         parts = [f"SCAN_FRAME {self.source.columns}"]
         parts += [f"FILTER {f}" for f in self.filters]
-        if self.keys is not None:
+        if self.keys == []:
+            parts.append(f"SELECT {[a.name for a in self.aggs]}")
+        elif self.keys is not None:
             parts.append(f"AGG keys={self.keys} maintain_order={self.maintain_order} aggs={[a.name for a in self.aggs]}")
         return " -> ".join(parts)
 
@@ -346,6 +348,28 @@ class LazyFrame:
         for k in keys:
             self._plan.source.column(k)
         return LazyGroupBy(self, keys, maintain_order)
+
+    def select(self, exprs: AggExpr | Sequence[AggExpr]) -> "LazyFrame":
+        """Ungrouped reductions of the filtered rows: SCAN_FRAME -> FILTER* ->
+        SELECT(col(c).sum(), ...), one output row (the reference's filtered
+        reduction region, dataframe_metal/filter_plan.mojo:149-200).  An empty
+        selection gives the reductions of no rows: sum 0 (null when min_count
+        > 0), count, len and null_count 0, mean, min, max, var and std null."""
+        if self._plan.keys is not None:
+            raise ValueError("a select after the aggregation is not part of this region")
+        if isinstance(exprs, AggExpr):
+            exprs = [exprs]
+        exprs = list(exprs)
+        if not exprs:
+            raise ValueError("select needs at least one reduction")
+        for e in exprs:
+            self._plan.source.column(e.column)
+        names = [e.name for e in exprs]
+        if len(set(names)) != len(names):
+            raise ValueError("duplicate output column names")
+        p = self._plan
+        plan = Plan(p.source, list(p.filters), [], exprs, False)
+        return LazyFrame(p.source, plan)
 
     def collect(self, engine: str = "accel") -> DataFrame:
         if engine != "accel":

@@ -414,7 +414,7 @@ def _execute_plan(plan: Plan, device: int) -> DataFrame:
 
 def _unsupported_reason(plan: Plan) -> str | None:
     if plan.keys is None:
-        return "the region has no grouped aggregation"
+        return "the region has no aggregation"
     try:
         bound = bind(plan)
     except (TypeError, ValueError, KeyError) as e:

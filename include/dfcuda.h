@@ -211,7 +211,7 @@ typedef struct dfc_query {
   uint32_t abi_version; /* DFC_ABI_VERSION */
   uint32_t flags;       /* DFC_Q_* */
   int32_t n_inputs;     /* columns the query reads; all have the same row count */
-  int32_t n_keys;       /* 1..4 */
+  int32_t n_keys;       /* 0..4; 0: ungrouped reductions, one output row even when no row is kept */
   dfc_column* const* inputs;
   const int32_t* keys;  /* n_keys indices into inputs */
   int32_t n_pred;       /* 0 keeps every row */

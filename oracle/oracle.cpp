@@ -550,7 +550,7 @@ int finalize(const orc_query& q, const Plan& plan, const std::vector<Group>& gro
 }
 
 int validate(const orc_query* q) {
-  if (!q || q->n_keys < 1 || q->n_keys > 4 || q->n_inputs < 1) return fail(DFC_INVALID, "bad query");
+  if (!q || q->n_keys < 0 || q->n_keys > 4 || q->n_inputs < 1) return fail(DFC_INVALID, "bad query");
   uint64_t rows = q->inputs[0].rows;
   for (int i = 0; i < q->n_inputs; ++i)
     if (q->inputs[i].rows != rows) return fail(DFC_INVALID, "row counts differ");
@@ -585,6 +585,23 @@ void scan_range(const orc_query& q, const Plan& plan, uint64_t lo, uint64_t hi, 
   }
 }
 
+// Ungrouped reductions (no key columns; the filtered reduction region
+// SCAN_FRAME -> FILTER* -> SELECT, dataframe_metal/filter_plan.mojo:149-200)
+// always have one row: with no row kept it holds the reductions of nothing,
+// the states at their initial values (function.mojo:187-254), finished as
+// for an empty group (sum 0 unless min_count > 0, mean/min/max/var null).
+void ungrouped_row(const orc_query& q, const Plan& plan, std::vector<Group>& groups, std::vector<GroupKey>& keys,
+                   std::vector<uint64_t>& key_rows) {
+  if (q.n_keys != 0 || !groups.empty()) return;
+  Group g;
+  g.first_row = 0;
+  g.len = 0;
+  g.vals.resize(plan.value_cols.size());
+  groups.push_back(std::move(g));
+  keys.push_back(GroupKey{});
+  key_rows.push_back(0);
+}
+
 }  // namespace
 
 extern "C" {
@@ -596,6 +613,7 @@ int32_t orc_groupby(const orc_query* q, orc_result** out) {
   GroupTable t;
   std::vector<uint64_t> key_rows;
   scan_range(*q, plan, 0, q->inputs[0].rows, t, key_rows);
+  ungrouped_row(*q, plan, t.groups, t.keys, key_rows);
   auto r = std::make_unique<orc_result>();
   st = finalize(*q, plan, t.groups, t.keys, key_rows, r.get());
   if (st) return st;
@@ -690,6 +708,7 @@ int32_t orc_groupby_parallel(const orc_query* q, int32_t threads, orc_result** o
     key_rows.push_back(prows[p][i]);
     if (at[p] < pgroups[p].size()) heap.push({pgroups[p][at[p]].first_row, p});
   }
+  ungrouped_row(*q, plan, groups, keys, key_rows);
   auto r = std::make_unique<orc_result>();
   st = finalize(*q, plan, groups, keys, key_rows, r.get());
   if (st) return st;

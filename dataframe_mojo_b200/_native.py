@@ -152,6 +152,7 @@ SIGNATURES = [
     ("dfc_installed", C.c_int32, []),
     ("dfc_device_count", C.c_int32, []),
     ("dfc_device_info_get", C.c_int, [C.c_int32, C.POINTER(DeviceInfo)]),
+    ("dfc_set_memory_limit", C.c_int, [C.c_int32, C.c_int64]),
     (
         "dfc_column_register",
         C.c_int,

@@ -166,6 +166,20 @@ std::map<std::vector<uint64_t>, double> g_joint;
 std::map<std::vector<uint64_t>, std::pair<double, double>> g_skew;
 std::atomic<uint64_t> g_column_serial{0};
 
+// dfc_set_memory_limit: the most bytes one query may hold on a device
+// (working memory and result columns); <= 0 none.
+std::atomic<int64_t> g_memory_limit[64];
+
+// Host-side fault injection (DFCUDA_FAULT, read on every call): `alloc` fails
+// the query's working-memory allocation, `capacity` makes the first attempt
+// report a full table (the regrowth path reruns it), `timeout` makes the
+// host's bounded wait give up at once, `overflow` reports a checked integer
+// sum overflow.  Nothing is injected on the GPU.
+bool fault_is(const char* what) {
+  const char* f = getenv("DFCUDA_FAULT");
+  return f && strcmp(f, what) == 0;
+}
+
 // The library's own stream-ordered memory pool per device.  Freed query
 // memory stays cached in it (queries reuse it without returning to the
 // driver); the device's default pool, which other code in the process may
@@ -295,6 +309,7 @@ double wait_limit_seconds() {
 
 // Host-side bounded wait on the stream's work (cudaEventQuery polling).
 dfc_status wait_bounded(cudaStream_t stream) {
+  if (fault_is("timeout")) return fail(DFC_TIMEOUT, "device work did not finish within the wait limit (injected by DFCUDA_FAULT=timeout)");
   // One completion event per thread and device, created on first use.
   thread_local std::map<int, cudaEvent_t> events;
   int dev = 0;
@@ -1119,6 +1134,7 @@ struct Scratch {
     return DFC_OK;
   }
   dfc_status commit(const char* what) {
+    if (fault_is("alloc")) return fail(DFC_OOM, std::string(what) + ": allocation failed (injected by DFCUDA_FAULT=alloc)");
     cudaError_t e = pool_alloc(&block, std::max<size_t>(total, 256), stream);
     if (e != cudaSuccess) {
       block = nullptr;
@@ -1392,11 +1408,24 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   if ((st = S.alloc(&bsums, chunks * 4, "prefix chunks"))) return S.release(), st;
   if ((st = S.alloc(&perm, recs * 4, "group permutation"))) return S.release(), st;
   if ((st = S.alloc(&firsts, recs * 4, "first rows"))) return S.release(), st;
-  if ((st = S.commit("query working memory"))) return S.release(), st;
   // Output columns sized for the group capacity (the group count is known
   // only on the device; the host reads it once, at the end).
   // Ungrouped reductions always give one row.
   const uint64_t out_rows = std::max<uint64_t>(P.sp.n_keys == 0 ? 1 : 0, std::min<uint64_t>(P.rows, recs));
+  // The device's memory limit (DATAFRAME_ACCEL_MEMORY_LIMIT through
+  // dfc_set_memory_limit): rejected before the query's kernels are submitted.
+  if (const int64_t limit = g_memory_limit[P.device].load(); limit > 0) {
+    uint64_t need = S.total;
+    for (int c = 0; c < P.n_out; ++c) need += out_rows * dtype_size(P.out_dtype[c]) + ((out_rows + 31) / 32) * 4 + 512;
+    if (need > (uint64_t)limit) {
+      S.release();
+      char msg[200];
+      snprintf(msg, sizeof msg, "the query needs %llu bytes of device memory; the memory limit is %lld",
+               (unsigned long long)need, (long long)limit);
+      return fail(DFC_UNSUPPORTED, msg);
+    }
+  }
+  if ((st = S.commit("query working memory"))) return S.release(), st;
   std::vector<ResultCol> rc;
   void* out_slab = nullptr;
   {
@@ -1641,7 +1670,8 @@ DFC_API dfc_status dfc_device_info_get(int32_t ordinal, dfc_device_info* out) {
   out->cc_minor = prop.minor;
   out->total_bytes = prop.totalGlobalMem;
   out->budget_bytes = -1;
-  const char* lim = getenv("DATAFRAME_ACCEL_MEMORY_LIMIT");
+  if (ordinal < 64 && g_memory_limit[ordinal].load() > 0) out->budget_bytes = g_memory_limit[ordinal].load();
+  const char* lim = out->budget_bytes > 0 ? nullptr : getenv("DATAFRAME_ACCEL_MEMORY_LIMIT");
   if (lim && *lim) {
     char* end = nullptr;
     long long v = strtoll(lim, &end, 10);
@@ -1649,6 +1679,25 @@ DFC_API dfc_status dfc_device_info_get(int32_t ordinal, dfc_device_info* out) {
   }
   snprintf(out->name, sizeof(out->name), "%s", prop.name);
   return DFC_OK;
+}
+
+DFC_API dfc_status dfc_set_memory_limit(int32_t device, int64_t bytes) {
+  if (device < 0 || device >= 64) return fail(DFC_INVALID, "device ordinal out of range");
+  g_memory_limit[device].store(bytes > 0 ? bytes : 0);
+  return DFC_OK;
+}
+
+// Whether `p` is device memory of `device` (not host, managed or another
+// GPU's memory): the kernels stream borrowed columns with bulk copies, which
+// must read this GPU's own memory.
+bool device_memory_of(const void* p, int device) {
+  if (!p) return true;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice && a.device == device;
 }
 
 DFC_API dfc_status dfc_column_register(int32_t device, dfc_dtype dtype, uint64_t rows, const void* values,
@@ -1663,6 +1712,9 @@ DFC_API dfc_status dfc_column_register(int32_t device, dfc_dtype dtype, uint64_t
   DeviceState* ds;
   dfc_status st = device_ready(device, &ds);
   if (st) return st;
+  if (flags == DFC_COLUMN_DEVICE && rows > 0 && !device_memory_of(values, device))
+    return fail(DFC_INVALID, "DFC_COLUMN_DEVICE values must be device memory of the column's device "
+                             "(host, managed or another GPU's memory is not accepted)");
   DeviceGuard guard(device);
   cudaStream_t stream = thread_stream(device);
   auto* c = new dfc_column();
@@ -1794,6 +1846,15 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
   for (int attempt = 0; attempt < 6; ++attempt) {
     bool grow = false;
     st = run_attempt(query, P, ds, stream, slots, factor, partitioned ? &pp : nullptr, out, &grow, host_ctl);
+    if (st == DFC_OK && attempt == 0 && fault_is("capacity")) {
+      // Injected: the first attempt reports a full table and is regrown.
+      dfc_result_free(*out);
+      *out = nullptr;
+      host_ctl->status[0] = ST_CAPACITY;
+      host_ctl->status[1] = partitioned ? CAP_AGG_TABLE : 0u;
+      grow = true;
+      st = DFC_CAPACITY;
+    }
     if (!grow) break;
     t_timings.retries += 1;
     if (host_ctl->status[0] & ST_F32_RANGE) {
@@ -1830,6 +1891,17 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
   }
   if (st == DFC_CAPACITY) return fail(DFC_CAPACITY, "group table capacity exhausted after regrowth");
   if (st) return st;
+  if (fault_is("overflow")) {
+    // Injected: the first integer sum reports the CPU's overflow error.
+    for (int a = 0; a < query->n_aggs; ++a) {
+      const int idt = P.out_agg_input_dtype[a];
+      if (query->aggs[a].op == DFC_AGG_SUM && !is_float(idt)) {
+        dfc_result_free(*out);
+        *out = nullptr;
+        return fail(DFC_DATA_OVERFLOW, overflow_message(idt));
+      }
+    }
+  }
   learn_groups(P, (*out)->rows);
   t_timings.groups = (*out)->rows;
   t_timings.regime = partitioned ? 2 : (P.sp.smem_slots ? 1 : 0);
@@ -2023,6 +2095,9 @@ DFC_API dfc_status dfc_groupby_noalloc(const dfc_query* query, int32_t device, u
     if (rows > 0 && !d.values) return fail(DFC_INVALID, "null values");
     if (((uintptr_t)d.values & 15u) != 0 || ((uintptr_t)d.validity & 15u) != 0)
       return fail(DFC_INVALID, "column values and validity must be 16-byte aligned");
+    if (rows > 0 && (!device_memory_of(d.values, device) || !device_memory_of(d.validity, device)))
+      return fail(DFC_INVALID, "column values and validity must be device memory of `device` "
+                               "(host, managed or another GPU's memory is not accepted)");
     cols[i].device = device;
     cols[i].dtype = (dfc_dtype)d.dtype;
     cols[i].rows = rows;
@@ -2035,8 +2110,11 @@ DFC_API dfc_status dfc_groupby_noalloc(const dfc_query* query, int32_t device, u
   Plan P;
   dfc_status st = plan_query(&q, P);
   if (st) return st;
-  for (int c = 0; c < P.n_out; ++c)
+  for (int c = 0; c < P.n_out; ++c) {
     if (capacity > 0 && (!outputs[c].values || !outputs[c].validity)) return fail(DFC_INVALID, "null output buffer");
+    if (capacity > 0 && (!device_memory_of(outputs[c].values, device) || !device_memory_of(outputs[c].validity, device)))
+      return fail(DFC_INVALID, "output buffers must be device memory of `device`");
+  }
   DeviceState* ds;
   if ((st = device_ready(P.device, &ds))) return st;
   DeviceGuard guard(P.device);

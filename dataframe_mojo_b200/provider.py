@@ -400,6 +400,9 @@ def _region_plan(plan) -> Plan:
 def _execute_plan(plan: Plan, device: int) -> DataFrame:
     bound = bind(plan)
     flags = _regime_flags()
+    # DATAFRAME_ACCEL_MEMORY_LIMIT bounds each query's device memory: a query
+    # that would need more is rejected before submission (DFC_UNSUPPORTED).
+    _check(N.lib().dfc_set_memory_limit(device, max(_memory_limit(), 0)))
     cols = [DeviceColumn(s, device) for s in bound.series]
     try:
         result = run_bound(bound, cols, flags=flags)

@@ -124,11 +124,21 @@ DFC_API dfc_status dfc_device_info_get(int32_t ordinal, dfc_device_info* out);
 /* ------------------------------------------------------------------------ */
 typedef struct dfc_column dfc_column;
 
+/* The most bytes one query may hold on `device` (its working memory and its
+ * result columns); a query that would need more is rejected with
+ * DFC_UNSUPPORTED before its kernels are submitted.  <= 0: no limit.  The
+ * provider sets it from DATAFRAME_ACCEL_MEMORY_LIMIT, the name the
+ * reference's contract keeps (docs/design/accelerator-contract.md:168-171);
+ * dfc_device_info_get reports it as budget_bytes. */
+DFC_API dfc_status dfc_set_memory_limit(int32_t device, int64_t bytes);
+
 /* values/validity point to host memory: the library copies them into HBM
  * (validity normalised to bit offset 0) and keeps them resident. */
 #define DFC_COLUMN_HOST 0u
 /* values points to device memory the caller owns and keeps alive until
- * dfc_column_release; only the validity bitmap is copied (normalised). */
+ * dfc_column_release; only the validity bitmap is copied (normalised).  It
+ * must be device memory of `device` (cudaPointerGetAttributes): host,
+ * managed or another GPU's memory is rejected with DFC_INVALID. */
 #define DFC_COLUMN_DEVICE 1u
 
 /* validity may be NULL (every row valid).  validity_bit_offset is the bit

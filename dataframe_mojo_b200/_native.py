@@ -27,6 +27,7 @@ LT, LE, GT, GE, EQ, NE = range(1, 7)
 
 # aggregations
 AGG_COUNT, AGG_SUM, AGG_MEAN, AGG_MIN, AGG_MAX, AGG_VAR, AGG_STD, AGG_LEN, AGG_NULL_COUNT = range(1, 10)
+AGG_FIRST, AGG_LAST, AGG_N_UNIQUE = 10, 11, 12
 
 # query flags
 Q_MAINTAIN_ORDER = 1

@@ -142,6 +142,7 @@ struct ScanParams {
   uint32_t smem_cluster;  // CTAs sharing one table; 0 or 1: each CTA its own
   int32_t track_first;  // maintain_order: first row lowered by atomic min
   int32_t off_len;      // u32 rows of the group, -1 absent
+  int32_t off_last;     // u32 the group's latest row + 1 (LAST), -1 absent
   int32_t rec_words;    // stride / 8
   // Value fields (bit v) whose sum and shifted square sum accumulate in the
   // shared-memory tables as compensated FP32 pairs {s, c} (Float32 columns),

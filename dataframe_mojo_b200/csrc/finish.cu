@@ -258,6 +258,19 @@ __device__ uint64_t output_cell(const FinishParams& f, const OutCol& oc, const u
       }
       return b;
     }
+    case DFC_AGG_FIRST:
+    case DFC_AGG_LAST: {
+      // The value at the group's first (last) kept row, null when that
+      // row's value is; the identity record has neither row.
+      const uint32_t r = oc.op == DFC_AGG_FIRST ? ~*reinterpret_cast<const uint32_t*>(rec + kRecFirst)
+                                                 : *reinterpret_cast<const uint32_t*>(rec + p.off_last) - 1u;
+      const DevColumn& col = p.cols[vf.input];
+      if (r >= p.rows || (col.validity && !bit_valid(col.validity, r))) {
+        *ok = false;
+        return 0;
+      }
+      return load_bits(col.values, col.size, r);
+    }
     case DFC_AGG_VAR:
     case DFC_AGG_STD: {
       const int64_t n = (int64_t)count;

@@ -554,11 +554,13 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
   };
   std::vector<Need> needs;
   int val_of_agg[kMaxAggs];
-  bool track_len = false;
+  bool track_len = false, track_first_row = false, track_last = false;
   for (int a = 0; a < q->n_aggs; ++a) {
     const dfc_agg& ag = q->aggs[a];
     if (ag.column < 0 || ag.column >= q->n_inputs) return fail(DFC_INVALID, "aggregation column out of range");
-    if (ag.op < DFC_AGG_COUNT || ag.op > DFC_AGG_NULL_COUNT) return fail(DFC_UNSUPPORTED, "unsupported aggregation");
+    if (ag.op == DFC_AGG_N_UNIQUE)
+      return fail(DFC_UNSUPPORTED, "n_unique runs through dfc_groupby (two device group-bys)");
+    if (ag.op < DFC_AGG_COUNT || ag.op > DFC_AGG_LAST) return fail(DFC_UNSUPPORTED, "unsupported aggregation");
     if ((ag.op == DFC_AGG_VAR || ag.op == DFC_AGG_STD) && ag.ddof < 0) return fail(DFC_INVALID, "negative ddof");
     int v = -1;
     for (size_t j = 0; j < needs.size(); ++j)
@@ -576,6 +578,8 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
       case DFC_AGG_MAX: n.mx = true; break;
       case DFC_AGG_VAR: case DFC_AGG_STD: n.m2 = true; n.sum = true; break;
       case DFC_AGG_LEN: case DFC_AGG_NULL_COUNT: track_len = true; break;
+      case DFC_AGG_FIRST: track_first_row = true; break;
+      case DFC_AGG_LAST: track_last = true; break;
       default: break;
     }
   }
@@ -588,6 +592,11 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
   sp.off_len = -1;
   if (track_len) {
     sp.off_len = off;
+    off += 4;
+  }
+  sp.off_last = -1;
+  if (track_last) {
+    sp.off_last = off;
     off += 4;
   }
   for (int j = 0; j < sp.n_vals; ++j) {
@@ -624,7 +633,8 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
     for (int j = 0; j < sp.n_vals; ++j)
       if (sp.vals[j].dtype == DFC_FLOAT32 && sp.vals[j].off_sum >= 0) sp.comp_mask |= 1u << j;
   sp.rec_words = sp.rec_stride / 8;
-  sp.track_first = (q->flags & DFC_Q_MAINTAIN_ORDER) ? 1 : 0;
+  // FIRST reads the group's earliest kept row, which maintain_order tracks.
+  sp.track_first = ((q->flags & DFC_Q_MAINTAIN_ORDER) || track_first_row) ? 1 : 0;
 
   // Output columns: keys, then one per aggregation.
   FinishParams& fp = P.fp;
@@ -649,7 +659,7 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
     switch (ag.op) {
       case DFC_AGG_COUNT: case DFC_AGG_LEN: case DFC_AGG_NULL_COUNT: oc.dtype = DFC_INT64; break;
       case DFC_AGG_SUM: oc.dtype = sum_dtype(idt); break;
-      case DFC_AGG_MIN: case DFC_AGG_MAX: oc.dtype = idt; break;
+      case DFC_AGG_MIN: case DFC_AGG_MAX: case DFC_AGG_FIRST: case DFC_AGG_LAST: oc.dtype = idt; break;
       default: oc.dtype = DFC_FLOAT64; break;
     }
     P.out_agg_input_dtype[a] = idt;
@@ -1797,7 +1807,12 @@ DFC_API int32_t dfc_column_null_count(const dfc_column* column) {
   return column ? (int32_t)std::min<uint64_t>(column->null_count, INT32_MAX) : 0;
 }
 
-DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
+}  // extern "C"
+
+namespace {
+
+// One group-by through the planner (every aggregation but N_UNIQUE).
+dfc_status groupby_one(const dfc_query* query, dfc_result** out) {
   if (!out) return fail(DFC_INVALID, "null output");
   *out = nullptr;
   t_timings = dfc_timings{};
@@ -1909,6 +1924,178 @@ DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
   t_timings.compensated = P.sp.smem_slots ? (int32_t)P.sp.comp_mask : 0;
   t_timings.total_ns = std::chrono::duration<double, std::nano>(std::chrono::steady_clock::now() - t0).count();
   return DFC_OK;
+}
+
+// A result column as a query input, read in place (result validity is
+// already 32-bit words at bit offset 0, the normalised form).
+dfc_column result_input(const dfc_result* r, int i) {
+  dfc_column c;
+  c.serial = ++g_column_serial;
+  c.device = r->device;
+  c.dtype = r->cols[i].dtype;
+  c.rows = r->rows;
+  c.values = r->cols[i].values;
+  c.validity = r->cols[i].has_nulls ? r->cols[i].validity : nullptr;
+  c.null_count = r->cols[i].has_nulls ? 1 : 0;
+  return c;
+}
+
+// N_UNIQUE(v) by two device group-bys: the distinct (keys, v) tuples of the
+// kept rows, then the rows of that result per key tuple (LEN).  Both run in
+// first-appearance order: a group's first tuple comes at the group's first
+// row, so the second result's rows line up with the main query's groups.
+// The main query (maintain_order forced) gives the keys and every other
+// aggregation; the result is assembled in the query's column order.
+dfc_status groupby_with_n_unique(const dfc_query* q, dfc_result** out) {
+  *out = nullptr;
+  if (q->n_aggs < 0 || q->n_aggs > kMaxAggs || !q->aggs) return fail(DFC_INVALID, "bad aggregation list");
+  std::vector<dfc_agg> main_aggs;
+  std::vector<int> where(q->n_aggs), nu_cols;
+  for (int a = 0; a < q->n_aggs; ++a) {
+    if (q->aggs[a].op != DFC_AGG_N_UNIQUE) {
+      where[a] = (int)main_aggs.size();
+      main_aggs.push_back(q->aggs[a]);
+      continue;
+    }
+    const int v = q->aggs[a].column;
+    if (v < 0 || v >= q->n_inputs) return fail(DFC_INVALID, "aggregation column out of range");
+    int slot = -1;
+    for (size_t u = 0; u < nu_cols.size(); ++u)
+      if (nu_cols[u] == v) slot = (int)u;
+    if (slot < 0) {
+      slot = (int)nu_cols.size();
+      nu_cols.push_back(v);
+    }
+    where[a] = -1 - slot;
+  }
+  if (main_aggs.empty()) main_aggs.push_back(dfc_agg{DFC_AGG_LEN, q->n_keys > 0 ? q->keys[0] : 0, 0, 0});
+  dfc_query q0 = *q;
+  q0.flags |= DFC_Q_MAINTAIN_ORDER;
+  q0.aggs = main_aggs.data();
+  q0.n_aggs = (int32_t)main_aggs.size();
+  dfc_result* r0 = nullptr;
+  dfc_status st = groupby_one(&q0, &r0);
+  if (st) return st;
+  const dfc_timings main_timings = t_timings;
+  int launches = t_timings.launches;
+  std::vector<dfc_result*> counts(nu_cols.size(), nullptr);
+  auto release = [&]() {
+    dfc_result_free(r0);
+    for (dfc_result* r : counts) dfc_result_free(r);
+  };
+  const uint32_t regime_flags = q->flags & (DFC_Q_FORCE_GLOBAL | DFC_Q_FORCE_SHARED | DFC_Q_FORCE_PARTITIONED);
+  for (size_t u = 0; u < nu_cols.size(); ++u) {
+    const int v = nu_cols[u];
+    int keys1[kMaxKeys + 1];
+    int n1 = 0, vpos = -1;
+    for (int k = 0; k < q->n_keys; ++k) {
+      keys1[n1++] = q->keys[k];
+      if (q->keys[k] == v) vpos = k;
+    }
+    if (vpos < 0) {
+      if (n1 >= kMaxKeys) {
+        release();
+        return fail(DFC_UNSUPPORTED, "n_unique of a non-key column with four keys");
+      }
+      vpos = n1;
+      keys1[n1++] = v;
+    }
+    dfc_query q1 = *q;
+    q1.flags = DFC_Q_MAINTAIN_ORDER | regime_flags;
+    q1.keys = keys1;
+    q1.n_keys = n1;
+    q1.aggs = nullptr;
+    q1.n_aggs = 0;
+    dfc_result* r1 = nullptr;
+    if ((st = groupby_one(&q1, &r1))) {
+      release();
+      return st;
+    }
+    launches += t_timings.launches;
+    dfc_column c1[kMaxKeys + 1];
+    dfc_column* p1[kMaxKeys + 1];
+    int keys2[kMaxKeys];
+    for (int i = 0; i < n1; ++i) {
+      c1[i] = result_input(r1, i);
+      p1[i] = &c1[i];
+    }
+    for (int k = 0; k < q->n_keys; ++k) keys2[k] = k;
+    const dfc_agg len{DFC_AGG_LEN, vpos, 0, 0};
+    dfc_query q2 = {};
+    q2.abi_version = DFC_ABI_VERSION;
+    q2.flags = DFC_Q_MAINTAIN_ORDER | regime_flags;
+    q2.n_inputs = n1;
+    q2.n_keys = q->n_keys;
+    q2.inputs = p1;
+    q2.keys = keys2;
+    q2.n_aggs = 1;
+    q2.aggs = &len;
+    q2.stream = q->stream;
+    st = groupby_one(&q2, &counts[u]);
+    launches += t_timings.launches;
+    dfc_result_free(r1);
+    if (st) {
+      release();
+      return st;
+    }
+    if (counts[u]->rows != r0->rows) {
+      release();
+      return fail(DFC_DEVICE, "n_unique: the distinct-value counts do not line up with the groups");
+    }
+  }
+  // The result: keys and aggregations in the query's order, each column
+  // copied into one new allocation.
+  auto* r = new dfc_result();
+  r->device = r0->device;
+  r->rows = r0->rows;
+  DeviceGuard guard(r0->device);
+  cudaStream_t stream = q->stream ? static_cast<cudaStream_t>(q->stream) : thread_stream(r0->device);
+  std::vector<const ResultCol*> src;
+  for (int k = 0; k < q->n_keys; ++k) src.push_back(&r0->cols[k]);
+  for (int a = 0; a < q->n_aggs; ++a)
+    src.push_back(where[a] >= 0 ? &r0->cols[q->n_keys + where[a]] : &counts[-1 - where[a]]->cols[q->n_keys]);
+  auto piece = [](uint64_t bytes) { return (std::max<uint64_t>(bytes, 256) + 255) & ~(uint64_t)255; };
+  const uint64_t rows = r->rows, vwords = (rows + 31) / 32;
+  uint64_t total = 0;
+  for (const ResultCol* c : src) total += piece(rows * dtype_size(c->dtype)) + piece(vwords * 4);
+  cudaError_t e = pool_alloc(&r->slab, std::max<uint64_t>(total, 256), stream);
+  unsigned char* at = static_cast<unsigned char*>(r->slab);
+  for (const ResultCol* c : src) {
+    if (e != cudaSuccess) break;
+    ResultCol rc;
+    rc.dtype = c->dtype;
+    rc.has_nulls = c->has_nulls;
+    rc.values = at;
+    at += piece(rows * dtype_size(c->dtype));
+    rc.validity = reinterpret_cast<uint32_t*>(at);
+    at += piece(vwords * 4);
+    if (rows) e = cudaMemcpyAsync(rc.values, c->values, rows * dtype_size(c->dtype), cudaMemcpyDeviceToDevice, stream);
+    if (e == cudaSuccess && rows) e = cudaMemcpyAsync(rc.validity, c->validity, vwords * 4, cudaMemcpyDeviceToDevice, stream);
+    r->cols.push_back(rc);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  release();
+  if (e != cudaSuccess) {
+    dfc_result_free(r);
+    return cuda_fail(e, "n_unique result assembly");
+  }
+  t_timings = main_timings;
+  t_timings.launches = launches;
+  *out = r;
+  return DFC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+DFC_API dfc_status dfc_groupby(const dfc_query* query, dfc_result** out) {
+  if (!out) return fail(DFC_INVALID, "null output");
+  *out = nullptr;
+  if (query && query->aggs)
+    for (int a = 0; a < query->n_aggs && a < kMaxAggs; ++a)
+      if (query->aggs[a].op == DFC_AGG_N_UNIQUE) return groupby_with_n_unique(query, out);
+  return groupby_one(query, out);
 }
 
 DFC_API uint64_t dfc_result_rows(const dfc_result* result) { return result ? result->rows : 0; }

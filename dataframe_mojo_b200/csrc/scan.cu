@@ -803,9 +803,14 @@ __device__ __forceinline__ void group_update(const ScanParams& p, const Rec& rec
     const uint32_t first =
         group_reduce<uint32_t>(grp, maxpop, row, 0xFFFFFFFFu, loc, [](uint32_t a, uint32_t b2) { return a < b2 ? a : b2; },
                                one);
+    // The group's latest row + 1 (LAST; 0 = none).
+    const uint32_t last = p.off_last >= 0 ? group_reduce<uint32_t>(grp, maxpop, row + 1u, 0u, loc,
+                                                                   [](uint32_t a, uint32_t b2) { return a > b2 ? a : b2; }, one)
+                                          : 0u;
     if (leader) {
       rec.max_u32(kRecFirst, ~first);
       if (p.off_len >= 0) rec.add_u32(p.off_len, (uint32_t)__popc(grp));
+      if (p.off_last >= 0) rec.max_u32(p.off_last, last);
     }
     for (int v = 0; v < p.n_vals; ++v) {
       const ValField& f = p.vals[v];
@@ -968,9 +973,11 @@ __device__ bool collapse_largest(const ScanParams& p, unsigned char* rec, uint32
   unsigned char* const grec = reinterpret_cast<unsigned char*>(
       __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(rec), lead));
   const uint32_t first = __reduce_min_sync(0xffffffffu, in ? row : 0xFFFFFFFFu);
+  const uint32_t last = __reduce_max_sync(0xffffffffu, in ? row + 1u : 0u);
   if (leader) {
     atomicMax(reinterpret_cast<uint32_t*>(grec + kRecFirst), ~first);
     if (p.off_len >= 0) atomicAdd(reinterpret_cast<uint32_t*>(grec + p.off_len), (uint32_t)__popc(big));
+    if (p.off_last >= 0) atomicMax(reinterpret_cast<uint32_t*>(grec + p.off_last), last);
   }
   for (int v = 0; v < p.n_vals; ++v) {
     const ValField& f = p.vals[v];
@@ -1242,6 +1249,11 @@ __device__ __forceinline__ void consume_rows(const ScanParams& p, const Step& s,
     for (int j = 0; j < kR; ++j)
       if (sel[j]) red_add_u32(record_at(p, gid[j]) + p.off_len, 1u);
   }
+  if (p.off_last >= 0) {
+#pragma unroll
+    for (int j = 0; j < kR; ++j)
+      if (sel[j]) atomicMax(reinterpret_cast<uint32_t*>(record_at(p, gid[j]) + p.off_last), rows[j] + 1u);
+  }
   for (int v = 0; v < p.n_vals; ++v) {
     const ValField& f = p.vals[v];
     const ColRef cr = col_ref(p, s, f.input);
@@ -1460,6 +1472,7 @@ __device__ void merge_into(const ScanParams& p, const unsigned char* src, uint32
   unsigned char* dst = record_at(p, gid);
   if (p.track_first) atomicMax(reinterpret_cast<uint32_t*>(dst + kRecFirst), first_enc);
   if (p.off_len >= 0) red_add_u32(dst + p.off_len, *reinterpret_cast<const uint32_t*>(src + p.off_len));
+  if (p.off_last >= 0) atomicMax(reinterpret_cast<uint32_t*>(dst + p.off_last), *reinterpret_cast<const uint32_t*>(src + p.off_last));
   const uint32_t flags = *reinterpret_cast<const uint32_t*>(src + kRecFlags);
   if (flags) red_or_u32(dst + kRecFlags, flags);
   for (int v = 0; v < p.n_vals; ++v) {
@@ -2150,6 +2163,7 @@ __device__ __forceinline__ void fold_rows(const ScanParams& p, unsigned char* ta
     if (!on[j]) continue;
     rec_max_u32<true>(recs[j] + kRecFirst, ~row[j]);
     if (p.off_len >= 0) rec_add_u32<true>(recs[j] + p.off_len, 1u);
+    if (p.off_last >= 0) rec_max_u32<true>(recs[j] + p.off_last, row[j] + 1u);
   }
   for (int v = 0; v < p.n_vals; ++v) {
     bool ok[kBR];

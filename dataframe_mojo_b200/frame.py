@@ -285,6 +285,18 @@ class Col:
     def null_count(self) -> AggExpr:
         return AggExpr(N.AGG_NULL_COUNT, self.name, self.name)
 
+    def first(self) -> AggExpr:
+        """The value at the group's first kept row (null when that value is)."""
+        return AggExpr(N.AGG_FIRST, self.name, self.name)
+
+    def last(self) -> AggExpr:
+        """The value at the group's last kept row (null when that value is)."""
+        return AggExpr(N.AGG_LAST, self.name, self.name)
+
+    def n_unique(self) -> AggExpr:
+        """Distinct values of the group: null is one value, NaN one, -0.0 == 0.0."""
+        return AggExpr(N.AGG_N_UNIQUE, self.name, self.name)
+
     def var(self, ddof: int = 1) -> AggExpr:
         return AggExpr(N.AGG_VAR, self.name, self.name, ddof=ddof)
 

@@ -199,7 +199,16 @@ typedef enum dfc_agg_op {
   DFC_AGG_VAR = 6,        /* Float64, M2 / (n - ddof); null when n <= ddof */
   DFC_AGG_STD = 7,
   DFC_AGG_LEN = 8,        /* rows of the group, Int64 */
-  DFC_AGG_NULL_COUNT = 9  /* null values, Int64 */
+  DFC_AGG_NULL_COUNT = 9, /* null values, Int64 */
+  /* The value at the group's first (last) row among the rows the filter
+   * kept, null when that row's value is null; the input type
+   * (dataframe/aggregation/function.mojo:997-1013, 1586-1600, 2637-2650). */
+  DFC_AGG_FIRST = 10,
+  DFC_AGG_LAST = 11,
+  /* Distinct values of the group, Int64: null counts as one value, every
+   * NaN is one value and -0.0 == 0.0, the key equality
+   * (function.mojo:620-625; tests/public_contracts/test_approx_n_unique.mojo:60-80). */
+  DFC_AGG_N_UNIQUE = 12
 } dfc_agg_op;
 
 typedef struct dfc_agg {

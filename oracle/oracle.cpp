@@ -35,6 +35,7 @@
 #include <queue>
 #include <string>
 #include <thread>
+#include <unordered_set>
 #include <vector>
 
 namespace {
@@ -225,10 +226,16 @@ struct ValueState {
   double min_f = 0, max_f = 0;
   int64_t wn = 0;         // Welford count / mean / m2
   double wmean = 0, wm2 = 0;
+  // N_UNIQUE (_K_DISTINCT, function.mojo:620-625): the distinct valid values
+  // by key equality (key_word) and whether a null was seen (null counts as a
+  // value, tests/public_contracts/test_approx_n_unique.mojo:60-80).
+  std::unordered_set<uint64_t> uniq;
+  bool uniq_null = false;
 };
 
 struct Group {
   uint64_t first_row;
+  uint64_t last_row = 0;  // LAST: the group's latest kept row (function.mojo:1586-1600)
   int64_t len;
   std::vector<ValueState> vals;
 };
@@ -296,6 +303,7 @@ struct GroupTable {
 struct Plan {
   std::vector<int> value_cols;      // distinct input indices that aggregations read
   std::vector<int> agg_value_slot;  // per aggregation, index into value_cols
+  std::vector<bool> uniq;           // per value column: an N_UNIQUE reads it
 };
 
 Plan make_plan(const orc_query& q) {
@@ -311,6 +319,9 @@ Plan make_plan(const orc_query& q) {
     }
     p.agg_value_slot.push_back(slot);
   }
+  p.uniq.assign(p.value_cols.size(), false);
+  for (int a = 0; a < q.n_aggs; ++a)
+    if (q.aggs[a].op == DFC_AGG_N_UNIQUE) p.uniq[p.agg_value_slot[a]] = true;
   return p;
 }
 
@@ -486,14 +497,37 @@ int finalize(const orc_query& q, const Plan& plan, const std::vector<Group>& gro
     OutColumn out;
     int odt;
     switch (agg.op) {
-      case DFC_AGG_COUNT: case DFC_AGG_LEN: case DFC_AGG_NULL_COUNT: odt = DFC_INT64; break;
+      case DFC_AGG_COUNT: case DFC_AGG_LEN: case DFC_AGG_NULL_COUNT: case DFC_AGG_N_UNIQUE: odt = DFC_INT64; break;
       case DFC_AGG_SUM: odt = sum_dtype(c.dtype); break;
-      case DFC_AGG_MIN: case DFC_AGG_MAX: odt = c.dtype; break;
+      case DFC_AGG_MIN: case DFC_AGG_MAX: case DFC_AGG_FIRST: case DFC_AGG_LAST: odt = c.dtype; break;
       default: odt = DFC_FLOAT64; break;
     }
     out.dtype = odt;
     out.bytes.assign(G * dtype_size(odt), 0);
     out.valid.assign(G, 0);
+    if (agg.op == DFC_AGG_FIRST || agg.op == DFC_AGG_LAST) {
+      // The value at the group's first (last) kept row, null when that row's
+      // value is null (function.mojo:997-1013, 2637-2650).
+      const size_t sz = dtype_size(c.dtype);
+      for (size_t g = 0; g < G; ++g) {
+        const uint64_t row = agg.op == DFC_AGG_FIRST ? groups[g].first_row : groups[g].last_row;
+        const bool valid = groups[g].len > 0 && col_valid(c, row);
+        out.valid[g] = valid;
+        if (valid) std::memcpy(out.bytes.data() + g * sz, (const uint8_t*)c.values + row * sz, sz);
+      }
+      r->cols.push_back(std::move(out));
+      continue;
+    }
+    if (agg.op == DFC_AGG_N_UNIQUE) {
+      for (size_t g = 0; g < G; ++g) {
+        const ValueState& s = groups[g].vals[slot];
+        const int64_t n = (int64_t)s.uniq.size() + (s.uniq_null ? 1 : 0);
+        std::memcpy(out.bytes.data() + g * 8, &n, 8);
+        out.valid[g] = 1;
+      }
+      r->cols.push_back(std::move(out));
+      continue;
+    }
     for (size_t g = 0; g < G; ++g) {
       const ValueState& s = groups[g].vals[slot];
       bool ok = true;
@@ -578,9 +612,15 @@ void scan_range(const orc_query& q, const Plan& plan, uint64_t lo, uint64_t hi, 
     }
     Group& grp = t.groups[g];
     grp.len += 1;
+    grp.last_row = row;
     for (size_t v = 0; v < nv; ++v) {
       const orc_column& c = q.inputs[plan.value_cols[v]];
-      if (col_valid(c, row)) update_value(grp.vals[v], c, row);
+      const bool valid = col_valid(c, row);
+      if (valid) update_value(grp.vals[v], c, row);
+      if (plan.uniq[v]) {
+        if (valid) grp.vals[v].uniq.insert(key_word(c, row));
+        else grp.vals[v].uniq_null = true;
+      }
     }
   }
 }
@@ -675,6 +715,11 @@ int32_t orc_groupby_parallel(const orc_query* q, int32_t threads, orc_result** o
               } else {
                 Group& dst = merged.groups[m];
                 dst.len += src.len;
+                dst.last_row = std::max(dst.last_row, src.last_row);
+                for (size_t v = 0; v < dst.vals.size(); ++v) {
+                  dst.vals[v].uniq.insert(src.vals[v].uniq.begin(), src.vals[v].uniq.end());
+                  dst.vals[v].uniq_null = dst.vals[v].uniq_null || src.vals[v].uniq_null;
+                }
                 for (size_t v = 0; v < dst.vals.size(); ++v) combine_value(dst.vals[v], src.vals[v], floating[v]);
               }
             }

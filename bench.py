@@ -300,50 +300,74 @@ def _register(tensor, dtype_code, rows, valid_bytes=None):
     return type("DeviceHandle", (), {"handle": h})()
 
 
-def batched_jobs(device: str, nq: int):
-    """The batched configuration's queries: nq independent queries (rows
-    log-uniform 1K-20M; one Int64 key, cardinality log-uniform 1-2M, uniform
-    or Zipf s=1.2; Int64 and Float32 values with 2% nulls; filter on the Int64
-    value against a random threshold), seeds 4 + query id.  Returns the jobs
-    (bound plan, registered columns), what keeps their buffers alive, the
-    total rows and per query (rows, cardinality, zipf)."""
-    import torch
-    from dataframe_mojo_b200 import _native as native
-    from dataframe_mojo_b200.frame import bind
-    from dataframe_mojo_b200.frame import DataFrame, Series, col
-
+def batched_specs(nq: int) -> list[dict]:
+    """The batched configuration's query shapes, in order: rows log-uniform
+    1K-20M; one Int64 key of cardinality log-uniform 1-2M, uniform or Zipf
+    s=1.2; a filter on the Int64 value against a random threshold."""
     rng = np.random.default_rng(4)
-    shape = DataFrame([Series("k", np.zeros(1, np.int64)), Series("a", np.zeros(1, np.int64)),
-                       Series("b", np.zeros(1, np.float32))])
-    jobs, keep, total, info = [], [], 0, []
-    for q in range(nq):
+    specs = []
+    for _ in range(nq):
         rows = int(math.exp(rng.uniform(math.log(1e3), math.log(2e7))))
         card = max(1, int(math.exp(rng.uniform(0.0, math.log(2e6)))))
         zipf = bool(rng.integers(0, 2))
         thr = int(rng.integers(-1000, 1000))
-        g = torch.Generator(device=device)
-        g.manual_seed(4 + q)
-        if zipf:
-            w = torch.arange(1, card + 1, device=device, dtype=torch.float64).pow(-1.2)
-            cdf = torch.cumsum(w, 0)
-            cdf /= cdf[-1].clone()
-            u = torch.rand(rows, generator=g, device=device, dtype=torch.float64)
-            k = torch.searchsorted(cdf, u).clamp_(max=card - 1)
-        else:
-            k = torch.randint(0, card, (rows,), generator=g, device=device)
-        a = torch.randint(-1000, 1001, (rows,), generator=g, device=device)
-        b = torch.randn(rows, generator=g, device=device, dtype=torch.float32)
-        va = pack_bits_torch(torch.rand(rows, generator=g, device=device) >= 0.02)
-        vb = pack_bits_torch(torch.rand(rows, generator=g, device=device) >= 0.02)
-        plan = shape.lazy().filter(col("a") > thr).group_by("k", maintain_order=True).agg(
-            [col("a").sum().alias("sa"), col("b").mean().alias("mb"), col("a").min().alias("lo"),
-             col("b").max().alias("hi"), col("b").count().alias("n")])
-        bound = bind(plan.plan)
-        hs = {"k": _register(k, native.INT64, rows), "a": _register(a, native.INT64, rows, va),
-              "b": _register(b, native.FLOAT32, rows, vb)}
-        keep.append((k, a, b, va, vb, hs))
+        specs.append({"rows": rows, "card": card, "zipf": zipf, "thr": thr})
+    return specs
+
+
+def batched_columns(q: int, spec: dict, device: str) -> dict:
+    """Query q's columns (seed 4 + q): key k, Int64 value a and Float32 value
+    b with 2% nulls each (validity as packed LSB-first bytes)."""
+    import torch
+
+    rows, card = spec["rows"], spec["card"]
+    g = torch.Generator(device=device)
+    g.manual_seed(4 + q)
+    if spec["zipf"]:
+        w = torch.arange(1, card + 1, device=device, dtype=torch.float64).pow(-1.2)
+        cdf = torch.cumsum(w, 0)
+        cdf /= cdf[-1].clone()
+        u = torch.rand(rows, generator=g, device=device, dtype=torch.float64)
+        k = torch.searchsorted(cdf, u).clamp_(max=card - 1)
+    else:
+        k = torch.randint(0, card, (rows,), generator=g, device=device)
+    a = torch.randint(-1000, 1001, (rows,), generator=g, device=device)
+    b = torch.randn(rows, generator=g, device=device, dtype=torch.float32)
+    va = torch.rand(rows, generator=g, device=device) >= 0.02
+    vb = torch.rand(rows, generator=g, device=device) >= 0.02
+    return {"k": k, "a": a, "b": b, "va": va, "vb": vb}
+
+
+def batched_plan(frame_like, thr: int):
+    from dataframe_mojo_b200.frame import col
+
+    return frame_like.lazy().filter(col("a") > thr).group_by("k", maintain_order=True).agg(
+        [col("a").sum().alias("sa"), col("b").mean().alias("mb"), col("a").min().alias("lo"),
+         col("b").max().alias("hi"), col("b").count().alias("n")])
+
+
+def batched_jobs(device: str, nq: int):
+    """The batched configuration's queries (batched_specs, batched_columns):
+    the jobs (bound plan, registered columns), what keeps their buffers
+    alive, the total rows and per query (rows, cardinality, zipf)."""
+    import torch
+    from dataframe_mojo_b200 import _native as native
+    from dataframe_mojo_b200.frame import bind
+    from dataframe_mojo_b200.frame import DataFrame, Series
+
+    shape = DataFrame([Series("k", np.zeros(1, np.int64)), Series("a", np.zeros(1, np.int64)),
+                       Series("b", np.zeros(1, np.float32))])
+    jobs, keep, total, info = [], [], 0, []
+    for q, spec in enumerate(batched_specs(nq)):
+        c = batched_columns(q, spec, device)
+        rows = spec["rows"]
+        va, vb = pack_bits_torch(c["va"]), pack_bits_torch(c["vb"])
+        bound = bind(batched_plan(shape, spec["thr"]).plan)
+        hs = {"k": _register(c["k"], native.INT64, rows), "a": _register(c["a"], native.INT64, rows, va),
+              "b": _register(c["b"], native.FLOAT32, rows, vb)}
+        keep.append((c, va, vb, hs))
         jobs.append((bound, [hs[n] for n in bound.names]))
-        info.append((rows, card, zipf))
+        info.append((rows, spec["card"], spec["zipf"]))
         total += rows
     torch.cuda.synchronize()
     return jobs, keep, total, info
@@ -393,6 +417,35 @@ def batched_form(device: str, nq: int) -> dict:
     }
 
 
+def served_sizes() -> list[int]:
+    """Rows of the served configuration's 8 resident tables (seeds 5 + table id)."""
+    return [int(x) for x in np.geomspace(1e7, 2e8, 8)]
+
+
+SERVED_AGGS = ("sum", "mean", "min", "max", "count", "var")
+
+
+def served_requests(nreq: int, rate: float = 2000.0):
+    """The served configuration's requests, in order: table, key subset
+    ({k1}, {k2} or {k1, k2}), aggregation list and threshold (p < t); and
+    their Poisson arrival times at `rate` per second."""
+    rng = np.random.default_rng(5)
+    specs = []
+    for _ in range(nreq):
+        t = int(rng.integers(0, len(served_sizes())))
+        keys = [["k1"], ["k2"], ["k1", "k2"]][int(rng.integers(0, 3))]
+        pick = [a for a in SERVED_AGGS if rng.random() < 0.5] or [SERVED_AGGS[0]]
+        specs.append({"table": t, "keys": keys, "aggs": pick, "thr": int(rng.integers(1, 100))})
+    return specs, np.cumsum(rng.exponential(1.0 / rate, nreq))
+
+
+def served_plan(frame_like, spec: dict):
+    from dataframe_mojo_b200.frame import col
+
+    return frame_like.lazy().filter(col("p") < spec["thr"]).group_by(spec["keys"], maintain_order=True).agg(
+        [getattr(col("v"), n)().alias(n) for n in spec["aggs"]])
+
+
 def served_form(device: str, nreq: int, rate: float = 2000.0, inflight: int = 32) -> dict:
     """The served configuration: 8 resident tables of 10M-200M rows (the
     100M-row workload's schema, seeds 5 + table id), nreq requests arriving
@@ -407,7 +460,7 @@ def served_form(device: str, nreq: int, rate: float = 2000.0, inflight: int = 32
     from dataframe_mojo_b200.frame import bind
     from dataframe_mojo_b200.frame import DataFrame, Series, col
 
-    sizes = [int(x) for x in np.geomspace(1e7, 2e8, 8)]
+    sizes = served_sizes()
     tables = []
     for t, n in enumerate(sizes):
         c = generate(n, 5 + t, device)
@@ -416,21 +469,13 @@ def served_form(device: str, nreq: int, rate: float = 2000.0, inflight: int = 32
               "v": _register(c["v"], native.FLOAT64, n, vb), "p": _register(c["p"], native.INT32, n)}
         tables.append((c, vb, hs))
     torch.cuda.synchronize()
-    rng = np.random.default_rng(5)
     shape = DataFrame([Series("k1", np.zeros(1, np.int32)), Series("k2", np.zeros(1, np.uint32)),
                        Series("v", np.zeros(1)), Series("p", np.zeros(1, np.int32))])
-    aggs_all = [("sum", lambda v: v.sum()), ("mean", lambda v: v.mean()), ("min", lambda v: v.min()),
-                ("max", lambda v: v.max()), ("count", lambda v: v.count()), ("var", lambda v: v.var())]
+    specs, arrivals = served_requests(nreq, rate)
     reqs = []
-    for i in range(nreq):
-        t = int(rng.integers(0, len(tables)))
-        keys = [["k1"], ["k2"], ["k1", "k2"]][int(rng.integers(0, 3))]
-        pick = [a for a in aggs_all if rng.random() < 0.5] or [aggs_all[0]]
-        plan = shape.lazy().filter(col("p") < int(rng.integers(1, 100))).group_by(keys, maintain_order=True).agg(
-            [f(col("v")).alias(n) for n, f in pick])
+    for t, plan in ((sp["table"], served_plan(shape, sp)) for sp in specs):
         bound = bind(plan.plan)
         reqs.append((bound, [tables[t][2][n] for n in bound.names]))
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
 
     # Warm-up: every table once (statistics, learned group counts).
     for bound, cl in reqs[: min(nreq, 16)]:

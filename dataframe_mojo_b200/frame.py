@@ -54,15 +54,43 @@ class Series:
     reference's columns and the provider use) and unpacks it to the bool
     mask only when `valid` is first read."""
 
-    def __init__(self, name: str, values, valid=None, dtype=None):
+    def __init__(self, name: str, values, valid=None, dtype=None, categories=None):
+        """`values`: a numeric array, or strings (a String column, values of
+        dtype object).  With `categories` the column is a Categorical: values
+        are UInt32 codes into that dictionary of strings
+        (dataframe/categorical.mojo:1-17)."""
         arr = np.asarray(values, dtype=dtype)
         if arr.ndim != 1:
             raise ValueError("a Series is one-dimensional")
-        dfc_dtype(arr.dtype)
+        if arr.dtype.kind in "OUS":
+            if categories is not None:
+                raise TypeError("a Categorical's values are UInt32 codes")
+            arr = arr.astype(object)
+        else:
+            dfc_dtype(arr.dtype)
+        if categories is not None:
+            if arr.dtype != np.uint32:
+                raise TypeError("a Categorical's codes are UInt32")
+            categories = np.asarray(categories, dtype=object)
         self.name = name
         self.values = np.ascontiguousarray(arr)
+        self.categories = categories
         self._bits = None
         self.valid = valid
+
+    @property
+    def is_string(self) -> bool:
+        return self.values.dtype == object
+
+    @property
+    def is_categorical(self) -> bool:
+        return self.categories is not None
+
+    def decoded(self) -> np.ndarray:
+        """The column's strings (String or Categorical columns)."""
+        if self.is_categorical:
+            return self.categories[self.values]
+        return self.values
 
     @classmethod
     def from_bits(cls, name: str, values, bits: np.ndarray | None) -> "Series":
@@ -117,18 +145,27 @@ class Series:
         return self.valid is None or bool(self.valid[i])
 
     def item(self, i: int):
-        return self.values[i].item() if self.is_valid(i) else None
+        if not self.is_valid(i):
+            return None
+        if self.is_categorical:
+            return self.categories[self.values[i]]
+        v = self.values[i]
+        return v if self.is_string else v.item()
 
     def to_list(self) -> list:
         return [self.item(i) for i in range(len(self))]
 
     def slice(self, offset: int, length: int) -> "Series":
         v = None if self.valid is None else self.valid[offset : offset + length]
-        return Series(self.name, self.values[offset : offset + length], v)
+        return Series(self.name, self.values[offset : offset + length], v, categories=self.categories)
 
     def equals(self, other: "Series") -> bool:
         """Same name, dtype, length, nulls and values (NaN equals NaN)."""
         if self.name != other.name or self.dtype != other.dtype or len(self) != len(other):
+            return False
+        if self.is_categorical != other.is_categorical:
+            return False
+        if self.is_categorical and not np.array_equal(self.categories, other.categories):
             return False
         va = np.ones(len(self), bool) if self.valid is None else self.valid
         vb = np.ones(len(other), bool) if other.valid is None else other.valid
@@ -439,6 +476,9 @@ class Bound:
     aggs: list[tuple]                # (op, column index, ddof, min_count)
     out_names: list[str]
     maintain_order: bool
+    # Output column index -> ("categorical" | "string", dictionary): columns
+    # that come back as codes and are decoded (decode_outputs).
+    decoders: dict = field(default_factory=dict)
 
 
 def _bind_literal(series: Series, value):
@@ -458,17 +498,55 @@ def _bind_literal(series: Series, value):
     return ("u", int(value)) if series.dtype == np.uint64 else ("i", int(value))
 
 
+# Aggregations that read a String or Categorical column through its codes
+# (they need only equality or the row's value).
+_CODED_AGGS = {N.AGG_COUNT, N.AGG_LEN, N.AGG_NULL_COUNT, N.AGG_N_UNIQUE, N.AGG_FIRST, N.AGG_LAST}
+
+
+def _coded(s: Series) -> tuple[Series, str, np.ndarray]:
+    """A String or Categorical column as UInt32 codes.  A Categorical keys by
+    canonical codes (every code mapped to the first code with the same label,
+    so repeated labels are one group) and keeps its dictionary; a String
+    column is dictionary-encoded here and decoded back after the query (the
+    reference groups a dictionary-coded String key by its codes and returns
+    strings: dataframe/aggregation/group_by.mojo:307-317, 344-356)."""
+    valid = s.valid
+    if s.is_categorical:
+        labels = s.categories
+        first: dict = {}
+        canon = np.array([first.setdefault(lab, i) for i, lab in enumerate(labels)], dtype=np.uint32)
+        raw = s.values if valid is None else np.where(valid, s.values, 0).astype(np.uint32)
+        codes = canon[raw] if len(labels) else np.zeros(len(s), np.uint32)
+        return Series(s.name, codes, valid), "categorical", labels
+    filled = s.values if valid is None else np.where(valid, s.values, "")
+    uniques, inverse = np.unique(filled.astype(str).astype(object), return_inverse=True)
+    return Series(s.name, inverse.astype(np.uint32), valid), "string", uniques
+
+
+def _code_literal(kind: str, table: np.ndarray, value) -> int:
+    """The code a string literal compares as: its (canonical) code, or one no
+    row holds when the dictionary lacks it."""
+    hits = np.flatnonzero(table == value) if len(table) else []
+    return int(hits[0]) if len(hits) else len(table)
+
+
 def bind(plan: Plan) -> Bound:
     if plan.keys is None:
         raise ValueError("the plan has no aggregation")
     src = plan.source
     names: list[str] = []
+    coded: dict[str, tuple] = {}
 
     def idx(name: str) -> int:
         if name not in names:
-            src.column(name)
+            s = src.column(name)
+            if s.is_string or s.is_categorical:
+                coded[name] = _coded(s)
             names.append(name)
         return names.index(name)
+
+    def series(name: str) -> Series:
+        return coded[name][0] if name in coded else src.column(name)
 
     keys = [idx(k) for k in plan.keys]
     prog: list[tuple] = []
@@ -476,7 +554,13 @@ def bind(plan: Plan) -> Bound:
     def emit(p: Pred):
         if p.kind == "cmp":
             i = idx(p.column)
-            prog.append((N.PRED_CMP, i, _CMP[p.op], _bind_literal(src.column(p.column), p.literal)))
+            if p.column in coded:
+                if p.op not in ("==", "!="):
+                    raise TypeError(f"only == and != compare a String or Categorical column ({p.column})")
+                _, kind, table = coded[p.column]
+                prog.append((N.PRED_CMP, i, _CMP[p.op], ("i", _code_literal(kind, table, p.literal))))
+            else:
+                prog.append((N.PRED_CMP, i, _CMP[p.op], _bind_literal(src.column(p.column), p.literal)))
         elif p.kind == "is_null":
             prog.append((N.PRED_IS_NULL, idx(p.column), 0, ("i", 0)))
         elif p.kind == "is_not_null":
@@ -498,15 +582,50 @@ def bind(plan: Plan) -> Bound:
         if i > 0:
             prog.append((N.PRED_AND, 0, 0, ("i", 0)))
     aggs = [(a.op, idx(a.column), a.ddof, a.min_count) for a in plan.aggs]
+    decoders: dict = {}
+    for k, name in enumerate(plan.keys):
+        if name in coded:
+            decoders[k] = coded[name][1:]
+    for j, a in enumerate(plan.aggs):
+        if a.column in coded:
+            if a.op not in _CODED_AGGS:
+                raise TypeError(f"this aggregation does not read a String or Categorical column ({a.column})")
+            if a.op in (N.AGG_FIRST, N.AGG_LAST):
+                decoders[len(plan.keys) + j] = coded[a.column][1:]
     return Bound(
         names=names,
-        series=[src.column(n) for n in names],
+        series=[series(n) for n in names],
         keys=keys,
         pred=prog,
         aggs=aggs,
         out_names=list(plan.keys) + [a.name for a in plan.aggs],
         maintain_order=plan.maintain_order,
+        decoders=decoders,
     )
+
+
+def decode_outputs(bound: Bound, frame: DataFrame) -> DataFrame:
+    """Result columns that came back as codes: a Categorical keeps its
+    dictionary, a String column gets its strings back."""
+    if not bound.decoders:
+        return frame
+    cols = []
+    for i, name in enumerate(frame.columns):
+        s = frame[name]
+        if i not in bound.decoders:
+            cols.append(s)
+            continue
+        kind, table = bound.decoders[i]
+        valid = s.valid
+        codes = s.values.astype(np.uint32)
+        if kind == "categorical":
+            cols.append(Series(name, codes, valid, categories=table))
+        else:
+            strings = np.empty(len(s), dtype=object)
+            ok = np.ones(len(s), bool) if valid is None else valid
+            strings[ok] = table[codes[ok]] if len(table) else None
+            cols.append(Series(name, strings, valid))
+    return DataFrame(cols)
 
 
 def pack_validity(valid: np.ndarray | None) -> np.ndarray | None:

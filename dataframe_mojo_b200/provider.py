@@ -28,7 +28,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _native as N
-from .frame import Bound, DataFrame, LazyFrame, Plan, Series, bind, dfc_dtype, np_dtype
+from .frame import Bound, DataFrame, LazyFrame, Plan, Series, bind, decode_outputs, dfc_dtype, np_dtype
 
 BACKEND = "cuda"
 MEMORY_DISCRETE = 1
@@ -407,7 +407,7 @@ def _execute_plan(plan: Plan, device: int) -> DataFrame:
     try:
         result = run_bound(bound, cols, flags=flags)
         try:
-            return result.to_frame()
+            return decode_outputs(bound, result.to_frame())
         finally:
             result.free()
     finally:

@@ -12,7 +12,7 @@ from pathlib import Path
 import numpy as np
 
 from dataframe_mojo_b200 import _native as N
-from dataframe_mojo_b200.frame import Bound, DataFrame, Plan, Series, bind, np_dtype, pack_validity
+from dataframe_mojo_b200.frame import Bound, DataFrame, Plan, Series, bind, decode_outputs, np_dtype, pack_validity
 
 LIB_PATH = Path(__file__).resolve().parent / "_build" / "liboracle.so"
 
@@ -147,7 +147,7 @@ def run(plan_or_bound, threads: int | None = None):
         )
     finally:
         h.orc_result_free(out)
-    return DataFrame(series), first
+    return decode_outputs(bound, DataFrame(series)), first
 
 
 def N_dtype(s: Series) -> int:

@@ -186,6 +186,7 @@ SIGNATURES = [
     ("dfc_result_copy_to_host", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     ("dfc_result_free", None, [C.c_void_p]),
     ("dfc_result_residence", C.c_void_p, [C.c_void_p, C.c_int32]),
+    ("dfc_result_validity_residence", C.c_void_p, [C.c_void_p, C.c_int32]),
     ("dfc_residence_to_host", C.c_int32, [C.c_void_p, C.c_void_p, C.c_int64]),
     ("dfc_residence_release", None, [C.c_void_p]),
     ("dfc_last_timings", C.c_int, [C.POINTER(Timings)]),

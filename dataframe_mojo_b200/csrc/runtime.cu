@@ -1722,8 +1722,8 @@ DFC_API dfc_status dfc_column_register(int32_t device, dfc_dtype dtype, uint64_t
   DeviceState* ds;
   dfc_status st = device_ready(device, &ds);
   if (st) return st;
-  if (flags == DFC_COLUMN_DEVICE && rows > 0 && !device_memory_of(values, device))
-    return fail(DFC_INVALID, "DFC_COLUMN_DEVICE values must be device memory of the column's device "
+  if (flags == DFC_COLUMN_DEVICE && rows > 0 && (!device_memory_of(values, device) || !device_memory_of(validity, device)))
+    return fail(DFC_INVALID, "DFC_COLUMN_DEVICE values and validity must be device memory of the column's device "
                              "(host, managed or another GPU's memory is not accepted)");
   DeviceGuard guard(device);
   cudaStream_t stream = thread_stream(device);
@@ -2145,22 +2145,31 @@ DFC_API void dfc_result_free(dfc_result* result) {
 struct Residence {
   dfc_result* result;
   int32_t column;
+  bool validity;  // the column's LSB-first validity bitmap instead of its values
 };
 
 DFC_API void* dfc_result_residence(dfc_result* result, int32_t i) {
   if (!result || i < 0 || i >= (int32_t)result->cols.size()) return nullptr;
   result->refs.fetch_add(1);
-  return new Residence{result, i};
+  return new Residence{result, i, false};
+}
+
+DFC_API void* dfc_result_validity_residence(dfc_result* result, int32_t i) {
+  if (!result || i < 0 || i >= (int32_t)result->cols.size() || !result->cols[i].has_nulls) return nullptr;
+  result->refs.fetch_add(1);
+  return new Residence{result, i, true};
 }
 
 DFC_API int32_t dfc_residence_to_host(void* ctx, void* host_dst, int64_t bytes) {
   auto* r = static_cast<Residence*>(ctx);
   if (!r || !host_dst || bytes < 0) return 1;
   const ResultCol& c = r->result->cols[r->column];
-  const int64_t have = (int64_t)(r->result->rows * dtype_size(c.dtype));
+  const uint64_t rows = r->result->rows;
+  const int64_t have = r->validity ? (int64_t)((rows + 7) / 8) : (int64_t)(rows * dtype_size(c.dtype));
   if (bytes > have) return 1;
   DeviceGuard guard(r->result->device);
-  if (bytes && cudaMemcpy(host_dst, c.values, (size_t)bytes, cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+  const void* src = r->validity ? static_cast<const void*>(c.validity) : c.values;
+  if (bytes && cudaMemcpy(host_dst, src, (size_t)bytes, cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
   return 0;
 }
 

@@ -22,13 +22,15 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import threading
 import time
 from dataclasses import dataclass
 
 import numpy as np
 
 from . import _native as N
-from .frame import Bound, DataFrame, LazyFrame, Plan, Series, bind, decode_outputs, dfc_dtype, np_dtype
+from .frame import (Bound, DataFrame, LazyFrame, Plan, Series, bind, bits_all_set, decode_outputs, dfc_dtype,
+                    np_dtype, unpack_validity)
 
 BACKEND = "cuda"
 MEMORY_DISCRETE = 1
@@ -167,6 +169,25 @@ class DeviceColumn:
         self.handle = handle
         return self
 
+    @classmethod
+    def from_resident(cls, series: "ResidentSeries", device: int | None = None) -> "DeviceColumn":
+        """A resident result column as the input of a following query, read
+        in place on the device (no host round trip); the column keeps the
+        series, and so its device buffers, alive."""
+        self = cls.__new__(cls)
+        self.name, self.dtype, self.rows = series.name, series.dtype, len(series)
+        self.device = series.device if device is None else device
+        self._keep = series
+        handle = C.c_void_p()
+        _check(
+            N.lib().dfc_column_register(
+                self.device, dfc_dtype(series.dtype), self.rows, series.device_values if self.rows else None,
+                series.device_validity, 0, N.COLUMN_DEVICE, C.byref(handle)
+            )
+        )
+        self.handle = handle
+        return self
+
     @property
     def null_count(self) -> int:
         return int(N.lib().dfc_column_null_count(self.handle)) if self.handle else 0
@@ -183,13 +204,93 @@ class DeviceColumn:
             pass
 
 
+class ResidentSeries(Series):
+    """A result column left in device memory, the shape of the reference's
+    `_DeviceResidence` (dataframe/storage/residence.mojo:20-72): an opaque
+    handle with C-ABI callbacks (dfc_residence_to_host / _release).  The
+    first host read of values or validity copies them once, under a lock;
+    the device buffers stay until the series is released, so a following
+    device query reads them in place (DeviceColumn.from_resident)."""
+
+    def __init__(self, name: str, result: "DeviceResult", i: int):
+        lib = N.lib()
+        dtype, vals, valid = result.column_info(i)
+        self.name = name
+        self.categories = None
+        self.device = result.device
+        self._dtype = np.dtype(dtype)
+        self._rows = result.rows
+        self.device_values = vals
+        self.device_validity = valid
+        self._ctx = lib.dfc_result_residence(result.handle, i)
+        self._vctx = lib.dfc_result_validity_residence(result.handle, i) if valid else None
+        self._lock = threading.Lock()
+        self._host = None
+        self._bits = None
+        self._valid = None
+
+    def on_host(self) -> bool:
+        return self._host is not None
+
+    def _copy(self) -> None:
+        with self._lock:
+            if self._host is not None:
+                return
+            lib = N.lib()
+            values = np.empty(self._rows, dtype=self._dtype)
+            if self._rows and lib.dfc_residence_to_host(self._ctx, values.ctypes.data, values.nbytes) != 0:
+                raise ProviderError(N.DEVICE, "copying a device result column to the host failed")
+            if self._vctx:
+                bits = np.empty((self._rows + 7) // 8, dtype=np.uint8)
+                if self._rows and lib.dfc_residence_to_host(self._vctx, bits.ctypes.data, bits.nbytes) != 0:
+                    raise ProviderError(N.DEVICE, "copying a device validity bitmap to the host failed")
+                if not bits_all_set(bits, self._rows):
+                    self._bits = bits
+            self._host = values
+
+    @property
+    def values(self) -> np.ndarray:
+        self._copy()
+        return self._host
+
+    @property
+    def valid(self) -> np.ndarray | None:
+        self._copy()
+        if self._bits is not None:
+            self._valid = unpack_validity(self._bits, self._rows)
+            self._bits = None
+        return self._valid
+
+    @property
+    def dtype(self) -> np.dtype:
+        return self._dtype
+
+    def __len__(self) -> int:
+        return self._rows
+
+    def release(self) -> None:
+        lib = N.lib()
+        for attr in ("_ctx", "_vctx"):
+            ctx = getattr(self, attr, None)
+            if ctx:
+                lib.dfc_residence_release(ctx)
+                setattr(self, attr, None)
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
 class DeviceResult:
     """A query result resident on the device: key columns then one column per
     aggregation.  ``to_frame`` copies it to the host."""
 
-    def __init__(self, handle: C.c_void_p, names: list[str]):
+    def __init__(self, handle: C.c_void_p, names: list[str], device: int = 0):
         self.handle = handle
         self.names = names
+        self.device = device
         self.rows = int(N.lib().dfc_result_rows(handle))
 
     def column_info(self, i: int) -> tuple[np.dtype, int, int | None]:
@@ -198,6 +299,11 @@ class DeviceResult:
         valid = C.c_void_p()
         _check(N.lib().dfc_result_column(self.handle, i, C.byref(dt), C.byref(vals), C.byref(valid)))
         return np_dtype(dt.value), vals.value, valid.value
+
+    def to_resident(self) -> DataFrame:
+        """The result as a frame of ResidentSeries: nothing is copied until a
+        column is read on the host."""
+        return DataFrame([ResidentSeries(name, self, i) for i, name in enumerate(self.names)])
 
     def to_frame(self, into: dict | None = None) -> DataFrame:
         """Copies the result to host memory.  `into` maps column names to
@@ -277,7 +383,7 @@ def run_bound(bound: Bound, columns: list[DeviceColumn], stream: int | None = No
     q = _query_struct(bound, [c.handle for c in columns], stream, flags)
     out = C.c_void_p()
     _check(N.lib().dfc_groupby(C.byref(q), C.byref(out)))
-    return DeviceResult(out, bound.out_names)
+    return DeviceResult(out, bound.out_names, getattr(columns[0], "device", 0) if columns else 0)
 
 
 def run_batch(jobs: list, stream: int | None = None, flags: int = 0) -> list:
@@ -406,6 +512,7 @@ def _execute_plan(plan: Plan, device: int) -> DataFrame:
     cols = [DeviceColumn(s, device) for s in bound.series]
     try:
         result = run_bound(bound, cols, flags=flags)
+        _record_run(plan, last_timings()["total_ns"])
         try:
             return decode_outputs(bound, result.to_frame())
         finally:
@@ -595,18 +702,92 @@ def pipeline_supports(pipeline, device: int) -> bool:
         return False
 
 
+# Device-time calibration, per layout (the region with its literals left
+# out): nanoseconds per input byte, from this provider's own timed queries
+# (dfc_last_timings total).  Before a layout has run, the model measured for
+# this provider on B200: the 100M-row filtered group-by (2.0125 GB of input
+# columns) took 7.3 ms, and a query's fixed cost (planning, statistics,
+# launches, result) is about 0.3 ms.
+_DEFAULT_NS_PER_BYTE = 7.0e6 / 2.0125e9
+_FIXED_NS = 3.0e5
+_calibration: dict[str, list[float]] = {}
+_calibration_lock = threading.Lock()
+
+
+def _layout_key(plan: Plan) -> str:
+    src = plan.source
+    cols = sorted({f.column for f in plan.filters if getattr(f, "column", None)} | set(plan.keys or [])
+                  | {a.column for a in plan.aggs or []})
+    types = ",".join(f"{c}:{src.column(c).dtype}" for c in cols)
+    filt = ";".join(f.kind + getattr(f, "op", "") for f in plan.filters)
+    aggs = ",".join(f"{a.op}:{a.column}" for a in plan.aggs or [])
+    return f"cuda:groupby:v2:{types}|{filt}|{plan.keys}|{aggs}"
+
+
+def _input_bytes(plan: Plan, rows: int | None = None) -> int:
+    bound = bind(plan)
+    n = len(bound.series[0]) if rows is None and bound.series else (rows or 0)
+    per_row = sum(s.dtype.itemsize + (0.125 if s.has_nulls else 0.0) for s in bound.series)
+    return int(n * per_row)
+
+
+def _record_run(plan: Plan, device_ns: float) -> None:
+    nbytes = _input_bytes(plan)
+    if nbytes <= 0 or device_ns <= _FIXED_NS:
+        return
+    rate = (device_ns - _FIXED_NS) / nbytes
+    with _calibration_lock:
+        old = _calibration.get(_layout_key(plan))
+        _calibration[_layout_key(plan)] = [rate if old is None else 0.5 * old[0] + 0.5 * rate,
+                                           1.0 if old is None else old[1] + 1.0]
+
+
 def pipeline_estimate(pipeline, device: int, features: PipelineFeatures | None = None) -> float:
-    """Estimated device ns excluding input/output moves; -1 when unmeasured."""
-    return -1.0
+    """Estimated device nanoseconds of the pipeline's region, input and
+    output moves excluded (those are transfer_model's): fixed cost plus the
+    layout's calibrated ns per input byte; -1 when the region is not one this
+    provider runs."""
+    try:
+        p = _region_plan(pipeline)
+        if _unsupported_reason(p) is not None:
+            return -1.0
+        nbytes = features.input_bytes if features and features.input_bytes > 0 else _input_bytes(
+            p, features.rows if features and features.rows > 0 else None)
+        with _calibration_lock:
+            cal = _calibration.get(_layout_key(p))
+        return _FIXED_NS + nbytes * (cal[0] if cal else _DEFAULT_NS_PER_BYTE)
+    except Exception:
+        return -1.0
 
 
 def pipeline_costs(pipeline, device: int, features: PipelineFeatures | None = None) -> tuple[float, float]:
+    """(matched CPU ns, device ns): -1 for the CPU keeps the core's generic
+    calibration (dataframe/lazy_api.mojo:2537-2541)."""
     return -1.0, pipeline_estimate(pipeline, device, features)
 
 
 def run_pipeline(pipeline, device: int) -> DataFrame:
+    """Runs the region and leaves its result on the device: a frame of
+    ResidentSeries, copied to the host column by column when first read
+    (the reference's device-resident pipeline output,
+    dataframe/storage/residence.mojo:33-147).  Columns decoded from
+    dictionary codes are read on the host at once."""
     p = _region_plan(pipeline)
     reason = _unsupported_reason(p)
     if reason:
         raise UnsupportedError(N.UNSUPPORTED, f"accelerator cannot run this pipeline: {reason}")
-    return _execute_plan(p, device)
+    bound = bind(p)
+    _check(N.lib().dfc_set_memory_limit(device, max(_memory_limit(), 0)))
+    cols = [DeviceColumn(s, device) for s in bound.series]
+    try:
+        result = run_bound(bound, cols, flags=_regime_flags())
+        t = last_timings()
+        try:
+            frame = result.to_resident()
+        finally:
+            result.free()  # the resident columns hold their own references
+    finally:
+        for c in cols:
+            c.release()
+    _record_run(p, t["total_ns"])
+    return decode_outputs(bound, frame)

@@ -135,10 +135,11 @@ DFC_API dfc_status dfc_set_memory_limit(int32_t device, int64_t bytes);
 /* values/validity point to host memory: the library copies them into HBM
  * (validity normalised to bit offset 0) and keeps them resident. */
 #define DFC_COLUMN_HOST 0u
-/* values points to device memory the caller owns and keeps alive until
- * dfc_column_release; only the validity bitmap is copied (normalised).  It
- * must be device memory of `device` (cudaPointerGetAttributes): host,
- * managed or another GPU's memory is rejected with DFC_INVALID. */
+/* values (and validity, when given) point to device memory the caller owns
+ * and keeps alive until dfc_column_release; only the validity bitmap is
+ * copied (normalised).  Both must be device memory of `device`
+ * (cudaPointerGetAttributes): host, managed or another GPU's memory is
+ * rejected with DFC_INVALID. */
 #define DFC_COLUMN_DEVICE 1u
 
 /* validity may be NULL (every row valid).  validity_bit_offset is the bit
@@ -396,6 +397,9 @@ DFC_API void dfc_result_free(dfc_result* result);
  * handle made by dfc_result_residence(result, i). to_host returns 0 on
  * success; release frees the handle (the result keeps its own reference). */
 DFC_API void* dfc_result_residence(dfc_result* result, int32_t i);
+/* The same for column i's validity bitmap (ceil(rows / 8) LSB-first bytes);
+ * NULL when the column has no nulls. */
+DFC_API void* dfc_result_validity_residence(dfc_result* result, int32_t i);
 DFC_API int32_t dfc_residence_to_host(void* ctx, void* host_dst, int64_t bytes);
 DFC_API void dfc_residence_release(void* ctx);
 

@@ -719,7 +719,10 @@ def _layout_key(plan: Plan) -> str:
     cols = sorted({f.column for f in plan.filters if getattr(f, "column", None)} | set(plan.keys or [])
                   | {a.column for a in plan.aggs or []})
     types = ",".join(f"{c}:{src.column(c).dtype}" for c in cols)
-    filt = ";".join(f.kind + getattr(f, "op", "") for f in plan.filters)
+    def shape(f) -> str:
+        return f.kind + (f.op or "") + "(" + ",".join(shape(a) for a in f.args) + ")"
+
+    filt = ";".join(shape(f) for f in plan.filters)
     aggs = ",".join(f"{a.op}:{a.column}" for a in plan.aggs or [])
     return f"cuda:groupby:v2:{types}|{filt}|{plan.keys}|{aggs}"
 

@@ -512,7 +512,7 @@ def _execute_plan(plan: Plan, device: int) -> DataFrame:
     cols = [DeviceColumn(s, device) for s in bound.series]
     try:
         result = run_bound(bound, cols, flags=flags)
-        _record_run(plan, last_timings()["total_ns"])
+        _record_run(plan, last_timings()["total_ns"], bound)
         try:
             return decode_outputs(bound, result.to_frame())
         finally:
@@ -727,15 +727,15 @@ def _layout_key(plan: Plan) -> str:
     return f"cuda:groupby:v2:{types}|{filt}|{plan.keys}|{aggs}"
 
 
-def _input_bytes(plan: Plan, rows: int | None = None) -> int:
-    bound = bind(plan)
+def _input_bytes(plan: Plan, rows: int | None = None, bound: Bound | None = None) -> int:
+    bound = bound or bind(plan)
     n = len(bound.series[0]) if rows is None and bound.series else (rows or 0)
     per_row = sum(s.dtype.itemsize + (0.125 if s.has_nulls else 0.0) for s in bound.series)
     return int(n * per_row)
 
 
-def _record_run(plan: Plan, device_ns: float) -> None:
-    nbytes = _input_bytes(plan)
+def _record_run(plan: Plan, device_ns: float, bound: Bound | None = None) -> None:
+    nbytes = _input_bytes(plan, bound=bound)
     if nbytes <= 0 or device_ns <= _FIXED_NS:
         return
     rate = (device_ns - _FIXED_NS) / nbytes
@@ -792,5 +792,5 @@ def run_pipeline(pipeline, device: int) -> DataFrame:
     finally:
         for c in cols:
             c.release()
-    _record_run(p, t["total_ns"])
+    _record_run(p, t["total_ns"], bound)
     return decode_outputs(bound, frame)

@@ -184,6 +184,7 @@ SIGNATURES = [
         [C.c_void_p, C.c_int32, C.POINTER(C.c_int), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)],
     ),
     ("dfc_result_copy_to_host", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    ("dfc_result_copy_to_device", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     ("dfc_result_free", None, [C.c_void_p]),
     ("dfc_result_residence", C.c_void_p, [C.c_void_p, C.c_int32]),
     ("dfc_result_validity_residence", C.c_void_p, [C.c_void_p, C.c_int32]),

@@ -2126,6 +2126,24 @@ DFC_API dfc_status dfc_result_copy_to_host(const dfc_result* result, int32_t i, 
   return DFC_OK;
 }
 
+DFC_API dfc_status dfc_result_copy_to_device(const dfc_result* result, int32_t i, void* values, uint8_t* validity) {
+  if (!result || i < 0 || i >= (int32_t)result->cols.size()) return fail(DFC_INVALID, "bad result column");
+  const ResultCol& c = result->cols[i];
+  DeviceGuard guard(result->device);
+  const size_t n = result->rows;
+  if (n && (!device_memory_of(values, result->device) || !device_memory_of(validity, result->device)))
+    return fail(DFC_INVALID, "result copy targets must be device memory of the result's device");
+  cudaStream_t stream = thread_stream(result->device);
+  if (values && n)
+    CK(cudaMemcpyAsync(values, c.values, n * dtype_size(c.dtype), cudaMemcpyDeviceToDevice, stream), "result copy");
+  if (validity && n) {
+    if (c.has_nulls) CK(cudaMemcpyAsync(validity, c.validity, (n + 7) / 8, cudaMemcpyDeviceToDevice, stream), "result copy");
+    else CK(cudaMemsetAsync(validity, 0xFF, (n + 7) / 8, stream), "result copy");
+  }
+  CK(cudaStreamSynchronize(stream), "result copy");
+  return DFC_OK;
+}
+
 DFC_API void dfc_result_free(dfc_result* result) {
   if (!result) return;
   if (result->refs.fetch_sub(1) != 1) return;

@@ -1,26 +1,32 @@
 """Sharded group-by: the rows split across ranks (one process per GPU), each
 rank aggregating its own rows on its own GPU, one exchange of the partial
-groups, and a merge that restores the result of one query over all rows.
+groups by key, and a merge on the device that restores the result of one
+query over all rows (the reference's parallel design: per-worker partial
+tables merged by partition, dataframe/aggregation/hash_table.mojo:11-47).
 
-Order: every rank's result is in first-appearance order of its own rows, and
-rank r's rows all come after rank r-1's.  Concatenating the partial results
-in rank order therefore puts each group's first occurrence at its global
-first appearance, so the merged groups are ordered by the position of their
-first occurrence in that concatenation (maintain_order=True; without it the
-order is not part of the result).
-
-Partial states: each rank runs the query with aggregations a merge can
-combine -- counts, rows, null counts, integer sums (sum types are exact),
-means (a Float column's sum is rebuilt as mean x count in FP64, since a
-Float32 sum is a Float32 result), population variances (M2 = var0 x n, merged
-by Chan et al.'s pairwise update), minima and maxima -- and the merge
-finishes the requested aggregations from them, with the same null, NaN,
-signed-zero and overflow rules as the single-GPU path.
-
-The exchange is one all-gather of the partial results
-(`torch.distributed.all_gather_object`), which works on the NCCL and gloo
-backends alike; the merge runs on the host.  Partial results hold one row
-per group and rank, far fewer bytes than the rows the ranks aggregated.
+1. Partials.  Each rank runs the query over its contiguous rows with
+   aggregations a merge can combine -- counts, rows, null counts, integer
+   sums (sum types are exact), means (a Float column's sum is rebuilt as
+   mean x count in FP64), population variances (M2 = var0 x n) and extrema
+   -- in first-appearance order (partial_plan).  On GPUs the partial result
+   stays on the device (dfc_result_copy_to_device into torch tensors).
+2. Exchange.  Every partial row goes to the rank that owns its key (a hash
+   of the canonical key words: NaN one value, -0.0 == 0.0, nulls equal):
+   one all_to_all_single of a packed int64 matrix (NCCL over NVLink on GPUs,
+   gloo on CPU), after one of the row counts.  No TMA or bulk copy reads
+   another GPU's memory.  A row carries its position (rank << 32 | index in
+   its rank's partial result): rank r's rows all come after rank r-1's, so
+   the smallest position of a group is its global first appearance.
+3. Owner merge, on the owner's device (torch tensors): groups by torch.unique
+   over the key words; exact integer sums from 32-bit halves (the split the
+   reference's Metal kernels use, dataframe_metal/accelerator/gpu/
+   filter_sum.mojo:8-14) checked against the sum type with the CPU's
+   overflow message; float sums; Chan et al.'s update for M2 (the combine of
+   dataframe/aggregation/function.mojo:1736-1758); extrema with the
+   single-GPU null, NaN, tie and signed-zero rules; key values from the
+   group's first row.
+4. Order.  The owners' finished rows (one per group) are all-gathered and
+   ordered by their groups' first position (maintain_order=True).
 """
 from __future__ import annotations
 
@@ -84,170 +90,465 @@ def partial_plan(plan: Plan, part: DataFrame) -> tuple[Plan, dict, str]:
     return sub, parts, rows_name
 
 
-def _key_bytes(cols: list[Series]) -> np.ndarray:
-    """One fixed-width byte string per row: per key column a validity byte and
-    the value bytes (0 when null; NaN canonical and -0.0 as 0.0 for floats,
-    the keys' equality)."""
-    n = len(cols[0]) if cols else 0
-    pieces = []
-    for s in cols:
-        valid = np.ones(n, bool) if s.valid is None else s.valid
-        v = s.values.copy()
-        if v.dtype.kind == "f":
-            v = np.where(np.isnan(v), np.array(np.nan, v.dtype), v).astype(v.dtype)
-            v = np.where(v == 0, np.zeros(1, v.dtype), v).astype(v.dtype)
-        raw = np.ascontiguousarray(v).view(np.uint8).reshape(n, v.dtype.itemsize).copy()
-        raw[~valid] = 0
-        pieces.append(valid[:, None].astype(np.uint8))
-        pieces.append(raw)
-    mat = np.ascontiguousarray(np.concatenate(pieces, axis=1)) if pieces else np.zeros((n, 1), np.uint8)
-    return mat.view(np.dtype((np.void, mat.shape[1]))).ravel()
+# ---------------------------------------------------------------------------
+# Columns as int64 tensors: the raw bits of 8-byte values, narrower ones
+# widened (signed types sign-extended, Float32 through its Int32 bits), so
+# every column fits one int64 column of the exchanged matrix and decodes back
+# exactly.
+# ---------------------------------------------------------------------------
+def _encode_np(values: np.ndarray) -> np.ndarray:
+    dt = values.dtype
+    if dt.itemsize == 8:
+        return np.ascontiguousarray(values).view(np.int64)
+    if dt == np.float32:
+        return np.ascontiguousarray(values).view(np.int32).astype(np.int64)
+    return values.astype(np.int64)
 
 
-def _cat(parts: list[DataFrame], name: str) -> Series:
-    vals = np.concatenate([p[name].values for p in parts])
-    if all(p[name].valid is None for p in parts):
-        return Series(name, vals)
-    valid = np.concatenate([np.ones(p.height, bool) if p[name].valid is None else p[name].valid for p in parts])
-    return Series(name, vals, valid)
+def _decode_np(bits: np.ndarray, dt: np.dtype) -> np.ndarray:
+    dt = np.dtype(dt)
+    bits = np.ascontiguousarray(bits, dtype=np.int64)
+    if dt.itemsize == 8:
+        return bits.view(dt)
+    if dt == np.float32:
+        return bits.astype(np.int32).view(np.float32)
+    return bits.astype(dt)
 
 
-def _valid(s: Series) -> np.ndarray:
-    return np.ones(len(s), bool) if s.valid is None else s.valid
+class _Cols:
+    """Partial columns on one device: name -> (int64 bits, valid mask, dtype)."""
+
+    def __init__(self):
+        self.bits: dict = {}
+        self.valid: dict = {}
+        self.dtype: dict = {}
+
+    def add(self, name, bits, valid, dtype):
+        self.bits[name], self.valid[name], self.dtype[name] = bits, valid, np.dtype(dtype)
+
+    def rows(self) -> int:
+        return int(next(iter(self.bits.values())).shape[0]) if self.bits else 0
 
 
-def merge_partials(plan: Plan, parts: list[DataFrame], spec: dict, rows_name: str) -> DataFrame:
-    """The query's result from the ranks' partial results, `parts` in rank
-    order."""
-    from .provider import DataFaultError, ProviderError
+def _frame_cols(frame: DataFrame, device) -> _Cols:
+    import torch
 
-    keys = [_cat(parts, k) for k in plan.keys]
-    total = sum(p.height for p in parts)
-    kb = _key_bytes(keys)
-    _, first, inv = np.unique(kb, return_index=True, return_inverse=True)
-    inv = inv.ravel()
-    # Groups in order of their first occurrence; rows sorted by group, rank order kept.
-    order_groups = np.argsort(first, kind="stable")
-    rank_of = np.empty_like(order_groups)
-    rank_of[order_groups] = np.arange(len(order_groups))
-    gid = rank_of[inv] if total else inv
-    rows = np.argsort(gid, kind="stable")
-    gsorted = gid[rows]
-    starts = np.flatnonzero(np.r_[True, gsorted[1:] != gsorted[:-1]]) if total else np.zeros(0, np.int64)
-    G = len(starts)
-    firsts = rows[starts]
+    cols = _Cols()
+    for c in frame.columns:
+        s = frame[c]
+        bits = torch.from_numpy(_encode_np(s.values).copy()).to(device)
+        valid = torch.ones(len(s), dtype=torch.bool, device=device) if s.valid is None else \
+            torch.from_numpy(np.asarray(s.valid, dtype=bool).copy()).to(device)
+        cols.add(c, bits, valid, s.dtype)
+    return cols
 
-    def red_add(a):
-        return np.add.reduceat(a[rows], starts) if G else np.zeros(0, a.dtype)
 
-    out_cols = [Series(k.name, k.values[firsts], None if k.valid is None else k.valid[firsts]) for k in keys]
+def _result_cols(result, device) -> _Cols:
+    """A device result's columns as torch tensors on `device`, copied device
+    to device (dfc_result_copy_to_device)."""
+    import torch
+
+    lib = N.lib()
+    cols = _Cols()
+    rows = result.rows
+    for i, name in enumerate(result.names):
+        dt, _, _ = result.column_info(i)
+        raw = torch.empty(max(rows, 1), dtype=_TORCH_DTYPE[np.dtype(dt)], device=device)
+        vbytes = torch.empty(max((rows + 7) // 8, 1), dtype=torch.uint8, device=device)
+        st = lib.dfc_result_copy_to_device(result.handle, i, raw.data_ptr(), vbytes.data_ptr())
+        if st != N.OK:
+            from .provider import _error
+
+            raise _error(st, N.last_error())
+        raw = raw[:rows]
+        if np.dtype(dt).itemsize == 8:
+            bits = raw.view(torch.int64)
+        elif np.dtype(dt) == np.float32:
+            bits = raw.view(torch.int32).to(torch.int64)
+        else:
+            bits = raw.to(torch.int64)
+            if np.dtype(dt).kind == "u":  # torch reads UInt16/UInt32 through signed views
+                bits &= (1 << (8 * np.dtype(dt).itemsize)) - 1
+        shifts = torch.arange(8, device=device, dtype=torch.uint8)
+        valid = ((vbytes.unsqueeze(1) >> shifts) & 1).reshape(-1)[:rows].bool()
+        cols.add(name, bits, valid, dt)
+    return cols
+
+
+def _torch_dtypes():
+    import torch
+
+    return {np.dtype(np.int8): torch.int8, np.dtype(np.int16): torch.int16, np.dtype(np.int32): torch.int32,
+            np.dtype(np.int64): torch.int64, np.dtype(np.uint8): torch.uint8, np.dtype(np.uint16): torch.int16,
+            np.dtype(np.uint32): torch.int32, np.dtype(np.uint64): torch.int64, np.dtype(np.float32): torch.float32,
+            np.dtype(np.float64): torch.float64}
+
+
+class _LazyDtypes(dict):
+    def __missing__(self, key):
+        self.update(_torch_dtypes())
+        return dict.__getitem__(self, key)
+
+
+_TORCH_DTYPE = _LazyDtypes()
+
+
+# ---------------------------------------------------------------------------
+# Keys: canonical words (every NaN one value, -0.0 == 0.0, a null key's word
+# 0 with its null flag), their hash to an owner rank, and the exchange.
+# ---------------------------------------------------------------------------
+_CANON_F64 = 0x7FF8000000000000
+_CANON_F32 = 0x7FC00000
+_MIX1 = -0x61C8864680B583EB  # 0x9E3779B97F4A7C15 as a signed 64-bit value
+_MIX2 = -0x40A7B892E31B1A47  # 0xBF58476D1CE4E5B9
+
+
+def _canonical(cols: _Cols, name: str):
+    import torch
+
+    bits, valid, dt = cols.bits[name], cols.valid[name], cols.dtype[name]
+    if dt == np.float64:
+        f = bits.view(torch.float64)
+        bits = torch.where(torch.isnan(f), torch.full_like(bits, _CANON_F64), torch.where(f == 0, torch.zeros_like(bits), bits))
+    elif dt == np.float32:
+        f = bits.to(torch.int32).view(torch.float32)
+        bits = torch.where(torch.isnan(f), torch.full_like(bits, _CANON_F32), torch.where(f == 0, torch.zeros_like(bits), bits))
+    return torch.where(valid, bits, torch.zeros_like(bits)), valid
+
+
+def _key_matrix(cols: _Cols, keys: list[str]):
+    """One row per partial row: the canonical key words and a null flag word."""
+    import torch
+
+    n = cols.rows()
+    words, nulls = [], torch.zeros(n, dtype=torch.int64, device=_device_of(cols))
+    for k, name in enumerate(keys):
+        w, valid = _canonical(cols, name)
+        words.append(w)
+        nulls |= (~valid).to(torch.int64) << k
+    return torch.stack(words + [nulls], dim=1) if words else nulls.unsqueeze(1)
+
+
+def _device_of(cols: _Cols):
+    return next(iter(cols.bits.values())).device
+
+
+def _owner(keymat, world: int):
+    """The rank owning each row's key: a multiply-xorshift hash of its words."""
+    import torch
+
+    h = torch.zeros(keymat.shape[0], dtype=torch.int64, device=keymat.device)
+    for j in range(keymat.shape[1]):
+        h = (h ^ keymat[:, j]) * _MIX1
+        h = h ^ ((h >> 31) & ((1 << 33) - 1))
+        h = h * _MIX2
+    return (h & 0x7FFFFFFFFFFFFFFF) % world
+
+
+def _exchange(cols: _Cols, keys: list[str], rank: int, world: int, group=None):
+    """Sends every partial row to its key's owner: returns the rows this rank
+    owns (in source-rank order, each rank's in its partial order) and their
+    positions (rank << 32 | index in the sender's partial result)."""
+    import torch
+    import torch.distributed as dist
+
+    dev = _device_of(cols)
+    n = cols.rows()
+    names = list(cols.bits)
+    pos = (torch.arange(n, dtype=torch.int64, device=dev) | (rank << 32))
+    owner = _owner(_key_matrix(cols, keys), world) if n else torch.zeros(0, dtype=torch.int64, device=dev)
+    order = torch.argsort(owner, stable=True)
+    counts = torch.bincount(owner, minlength=world).to(torch.int64)
+    validbits = torch.zeros(n, dtype=torch.int64, device=dev)
+    for i, c in enumerate(names):
+        validbits |= cols.valid[c].to(torch.int64) << i
+    mat = torch.stack([cols.bits[c] for c in names] + [validbits, pos], dim=1)[order].contiguous()
+    recv = torch.empty_like(counts)
+    dist.all_to_all_single(recv, counts, group=group)
+    out = torch.empty((int(recv.sum().item()), mat.shape[1]), dtype=torch.int64, device=dev)
+    dist.all_to_all_single(out, mat, recv.tolist(), counts.tolist(), group=group)
+    got = _Cols()
+    for i, c in enumerate(names):
+        got.add(c, out[:, i].contiguous(), ((out[:, len(names)] >> i) & 1).bool(), cols.dtype[c])
+    return got, out[:, len(names) + 1].contiguous()
+
+
+# ---------------------------------------------------------------------------
+# Owner merge (torch, on the owner's device).
+# ---------------------------------------------------------------------------
+def _overflow_message(input_dtype: np.dtype) -> str:
+    """The CPU provider's text (dataframe/aggregation/function.mojo:2798, 2914)."""
+    dt = np.dtype(input_dtype)
+    if dt == np.int64:
+        return "Int64 expression sum overflow"
+    sum_dt = np.dtype(np.int64) if dt.itemsize <= 2 and dt.kind in "iu" else dt
+    return f"{sum_dt.name} expression sum overflow"
+
+
+def _exact_sum(bits, inv, G: int, signed: bool):
+    """Exact per-group totals of 64-bit integers from their 32-bit halves
+    (each half's sum fits int64 for fewer than 2^31 rows): (high, low) with
+    total = high * 2^32 + low, low in [0, 2^32)."""
+    import torch
+
+    lo = bits & 0xFFFFFFFF
+    hi = (bits >> 32) if signed else ((bits >> 32) & 0xFFFFFFFF)
+    los = torch.zeros(G, dtype=torch.int64, device=bits.device).index_add_(0, inv, lo)
+    his = torch.zeros(G, dtype=torch.int64, device=bits.device).index_add_(0, inv, hi)
+    return his + (los >> 32), los & 0xFFFFFFFF
+
+
+def _merge_extreme(bits, valid, dt: np.dtype, inv, G: int, is_min: bool):
+    """Minimum (maximum) of the partial extrema per group: nulls skipped, NaN
+    only when every valid partial is NaN, a zero extremum keeps the sign of
+    the zeros seen (both signs: the CPU adjudicates)."""
+    import torch
+
+    from .provider import DataFaultError
+
+    dev = bits.device
+    red = "amin" if is_min else "amax"
+    anyvalid = torch.zeros(G, dtype=torch.int32, device=dev).scatter_reduce_(0, inv, valid.to(torch.int32), "amax")
+    if dt.kind == "f":
+        v = bits.view(torch.float64) if dt == np.float64 else bits.to(torch.int32).view(torch.float32).to(torch.float64)
+        finite = valid & ~torch.isnan(v)
+        fill = float("inf") if is_min else float("-inf")
+        x = torch.where(finite, v, torch.full_like(v, fill))
+        best = torch.full((G,), fill, dtype=torch.float64, device=dev).scatter_reduce_(0, inv, x, red)
+        has = torch.zeros(G, dtype=torch.int32, device=dev).scatter_reduce_(0, inv, finite.to(torch.int32), "amax") > 0
+        out = torch.where(has, best, torch.full_like(best, float("nan")))
+        zero = has & (best == 0)
+        if bool(zero.any()):
+            z = finite & (v == 0)
+            neg = (z & torch.signbit(v)).to(torch.int32)
+            pos = (z & ~torch.signbit(v)).to(torch.int32)
+            gneg = torch.zeros(G, dtype=torch.int32, device=dev).scatter_reduce_(0, inv, neg, "amax") > 0
+            gpos = torch.zeros(G, dtype=torch.int32, device=dev).scatter_reduce_(0, inv, pos, "amax") > 0
+            if bool((zero & gneg & gpos).any()):
+                raise DataFaultError(N.DATA_FAULT, "Mojo GPU data fault: mixed signed-zero extrema; the CPU adjudicates")
+            out = torch.where(zero & gneg, torch.full_like(out, -0.0), out)
+        if dt == np.float64:
+            obits = out.view(torch.int64)
+        else:
+            obits = out.to(torch.float32).view(torch.int32).to(torch.int64)
+        return obits, anyvalid > 0
+    if dt == np.uint64:
+        # Unsigned order through the sign-flipped bits.
+        x = torch.where(valid, bits ^ (-(1 << 63)), torch.full_like(bits, (1 << 63) - 1 if is_min else -(1 << 63)))
+        best = torch.full((G,), (1 << 63) - 1 if is_min else -(1 << 63), dtype=torch.int64, device=dev)
+        best = best.scatter_reduce_(0, inv, x, red)
+        return best ^ (-(1 << 63)), anyvalid > 0
+    info = np.iinfo(dt)
+    fill = int(info.max) if is_min else int(info.min)
+    x = torch.where(valid, bits, torch.full_like(bits, fill))
+    best = torch.full((G,), fill, dtype=torch.int64, device=dev).scatter_reduce_(0, inv, x, red)
+    return best, anyvalid > 0
+
+
+def _merge_owned(plan: Plan, cols: _Cols, pos, spec: dict, rows_name: str):
+    """The finished rows of the groups this rank owns: per output column
+    (int64 bits, valid, dtype), and each group's first position."""
+    import torch
+
+    from .provider import ProviderError
+
+    dev = pos.device
+    n = int(pos.shape[0])
+    src = plan.source
+    out_dtypes = _output_dtypes(plan)
+    if n == 0:
+        empty = torch.zeros(0, dtype=torch.int64, device=dev)
+        return [(empty, empty.bool(), dt) for dt in out_dtypes], empty
+    keymat = _key_matrix(cols, plan.keys)
+    _, inv = torch.unique(keymat, dim=0, return_inverse=True)
+    inv = inv.reshape(-1)
+    G = int(inv.max().item()) + 1
+    first = torch.full((G,), n, dtype=torch.int64, device=dev).scatter_reduce_(
+        0, inv, torch.arange(n, dtype=torch.int64, device=dev), "amin")
+    first_pos = pos[first]
+
+    def add(x, dtype=torch.int64):
+        return torch.zeros(G, dtype=dtype, device=dev).index_add_(0, inv, x)
+
+    out = [(cols.bits[k][first], cols.valid[k][first], cols.dtype[k]) for k in plan.keys]
     merged = {}
     for c, p in spec.items():
-        n = red_add(_cat(parts, p.count).values.astype(np.int64))
-        d = {"n": n}
+        d = {"n": add(cols.bits[p.count])}
+        ni = cols.bits[p.count].to(torch.float64)
         if p.mean is not None:
-            m = _cat(parts, p.mean)
-            ni = _cat(parts, p.count).values.astype(np.float64)
-            mv = np.where(_valid(m), m.values, 0.0)
-            d["fsum"] = red_add(mv * ni)
+            mv = torch.where(cols.valid[p.mean], cols.bits[p.mean].view(torch.float64), torch.zeros_like(ni))
+            d["fsum"] = add(mv * ni, torch.float64)
             if p.var0 is not None:
-                v0 = _cat(parts, p.var0)
-                mean = np.divide(d["fsum"], n, out=np.zeros(G), where=n > 0)
-                dev = mv - mean[gid]
-                m2i = np.where(_valid(v0), v0.values, 0.0) * ni + ni * dev * dev
-                d["m2"] = red_add(m2i)
-                d["mean"] = mean
+                mean = torch.where(d["n"] > 0, d["fsum"] / d["n"].clamp(min=1).to(torch.float64), torch.zeros_like(d["fsum"]))
+                dev_ = mv - mean[inv]
+                v0 = torch.where(cols.valid[p.var0], cols.bits[p.var0].view(torch.float64), torch.zeros_like(ni))
+                d["m2"] = add(v0 * ni + ni * dev_ * dev_, torch.float64)
         if p.isum is not None:
-            s = _cat(parts, p.isum)
-            vals = np.where(_valid(s), s.values, 0)
-            approx = red_add(vals.astype(np.float64))
-            exact = red_add(vals)
-            limit = 2.0**63 if vals.dtype == np.int64 else 2.0**64
-            if np.any(np.abs(approx) >= limit * (1 - 1e-12)):
-                raise ProviderError(N.DATA_OVERFLOW, f"{'Int64' if vals.dtype == np.int64 else 'UInt64'} expression sum overflow")
-            d["isum"] = exact
+            sdt = cols.dtype[p.isum]
+            bits = torch.where(cols.valid[p.isum], cols.bits[p.isum], torch.zeros_like(cols.bits[p.isum]))
+            hi, lo = _exact_sum(bits, inv, G, signed=sdt.kind == "i")
+            d["isum"] = (hi, lo, sdt)
         for side in ("lo", "hi"):
             name = getattr(p, side)
-            if name is None:
-                continue
-            s = _cat(parts, name)
-            d[side] = _merge_extreme(s, rows, starts, gid, side == "lo", DataFaultError)
+            if name is not None:
+                d[side] = _merge_extreme(cols.bits[name], cols.valid[name], cols.dtype[name], inv, G, side == "lo")
         if p.nulls is not None:
-            d["nulls"] = red_add(_cat(parts, p.nulls).values.astype(np.int64))
+            d["nulls"] = add(cols.bits[p.nulls])
         merged[c] = d
-    nrows = red_add(_cat(parts, rows_name).values.astype(np.int64))
-
-    src = plan.source
-    for a in plan.aggs:
+    nrows = add(cols.bits[rows_name])
+    true = torch.ones(G, dtype=torch.bool, device=dev)
+    for a, odt in zip(plan.aggs, out_dtypes[len(plan.keys):]):
         d = merged[a.column]
         idt = src.column(a.column).dtype
-        n = d["n"]
+        cnt = d["n"]
         if a.op == N.AGG_COUNT:
-            out_cols.append(Series(a.name, n.astype(np.int64)))
+            out.append((cnt, true, odt))
         elif a.op == N.AGG_LEN:
-            out_cols.append(Series(a.name, nrows.astype(np.int64)))
+            out.append((nrows, true, odt))
         elif a.op == N.AGG_NULL_COUNT:
-            out_cols.append(Series(a.name, d["nulls"].astype(np.int64)))
+            out.append((d["nulls"], true, odt))
         elif a.op == N.AGG_SUM:
-            valid = n >= a.min_count
+            valid = cnt >= a.min_count
             if idt.kind == "f":
-                vals = np.where(valid, d["fsum"], 0.0).astype(idt)
+                s = torch.where(valid, d["fsum"], torch.zeros_like(d["fsum"]))
+                bits = s.view(torch.int64) if odt == np.float64 else s.to(torch.float32).view(torch.int32).to(torch.int64)
             else:
-                vals = np.where(valid, d["isum"], 0)
-            out_cols.append(Series(a.name, vals, valid if not valid.all() else None))
+                hi, lo, sdt = d["isum"]
+                bits = _checked_total(hi, lo, sdt, valid, idt, ProviderError)
+            out.append((torch.where(valid, bits, torch.zeros_like(bits)), valid, odt))
         elif a.op == N.AGG_MEAN:
-            tot = d["fsum"] if idt.kind == "f" else d["isum"].astype(np.float64)
-            valid = n > 0
-            out_cols.append(Series(a.name, np.divide(tot, n, out=np.zeros(G), where=valid), valid))
+            valid = cnt > 0
+            if idt.kind == "f":
+                tot = d["fsum"]
+            else:
+                hi, lo, sdt = d["isum"]
+                tot = hi.to(torch.float64) * 4294967296.0 + lo.to(torch.float64)
+            m = torch.where(valid, tot / cnt.clamp(min=1).to(torch.float64), torch.zeros_like(tot))
+            out.append((m.view(torch.int64), valid, odt))
         elif a.op in (N.AGG_VAR, N.AGG_STD):
-            valid = n > a.ddof
-            var = np.divide(d["m2"], n - a.ddof, out=np.zeros(G), where=valid)
-            vals = np.sqrt(var) if a.op == N.AGG_STD else var
-            out_cols.append(Series(a.name, vals, valid))
+            valid = cnt > a.ddof
+            var = torch.where(valid, d["m2"] / (cnt - a.ddof).clamp(min=1).to(torch.float64), torch.zeros_like(d["m2"]))
+            v = torch.sqrt(var) if a.op == N.AGG_STD else var
+            out.append((v.view(torch.int64), valid, odt))
         elif a.op in (N.AGG_MIN, N.AGG_MAX):
-            vals, valid = d["lo" if a.op == N.AGG_MIN else "hi"]
-            out_cols.append(Series(a.name, vals, valid))
+            bits, valid = d["lo" if a.op == N.AGG_MIN else "hi"]
+            out.append((bits, valid, odt))
         else:
             raise ValueError(f"aggregation {a.op} is not supported in a sharded query")
-    return DataFrame(out_cols)
+    return out, first_pos
 
 
-def _merge_extreme(s: Series, rows, starts, gid, is_min: bool, fault):
-    """Minimum (or maximum) of the ranks' extrema per group: nulls skipped,
-    NaN only when every valid partial is NaN, on equal values the earliest
-    rank's kept; mixed signed zeros as the extreme are a data fault."""
-    G = len(starts)
-    valid = _valid(s)
-    v = s.values
-    if G == 0:
-        return v[:0], np.zeros(0, bool)
-    anyvalid = np.logical_or.reduceat(valid[rows], starts)
-    if v.dtype.kind == "f":
-        finite = valid & ~np.isnan(v)
-        fill = np.inf if is_min else -np.inf
-        x = np.where(finite, v, fill).astype(np.float64)
-        best = (np.minimum if is_min else np.maximum).reduceat(x[rows], starts)
-        has = np.logical_or.reduceat(finite[rows], starts)
-        out = np.where(has, best, np.nan).astype(v.dtype)
-        # Zero extremes: the earliest partial's sign, or a fault when both occur.
-        zero = has & (best == 0)
-        if zero.any():
-            z = finite & (v == 0)
-            neg = z & np.signbit(v)
-            pos = z & ~np.signbit(v)
-            gneg = np.logical_or.reduceat(neg[rows], starts)
-            gpos = np.logical_or.reduceat(pos[rows], starts)
-            if np.any(zero & gneg & gpos):
-                raise fault("Mojo GPU data fault: mixed signed-zero extrema; the CPU adjudicates")
-            out = np.where(zero & gneg, np.array(-0.0, v.dtype), out)
-        return out, anyvalid
-    info = np.iinfo(v.dtype)
-    fill = info.max if is_min else info.min
-    x = np.where(valid, v, fill).astype(v.dtype)
-    best = (np.minimum if is_min else np.maximum).reduceat(x[rows], starts)
-    return best.astype(v.dtype), anyvalid
+def _checked_total(hi, lo, sdt: np.dtype, valid, idt: np.dtype, error):
+    """The exact total's bits when it fits the sum type, else the CPU's
+    overflow error."""
+    import torch
+
+    if sdt.kind == "u":
+        ok = (hi >= 0) & (hi < (1 << 32)) if sdt.itemsize == 8 else (hi == 0)
+    else:
+        ok = (hi >= -(1 << 31)) & (hi < (1 << 31)) if sdt.itemsize == 8 else (
+            (hi == 0) & (lo < (1 << 31))) | ((hi == -1) & (lo >= (1 << 31)))
+    if bool((valid & ~ok).any()):
+        raise error(N.DATA_OVERFLOW, _overflow_message(idt))
+    return (hi << 32) | lo
 
 
+def _output_dtypes(plan: Plan) -> list[np.dtype]:
+    src = plan.source
+    out = [src.column(k).dtype for k in plan.keys]
+    for a in plan.aggs:
+        idt = src.column(a.column).dtype
+        if a.op in (N.AGG_COUNT, N.AGG_LEN, N.AGG_NULL_COUNT):
+            out.append(np.dtype(np.int64))
+        elif a.op == N.AGG_SUM:
+            out.append(idt if idt.kind == "f" or idt.itemsize >= 4 else np.dtype(np.int64))
+        elif a.op in (N.AGG_MIN, N.AGG_MAX):
+            out.append(idt)
+        else:
+            out.append(np.dtype(np.float64))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Order and assembly.
+# ---------------------------------------------------------------------------
+def _pack(columns, first_pos):
+    """One int64 matrix per owner: the output columns' bits, a word of their
+    validity bits and each group's first position."""
+    import torch
+
+    validbits = torch.zeros(first_pos.shape[0], dtype=torch.int64, device=first_pos.device)
+    for i, (_, valid, _) in enumerate(columns):
+        validbits |= valid.to(torch.int64) << i
+    return torch.stack([b for b, _, _ in columns] + [validbits, first_pos], dim=1)
+
+
+def _assemble(plan: Plan, mat, dtypes) -> DataFrame:
+    """The host frame of the finished rows, ordered by first position."""
+    import torch
+
+    mat = mat[torch.argsort(mat[:, -1])]
+    host = mat.cpu().numpy()
+    names = list(plan.keys) + [a.name for a in plan.aggs]
+    width = len(names)
+    cols = []
+    for i, (name, dt) in enumerate(zip(names, dtypes)):
+        valid = ((host[:, width] >> i) & 1).astype(bool)
+        cols.append(Series(name, _decode_np(host[:, i], dt), None if valid.all() else valid))
+    return DataFrame(cols)
+
+
+def _gather_ordered(plan: Plan, columns, first_pos, group=None) -> DataFrame:
+    """Every owner's finished rows on every rank (one all_gather of the
+    packed matrices, padded to the largest), ordered by first position."""
+    import torch
+    import torch.distributed as dist
+
+    mat = _pack(columns, first_pos).contiguous()
+    dev = mat.device
+    world = dist.get_world_size(group)
+    n = torch.tensor([mat.shape[0]], dtype=torch.int64, device=dev)
+    sizes = [torch.zeros_like(n) for _ in range(world)]
+    dist.all_gather(sizes, n, group=group)
+    sizes = [int(s.item()) for s in sizes]
+    pad = torch.zeros((max(max(sizes), 1), mat.shape[1]), dtype=torch.int64, device=dev)
+    pad[: mat.shape[0]] = mat
+    bufs = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(bufs, pad, group=group)
+    return _assemble(plan, torch.cat([b[:s] for b, s in zip(bufs, sizes)]), [dt for _, _, dt in columns])
+
+
+def _take(cols: _Cols, idx) -> _Cols:
+    out = _Cols()
+    for c in cols.bits:
+        out.add(c, cols.bits[c][idx], cols.valid[c][idx], cols.dtype[c])
+    return out
+
+
+def _concat(parts: list[_Cols]) -> _Cols:
+    import torch
+
+    out = _Cols()
+    for c in parts[0].bits:
+        out.add(c, torch.cat([p.bits[c] for p in parts]), torch.cat([p.valid[c] for p in parts]), parts[0].dtype[c])
+    return out
+
+
+def _check_shardable(plan: Plan) -> None:
+    if plan.keys is None or not plan.keys or plan.aggs is None:
+        raise ValueError("a sharded query is a group-by with at least one key")
+    src = plan.source
+    for name in set(plan.keys) | {a.column for a in plan.aggs}:
+        s = src.column(name)
+        if s.is_string or s.is_categorical:
+            raise ValueError(f"column {name!r}: a sharded query reads numeric columns")
+    if len(plan.keys) + len(plan.aggs) > 62:
+        raise ValueError("a sharded query has at most 62 output columns")
+
+
+# ---------------------------------------------------------------------------
+# Entry points.
+# ---------------------------------------------------------------------------
 def split_rows(frame: DataFrame, world: int) -> list[DataFrame]:
     """Contiguous row ranges, one per rank."""
     bounds = np.linspace(0, frame.height, world + 1).astype(np.int64)
@@ -259,21 +560,68 @@ def split_rows(frame: DataFrame, world: int) -> list[DataFrame]:
     return out
 
 
-def execute_sharded(lazy: LazyFrame | Plan, rank: int, world: int, run=None, group=None) -> DataFrame:
-    """The query over all ranks' rows: this rank aggregates its contiguous
-    share of `lazy`'s source frame with `run` (default: the device provider),
-    the partial results are all-gathered, and every rank merges them."""
-    import torch.distributed as dist
+def merge_partials(plan: Plan, parts: list, spec: dict, rows_name: str, owners: int | None = None,
+                   device=None) -> DataFrame:
+    """The query's result from the ranks' partial results in one process:
+    `parts` in rank order, host DataFrames or DeviceResults (read on their
+    device).  The rows are routed to `owners` owners (default one per part)
+    by the exchange's key hash, each owner's rows merged as that rank would,
+    and the finished rows ordered by first position."""
+    import torch
+
+    from .provider import DeviceResult
+
+    _check_shardable(plan)
+    if device is None:
+        on_gpu = [p for p in parts if isinstance(p, DeviceResult)]
+        device = torch.device("cuda", on_gpu[0].device) if on_gpu else torch.device("cpu")
+    cols, pos = [], []
+    for r, p in enumerate(parts):
+        c = _result_cols(p, device) if isinstance(p, DeviceResult) else _frame_cols(p, device)
+        cols.append(c)
+        pos.append(torch.arange(c.rows(), dtype=torch.int64, device=device) | (r << 32))
+    allc, allpos = _concat(cols), torch.cat(pos)
+    owners = len(parts) if owners is None else owners
+    owner = _owner(_key_matrix(allc, plan.keys), owners)
+    mats, dtypes = [], _output_dtypes(plan)
+    for o in range(owners):
+        idx = torch.nonzero(owner == o).reshape(-1)
+        columns, first_pos = _merge_owned(plan, _take(allc, idx), allpos[idx], spec, rows_name)
+        mats.append(_pack(columns, first_pos))
+    return _assemble(plan, torch.cat(mats), dtypes)
+
+
+def execute_sharded(lazy: LazyFrame | Plan, rank: int, world: int, run=None, group=None, device=None) -> DataFrame:
+    """The query over all ranks' rows, called by every rank of `group`:
+    this rank aggregates its contiguous share of the source frame -- on its
+    GPU (`device`, default torch's current CUDA device) with the result kept
+    there, or with `run(plan) -> DataFrame` (tests: the oracle, on CPU
+    tensors) -- the partial rows go to their keys' owners, each owner merges
+    its groups, and every rank returns the whole result."""
+    import torch
 
     plan = lazy.plan if isinstance(lazy, LazyFrame) else lazy
+    _check_shardable(plan)
     part = split_rows(plan.source, world)[rank]
     sub, spec, rows_name = partial_plan(plan, part)
     if run is None:
-        from .provider import execute
+        from .frame import bind
+        from .provider import DeviceColumn, _regime_flags, run_bound
 
-        def run(p):
-            return execute(p)[0]
-    mine = run(sub)
-    gathered = [None] * world
-    dist.all_gather_object(gathered, mine, group=group)
-    return merge_partials(plan, gathered, spec, rows_name)
+        index = torch.cuda.current_device() if device is None else int(device)
+        bound = bind(sub)
+        inputs = [DeviceColumn(s, index) for s in bound.series]
+        try:
+            result = run_bound(bound, inputs, flags=_regime_flags())
+            try:
+                cols = _result_cols(result, torch.device("cuda", index))
+            finally:
+                result.free()
+        finally:
+            for c in inputs:
+                c.release()
+    else:
+        cols = _frame_cols(run(sub), torch.device("cpu") if device is None else device)
+    got, pos = _exchange(cols, plan.keys, rank, world, group)
+    columns, first_pos = _merge_owned(plan, got, pos, spec, rows_name)
+    return _gather_ordered(plan, columns, first_pos, group)

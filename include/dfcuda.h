@@ -390,6 +390,11 @@ DFC_API dfc_status dfc_result_column(const dfc_result* result, int32_t i, dfc_dt
  * (all ones when the column has no nulls). */
 DFC_API dfc_status dfc_result_copy_to_host(const dfc_result* result, int32_t i, void* values,
                                            uint8_t* validity);
+/* The same into device memory of the result's device (a following device
+ * step's buffers, e.g. the sharded group-by's exchange): device-to-device
+ * copies, waited for. */
+DFC_API dfc_status dfc_result_copy_to_device(const dfc_result* result, int32_t i, void* values,
+                                             uint8_t* validity);
 DFC_API void dfc_result_free(dfc_result* result);
 
 /* Residence callbacks in the shape of the reference's _DeviceResidence

@@ -45,6 +45,7 @@ DISTINCT = 1_000_000
 ZIPF_S = 1.1
 CODES = 64
 BYTES_PER_ROW = 4 + 4 + 8 + 4 + 1 / 8  # k1, k2, v, p, v's validity bit
+COUNT_BYTES_PER_ROW = 4 + 4 + 4  # the counting pass reads the keys and the filter column
 METRIC = "group-by rows/s"
 WORKLOAD = (
     "100M-row filtered group-by: keys (Int32 Zipf s=1.1 over 1M, UInt32 codes of 64), "
@@ -176,14 +177,67 @@ class Clocks:
         }
 
 
-def traffic_per_launch() -> float | None:
-    """DRAM bytes of one scan launch from the committed ncu summary, if any."""
-    p = ROOT / "profiles" / "scan_kernel_traffic.json"
+def traffic_per_launch(kernel: str) -> float | None:
+    """DRAM bytes of one full-size launch of `kernel` from the committed ncu
+    summaries (a smaller capture scaled by rows), if any."""
+    p = ROOT / "profiles" / "kernel_traffic.json"
     try:
-        d = json.loads(p.read_text())
-        return float(d["dram_bytes_per_full_launch"])
+        return float(json.loads(p.read_text())[kernel]["dram_bytes_per_full_launch"])
     except Exception:
         return None
+
+
+def roofline_of(step_t: list[dict], rows: int) -> dict:
+    """HBM roofline from the library's CUDA-event timings of the timed steps.
+
+    Radix-partitioned regime, per pass (algorithmic bytes per launch):
+    counting pass rows x 12 B (keys and filter column); placement (pass A)
+    rows x 20.125 B read + kept rows x placed row bytes written; aggregation
+    (pass B) kept rows x placed row bytes read (the groups' records, about
+    groups x 64 B, left out).  The dominant pass is the roofline's kernel;
+    "query" is the single-pass minimum (rows x 20.125 B) over the query's
+    whole device time.  Table regimes: one scan kernel, rows x 20.125 B."""
+    peak, peak_kind = measured_hbm_gbs()
+
+    def mean_s(k):
+        return float(np.mean([t[k] for t in step_t])) * 1e-9
+
+    last = step_t[-1]
+    in_bytes = rows * BYTES_PER_ROW
+    if last["regime"] == 2:
+        kept, rb = last["kept_rows"], last["placed_row_bytes"]
+        passes = {
+            "partition_count": (rows * COUNT_BYTES_PER_ROW, mean_s("count_ns")),
+            "partition_kernel": (in_bytes + kept * rb, mean_s("place_ns")),
+            "partition_aggregate": (kept * rb, mean_s("aggregate_ns")),
+        }
+        extra = {"kept_rows": kept, "placed_row_bytes": rb, "partitions": last["partitions"]}
+    else:
+        passes = {"scan_kernel": (in_bytes, mean_s("scan_ns"))}
+        extra = {}
+    dominant = max(passes, key=lambda k: passes[k][1])
+    b, s = passes[dominant]
+    achieved = b / s / 1e9
+    query_s = mean_s("scan_ns") + mean_s("aggregate_ns") + mean_s("finish_ns")
+    return {
+        "bound": "hbm",
+        "kernel": dominant,
+        "achieved": achieved,
+        "peak": peak,
+        "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+        "unit": "GB/s",
+        "frac": achieved / peak,
+        "traffic": traffic_per_launch(dominant),
+        "algorithmic_bytes": b,
+        "kernel_ms": s * 1e3,
+        "regime": ["global table", "shared-memory tables", "radix-partitioned"][last["regime"]],
+        "passes": {k: {"algorithmic_bytes": pb, "ms": ps * 1e3, "gbs": pb / ps / 1e9, "frac": pb / ps / 1e9 / peak,
+                       "traffic": traffic_per_launch(k)} for k, (pb, ps) in passes.items()},
+        "finish_ms": mean_s("finish_ns") * 1e3,
+        "query": {"single_pass_bytes": in_bytes, "device_ms": query_s * 1e3, "gbs": in_bytes / query_s / 1e9,
+                  "frac": in_bytes / query_s / 1e9 / peak},
+        **extra,
+    }
 
 
 def cpu_baseline(frame_np, sample_rows: int, threads: int) -> dict:
@@ -734,7 +788,7 @@ def main() -> int:
     torch.cuda.synchronize()
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
-    scan_ns = []
+    step_t = []
     launches = 0
     start.record(stream)
     for _ in range(args.steps):
@@ -743,7 +797,7 @@ def main() -> int:
         # the memory pool at a steady size.
         r = step()
         t = provider.last_timings()
-        scan_ns.append(t["scan_ns"])
+        step_t.append(t)
         launches += t["launches"]
         r.free()
     end.record(stream)
@@ -758,23 +812,7 @@ def main() -> int:
     ms_max = float(ms_t.item())
     value = rows * world / (ms_max * 1e-3)
 
-    # Roofline of the scan kernel: algorithmic bytes / its event-timed duration.
-    peak, peak_kind = measured_hbm_gbs()
-    scan_s = float(np.mean(scan_ns)) * 1e-9
-    algo_bytes = rows * BYTES_PER_ROW
-    achieved = algo_bytes / scan_s / 1e9
-    roofline = {
-        "bound": "hbm",
-        "kernel": "scan_kernel_global",
-        "achieved": achieved,
-        "peak": peak,
-        "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-        "unit": "GB/s",
-        "frac": achieved / peak,
-        "traffic": traffic_per_launch(),
-        "algorithmic_bytes": algo_bytes,
-        "scan_ms": scan_s * 1e3,
-    }
+    roofline = roofline_of(step_t, rows)
 
     # End to end through the C ABI with host buffers (pinned).
     host = {n: cols[n].cpu().pin_memory() for n in ("k1", "k2", "v", "p")}

@@ -102,6 +102,8 @@ class Timings(C.Structure):
         ("compensated", C.c_int32),
         ("count_ns", C.c_double),
         ("place_ns", C.c_double),
+        ("kept_rows", C.c_uint64),
+        ("placed_row_bytes", C.c_uint64),
     ]
 
 

@@ -1180,7 +1180,8 @@ struct Control {
   uint32_t overflow_agg;
   uint32_t alloc;
   uint32_t part_next;
-  uint32_t pad[4];
+  uint32_t part_kept;  // radix-partitioned regime: rows the filter kept (the counting pass's total)
+  uint32_t pad[3];
   uint32_t has_nulls[kMaxOut];
 };
 
@@ -1485,6 +1486,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
     sp.part_order = static_cast<uint32_t*>(part_order);
     sp.agg_slots = pp->agg_slots;
     sp.part_next = &dctl->part_next;
+    sp.part_kept = &dctl->part_kept;
   }
 
   cudaEvent_t* ev = attempt_events(P.device);
@@ -1578,6 +1580,8 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   if (pp) {
     t_timings.count_ns += ms_count * 1e6;
     t_timings.place_ns += (ms_scan - ms_count - ms_offsets) * 1e6;
+    t_timings.kept_rows = host_ctl->part_kept;
+    t_timings.placed_row_bytes = 8u * pp->words;
   }
   if (getenv("DFC_TRACE")) {
     fprintf(stderr,

@@ -1868,6 +1868,7 @@ __global__ void __launch_bounds__(1024) partition_offsets(const __grid_constant_
     uint32_t t = 0;
     for (int w = 0; w < (int)(blockDim.x / 32); ++w) t += s_warp[w];
     s_total = t;
+    *p.part_kept = t;
   }
   uint32_t run = before + x - sum;
   for (uint32_t k = 0; k < per; ++k) {

@@ -471,6 +471,8 @@ def last_timings() -> dict:
         "compensated": int(t.compensated),
         "count_ns": t.count_ns,
         "place_ns": t.place_ns,
+        "kept_rows": int(t.kept_rows),
+        "placed_row_bytes": int(t.placed_row_bytes),
     }
 
 

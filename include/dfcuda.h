@@ -425,6 +425,8 @@ typedef struct dfc_timings {
   int32_t compensated;  /* value fields accumulated as compensated FP32 partials (bit per field) */
   double count_ns;      /* radix-partitioned regime: the counting pass (part of scan_ns) */
   double place_ns;      /* radix-partitioned regime: the pass placing rows into partitions (part of scan_ns) */
+  uint64_t kept_rows;        /* radix-partitioned regime: rows the filter kept (each placed once) */
+  uint64_t placed_row_bytes; /* radix-partitioned regime: bytes of one placed row */
 } dfc_timings;
 DFC_API dfc_status dfc_last_timings(dfc_timings* out);
 

@@ -1730,6 +1730,14 @@ DFC_API dfc_status dfc_column_register(int32_t device, dfc_dtype dtype, uint64_t
     return fail(DFC_INVALID, "DFC_COLUMN_DEVICE values and validity must be device memory of the column's device "
                              "(host, managed or another GPU's memory is not accepted)");
   DeviceGuard guard(device);
+  if (flags == DFC_COLUMN_DEVICE && rows > 0) {
+    // A borrowed column may have been written on any stream of the device,
+    // none of which orders before this thread's non-blocking stream (the
+    // validity bitmap is read here, the values by later queries): wait for
+    // the device's queued work first.
+    const cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_fail(e, "device column producer");
+  }
   cudaStream_t stream = thread_stream(device);
   auto* c = new dfc_column();
   c->serial = ++g_column_serial;

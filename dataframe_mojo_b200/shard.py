@@ -155,6 +155,9 @@ def _result_cols(result, device) -> _Cols:
         dt, _, _ = result.column_info(i)
         raw = torch.empty(max(rows, 1), dtype=_TORCH_DTYPE[np.dtype(dt)], device=device)
         vbytes = torch.empty(max((rows + 7) // 8, 1), dtype=torch.uint8, device=device)
+        # The library copies on its own stream: torch's queued work on these
+        # blocks (they may be reused) completes first.
+        torch.cuda.current_stream(device).synchronize()
         st = lib.dfc_result_copy_to_device(result.handle, i, raw.data_ptr(), vbytes.data_ptr())
         if st != N.OK:
             from .provider import _error

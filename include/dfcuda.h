@@ -139,7 +139,10 @@ DFC_API dfc_status dfc_set_memory_limit(int32_t device, int64_t bytes);
  * and keeps alive until dfc_column_release; only the validity bitmap is
  * copied (normalised).  Both must be device memory of `device`
  * (cudaPointerGetAttributes): host, managed or another GPU's memory is
- * rejected with DFC_INVALID. */
+ * rejected with DFC_INVALID.  Registration first waits for the device's
+ * queued work (cudaDeviceSynchronize), so values written on any stream
+ * before the call are the ones read; writes after it must be ordered before
+ * the query's stream (dfc_query.stream) by the caller. */
 #define DFC_COLUMN_DEVICE 1u
 
 /* validity may be NULL (every row valid).  validity_bit_offset is the bit

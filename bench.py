@@ -266,9 +266,20 @@ def cpu_baseline(frame_np, sample_rows: int, threads: int) -> dict:
         "value": sample_rows / t,
         "unit": "rows/s",
         "cores": threads,
+        "physical_cores": physical_cores(),
         "kind": "port",
         "sample": f"first {sample_rows:,} rows of the workload, median of 3 runs, {t:.3f} s each",
     }
+
+
+def physical_cores() -> int | None:
+    """Physical cores of the host (the threads used may count SMT siblings)."""
+    try:
+        import psutil
+
+        return psutil.cpu_count(logical=False)
+    except Exception:
+        return None
 
 
 def host_numpy(cols):
@@ -330,6 +341,7 @@ def run_reference(args, rank: int, world: int) -> int:
             "value": value,
             "unit": "rows/s",
             "cores": threads,
+            "physical_cores": physical_cores(),
             "kind": "port",
             "sample": f"{rows:,} rows of the workload per step (the full 100M-row query does not fit a few-minute run)",
         },
@@ -435,12 +447,23 @@ def batched_form(device: str, nq: int) -> dict:
     from dataframe_mojo_b200 import _native as native
     from dataframe_mojo_b200 import provider
 
-    jobs, keep, total, _ = batched_jobs(device, nq)
+    jobs, keep, total, info = batched_jobs(device, nq)
+    # Where the plain path's time goes, by query size: the library's device
+    # time (scan, aggregation and finish events) and the host's per query.
+    account = {k: {"queries": 0, "rows": 0, "device_ms": 0.0, "wall_ms": 0.0}
+               for k in ("over_1M_rows", "1M_rows_or_fewer")}
 
     def plain():
-        for bd, cl in jobs:
+        for (bd, cl), (rows, _, _) in zip(jobs, info):
+            t0 = time.perf_counter()
             r = provider.run_bound(bd, cl)
+            t = provider.last_timings()
             r.free()
+            a = account["over_1M_rows" if rows > 1_000_000 else "1M_rows_or_fewer"]
+            a["queries"] += 1
+            a["rows"] += rows
+            a["device_ms"] += (t["scan_ns"] + t["aggregate_ns"] + t["finish_ns"]) * 1e-6
+            a["wall_ms"] += (time.perf_counter() - t0) * 1e3
 
     def batched():
         for r in provider.run_batch(jobs):
@@ -450,6 +473,9 @@ def batched_form(device: str, nq: int) -> dict:
 
     times = {}
     for name, fn in (("plain", plain), ("batched", batched), ("plain", plain), ("batched", batched)):
+        if name == "plain":
+            for a in account.values():
+                a.update(queries=0, rows=0, device_ms=0.0, wall_ms=0.0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         fn()
@@ -468,6 +494,7 @@ def batched_form(device: str, nq: int) -> dict:
         "plain_rows_per_s": total / times["plain"],
         "batched_rows_per_s": total / times["batched"],
         "speedup": times["plain"] / times["batched"],
+        "plain_account": account,
     }
 
 
@@ -538,10 +565,10 @@ def served_form(device: str, nreq: int, rate: float = 2000.0, inflight: int = 32
         except provider.DataFaultError:
             pass
 
-    def plain():
+    def plain(arrivals, n):
         lat = []
         t0 = time.perf_counter()
-        for (bound, cl), at in zip(reqs, arrivals):
+        for (bound, cl), at in zip(reqs[:n], arrivals[:n]):
             while time.perf_counter() - t0 < at:
                 pass
             try:
@@ -551,18 +578,18 @@ def served_form(device: str, nreq: int, rate: float = 2000.0, inflight: int = 32
             lat.append(time.perf_counter() - t0 - at)
         return np.array(lat), time.perf_counter() - t0
 
-    def served():
+    def served(arrivals, n):
         server = provider.Server(max_inflight=inflight)
         lat = {}
         t0 = time.perf_counter()
         i = 0
-        while len(lat) < nreq:
+        while len(lat) < n:
             now = time.perf_counter() - t0
-            while i < nreq and arrivals[i] <= now:
+            while i < n and arrivals[i] <= now:
                 server.submit(reqs[i][0], reqs[i][1], i)
                 i += 1
             # Wait briefly for completions once every request is submitted.
-            for tag, res, _, _ in server.poll(wait_ms=0 if i < nreq else 2):
+            for tag, res, _, _ in server.poll(wait_ms=0 if i < n else 2):
                 if isinstance(res, provider.DataFaultError):
                     pass  # answered: the core adjudicates such a query on the CPU
                 elif isinstance(res, Exception):
@@ -572,10 +599,24 @@ def served_form(device: str, nreq: int, rate: float = 2000.0, inflight: int = 32
                 lat[tag] = time.perf_counter() - t0 - arrivals[tag]
         span = time.perf_counter() - t0
         server.close()
-        return np.array([lat[j] for j in range(nreq)]), span
+        return np.array([lat[j] for j in range(n)]), span
 
-    lp, sp_ = plain()
-    ls, ss = served()
+    def pct(lat):
+        return {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3)}
+
+    lp, sp_ = plain(arrivals, nreq)
+    ls, ss = served(arrivals, nreq)
+    # Latency under load: the first requests again, their Poisson arrivals
+    # rescaled to 50%, 80% and 100% of the served path's saturated rate.
+    capacity = nreq / ss
+    n_load = min(nreq, 150)
+    loads = {}
+    for frac in (0.5, 0.8, 1.0):
+        arr = np.asarray(arrivals[:n_load]) * (rate / (frac * capacity))
+        lpl, _ = plain(arr, n_load)
+        lsl, _ = served(arr, n_load)
+        loads[f"{int(frac * 100)}%"] = {"arrivals_per_s": frac * capacity, "requests": n_load,
+                                        "plain": pct(lpl), "served": pct(lsl)}
     for c, vb, hs in tables:
         for h in hs.values():
             native.lib().dfc_column_release(h.handle)
@@ -588,7 +629,90 @@ def served_form(device: str, nreq: int, rate: float = 2000.0, inflight: int = 32
         "served": {"p50_ms": float(np.percentile(ls, 50) * 1e3), "p99_ms": float(np.percentile(ls, 99) * 1e3),
                    "queries_per_s": nreq / ss},
         "throughput_ratio": (nreq / ss) / (nreq / sp_),
+        "latency_under_load": loads,
     }
+
+
+# The reference's published filtered sums (benchmarks/bench_handoff.mojo,
+# docs/apple-metal.md:453-457): 50M rows on an M1 Mac mini, best of 5 warm
+# collects, (CPU executor on 8 threads, Metal hand-off reading the column in
+# place) in ms.
+HANDOFF_PUBLISHED_MS = {"int32": (23.2, 9.4), "float32": (14.0, 9.7), "int64": (17.1, 16.5)}
+
+
+def handoff_values(dtype: str, rows: int, device: str):
+    """bench_handoff's column: x = (row * 7919) % spread - spread // 2, spread
+    7 for Int32 (so the filtered sum of any size fits Int32) and 2001 else."""
+    import torch
+
+    spread = 7 if dtype == "int32" else 2001
+    r = torch.arange(rows, dtype=torch.int64, device=device)
+    x = (r * 7919) % spread - spread // 2
+    return x.to({"int32": torch.int32, "float32": torch.float32, "int64": torch.int64}[dtype])
+
+
+def handoff_plan(frame_like):
+    from dataframe_mojo_b200.frame import col
+
+    return frame_like.lazy().filter(col("x") > 0).select(col("x").sum())
+
+
+def handoff_form(device: str, rows: int = 50_000_000, reps: int = 20) -> dict:
+    """The reference's published workload: filter(x > 0).select(x.sum()) over
+    one 50M-row column of each type.  `ms`: one query over the column
+    resident in HBM (the discrete-GPU form of reading it in place), CUDA
+    events around `reps` queries after 3 warm-ups; `e2e_ms`: the same from a
+    pinned host buffer (registration copy, query, result copy).  Best of the
+    reps, as the reference reports; the mean beside it."""
+    import torch
+
+    from dataframe_mojo_b200 import _native as native
+    from dataframe_mojo_b200 import provider
+    from dataframe_mojo_b200.frame import DataFrame, Series, bind
+
+    out = {}
+    codes = {"int32": (native.INT32, np.int32), "float32": (native.FLOAT32, np.float32),
+             "int64": (native.INT64, np.int64)}
+    stream = torch.cuda.Stream()
+    for name, (code, npdt) in codes.items():
+        x = handoff_values(name, rows, device)
+        torch.cuda.synchronize()
+        h = _register(x, code, rows)
+        bound = bind(handoff_plan(DataFrame([Series("x", np.zeros(1, npdt))])).plan)
+        cols = [h]
+        for _ in range(3):
+            provider.run_bound(bound, cols, stream=stream.cuda_stream).free()
+        times = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = provider.run_bound(bound, cols, stream=stream.cuda_stream)
+            e1.record(stream)
+            r.free()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        host = x.cpu().pin_memory()
+        e2e = []
+        for i in range(reps // 2 + 1):
+            t0 = time.perf_counter()
+            dc = provider.DeviceColumn.from_host_pointer("x", npdt, rows, host.data_ptr(), None, 0, 0)
+            r = provider.run_bound(bound, [dc])
+            total = r.to_frame().column(r.names[0]).values[0]
+            r.free()
+            dc.release()
+            if i:
+                e2e.append((time.perf_counter() - t0) * 1e3)
+        native.lib().dfc_column_release(h.handle)
+        cpu_ms, metal_ms = HANDOFF_PUBLISHED_MS[name]
+        best = float(min(times))
+        out[name] = {"ms": best, "mean_ms": float(np.mean(times)), "e2e_ms": float(min(e2e)),
+                     "gbs": rows * np.dtype(npdt).itemsize / best / 1e6, "sum": float(total),
+                     "published_m1_cpu_ms": cpu_ms, "published_m1_metal_ms": metal_ms,
+                     "vs_published_metal": metal_ms / best, "vs_published_cpu": cpu_ms / best}
+        del x, host
+        torch.cuda.empty_cache()
+    return {"config": f"filter(x > 0).select(x.sum()), {rows:,} rows per column (benchmarks/bench_handoff.mojo)",
+            "by_dtype": out}
 
 
 def precision_form(device: str, rows: int, reps: int = 5) -> dict:
@@ -695,7 +819,9 @@ def main() -> int:
     ap.add_argument("--served-requests", type=int, default=400, help="served form: requests (0: skip)")
     ap.add_argument("--served-inflight", type=int, default=32, help="served form: requests in flight at most")
     ap.add_argument("--precision-rows", type=int, default=100_000_000, help="precision form: rows (0: skip)")
-    ap.add_argument("--only", choices=["precision", "batched", "served"],
+    ap.add_argument("--handoff-rows", type=int, default=50_000_000,
+                    help="the reference's published filtered sums: rows per column (0: skip)")
+    ap.add_argument("--only", choices=["precision", "batched", "served", "handoff"],
                     help="run one configuration form alone and print its JSON object (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -708,6 +834,8 @@ def main() -> int:
             out = precision_form("cuda:0", args.precision_rows)
         elif args.only == "batched":
             out = batched_form("cuda:0", args.batch_queries)
+        elif args.only == "handoff":
+            out = handoff_form("cuda:0", args.handoff_rows)
         else:
             out = served_form("cuda:0", args.served_requests, inflight=args.served_inflight)
         print(json.dumps(out), flush=True)
@@ -909,7 +1037,7 @@ def main() -> int:
         lib.dfc_column_release(h)
     del cols
     torch.cuda.empty_cache()
-    batched = served = precision = None
+    batched = served = precision = handoff = None
     if world == 1 and args.precision_rows > 0:
         precision = precision_form(f"cuda:{local}", args.precision_rows)
         torch.cuda.empty_cache()
@@ -918,6 +1046,9 @@ def main() -> int:
         torch.cuda.empty_cache()
     if world == 1 and args.served_requests > 0:
         served = served_form(f"cuda:{local}", args.served_requests, inflight=args.served_inflight)
+        torch.cuda.empty_cache()
+    if world == 1 and args.handoff_rows > 0:
+        handoff = handoff_form(f"cuda:{local}", args.handoff_rows)
         torch.cuda.empty_cache()
     if world > 1:
         dist.barrier()
@@ -955,6 +1086,8 @@ def main() -> int:
             line["batched"] = batched
         if served is not None:
             line["served"] = served
+        if handoff is not None:
+            line["handoff"] = handoff
         print(json.dumps(line), flush=True)
     return 0
 

@@ -1219,8 +1219,11 @@ bool plan_partitions(const Plan& P, const DeviceState* ds, uint64_t est, PartPla
   const size_t rs = (size_t)sp.rec_stride + 8;  // the shared-memory record stride (scan.cu agg_stride)
   const double groups = (double)std::max<uint64_t>(est, 1);
   // Slots of a table in `bytes` (any count, a multiple of 32), besides the
-  // record of the all-ones key word.
-  auto slots_in = [&](size_t bytes) { return bytes / rs > 0 ? (uint64_t)(bytes / rs - 1) & ~(uint64_t)31 : 0ull; };
+  // record of the all-ones key word; each slot also takes a 4-byte entry of
+  // the claimed-slot list.
+  auto slots_in = [&](size_t bytes) {
+    return bytes > rs ? (uint64_t)((bytes - rs) / (rs + 4)) & ~(uint64_t)31 : 0ull;
+  };
   // DFC_PART_MIN_BITS=<n> raises the least partition count (tuning).
   if (const char* env = getenv("DFC_PART_MIN_BITS"))
     if (atoi(env) > 0) min_bits = std::max<uint32_t>(min_bits, (uint32_t)atoi(env));
@@ -1242,7 +1245,7 @@ bool plan_partitions(const Plan& P, const DeviceState* ds, uint64_t est, PartPla
     return false;
   pp.bits = bits;
   pp.agg_slots = (uint32_t)slots;
-  pp.agg_smem = (slots + 1) * rs;
+  pp.agg_smem = (slots + 1) * rs + slots * 4;
   pp.agg_ctas = (uint64_t)ds->sms * (two ? 2 : 1);
   // Counting pass: a ring of the key and filter columns only (they hold the
   // first bytes of every stage), then one counter per partition.

@@ -2053,7 +2053,8 @@ __global__ void __launch_bounds__(kPartThreads, 1) partition_kernel_quad(const _
 // bank pair (a 64-byte stride put all of a warp's accesses to one field in
 // two banks).  A row finds its record by linear probing from a hash of its
 // key word (independent of the partition hash).  A record is live once a row
-// set its first row.
+// set its first row; every claimed slot is, and claims append their slot to
+// a list after the table (S entries), so the copy-out visits only them.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ size_t agg_stride(const ScanParams& p) { return (size_t)p.rec_stride + 8; }
 
@@ -2066,8 +2067,8 @@ __device__ __forceinline__ void reset_record(unsigned char* rec, size_t rs) {
 // The shared-memory record of key word `kw` (claimed if new); false when the
 // table is seven-eighths full and the key is not in it.  Below that fill a
 // free slot always exists, so the probe ends within agg_slots steps.
-__device__ __forceinline__ bool agg_probe(const ScanParams& p, unsigned char* table, uint32_t* used, uint64_t kw,
-                                          unsigned char*& rec) {
+__device__ __forceinline__ bool agg_probe(const ScanParams& p, unsigned char* table, uint32_t* used, uint32_t* live,
+                                          uint64_t kw, unsigned char*& rec) {
   const uint32_t S = p.agg_slots;
   const size_t rs = agg_stride(p);
   if (kw == kEmpty) {
@@ -2089,7 +2090,12 @@ __device__ __forceinline__ bool agg_probe(const ScanParams& p, unsigned char* ta
     if (!hit && k == kEmpty) {
       if (*reinterpret_cast<volatile uint32_t*>(used) >= S - S / 8) return false;
       const unsigned long long prev = atomicCAS(key, kEmpty, kw);
-      if (prev == kEmpty) atomicAdd(used, 1u);
+      if (prev == kEmpty) {
+        // Each slot is claimed once, so fewer than S claims exist.
+        const uint32_t at = atomicAdd(used, 1u);
+        if (at < S) live[at] = s;
+        else part_check(p, CHK_SLOT);
+      }
       hit = prev == kEmpty || prev == kw;
     }
     if (hit) {
@@ -2108,7 +2114,7 @@ constexpr int kBR = 2;  // rows a pass B thread holds in flight
 // regime's update_rows on shared records); a warp's largest group of rows on
 // one record (a hot key) is first folded by butterflies (collapse_largest),
 // one atomic per field.
-__device__ __forceinline__ void fold_rows(const ScanParams& p, unsigned char* table, uint32_t* used,
+__device__ __forceinline__ void fold_rows(const ScanParams& p, unsigned char* table, uint32_t* used, uint32_t* live,
                                           const unsigned long long* rows, uint32_t n, uint32_t first, uint32_t stride) {
   const uint32_t W = p.part_words;
   bool on[kBR];
@@ -2134,7 +2140,7 @@ __device__ __forceinline__ void fold_rows(const ScanParams& p, unsigned char* ta
 #pragma unroll
   for (int j = 0; j < kBR; ++j) {
     recs[j] = table;
-    const bool hit = on[j] && agg_probe(p, table, used, kw[j], recs[j]);
+    const bool hit = on[j] && agg_probe(p, table, used, live, kw[j], recs[j]);
     lost |= on[j] && !hit;
     on[j] = hit;
   }
@@ -2159,10 +2165,17 @@ __device__ __forceinline__ void fold_rows(const ScanParams& p, unsigned char* ta
       maxpop = __reduce_max_sync(0xffffffffu, (unsigned)__popc(grp));
     }
   }
+  // A partition's rows arrive roughly in row order, so most rows do not
+  // lower their group's first row: the atomic only when they do (a new
+  // record's 0 always takes it).
+  uint32_t first_seen[kBR];
+#pragma unroll
+  for (int j = 0; j < kBR; ++j)
+    first_seen[j] = on[j] ? *reinterpret_cast<const volatile uint32_t*>(recs[j] + kRecFirst) : ~0u;
 #pragma unroll
   for (int j = 0; j < kBR; ++j) {
     if (!on[j]) continue;
-    rec_max_u32<true>(recs[j] + kRecFirst, ~row[j]);
+    if (~row[j] > first_seen[j]) rec_max_u32<true>(recs[j] + kRecFirst, ~row[j]);
     if (p.off_len >= 0) rec_add_u32<true>(recs[j] + p.off_len, 1u);
     if (p.off_last >= 0) rec_max_u32<true>(recs[j] + p.off_last, row[j] + 1u);
   }
@@ -2193,12 +2206,12 @@ __device__ __forceinline__ void fold_rows(const ScanParams& p, unsigned char* ta
 __global__ void __launch_bounds__(kAggThreads, 2) partition_aggregate(const __grid_constant__ ScanParams p) {
   extern __shared__ __align__(16) unsigned char table[];
   __shared__ uint32_t s_next, s_used, s_base, s_hole_lo, s_hole_hi, s_chunk_next, s_chunk_end;
-  __shared__ uint32_t s_warp[kAggThreads / 32];
   const uint32_t nparts = 1u << p.part_bits;
   const uint32_t S = p.agg_slots;
   const size_t rs = agg_stride(p);
   const size_t rw = (size_t)p.rec_stride / 8;  // words of a record
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t* const live = reinterpret_cast<uint32_t*>(table + (size_t)(S + 1) * rs);  // claimed slots, in claim order
+  unsigned char* const ones = table + (size_t)S * rs;  // the all-ones key word's record
   for (uint32_t s = threadIdx.x; s <= S; s += blockDim.x) reset_record(table + (size_t)s * rs, p.rec_stride);
   if (threadIdx.x == 0) {
     s_next = atomicAdd(p.part_next, 1u);
@@ -2221,27 +2234,16 @@ __global__ void __launch_bounds__(kAggThreads, 2) partition_aggregate(const __gr
     if (threadIdx.x == 0 && p.part_cursor[part] != n) part_check(p, CHK_RANGE);
     const unsigned long long* rows = p.part_buf + (uint64_t)p.part_start[part] * p.part_words;
     const uint32_t per = blockDim.x * (uint32_t)kBR;
-    for (uint32_t base = 0; base < n; base += per) fold_rows(p, table, &s_used, rows, n, base + threadIdx.x, blockDim.x);
+    for (uint32_t base = 0; base < n; base += per)
+      fold_rows(p, table, &s_used, live, rows, n, base + threadIdx.x, blockDim.x);
     __syncthreads();
-    // Live records: count, reserve (chunks of kRecChunk from p.alloc), copy
-    // out and reset.
-    uint32_t mine = 0;
-    for (uint32_t s = threadIdx.x; s <= S; s += blockDim.x)
-      mine += *reinterpret_cast<const uint32_t*>(table + (size_t)s * rs + kRecFirst) != 0u;
-    uint32_t x = mine;
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    if (lane == 31) s_warp[warp] = x;
-    __syncthreads();
+    // Live records: the claimed slots and the all-ones record when a row
+    // reached it.  Reserve (chunks of kRecChunk from p.alloc), copy out and
+    // reset.
+    const uint32_t n_live = min(s_used, S);
+    const bool ones_live = *reinterpret_cast<const uint32_t*>(ones + kRecFirst) != 0u;
     if (threadIdx.x == 0) {
-      uint32_t tot = 0;
-      for (int w = 0; w < (int)(blockDim.x / 32); ++w) {
-        const uint32_t t = s_warp[w];
-        s_warp[w] = tot;
-        tot += t;
-      }
+      const uint32_t tot = n_live + (ones_live ? 1u : 0u);
       s_hole_lo = s_hole_hi = 0;
       if (tot > s_chunk_end - s_chunk_next) {
         // The rest of the current chunk stays unused: holes for the finish.
@@ -2254,24 +2256,27 @@ __global__ void __launch_bounds__(kAggThreads, 2) partition_aggregate(const __gr
       }
       s_base = s_chunk_next;
       s_chunk_next += tot;
-      s_used = 0;
     }
     __syncthreads();
     for (uint32_t r = s_hole_lo + threadIdx.x; r < s_hole_hi; r += blockDim.x)
       if (r < p.recs_total) *reinterpret_cast<uint32_t*>(record_at(p, r) + kRecFirst) = 0u;
-    uint32_t dst = s_base + s_warp[warp] + x - mine;
-    for (uint32_t s = threadIdx.x; s <= S; s += blockDim.x) {
-      unsigned char* rec = table + (size_t)s * rs;
-      if (*reinterpret_cast<const uint32_t*>(rec + kRecFirst) == 0u) continue;
+    const uint32_t base_rec = s_base;
+    auto copy_out = [&](unsigned char* rec, uint32_t dst) {
       if (dst < p.recs_total) {
         unsigned long long* out = reinterpret_cast<unsigned long long*>(record_at(p, dst));
         const unsigned long long* in = reinterpret_cast<const unsigned long long*>(rec);
         for (size_t q = 0; q < rw; ++q) out[q] = in[q];
       }
       reset_record(rec, p.rec_stride);
-      ++dst;
+    };
+    for (uint32_t i = threadIdx.x; i < n_live; i += blockDim.x) {
+      const uint32_t s = live[i];
+      if (s < S) copy_out(table + (size_t)s * rs, base_rec + i);
+      else part_check(p, CHK_SLOT);
     }
-    __syncthreads();  // s_warp, s_base and the table are reused for the next partition
+    if (ones_live && threadIdx.x == blockDim.x - 1) copy_out(ones, base_rec + n_live);
+    __syncthreads();  // s_base, the list and the table are reused for the next partition
+    if (threadIdx.x == 0) s_used = 0;
   }
   // The unused rest of the last chunk: holes.
   for (uint32_t r = s_chunk_next + threadIdx.x; r < s_chunk_end; r += blockDim.x)

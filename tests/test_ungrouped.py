@@ -128,3 +128,20 @@ def test_gpu_ungrouped_int32_overflow_message():
     with pytest.raises(binding.OracleError) as eo:
         binding.run(frame.lazy().select(col("x").sum()))
     assert str(ei.value) == str(eo.value)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["int32", "float32", "int64"])
+def test_gpu_published_filtered_sum_workload(dtype):
+    """bench.py's handoff form: the reference's published filtered sum
+    (benchmarks/bench_handoff.mojo) on 5M rows, equal to the oracle (the
+    values are small integers, so every sum is exact)."""
+    import bench
+    from dataframe_mojo_b200 import provider
+
+    x = bench.handoff_values(dtype, 5_000_000, "cpu").numpy()
+    frame = DataFrame([Series("x", x)])
+    plan = bench.handoff_plan(frame)
+    dev = provider.execute(plan)[0]
+    ref, _ = binding.run(plan)
+    assert dev.equals(ref), (row(dev), row(ref))

@@ -104,6 +104,7 @@ class Timings(C.Structure):
         ("place_ns", C.c_double),
         ("kept_rows", C.c_uint64),
         ("placed_row_bytes", C.c_uint64),
+        ("direct_slots", C.c_uint64),
     ]
 
 

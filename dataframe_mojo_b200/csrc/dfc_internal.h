@@ -148,6 +148,13 @@ struct ScanParams {
   // shared-memory tables as compensated FP32 pairs {s, c} (Float32 columns),
   // merged into the FP64 global records; rows on the global path add in FP64.
   uint32_t comp_mask;
+  // Direct addressing of own tables (integer keys whose ranges together fit
+  // the table, dataframe/aggregation/perfect_hash.mojo:1-50): a key's slot is
+  // the sum over key columns of (value - dmin + 1, or 0 for null) << dshift;
+  // no hashing and no probing.  0: hashed tables.
+  int32_t direct;
+  int32_t dshift[kMaxKeys];
+  uint64_t dmin[kMaxKeys];  // each key's least value, as raw bits of its width
   // Tables.
   KeyEntry* table;
   uint64_t table_mask;

@@ -387,6 +387,8 @@ struct Plan {
   // Key skew from a 16K-row sample of the key words (-1: not measured): the
   // most frequent key's share and the share of the kHotSlots most frequent.
   double top1 = -1, top_hot = -1;
+  // Slots a direct-addressed own table needs (plan_direct; 0: not eligible).
+  uint64_t direct_slots = 0;
 };
 
 // The stage ring for tiles of `tile` rows (a power of two >= 128, so every
@@ -823,6 +825,41 @@ uint64_t estimate_groups(const dfc_query* q, const Plan& P, DeviceState* ds, cud
   return (uint64_t)std::max(1.0, est);
 }
 
+// Direct addressing (dataframe/aggregation/perfect_hash.mojo:1-50): integer
+// keys whose exact value ranges are known, each taking bit_width(range)
+// bits (0 for null, value - min + 1 otherwise), at most kDirectBits in all,
+// the first key highest.  Sets the kernel's fields and P.direct_slots; an
+// own table the regime picks then uses them instead of hashing.
+constexpr int kDirectBits = 12;
+void plan_direct(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_t stream) {
+  ScanParams& sp = P.sp;
+  sp.direct = 0;
+  P.direct_slots = 0;
+  if (sp.key_mode != KEY_PACKED || q->n_keys <= 0 || getenv("DFC_NO_DIRECT")) return;
+  int total = 0;
+  int shift[kMaxKeys] = {};
+  uint64_t mins[kMaxKeys] = {};
+  for (int k = q->n_keys - 1; k >= 0; --k) {
+    dfc_column* c = q->inputs[q->keys[k]];
+    if (is_float(c->dtype) || c->rows == 0) return;
+    if (ensure_stats(c, ds, stream) != DFC_OK || !c->have_stats || c->min_enc > c->max_enc) return;
+    const __int128 lo = order_value(c->min_enc, c->dtype);
+    const __int128 span = order_value(c->max_enc, c->dtype) - lo + 1;  // fields 1..span; 0 is null
+    if (span <= 0 || span >= ((__int128)1 << 31)) return;
+    int bits = 0;
+    while (((__int128)1 << bits) <= span) ++bits;
+    shift[k] = total;
+    total += bits;
+    if (total > kDirectBits) return;
+    mins[k] = (uint64_t)lo;  // two's complement: the kernel subtracts in the key's width
+  }
+  for (int k = 0; k < q->n_keys; ++k) {
+    sp.dshift[k] = shift[k];
+    sp.dmin[k] = mins[k];
+  }
+  P.direct_slots = 1ull << total;
+}
+
 // Per-CTA hot-key tables: slots, and the sampled share of rows their keys
 // must cover to be used when the groups do not fit a CTA.
 constexpr uint64_t kHotSlots = 512;
@@ -990,6 +1027,15 @@ bool plan_shared_at(Plan& P, DeviceState* ds, uint64_t est, uint32_t flags, bool
     if (want >= 2 || (!force && !hot && !sized)) return false;
     const uint64_t sslots =
         hot ? hot : next_pow2(std::max<uint64_t>(64, std::min<uint64_t>(est, kOwnTableGroups) * 2));
+    if (!hot && P.direct_slots > 0) {
+      // Direct addressing: every possible key its own slot, when that table
+      // still fits two CTAs per SM or is no larger than the hashed one.
+      const uint64_t dslots = std::max<uint64_t>(64, P.direct_slots);
+      if (total_for(dslots) <= ds->smem_optin && (total_for(dslots) <= ds->smem_half || dslots <= sslots)) {
+        sp.direct = 1;
+        return take(dslots, 1);
+      }
+    }
     // smem_optin already excludes the kernel's static shared memory.
     return total_for(sslots) <= ds->smem_optin && take(sslots, 1);
   }
@@ -1022,6 +1068,7 @@ bool plan_shared(Plan& P, DeviceState* ds, uint64_t est, uint32_t flags) {
   ScanParams& sp = P.sp;
   sp.smem_slots = 0;
   sp.smem_cluster = 1;
+  sp.direct = 0;
   if ((flags & DFC_Q_FORCE_GLOBAL) || sp.key_mode != KEY_PACKED) return false;
   const int tile0 = sp.tile_rows;
   for (bool own : {true, false}) {
@@ -1844,6 +1891,7 @@ dfc_status groupby_one(const dfc_query* query, dfc_result** out) {
   if (!host_ctl) CK(cudaMallocHost((void**)&host_ctl, sizeof(Control)), "pinned control block");
   const auto t_est = std::chrono::steady_clock::now();
   uint64_t est = estimate_groups(query, P, ds, stream);
+  plan_direct(query, P, ds, stream);
   const auto t_skew = std::chrono::steady_clock::now();
   // Regime: per-CTA shared-memory tables when the estimated groups fit in
   // shared memory at load <= 1/2 (two CTAs per SM if possible, else one);
@@ -1937,6 +1985,7 @@ dfc_status groupby_one(const dfc_query* query, dfc_result** out) {
   t_timings.regime = partitioned ? 2 : (P.sp.smem_slots ? 1 : 0);
   t_timings.cluster_ctas = P.sp.smem_slots ? (int32_t)std::max(1u, P.sp.smem_cluster) : 0;
   t_timings.compensated = P.sp.smem_slots ? (int32_t)P.sp.comp_mask : 0;
+  t_timings.direct_slots = P.sp.smem_slots && P.sp.direct ? P.sp.smem_slots : 0;
   t_timings.total_ns = std::chrono::duration<double, std::nano>(std::chrono::steady_clock::now() - t0).count();
   return DFC_OK;
 }
@@ -2591,6 +2640,7 @@ size_t arena_take(size_t& used, size_t bytes) {
 dfc_status size_item(const dfc_query* q, BatchItem& it, DeviceState* ds, cudaStream_t stream, size_t& used) {
   Plan& P = it.P;
   const uint64_t est = estimate_groups(q, P, ds, stream);
+  plan_direct(q, P, ds, stream);
   if (P.sp.key_mode == KEY_PACKED && est > kOwnAlwaysGroups && !(q->flags & DFC_Q_FORCE_GLOBAL))
     measure_skew(P, ds, stream);
   plan_shared(P, ds, est, q->flags);

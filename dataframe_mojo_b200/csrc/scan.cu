@@ -604,10 +604,39 @@ struct ClusterRec {
   }
 };
 
+// The direct-addressed slot of packed key word `kw` (ScanParams::direct).
+__device__ __forceinline__ uint32_t direct_slot(const ScanParams& p, uint64_t kw) {
+  uint32_t s = 0;
+  for (int k = 0; k < p.n_keys; ++k) {
+    const KeyField& kf = p.keys[k];
+    if (kf.null_bit >= 0 && ((kw >> kf.null_bit) & 1ull)) continue;  // null: field 0
+    const uint64_t mask = kf.bits == 64 ? ~0ull : ((1ull << kf.bits) - 1ull);
+    const uint64_t raw = (kw >> kf.shift) & mask;
+    // The key's own wrap-around subtraction: values lie in [dmin, dmin + span).
+    s += (uint32_t)(((raw - p.dmin[k]) & mask) + 1ull) << p.dshift[k];
+  }
+  return s;
+}
+
 // The record of key word `kw` in this CTA's own table (claimed if new);
 // false when the key is absent and the table is three-quarters full.
+// Direct-addressed tables hold every key's slot, so they never fill.
 __device__ __forceinline__ bool smem_probe(const ScanParams& p, const SmemTable& st, uint64_t kw, OwnRec& rec) {
   if (kw == kEmpty) return false;
+  if (p.direct) {
+    const uint32_t s = direct_slot(p, kw);
+    if (s >= p.smem_slots) return false;  // outside the planned ranges: the global path
+    unsigned long long* key = &st.keys[s];
+    const unsigned long long k = *reinterpret_cast<volatile unsigned long long*>(key);
+    if (k != kw) {
+      if (k != kEmpty) return false;
+      const unsigned long long prev = atomicCAS(key, kEmpty, kw);
+      if (prev == kEmpty) atomicAdd(st.used, 1u);
+      else if (prev != kw) return false;
+    }
+    rec.p = st.recs + (size_t)s * p.rec_stride;
+    return true;
+  }
   const uint32_t mask = p.smem_slots - 1;
   uint32_t s = (uint32_t)mix64(kw ^ 0x9FB21C651E98DF25ull) & mask;
   for (int probe = 0; probe < 32; ++probe) {

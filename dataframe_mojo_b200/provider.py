@@ -473,6 +473,7 @@ def last_timings() -> dict:
         "place_ns": t.place_ns,
         "kept_rows": int(t.kept_rows),
         "placed_row_bytes": int(t.placed_row_bytes),
+        "direct_slots": int(t.direct_slots),
     }
 
 

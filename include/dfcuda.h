@@ -430,6 +430,7 @@ typedef struct dfc_timings {
   double place_ns;      /* radix-partitioned regime: the pass placing rows into partitions (part of scan_ns) */
   uint64_t kept_rows;        /* radix-partitioned regime: rows the filter kept (each placed once) */
   uint64_t placed_row_bytes; /* radix-partitioned regime: bytes of one placed row */
+  uint64_t direct_slots;     /* shared-memory regime: slots of own tables addressed by key value (0: hashed) */
 } dfc_timings;
 DFC_API dfc_status dfc_last_timings(dfc_timings* out);
 

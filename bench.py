@@ -230,7 +230,7 @@ def roofline_of(step_t: list[dict], rows: int) -> dict:
         "traffic": traffic_per_launch(dominant),
         "algorithmic_bytes": b,
         "kernel_ms": s * 1e3,
-        "regime": ["global table", "shared-memory tables", "radix-partitioned"][last["regime"]],
+        "regime": ["global table", "shared-memory tables", "radix-partitioned", "ungrouped in registers"][last["regime"]],
         "passes": {k: {"algorithmic_bytes": pb, "ms": ps * 1e3, "gbs": pb / ps / 1e9, "frac": pb / ps / 1e9 / peak,
                        "traffic": traffic_per_launch(k)} for k, (pb, ps) in passes.items()},
         "finish_ms": mean_s("finish_ns") * 1e3,

@@ -153,6 +153,9 @@ struct ScanParams {
   // the sum over key columns of (value - dmin + 1, or 0 for null) << dshift;
   // no hashing and no probing.  0: hashed tables.
   int32_t direct;
+  // Ungrouped queries (no key) whose value columns fit the register path:
+  // scan_kernel_reduce instead of the own-table scan.
+  int32_t reduce;
   int32_t dshift[kMaxKeys];
   uint64_t dmin[kMaxKeys];  // each key's least value, as raw bits of its width
   // Tables.

@@ -15,10 +15,14 @@ constexpr int kFinishChunk = 4096;  // bitmap words per prefix-scan block
 // The scan, one kernel per table regime: the global table only, per-CTA
 // shared-memory tables, shared-memory tables pooled over a thread-block
 // cluster (launched with a cluster dimension of ScanParams::smem_cluster).
-enum ScanRegime : int { kScanGlobal = 0, kScanOwn = 1, kScanCluster = 2 };
+// kScanReduce: ungrouped queries (no key), every consumer thread folding its
+// rows into registers (ScanParams::reduce).
+enum ScanRegime : int { kScanGlobal = 0, kScanOwn = 1, kScanCluster = 2, kScanReduce = 3 };
 __global__ void scan_kernel_global(const __grid_constant__ ScanParams p);
 __global__ void scan_kernel_own(const __grid_constant__ ScanParams p);
 __global__ void scan_kernel_cluster(const __grid_constant__ ScanParams p);
+__global__ void scan_kernel_reduce(const __grid_constant__ ScanParams p);
+constexpr int kReduceVals = 2;  // value columns the register path holds
 // Radix-partitioned regime: the counting pass, the partition starts, pass A
 // (filter, keys, placement into partitions) and pass B (per-partition
 // aggregation in a shared-memory table, kAggThreads threads per CTA).

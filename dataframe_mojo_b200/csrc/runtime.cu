@@ -138,6 +138,7 @@ using ScanFn = void (*)(ScanParams);
 // The scan kernel for a planned query's table regime.
 ScanFn scan_fn(const ScanParams& sp) {
   if (!sp.smem_slots) return scan_kernel_global;
+  if (sp.reduce) return scan_kernel_reduce;
   return sp.smem_cluster > 1 ? scan_kernel_cluster : scan_kernel_own;
 }
 
@@ -230,13 +231,13 @@ dfc_status device_ready(int dev, DeviceState** out) {
     // Dynamic shared memory may use what the kernel's static buffers leave.
     cudaFuncAttributes fa;
     size_t scan_static = 0;
-    for (ScanFn f : {scan_kernel_global, scan_kernel_own, scan_kernel_cluster}) {
+    for (ScanFn f : {scan_kernel_global, scan_kernel_own, scan_kernel_cluster, scan_kernel_reduce}) {
       CK(cudaFuncGetAttributes(&fa, f), "cudaFuncGetAttributes");
       scan_static = std::max(scan_static, fa.sharedSizeBytes);
     }
     d.smem_optin = prop.sharedMemPerBlockOptin - scan_static;
     d.smem_half = (prop.sharedMemPerMultiprocessor - 2 * prop.reservedSharedMemPerBlock) / 2 - scan_static;
-    for (ScanFn f : {scan_kernel_global, scan_kernel_own, scan_kernel_cluster})
+    for (ScanFn f : {scan_kernel_global, scan_kernel_own, scan_kernel_cluster, scan_kernel_reduce})
       CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin),
          "cudaFuncSetAttribute");
     // Cluster tables pool the shared memory of up to 16 CTAs.
@@ -1069,12 +1070,20 @@ bool plan_shared(Plan& P, DeviceState* ds, uint64_t est, uint32_t flags) {
   sp.smem_slots = 0;
   sp.smem_cluster = 1;
   sp.direct = 0;
+  sp.reduce = 0;
   if ((flags & DFC_Q_FORCE_GLOBAL) || sp.key_mode != KEY_PACKED) return false;
   const int tile0 = sp.tile_rows;
   for (bool own : {true, false}) {
     for (int tile = tile0; tile >= std::min(tile0, 256); tile >>= 1) {
       if (tile != sp.tile_rows) layout_ring(P, tile);
-      if (plan_shared_at(P, ds, est, flags, own)) return true;
+      if (plan_shared_at(P, ds, est, flags, own)) {
+        // No key, an own table and value columns that fit the register
+        // path: per-thread states instead of per-row updates of one record.
+        // DFC_NO_REDUCE=1 keeps the per-row path (tuning).
+        sp.reduce = sp.n_keys == 0 && sp.smem_cluster <= 1 && sp.comp_mask == 0 && sp.n_vals <= kReduceVals &&
+                    !getenv("DFC_NO_REDUCE");
+        return true;
+      }
     }
   }
   if (sp.tile_rows != tile0) layout_ring(P, tile0);
@@ -1982,7 +1991,7 @@ dfc_status groupby_one(const dfc_query* query, dfc_result** out) {
   }
   learn_groups(P, (*out)->rows);
   t_timings.groups = (*out)->rows;
-  t_timings.regime = partitioned ? 2 : (P.sp.smem_slots ? 1 : 0);
+  t_timings.regime = partitioned ? 2 : (P.sp.smem_slots ? (P.sp.reduce ? 3 : 1) : 0);
   t_timings.cluster_ctas = P.sp.smem_slots ? (int32_t)std::max(1u, P.sp.smem_cluster) : 0;
   t_timings.compensated = P.sp.smem_slots ? (int32_t)P.sp.comp_mask : 0;
   t_timings.direct_slots = P.sp.smem_slots && P.sp.direct ? P.sp.smem_slots : 0;

@@ -1341,6 +1341,173 @@ __device__ void produce_tiles(const ScanParams& p, unsigned char* smem, uint64_t
   }
 }
 
+// ---------------------------------------------------------------------------
+// Ungrouped queries in registers (kScanReduce).  With no key every kept row
+// belongs to one group, and per-row atomics on one record serialise.  Each
+// consumer thread instead keeps the group's state for its own rows in
+// registers (the reference's Metal reductions keep per-thread partials too,
+// dataframe_metal/accelerator/gpu/filter_sum.mojo:1-20): count, exact
+// integer or FP64 sum, extrema codes, NaN and signed-zero flags, and shifted
+// moments about the thread's first value K_t.  A warp folds its lanes' states
+// by shuffles (moments re-centred on one lane's K), each warp folds its state
+// into the CTA's one shared-memory record with one atomic per field, and the
+// CTA's record merges into the global record as an own table does.
+// ---------------------------------------------------------------------------
+struct ReduceField {
+  uint32_t n, flags;
+  double sf;       // Float sum
+  __int128 si;     // integer sum
+  uint64_t emin;   // the largest complemented code (the minimum), 0 = none
+  uint64_t emax;   // the largest code, 0 = none
+  uint64_t k;      // K_t ^ kShiftTag, 0 = unset
+  double s1, s2;   // sums of (x - K_t) and (x - K_t)^2
+};
+struct ReduceState {
+  uint32_t first, last, len;  // least kept row, largest kept row + 1, kept rows
+  ReduceField f[kReduceVals];
+};
+
+__device__ __forceinline__ void reduce_init(ReduceState& st) {
+  st.first = 0xFFFFFFFFu;
+  st.last = st.len = 0;
+#pragma unroll
+  for (int v = 0; v < kReduceVals; ++v) {
+    ReduceField& f = st.f[v];
+    f.n = f.flags = 0;
+    f.sf = f.s1 = f.s2 = 0.0;
+    f.si = 0;
+    f.emin = f.emax = f.k = 0;
+  }
+}
+
+__device__ __forceinline__ void reduce_value(const ValField& vf, bool ok, uint64_t b, ReduceField& f) {
+  if (!ok) return;
+  const int dt = vf.dtype;
+  const bool isf = dt_float(dt);
+  const double xd = isf ? bits_to_f64(b, dt) : bits_as_double(b, dt);
+  const bool nan = isf && xd != xd;
+  ++f.n;
+  if (vf.off_sum >= 0) {
+    if (isf) f.sf += xd;
+    else f.si += dt == DFC_UINT64 ? (__int128)b : (__int128)bits_to_i64(b, dt);
+  }
+  if (vf.off_min >= 0 || vf.off_max >= 0) {
+    if (nan) {
+      f.flags |= 1u;
+    } else {
+      const uint64_t e = order_encode(b, dt);
+      if (~e > f.emin) f.emin = ~e;
+      if (e > f.emax) f.emax = e;
+      if (isf && xd == 0.0) f.flags |= signbit(xd) ? 4u : 2u;
+    }
+  }
+  if (vf.off_m2 >= 0) {
+    if (f.k == 0) f.k = (nan ? kCanonNaN : (uint64_t)__double_as_longlong(xd)) ^ kShiftTag;
+    const double d = xd - __longlong_as_double((long long)(f.k ^ kShiftTag));
+    f.s1 += d;
+    f.s2 += d * d;
+  }
+}
+
+// The lane's row r of tile k, kept by the filter.
+__device__ __forceinline__ void reduce_row(const ScanParams& p, const Step& s, int k, uint32_t r, ReduceState& st) {
+  const uint32_t row = (uint32_t)(s.start[k] + r);
+  st.first = min(st.first, row);
+  st.last = max(st.last, row + 1u);
+  ++st.len;
+#pragma unroll
+  for (int v = 0; v < kReduceVals; ++v) {
+    if (v >= p.n_vals) break;
+    const int c = p.vals[v].input;
+    const bool ok = valid_at(col_valid(p, s, k, c), r);
+    const uint64_t b = ok ? load_bits(col_values(p, s, k, c), p.cols[c].size, r) : 0ull;
+    reduce_value(p.vals[v], ok, b, st.f[v]);
+  }
+}
+
+__device__ __forceinline__ uint32_t warp_sum_u32(uint32_t v) { return __reduce_add_sync(0xffffffffu, v); }
+
+// The warp's states folded into the CTA's record `rec` (every lane calls it).
+__device__ __forceinline__ void reduce_flush(const ScanParams& p, ReduceState& st, const OwnRec& rec) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t first = __reduce_min_sync(0xffffffffu, st.first);
+  const uint32_t last = __reduce_max_sync(0xffffffffu, st.last);
+  const uint32_t len = warp_sum_u32(st.len);
+  if (len == 0) return;  // warp-uniform
+  if (lane == 0) {
+    rec.max_u32(kRecFirst, ~first);
+    if (p.off_len >= 0) rec.add_u32(p.off_len, len);
+    if (p.off_last >= 0) rec.max_u32(p.off_last, last);
+  }
+#pragma unroll
+  for (int v = 0; v < kReduceVals; ++v) {
+    if (v >= p.n_vals) break;
+    const ValField& vf = p.vals[v];
+    ReduceField& f = st.f[v];
+    const uint32_t n = warp_sum_u32(f.n);
+    const uint32_t flags = __reduce_or_sync(0xffffffffu, f.flags);
+    if (lane == 0) {
+      if (n) rec.add_u32(vf.off_count, n);
+      if (flags) rec.or_u32(kRecFlags, flags << (3 * v));
+    }
+    if (vf.off_sum >= 0) {
+      if (dt_float(vf.dtype)) {
+        const double sm = warp_sum_f64(f.sf);
+        if (lane == 0 && n) rec.add_f64(vf.off_sum, sm);
+      } else {
+        const __int128 exact = warp_sum_i128(f.si);
+        if (lane == 0 && n) {
+          if (vf.sum_kind == SUM_I64) {
+            rec.add_u64(vf.off_sum, (uint64_t)(int64_t)exact);
+          } else {
+            const uint64_t add_lo = (uint64_t)exact, add_hi = (uint64_t)(exact >> 64);
+            const uint64_t old = rec.add_u64(vf.off_sum, add_lo);
+            const uint64_t hi_add = add_hi + ((old + add_lo) < old ? 1ull : 0ull);
+            if (hi_add) rec.add_u64(vf.off_sum + 8, hi_add);
+          }
+        }
+      }
+    }
+    if (vf.off_min >= 0) {
+      const uint64_t m = warp_max_u64(f.emin);
+      if (lane == 0 && m) rec.max_u64(vf.off_min, m);
+    }
+    if (vf.off_max >= 0) {
+      const uint64_t m = warp_max_u64(f.emax);
+      if (lane == 0 && m) rec.max_u64(vf.off_max, m);
+    }
+    if (vf.off_m2 >= 0) {
+      // Moments re-centred on the first lane's K (sum (x - K)^2 = S2_t +
+      // 2 d S1_t + n_t d^2, d = K_t - K), then on the record's.
+      const uint32_t has = __ballot_sync(0xffffffffu, f.k != 0);
+      if (has) {
+        const uint64_t kw = __shfl_sync(0xffffffffu, f.k, __ffs(has) - 1);
+        double s1 = 0.0, s2 = 0.0;
+        if (f.k != 0) {
+          const double d = __longlong_as_double((long long)(f.k ^ kShiftTag)) -
+                           __longlong_as_double((long long)(kw ^ kShiftTag));
+          const double dn = (double)f.n;
+          s1 = d == 0.0 ? f.s1 : f.s1 + dn * d;
+          s2 = d == 0.0 ? f.s2 : f.s2 + 2.0 * d * f.s1 + dn * d * d;
+        }
+        s1 = warp_sum_f64(s1);
+        s2 = warp_sum_f64(s2);
+        if (lane == 0) {
+          uint64_t kr = rec.ld_u64(vf.off_shift);
+          if (kr == 0) {
+            const uint64_t prev = rec.cas_u64(vf.off_shift, 0ull, kw);
+            kr = prev == 0 ? kw : prev;
+          }
+          const double d = __longlong_as_double((long long)(kw ^ kShiftTag)) -
+                           __longlong_as_double((long long)(kr ^ kShiftTag));
+          const double dn = (double)n;
+          rec.add_f64(vf.off_m2, d == 0.0 ? s2 : s2 + 2.0 * d * s1 + dn * d * d);
+        }
+      }
+    }
+  }
+}
+
 // The scan body, specialised by table regime R (kScan*): each regime's
 // kernel carries only its own table code, which keeps the instruction
 // footprint of the hot loop small.
@@ -1378,6 +1545,8 @@ __device__ __forceinline__ void scan_body(const ScanParams& p) {
     uint4* recs = reinterpret_cast<uint4*>(st.recs);
     const uint32_t n16 = p.smem_slots * (uint32_t)p.rec_stride / 16;
     for (uint32_t i = threadIdx.x; i < n16; i += blockDim.x) recs[i] = make_uint4(0, 0, 0, 0);
+    // No key: the one group's key word is 0, its record slot 0.
+    if (R == kScanReduce && threadIdx.x == 0) st.keys[0] = 0ull;
   }
   __syncthreads();
   // A cluster table: every share is initialised before any CTA probes it.
@@ -1391,6 +1560,8 @@ __device__ __forceinline__ void scan_body(const ScanParams& p) {
     const uint32_t words = (uint32_t)(T / 32);
     uint32_t it = 0;   // tiles consumed
     uint32_t stp = 0;  // steps
+    ReduceState red;
+    if (R == kScanReduce) reduce_init(red);
     for (uint64_t t = blockIdx.x; t < p.tiles; t += (uint64_t)kTilesPerStep * gridDim.x, ++stp) {
       Step s;
       int nt = 0;
@@ -1416,6 +1587,26 @@ __device__ __forceinline__ void scan_body(const ScanParams& p) {
         const uint64_t left = p.rows - s.start[k];
         s.n[k] = (uint32_t)(left < T ? left : T);
         ++nt;
+      }
+      if constexpr (R == kScanReduce) {
+        // Each lane folds its kept rows of the warp's words into registers.
+        if (!failed) {
+          for (int k = 0; k < nt; ++k) {
+            for (uint32_t w = (uint32_t)(warp - 1); w < words; w += kScanConsumerWarps) {
+              const uint32_t bits = select_word(p, s, k, w);
+              if ((bits >> lane) & 1u) reduce_row(p, s, k, w * 32 + lane, red);
+            }
+          }
+        }
+        if (consumer_sync_or(failed || s_abort)) {
+          s_abort = 1;
+          break;
+        }
+        __syncwarp();
+        for (int k = 0; k < nt; ++k)
+          if (lane == 0) mbar_arrive(&empty[(it + k) % S]);
+        it += nt;
+        continue;
       }
       // 1 + 2: selection words and compaction into s_idx[b].
       const uint32_t b = stp % 3u;
@@ -1447,6 +1638,7 @@ __device__ __forceinline__ void scan_body(const ScanParams& p) {
         if (lane == 0) mbar_arrive(&empty[(it + k) % S]);
       it += nt;
     }
+    if (R == kScanReduce && p.smem_slots && !s_abort) reduce_flush(p, red, OwnRec{st.recs});
   }
   __syncthreads();
   // A cluster table: no CTA touches another's share after this barrier, so
@@ -1491,6 +1683,9 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel_own(const __grid_
 }
 __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel_cluster(const __grid_constant__ ScanParams p) {
   scan_body<kScanCluster>(p);
+}
+__global__ void __launch_bounds__(kScanThreads, 2) scan_kernel_reduce(const __grid_constant__ ScanParams p) {
+  scan_body<kScanReduce>(p);
 }
 
 // Merges one shared-memory record into global record `gid` (function.mojo:

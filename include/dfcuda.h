@@ -419,7 +419,7 @@ typedef struct dfc_timings {
   double total_ns;
   uint64_t groups;
   uint64_t table_slots;
-  int32_t regime;   /* 0 global table, 1 shared-memory tables, 2 radix-partitioned */
+  int32_t regime;   /* 0 global table, 1 shared-memory tables, 2 radix-partitioned, 3 ungrouped in registers */
   int32_t retries;  /* capacity regrowths */
   int32_t launches; /* kernels this library launched for the query */
   int32_t partitions;  /* radix-partitioned regime: partitions (else 0) */

@@ -145,3 +145,52 @@ def test_gpu_published_filtered_sum_workload(dtype):
     dev = provider.execute(plan)[0]
     ref, _ = binding.run(plan)
     assert dev.equals(ref), (row(dev), row(ref))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("columns", [1, 2, 3])
+def test_gpu_register_path_and_fallback(columns):
+    """Up to two value columns run in registers (regime 3: per-thread states
+    folded per warp and per CTA); a third value column takes the per-row
+    shared-memory path (regime 1).  NaN, signed zeros, nulls and a
+    far-from-zero mean (shifted moments re-centred across threads) against
+    the oracle."""
+    from dataframe_mojo_b200 import provider
+    from test_gpu_parity import compare_with_oracle
+
+    rng = np.random.default_rng(9100 + columns)
+    rows = 4_000_000
+    cols = [Series("p", rng.integers(0, 100, rows).astype(np.int32))]
+    aggs, floats, vars_ = [], [], []
+    for i in range(columns):
+        if i == 0:
+            x = 1e6 + rng.standard_normal(rows)
+            x[rng.random(rows) < 1e-6] = np.nan
+            x[rng.random(rows) < 0.001] = -0.0
+            vals = x
+        elif i == 1:
+            vals = rng.integers(-(2**40), 2**40, rows).astype(np.int64)
+        else:
+            vals = rng.standard_normal(rows).astype(np.float32)
+        cols.append(Series(f"v{i}", vals, rng.random(rows) > 0.05))
+        v = col(f"v{i}")
+        aggs += [v.sum().alias(f"s{i}"), v.count().alias(f"n{i}"), v.min().alias(f"lo{i}"), v.max().alias(f"hi{i}"),
+                 v.mean().alias(f"m{i}"), v.var().alias(f"var{i}"), v.first().alias(f"f{i}"), v.last().alias(f"l{i}")]
+        floats.append(f"m{i}")
+        vars_.append(f"var{i}")
+        if vals.dtype.kind == "f":
+            floats.append(f"s{i}")
+    plan = DataFrame(cols).lazy().filter(col("p") < 61).select(aggs + [col("v0").len().alias("len")])
+
+    def scales(ref):
+        out = {}
+        for i in range(columns):
+            n = ref[f"n{i}"].values.astype(np.float64)
+            m = np.maximum(np.abs(ref[f"lo{i}"].values.astype(np.float64)), np.abs(ref[f"hi{i}"].values.astype(np.float64)))
+            m = np.where(np.isfinite(m), m, 0.0)
+            out[f"s{i}"], out[f"m{i}"] = n * m, m
+        return out
+
+    compare_with_oracle(plan, f"register{columns}", float_cols=floats, var_cols=vars_, scales=scales)
+    provider.execute(plan)
+    assert provider.last_timings()["regime"] == (3 if columns <= 2 else 1)

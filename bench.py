@@ -997,8 +997,14 @@ def main() -> int:
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(e2e_stream)
     d2h = 0
+    step_host_ms, step_retries = [], []
     for _ in range(args.e2e_steps):
+        # Each step ends synchronised (its result copied to the host), so the
+        # host clock around it reads the step; the retries are the library's.
+        t0 = time.perf_counter()
         d2h = e2e_step()
+        step_host_ms.append(round((time.perf_counter() - t0) * 1e3, 3))
+        step_retries.append(provider.last_timings()["retries"])
     e1.record(e2e_stream)
     torch.cuda.synchronize()
     # One more step, after the timed ones and not part of them, read by the
@@ -1019,6 +1025,8 @@ def main() -> int:
         "steps": args.e2e_steps,
         "ms_per_step": float(et.item()),
         "phases_ms": {k: round(v, 3) for k, v in phases.items()},
+        "step_host_ms": step_host_ms,
+        "step_retries": step_retries,
     }
 
     cpu = None

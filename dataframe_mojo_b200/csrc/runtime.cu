@@ -1072,6 +1072,16 @@ bool plan_shared(Plan& P, DeviceState* ds, uint64_t est, uint32_t flags) {
   sp.direct = 0;
   sp.reduce = 0;
   if ((flags & DFC_Q_FORCE_GLOBAL) || sp.key_mode != KEY_PACKED) return false;
+  if (sp.n_keys == 0) {
+    // No key: one small own table, so the stage ring may take most of the
+    // shared memory of two CTAs per SM.  Narrow columns need the depth: a
+    // 4-stage ring of 4 KB tiles keeps too few bytes in flight per SM.
+    const size_t table = 64 * (8 + (size_t)sp.rec_stride) + 64;
+    const size_t per = (size_t)sp.stage_bytes + 2 * sizeof(uint64_t);
+    const size_t budget = ds->smem_half > table ? ds->smem_half - table : 0;
+    sp.stages = (int)std::max<size_t>(4, std::min<size_t>(16, budget / per));
+    P.smem = (size_t)sp.stages * per;
+  }
   const int tile0 = sp.tile_rows;
   for (bool own : {true, false}) {
     for (int tile = tile0; tile >= std::min(tile0, 256); tile >>= 1) {

@@ -1380,48 +1380,102 @@ __device__ __forceinline__ void reduce_init(ReduceState& st) {
   }
 }
 
-__device__ __forceinline__ void reduce_value(const ValField& vf, bool ok, uint64_t b, ReduceField& f) {
-  if (!ok) return;
-  const int dt = vf.dtype;
-  const bool isf = dt_float(dt);
-  const double xd = isf ? bits_to_f64(b, dt) : bits_as_double(b, dt);
-  const bool nan = isf && xd != xd;
-  ++f.n;
-  if (vf.off_sum >= 0) {
-    if (isf) f.sf += xd;
-    else f.si += dt == DFC_UINT64 ? (__int128)b : (__int128)bits_to_i64(b, dt);
-  }
-  if (vf.off_min >= 0 || vf.off_max >= 0) {
-    if (nan) {
-      f.flags |= 1u;
-    } else {
-      const uint64_t e = order_encode(b, dt);
-      if (~e > f.emin) f.emin = ~e;
-      if (e > f.emax) f.emax = e;
-      if (isf && xd == 0.0) f.flags |= signbit(xd) ? 4u : 2u;
+// A step's selection words of this warp: word w of tile k at [k * kRedWords +
+// i], w = warp - 1 + i * kScanConsumerWarps.
+constexpr int kRedWords = 4;  // 1,024-row tiles: 32 words over 8 consumer warps
+static_assert(kRedWords * kScanConsumerWarps * 32 >= kMaxTileRows, "a step's words per warp");
+
+// The lane's kept rows of value column v (type T) folded into `f`: one dtype
+// dispatch per step instead of one per row.
+template <typename T>
+__device__ __forceinline__ void reduce_words(const ScanParams& p, const Step& s, int nt, int v,
+                                             const uint32_t (&selw)[2 * kRedWords], ReduceField& f) {
+  constexpr bool kFloat = std::is_floating_point<T>::value;
+  const ValField& vf = p.vals[v];
+  const int c = vf.input;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool want_sum = vf.off_sum >= 0, want_ext = vf.off_min >= 0 || vf.off_max >= 0, want_m2 = vf.off_m2 >= 0;
+#pragma unroll
+  for (int k = 0; k < kTilesPerStep; ++k) {
+    if (k >= nt) break;
+    const unsigned char* vals = col_values(p, s, k, c);
+    const uint32_t* valid = col_valid(p, s, k, c);
+#pragma unroll
+    for (int i = 0; i < kRedWords; ++i) {
+      if (!((selw[k * kRedWords + i] >> lane) & 1u)) continue;
+      const uint32_t r = (uint32_t)(warp - 1 + i * kScanConsumerWarps) * 32u + (uint32_t)lane;
+      if (!valid_at(valid, r)) continue;
+      const T x = load_as<T>(vals, r);
+      const double xd = (double)x;
+      const bool nan = kFloat && xd != xd;
+      ++f.n;
+      if (want_sum) {
+        if constexpr (kFloat) f.sf += xd;
+        else f.si += (__int128)x;
+      }
+      if (want_ext) {
+        if (nan) {
+          f.flags |= 1u;
+        } else {
+          uint64_t e;
+          if constexpr (kFloat) {
+            const uint64_t u = xd == 0.0 ? 0ull : (uint64_t)__double_as_longlong(xd);
+            e = (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+            if (xd == 0.0) f.flags |= signbit(xd) ? 4u : 2u;
+          } else if constexpr (std::is_unsigned<T>::value) {
+            e = (uint64_t)x;
+          } else {
+            e = (uint64_t)(int64_t)x ^ 0x8000000000000000ull;
+          }
+          if (~e > f.emin) f.emin = ~e;
+          if (e > f.emax) f.emax = e;
+        }
+      }
+      if (want_m2) {
+        if (f.k == 0) f.k = (nan ? kCanonNaN : (uint64_t)__double_as_longlong(xd)) ^ kShiftTag;
+        const double d = xd - __longlong_as_double((long long)(f.k ^ kShiftTag));
+        f.s1 += d;
+        f.s2 += d * d;
+      }
     }
-  }
-  if (vf.off_m2 >= 0) {
-    if (f.k == 0) f.k = (nan ? kCanonNaN : (uint64_t)__double_as_longlong(xd)) ^ kShiftTag;
-    const double d = xd - __longlong_as_double((long long)(f.k ^ kShiftTag));
-    f.s1 += d;
-    f.s2 += d * d;
   }
 }
 
-// The lane's row r of tile k, kept by the filter.
-__device__ __forceinline__ void reduce_row(const ScanParams& p, const Step& s, int k, uint32_t r, ReduceState& st) {
-  const uint32_t row = (uint32_t)(s.start[k] + r);
-  st.first = min(st.first, row);
-  st.last = max(st.last, row + 1u);
-  ++st.len;
+// The warp's words of this step: selection, row bookkeeping, then each value
+// column by its type.
+__device__ __forceinline__ void reduce_step(const ScanParams& p, const Step& s, int nt, uint32_t words,
+                                            ReduceState& st) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t selw[2 * kRedWords];
+#pragma unroll
+  for (int k = 0; k < kTilesPerStep; ++k) {
+#pragma unroll
+    for (int i = 0; i < kRedWords; ++i) {
+      const uint32_t w = (uint32_t)(warp - 1 + i * kScanConsumerWarps);
+      selw[k * kRedWords + i] = (k < nt && w < words) ? select_word(p, s, k, w) : 0u;
+      if ((selw[k * kRedWords + i] >> lane) & 1u) {
+        const uint32_t row = (uint32_t)(s.start[k] + w * 32u + (uint32_t)lane);
+        st.first = min(st.first, row);
+        st.last = max(st.last, row + 1u);
+        ++st.len;
+      }
+    }
+  }
 #pragma unroll
   for (int v = 0; v < kReduceVals; ++v) {
     if (v >= p.n_vals) break;
-    const int c = p.vals[v].input;
-    const bool ok = valid_at(col_valid(p, s, k, c), r);
-    const uint64_t b = ok ? load_bits(col_values(p, s, k, c), p.cols[c].size, r) : 0ull;
-    reduce_value(p.vals[v], ok, b, st.f[v]);
+    switch (p.vals[v].dtype) {
+      case DFC_INT8: reduce_words<int8_t>(p, s, nt, v, selw, st.f[v]); break;
+      case DFC_INT16: reduce_words<int16_t>(p, s, nt, v, selw, st.f[v]); break;
+      case DFC_INT32: reduce_words<int32_t>(p, s, nt, v, selw, st.f[v]); break;
+      case DFC_INT64: reduce_words<int64_t>(p, s, nt, v, selw, st.f[v]); break;
+      case DFC_UINT8: reduce_words<uint8_t>(p, s, nt, v, selw, st.f[v]); break;
+      case DFC_UINT16: reduce_words<uint16_t>(p, s, nt, v, selw, st.f[v]); break;
+      case DFC_UINT32: reduce_words<uint32_t>(p, s, nt, v, selw, st.f[v]); break;
+      case DFC_UINT64: reduce_words<uint64_t>(p, s, nt, v, selw, st.f[v]); break;
+      case DFC_FLOAT32: reduce_words<float>(p, s, nt, v, selw, st.f[v]); break;
+      default: reduce_words<double>(p, s, nt, v, selw, st.f[v]); break;
+    }
   }
 }
 
@@ -1590,14 +1644,7 @@ __device__ __forceinline__ void scan_body(const ScanParams& p) {
       }
       if constexpr (R == kScanReduce) {
         // Each lane folds its kept rows of the warp's words into registers.
-        if (!failed) {
-          for (int k = 0; k < nt; ++k) {
-            for (uint32_t w = (uint32_t)(warp - 1); w < words; w += kScanConsumerWarps) {
-              const uint32_t bits = select_word(p, s, k, w);
-              if ((bits >> lane) & 1u) reduce_row(p, s, k, w * 32 + lane, red);
-            }
-          }
-        }
+        if (!failed) reduce_step(p, s, nt, words, red);
         if (consumer_sync_or(failed || s_abort)) {
           s_abort = 1;
           break;

@@ -1293,21 +1293,25 @@ bool plan_partitions(const Plan& P, const DeviceState* ds, uint64_t est, PartPla
   // DFC_PART_MIN_BITS=<n> raises the least partition count (tuning).
   if (const char* env = getenv("DFC_PART_MIN_BITS"))
     if (atoi(env) > 0) min_bits = std::max<uint32_t>(min_bits, (uint32_t)atoi(env));
+  // DFC_AGG_LOAD=<x> (tuning) replaces kAggLoad.
+  double load = kAggLoad;
+  if (const char* env = getenv("DFC_AGG_LOAD"))
+    if (atof(env) > 0.0 && atof(env) < 0.875) load = atof(env);
   auto bits_for = [&](uint64_t slots) {
     uint32_t b = std::max(kPartMinBits, min_bits);
-    while (b < (uint32_t)kPartMaxBits && groups / (double)(1ull << b) > (double)slots * kAggLoad) ++b;
+    while (b < (uint32_t)kPartMaxBits && groups / (double)(1ull << b) > (double)slots * load) ++b;
     return b;
   };
   // Two pass B CTAs per SM when their tables hold the groups, else one CTA
   // per SM with twice the table.
   uint64_t slots = slots_in(ds->agg_smem_half);
   uint32_t bits = bits_for(slots);
-  const bool two = slots >= 256 && groups / (double)(1ull << bits) <= (double)slots * kAggLoad;
+  const bool two = slots >= 256 && groups / (double)(1ull << bits) <= (double)slots * load;
   if (!two) {
     slots = slots_in(ds->agg_smem_optin);
     bits = bits_for(slots);
   }
-  if (slots < 64 || bits > (uint32_t)kPartMaxBits || groups / (double)(1ull << bits) > (double)slots * kAggLoad)
+  if (slots < 64 || bits > (uint32_t)kPartMaxBits || groups / (double)(1ull << bits) > (double)slots * load)
     return false;
   pp.bits = bits;
   pp.agg_slots = (uint32_t)slots;
@@ -1554,6 +1558,11 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
     sp.part_cursor = static_cast<uint32_t*>(part_cursor);
     sp.part_order = static_cast<uint32_t*>(part_order);
     sp.agg_slots = pp->agg_slots;
+    // DFC_AGG_COLLAPSE_MIN=<n> (tuning): the group size from which pass B
+    // folds a warp's rows of one key by butterflies (33: never).
+    sp.agg_collapse_min = 4;
+    if (const char* env = getenv("DFC_AGG_COLLAPSE_MIN"))
+      if (atoi(env) > 0) sp.agg_collapse_min = atoi(env);
     sp.part_next = &dctl->part_next;
     sp.part_kept = &dctl->part_kept;
   }

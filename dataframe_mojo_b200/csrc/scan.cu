@@ -2422,7 +2422,7 @@ __device__ __forceinline__ void fold_rows(const ScanParams& p, unsigned char* ta
     uint32_t grp = __match_any_sync(0xffffffffu, kw[j]) & __ballot_sync(0xffffffffu, on[j]);
     if (!on[j]) grp = 0;
     int maxpop = __reduce_max_sync(0xffffffffu, (unsigned)__popc(grp));
-    for (int round = 0; round < 2 && maxpop >= kCollapseMin; ++round) {
+    for (int round = 0; round < 2 && maxpop >= p.agg_collapse_min; ++round) {
       const unsigned long long* sp = src[j];
       const uint32_t flags = vf[j];
       const uint64_t first_val = v0[j];

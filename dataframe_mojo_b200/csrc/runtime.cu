@@ -1061,6 +1061,8 @@ bool plan_shared_at(Plan& P, DeviceState* ds, uint64_t est, uint32_t flags, bool
   return false;
 }
 
+bool plan_quad(ScanParams& sp);
+
 // Own tables, then cluster tables, each with the query's ring or else with
 // smaller tiles (down to 256 rows) that leave the tables more room; the ring
 // is restored when nothing fits.  Packed keys only; false: the global table
@@ -1092,6 +1094,9 @@ bool plan_shared(Plan& P, DeviceState* ds, uint64_t est, uint32_t flags) {
         // DFC_NO_REDUCE=1 keeps the per-row path (tuning).
         sp.reduce = sp.n_keys == 0 && sp.smem_cluster <= 1 && sp.comp_mask == 0 && sp.n_vals <= kReduceVals &&
                     !getenv("DFC_NO_REDUCE");
+        // Its rows four at a time when the filter is one range test
+        // (fast_rows; DFC_NO_QUAD=1 keeps one row per lane).
+        if (sp.reduce && !(plan_quad(sp) && !getenv("DFC_NO_QUAD"))) sp.fast_rows = 0;
         return true;
       }
     }

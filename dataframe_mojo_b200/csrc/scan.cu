@@ -1342,6 +1342,116 @@ __device__ void produce_tiles(const ScanParams& p, unsigned char* smem, uint64_t
 }
 
 // ---------------------------------------------------------------------------
+// The quad row path (ScanParams::fast_rows).  Consumer thread g of a step
+// takes rows 4 (g % 256) .. + 3 of the step's tile g / 256 (1024-row tiles),
+// reading each column's four values with one or two vector loads from the
+// stage; the filter is one range test per row and each key column is packed
+// by its size, with no per-row type dispatch.
+// ---------------------------------------------------------------------------
+static_assert(kTilesPerStep * kMaxTileRows / 4 == kPartConsumerThreads, "one quad per consumer thread and step");
+
+struct Quad {
+  int tile;                    // the step's tile, -1: none
+  uint32_t r0;                 // first row inside the tile
+  uint32_t in;                 // rows inside the tile (bits 0..3)
+  bool staged;
+  const unsigned char* stage;  // the tile's stage (staged tiles)
+  uint64_t start;              // the tile's first row
+};
+
+// The tile fields are chosen with compile-time indices (a runtime index
+// into Step would put it in local memory).
+__device__ __forceinline__ Quad quad_of(const Step& s, int nt) {
+  const uint32_t g = threadIdx.x - 32;
+  Quad q;
+  q.tile = (int)(g >> 8);
+  q.r0 = (g & 255u) * 4;
+  const bool second = q.tile != 0;
+  q.staged = second ? s.staged[1] : s.staged[0];
+  q.stage = second ? s.stage[1] : s.stage[0];
+  q.start = second ? s.start[1] : s.start[0];
+  const uint32_t n = second ? s.n[1] : s.n[0];
+  if (q.tile >= nt) {
+    q.tile = -1;
+    q.in = 0;
+    return q;
+  }
+  const uint32_t left = n > q.r0 ? n - q.r0 : 0u;
+  q.in = left >= 4 ? 0xFu : (1u << left) - 1u;
+  return q;
+}
+
+// Raw bits (zero-extended) of the quad's rows of column c.
+__device__ __forceinline__ void quad_load(const ScanParams& p, const Quad& q, int c, uint64_t (&x)[4]) {
+  const int size = p.cols[c].size;
+  if (q.staged) {
+    const unsigned char* at = q.stage + p.stage_off[c] + (size_t)q.r0 * size;
+    switch (size) {
+      case 8: {
+        const ulonglong2 a = reinterpret_cast<const ulonglong2*>(at)[0], b = reinterpret_cast<const ulonglong2*>(at)[1];
+        x[0] = a.x; x[1] = a.y; x[2] = b.x; x[3] = b.y;
+        return;
+      }
+      case 4: {
+        const uint4 a = *reinterpret_cast<const uint4*>(at);
+        x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+        return;
+      }
+      case 2: {
+        const uint2 a = *reinterpret_cast<const uint2*>(at);
+        x[0] = a.x & 0xFFFFu; x[1] = a.x >> 16; x[2] = a.y & 0xFFFFu; x[3] = a.y >> 16;
+        return;
+      }
+      default: {
+        const uint32_t a = *reinterpret_cast<const uint32_t*>(at);
+        x[0] = a & 0xFFu; x[1] = (a >> 8) & 0xFFu; x[2] = (a >> 16) & 0xFFu; x[3] = a >> 24;
+        return;
+      }
+    }
+  }
+  const unsigned char* vals = static_cast<const unsigned char*>(p.cols[c].values) + q.start * (uint64_t)size;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) x[i] = ((q.in >> i) & 1u) ? load_bits(vals, size, q.r0 + i) : 0ull;
+}
+
+// Validity bits of the quad's rows of column c (bits 0..3, rows outside the
+// tile 0).
+__device__ __forceinline__ uint32_t quad_valid(const ScanParams& p, const Quad& q, int c) {
+  const uint32_t* w;
+  if (q.staged) w = p.stage_voff[c] >= 0 ? reinterpret_cast<const uint32_t*>(q.stage + p.stage_voff[c]) : nullptr;
+  else w = p.cols[c].validity ? p.cols[c].validity + q.start / 32 : nullptr;
+  if (w == nullptr || q.in == 0) return q.in;
+  return (w[q.r0 >> 5] >> (q.r0 & 31u)) & q.in;
+}
+
+// Selected rows of the quad (bits 0..3).
+__device__ __forceinline__ uint32_t quad_select(const ScanParams& p, const Quad& q) {
+  if (p.fast_col < 0 || q.in == 0) return q.in;
+  const int c = p.fast_col;
+  uint64_t x[4];
+  quad_load(p, q, c, x);
+  const uint32_t valid = quad_valid(p, q, c);
+  const int dt = p.cols[c].dtype;
+  const int sh = 64 - 8 * p.cols[c].size;
+  uint32_t sel = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    bool v;
+    if (p.fast_kind == FAST_FLOAT) {
+      const double d = bits_to_f64(x[i], dt);
+      v = d >= p.fast_lo.f && d <= p.fast_hi.f;
+    } else if (p.fast_kind == FAST_UNSIGNED) {
+      v = x[i] >= p.fast_lo.u && x[i] <= p.fast_hi.u;
+    } else {
+      const int64_t xi = (int64_t)(x[i] << sh) >> sh;  // sign-extended from the column's size
+      v = xi >= p.fast_lo.i && xi <= p.fast_hi.i;
+    }
+    sel |= (uint32_t)(v != (p.fast_neg != 0)) << i;
+  }
+  return sel & valid;
+}
+
+// ---------------------------------------------------------------------------
 // Ungrouped queries in registers (kScanReduce).  With no key every kept row
 // belongs to one group, and per-row atomics on one record serialise.  Each
 // consumer thread instead keeps the group's state for its own rows in
@@ -1385,12 +1495,103 @@ __device__ __forceinline__ void reduce_init(ReduceState& st) {
 constexpr int kRedWords = 4;  // 1,024-row tiles: 32 words over 8 consumer warps
 static_assert(kRedWords * kScanConsumerWarps * 32 >= kMaxTileRows, "a step's words per warp");
 
+// One valid value of type T folded into `f`.
+template <typename T>
+__device__ __forceinline__ void reduce_one(const T x, bool want_sum, bool want_ext, bool want_m2, ReduceField& f) {
+  constexpr bool kFloat = std::is_floating_point<T>::value;
+  const double xd = (double)x;
+  const bool nan = kFloat && xd != xd;
+  ++f.n;
+  if (want_sum) {
+    if constexpr (kFloat) f.sf += xd;
+    else f.si += (__int128)x;
+  }
+  if (want_ext) {
+    if (nan) {
+      f.flags |= 1u;
+    } else {
+      uint64_t e;
+      if constexpr (kFloat) {
+        const uint64_t u = xd == 0.0 ? 0ull : (uint64_t)__double_as_longlong(xd);
+        e = (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+        if (xd == 0.0) f.flags |= signbit(xd) ? 4u : 2u;
+      } else if constexpr (std::is_unsigned<T>::value) {
+        e = (uint64_t)x;
+      } else {
+        e = (uint64_t)(int64_t)x ^ 0x8000000000000000ull;
+      }
+      if (~e > f.emin) f.emin = ~e;
+      if (e > f.emax) f.emax = e;
+    }
+  }
+  if (want_m2) {
+    if (f.k == 0) f.k = (nan ? kCanonNaN : (uint64_t)__double_as_longlong(xd)) ^ kShiftTag;
+    const double d = xd - __longlong_as_double((long long)(f.k ^ kShiftTag));
+    f.s1 += d;
+    f.s2 += d * d;
+  }
+}
+
+// The quad path (ScanParams::fast_rows, 1,024-row tiles): consumer thread g
+// takes rows 4g .. 4g + 3 of each of the step's tiles, the filter as one
+// range test per row and four values per column from one vector load.
+template <typename T>
+__device__ __forceinline__ void reduce_quad_field(const ValField& vf, uint32_t ok, const uint64_t (&x)[4],
+                                                  ReduceField& f) {
+  const bool want_sum = vf.off_sum >= 0, want_ext = vf.off_min >= 0 || vf.off_max >= 0, want_m2 = vf.off_m2 >= 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    if ((ok >> i) & 1u) reduce_one<T>(from_bits<T>(x[i]), want_sum, want_ext, want_m2, f);
+}
+
+__device__ __forceinline__ void reduce_step_quad(const ScanParams& p, const Step& s, int nt, ReduceState& st) {
+  const uint32_t g = threadIdx.x - 32;
+#pragma unroll
+  for (int k = 0; k < kTilesPerStep; ++k) {
+    if (k >= nt) break;
+    Quad q;
+    q.tile = k;
+    q.r0 = g * 4;
+    q.staged = k ? s.staged[1] : s.staged[0];
+    q.stage = k ? s.stage[1] : s.stage[0];
+    q.start = k ? s.start[1] : s.start[0];
+    const uint32_t n = k ? s.n[1] : s.n[0];
+    const uint32_t left = n > q.r0 ? n - q.r0 : 0u;
+    q.in = left >= 4 ? 0xFu : (1u << left) - 1u;
+    const uint32_t sel = quad_select(p, q);
+    if (!sel) continue;
+    const uint32_t row0 = (uint32_t)(q.start + q.r0);
+    st.first = min(st.first, row0 + (uint32_t)(__ffs(sel) - 1));
+    st.last = max(st.last, row0 + (uint32_t)(32 - __clz(sel)));
+    st.len += (uint32_t)__popc(sel);
+#pragma unroll
+    for (int v = 0; v < kReduceVals; ++v) {
+      if (v >= p.n_vals) break;
+      const ValField& vf = p.vals[v];
+      uint64_t x[4];
+      quad_load(p, q, vf.input, x);
+      const uint32_t ok = quad_valid(p, q, vf.input) & sel;
+      switch (vf.dtype) {
+        case DFC_INT8: reduce_quad_field<int8_t>(vf, ok, x, st.f[v]); break;
+        case DFC_INT16: reduce_quad_field<int16_t>(vf, ok, x, st.f[v]); break;
+        case DFC_INT32: reduce_quad_field<int32_t>(vf, ok, x, st.f[v]); break;
+        case DFC_INT64: reduce_quad_field<int64_t>(vf, ok, x, st.f[v]); break;
+        case DFC_UINT8: reduce_quad_field<uint8_t>(vf, ok, x, st.f[v]); break;
+        case DFC_UINT16: reduce_quad_field<uint16_t>(vf, ok, x, st.f[v]); break;
+        case DFC_UINT32: reduce_quad_field<uint32_t>(vf, ok, x, st.f[v]); break;
+        case DFC_UINT64: reduce_quad_field<uint64_t>(vf, ok, x, st.f[v]); break;
+        case DFC_FLOAT32: reduce_quad_field<float>(vf, ok, x, st.f[v]); break;
+        default: reduce_quad_field<double>(vf, ok, x, st.f[v]); break;
+      }
+    }
+  }
+}
+
 // The lane's kept rows of value column v (type T) folded into `f`: one dtype
 // dispatch per step instead of one per row.
 template <typename T>
 __device__ __forceinline__ void reduce_words(const ScanParams& p, const Step& s, int nt, int v,
                                              const uint32_t (&selw)[2 * kRedWords], ReduceField& f) {
-  constexpr bool kFloat = std::is_floating_point<T>::value;
   const ValField& vf = p.vals[v];
   const int c = vf.input;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1405,38 +1606,7 @@ __device__ __forceinline__ void reduce_words(const ScanParams& p, const Step& s,
       if (!((selw[k * kRedWords + i] >> lane) & 1u)) continue;
       const uint32_t r = (uint32_t)(warp - 1 + i * kScanConsumerWarps) * 32u + (uint32_t)lane;
       if (!valid_at(valid, r)) continue;
-      const T x = load_as<T>(vals, r);
-      const double xd = (double)x;
-      const bool nan = kFloat && xd != xd;
-      ++f.n;
-      if (want_sum) {
-        if constexpr (kFloat) f.sf += xd;
-        else f.si += (__int128)x;
-      }
-      if (want_ext) {
-        if (nan) {
-          f.flags |= 1u;
-        } else {
-          uint64_t e;
-          if constexpr (kFloat) {
-            const uint64_t u = xd == 0.0 ? 0ull : (uint64_t)__double_as_longlong(xd);
-            e = (u >> 63) ? ~u : (u | 0x8000000000000000ull);
-            if (xd == 0.0) f.flags |= signbit(xd) ? 4u : 2u;
-          } else if constexpr (std::is_unsigned<T>::value) {
-            e = (uint64_t)x;
-          } else {
-            e = (uint64_t)(int64_t)x ^ 0x8000000000000000ull;
-          }
-          if (~e > f.emin) f.emin = ~e;
-          if (e > f.emax) f.emax = e;
-        }
-      }
-      if (want_m2) {
-        if (f.k == 0) f.k = (nan ? kCanonNaN : (uint64_t)__double_as_longlong(xd)) ^ kShiftTag;
-        const double d = xd - __longlong_as_double((long long)(f.k ^ kShiftTag));
-        f.s1 += d;
-        f.s2 += d * d;
-      }
+      reduce_one<T>(load_as<T>(vals, r), want_sum, want_ext, want_m2, f);
     }
   }
 }
@@ -1643,8 +1813,11 @@ __device__ __forceinline__ void scan_body(const ScanParams& p) {
         ++nt;
       }
       if constexpr (R == kScanReduce) {
-        // Each lane folds its kept rows of the warp's words into registers.
-        if (!failed) reduce_step(p, s, nt, words, red);
+        // Each lane folds its kept rows into registers.
+        if (!failed) {
+          if (p.fast_rows) reduce_step_quad(p, s, nt, red);
+          else reduce_step(p, s, nt, words, red);
+        }
         if (consumer_sync_or(failed || s_abort)) {
           s_abort = 1;
           break;
@@ -1924,115 +2097,6 @@ __device__ __forceinline__ void ring_init(int S, uint64_t* full, uint64_t* empty
   __syncthreads();
 }
 
-// ---------------------------------------------------------------------------
-// The quad row path (ScanParams::fast_rows).  Consumer thread g of a step
-// takes rows 4 (g % 256) .. + 3 of the step's tile g / 256 (1024-row tiles),
-// reading each column's four values with one or two vector loads from the
-// stage; the filter is one range test per row and each key column is packed
-// by its size, with no per-row type dispatch.
-// ---------------------------------------------------------------------------
-static_assert(kTilesPerStep * kMaxTileRows / 4 == kPartConsumerThreads, "one quad per consumer thread and step");
-
-struct Quad {
-  int tile;                    // the step's tile, -1: none
-  uint32_t r0;                 // first row inside the tile
-  uint32_t in;                 // rows inside the tile (bits 0..3)
-  bool staged;
-  const unsigned char* stage;  // the tile's stage (staged tiles)
-  uint64_t start;              // the tile's first row
-};
-
-// The tile fields are chosen with compile-time indices (a runtime index
-// into Step would put it in local memory).
-__device__ __forceinline__ Quad quad_of(const Step& s, int nt) {
-  const uint32_t g = threadIdx.x - 32;
-  Quad q;
-  q.tile = (int)(g >> 8);
-  q.r0 = (g & 255u) * 4;
-  const bool second = q.tile != 0;
-  q.staged = second ? s.staged[1] : s.staged[0];
-  q.stage = second ? s.stage[1] : s.stage[0];
-  q.start = second ? s.start[1] : s.start[0];
-  const uint32_t n = second ? s.n[1] : s.n[0];
-  if (q.tile >= nt) {
-    q.tile = -1;
-    q.in = 0;
-    return q;
-  }
-  const uint32_t left = n > q.r0 ? n - q.r0 : 0u;
-  q.in = left >= 4 ? 0xFu : (1u << left) - 1u;
-  return q;
-}
-
-// Raw bits (zero-extended) of the quad's rows of column c.
-__device__ __forceinline__ void quad_load(const ScanParams& p, const Quad& q, int c, uint64_t (&x)[4]) {
-  const int size = p.cols[c].size;
-  if (q.staged) {
-    const unsigned char* at = q.stage + p.stage_off[c] + (size_t)q.r0 * size;
-    switch (size) {
-      case 8: {
-        const ulonglong2 a = reinterpret_cast<const ulonglong2*>(at)[0], b = reinterpret_cast<const ulonglong2*>(at)[1];
-        x[0] = a.x; x[1] = a.y; x[2] = b.x; x[3] = b.y;
-        return;
-      }
-      case 4: {
-        const uint4 a = *reinterpret_cast<const uint4*>(at);
-        x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
-        return;
-      }
-      case 2: {
-        const uint2 a = *reinterpret_cast<const uint2*>(at);
-        x[0] = a.x & 0xFFFFu; x[1] = a.x >> 16; x[2] = a.y & 0xFFFFu; x[3] = a.y >> 16;
-        return;
-      }
-      default: {
-        const uint32_t a = *reinterpret_cast<const uint32_t*>(at);
-        x[0] = a & 0xFFu; x[1] = (a >> 8) & 0xFFu; x[2] = (a >> 16) & 0xFFu; x[3] = a >> 24;
-        return;
-      }
-    }
-  }
-  const unsigned char* vals = static_cast<const unsigned char*>(p.cols[c].values) + q.start * (uint64_t)size;
-#pragma unroll
-  for (int i = 0; i < 4; ++i) x[i] = ((q.in >> i) & 1u) ? load_bits(vals, size, q.r0 + i) : 0ull;
-}
-
-// Validity bits of the quad's rows of column c (bits 0..3, rows outside the
-// tile 0).
-__device__ __forceinline__ uint32_t quad_valid(const ScanParams& p, const Quad& q, int c) {
-  const uint32_t* w;
-  if (q.staged) w = p.stage_voff[c] >= 0 ? reinterpret_cast<const uint32_t*>(q.stage + p.stage_voff[c]) : nullptr;
-  else w = p.cols[c].validity ? p.cols[c].validity + q.start / 32 : nullptr;
-  if (w == nullptr || q.in == 0) return q.in;
-  return (w[q.r0 >> 5] >> (q.r0 & 31u)) & q.in;
-}
-
-// Selected rows of the quad (bits 0..3).
-__device__ __forceinline__ uint32_t quad_select(const ScanParams& p, const Quad& q) {
-  if (p.fast_col < 0 || q.in == 0) return q.in;
-  const int c = p.fast_col;
-  uint64_t x[4];
-  quad_load(p, q, c, x);
-  const uint32_t valid = quad_valid(p, q, c);
-  const int dt = p.cols[c].dtype;
-  const int sh = 64 - 8 * p.cols[c].size;
-  uint32_t sel = 0;
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    bool v;
-    if (p.fast_kind == FAST_FLOAT) {
-      const double d = bits_to_f64(x[i], dt);
-      v = d >= p.fast_lo.f && d <= p.fast_hi.f;
-    } else if (p.fast_kind == FAST_UNSIGNED) {
-      v = x[i] >= p.fast_lo.u && x[i] <= p.fast_hi.u;
-    } else {
-      const int64_t xi = (int64_t)(x[i] << sh) >> sh;  // sign-extended from the column's size
-      v = xi >= p.fast_lo.i && xi <= p.fast_hi.i;
-    }
-    sel |= (uint32_t)(v != (p.fast_neg != 0)) << i;
-  }
-  return sel & valid;
-}
 
 // Packed key words of the quad's rows (packed key mode).
 __device__ __forceinline__ void quad_keys(const ScanParams& p, const Quad& q, uint64_t (&kw)[4]) {

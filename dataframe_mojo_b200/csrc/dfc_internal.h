@@ -190,6 +190,7 @@ struct ScanParams {
   uint32_t* part_next;     // pass B work counter
   uint32_t* part_kept;     // rows the counting pass kept (written by partition_offsets)
   int32_t agg_collapse_min;  // pass B: group size in a warp from which its rows fold by butterflies
+  int32_t collapse_min;      // the global-table scan: the same threshold
   // The quad row path of the counting pass and pass A (fast_rows = 1): every
   // lane takes four consecutive rows of a 1024-row tile with vector loads.
   // It needs integer key columns and no filter or one comparison, held in

@@ -636,6 +636,15 @@ dfc_status plan_query(const dfc_query* q, Plan& P) {
     for (int j = 0; j < sp.n_vals; ++j)
       if (sp.vals[j].dtype == DFC_FLOAT32 && sp.vals[j].off_sum >= 0) sp.comp_mask |= 1u << j;
   sp.rec_words = sp.rec_stride / 8;
+  // Group sizes in a warp from which the rows of one key fold by butterflies
+  // (one atomic per field) instead of per-lane atomics: the table scans and
+  // pass B.  DFC_COLLAPSE_MIN / DFC_AGG_COLLAPSE_MIN=<n> (tuning; 33: never).
+  sp.collapse_min = 4;
+  sp.agg_collapse_min = 12;
+  if (const char* env = getenv("DFC_COLLAPSE_MIN"))
+    if (atoi(env) > 0) sp.collapse_min = atoi(env);
+  if (const char* env = getenv("DFC_AGG_COLLAPSE_MIN"))
+    if (atoi(env) > 0) sp.agg_collapse_min = atoi(env);
   // FIRST reads the group's earliest kept row, which maintain_order tracks.
   sp.track_first = ((q->flags & DFC_Q_MAINTAIN_ORDER) || track_first_row) ? 1 : 0;
 
@@ -1563,11 +1572,6 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
     sp.part_cursor = static_cast<uint32_t*>(part_cursor);
     sp.part_order = static_cast<uint32_t*>(part_order);
     sp.agg_slots = pp->agg_slots;
-    // DFC_AGG_COLLAPSE_MIN=<n> (tuning): the group size from which pass B
-    // folds a warp's rows of one key by butterflies (33: never).
-    sp.agg_collapse_min = 4;
-    if (const char* env = getenv("DFC_AGG_COLLAPSE_MIN"))
-      if (atoi(env) > 0) sp.agg_collapse_min = atoi(env);
     sp.part_next = &dctl->part_next;
     sp.part_kept = &dctl->part_kept;
   }

@@ -1084,7 +1084,6 @@ __device__ bool collapse_largest(const ScanParams& p, unsigned char* rec, uint32
   return in;
 }
 
-constexpr int kCollapseMin = 4;  // group size from which a warp folds a group by butterfly
 
 // ---------------------------------------------------------------------------
 // 5. States in the global records.
@@ -1249,7 +1248,7 @@ __device__ __forceinline__ void consume_rows(const ScanParams& p, const Step& s,
     uint32_t grp = __match_any_sync(0xffffffffu, tag) & __ballot_sync(0xffffffffu, sel[j]);
     if (!sel[j]) grp = 0;
     int maxpop = __reduce_max_sync(0xffffffffu, (unsigned)__popc(grp));
-    for (int round = 0; round < 2 && maxpop >= kCollapseMin; ++round) {
+    for (int round = 0; round < 2 && maxpop >= p.collapse_min; ++round) {
       unsigned char* rec = record_at(p, sel[j] ? gid[j] : 0u);
       const RowRef xr = x[j];
       if (collapse_largest(p, rec, grp, maxpop, sel[j], rows[j], [&](int v, bool& ok, uint64_t& b) {

@@ -2274,10 +2274,24 @@ __device__ __forceinline__ void place_rows(const ScanParams& p, const bool (&on)
 // The row's key word, row word and first value, stored together once the
 // row's place is known (the other value columns are already written):
 // consecutive stores to one row let L2 merge them before the line leaves.
+// 24-byte rows (one value column) take two stores: of consecutive rows one
+// starts on a 16-byte boundary (its first two words go as one vector) and the
+// next on 8 mod 16 (its last two words do).  part_buf is 256-byte aligned.
 __device__ __forceinline__ void write_row(const ScanParams& p, unsigned long long* dst, uint64_t kw, uint32_t vflags,
                                           uint32_t row, uint64_t val0) {
+  const uint64_t w1 = (uint64_t)row | ((uint64_t)vflags << 32);
+  if (p.part_words == 3) {
+    if ((reinterpret_cast<uintptr_t>(dst) & 15u) == 0) {
+      *reinterpret_cast<ulonglong2*>(dst) = make_ulonglong2(kw, w1);
+      dst[2] = val0;
+    } else {
+      dst[0] = kw;
+      *reinterpret_cast<ulonglong2*>(dst + 1) = make_ulonglong2(w1, val0);
+    }
+    return;
+  }
   dst[0] = kw;
-  dst[1] = (uint64_t)row | ((uint64_t)vflags << 32);
+  dst[1] = w1;
   if (p.n_vals > 0) dst[2] = val0;
 }
 
@@ -2463,9 +2477,25 @@ __device__ __forceinline__ void fold_rows(const ScanParams& p, unsigned char* ta
     kw[j] = v0[j] = 0;
     row[j] = vf[j] = 0;
     if (!on[j]) continue;
-    kw[j] = __ldcs(src[j]);
-    const uint64_t w1 = __ldcs(src[j] + 1);
-    if (p.n_vals > 0) v0[j] = __ldcs(src[j] + 2);  // the first value column, loaded with the rest
+    uint64_t w1;
+    if (W == 3) {
+      // 24-byte rows: a 16-byte load of the aligned word pair and one 8-byte load.
+      if ((reinterpret_cast<uintptr_t>(src[j]) & 15u) == 0) {
+        const ulonglong2 a = __ldcs(reinterpret_cast<const ulonglong2*>(src[j]));
+        kw[j] = a.x;
+        w1 = a.y;
+        v0[j] = __ldcs(src[j] + 2);
+      } else {
+        kw[j] = __ldcs(src[j]);
+        const ulonglong2 b = __ldcs(reinterpret_cast<const ulonglong2*>(src[j] + 1));
+        w1 = b.x;
+        v0[j] = b.y;
+      }
+    } else {
+      kw[j] = __ldcs(src[j]);
+      w1 = __ldcs(src[j] + 1);
+      if (p.n_vals > 0) v0[j] = __ldcs(src[j] + 2);  // the first value column, loaded with the rest
+    }
     row[j] = (uint32_t)w1;
     vf[j] = (uint32_t)(w1 >> 32);
   }

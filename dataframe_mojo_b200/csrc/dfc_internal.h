@@ -184,6 +184,7 @@ struct ScanParams {
   unsigned long long* part_buf;
   uint32_t* part_totals;   // [partition] selected rows
   uint32_t* part_start;    // [partition] first row of the partition in part_buf
+  uint2* part_range;       // [partition] {part_start, part_totals}: pass A reads both with one load
   uint32_t* part_cursor;   // [partition] rows pass A placed (zeroed before pass A)
   uint32_t* part_order;    // pass B's order of the partitions: the large ones first
   uint32_t agg_slots;      // pass B table slots

@@ -1484,7 +1484,8 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   if (recs >= 0xFFFFFFE0ull) return fail(DFC_CAPACITY, "group capacity exceeds 2^32 - 32 records");
 
   void *table = nullptr, *records, *ctl, *bits, *prefix, *bsums, *perm, *firsts;
-  void *part_buf = nullptr, *part_totals = nullptr, *part_start = nullptr, *part_cursor = nullptr, *part_order = nullptr;
+  void *part_buf = nullptr, *part_totals = nullptr, *part_start = nullptr, *part_cursor = nullptr, *part_order = nullptr,
+       *part_range = nullptr;
   const uint64_t words = (P.rows + 31) / 32;
   const uint64_t chunks = std::max<uint64_t>(1, (words + kFinishChunk - 1) / kFinishChunk);
   const uint64_t nparts = pp ? (1ull << pp->bits) : 0;
@@ -1494,6 +1495,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
     if ((st = S.alloc(&part_buf, P.rows * pp->words * 8, "partition rows"))) return S.release(), st;
     if ((st = S.alloc(&part_totals, nparts * 4, "partition totals"))) return S.release(), st;
     if ((st = S.alloc(&part_start, nparts * 4, "partition starts"))) return S.release(), st;
+    if ((st = S.alloc(&part_range, nparts * 8, "partition ranges"))) return S.release(), st;
     if ((st = S.alloc(&part_cursor, nparts * 4, "partition cursors"))) return S.release(), st;
     if ((st = S.alloc(&part_order, nparts * 4, "partition order"))) return S.release(), st;
   } else {
@@ -1569,6 +1571,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
     sp.part_buf = static_cast<unsigned long long*>(part_buf);
     sp.part_totals = static_cast<uint32_t*>(part_totals);
     sp.part_start = static_cast<uint32_t*>(part_start);
+    sp.part_range = static_cast<uint2*>(part_range);
     sp.part_cursor = static_cast<uint32_t*>(part_cursor);
     sp.part_order = static_cast<uint32_t*>(part_order);
     sp.agg_slots = pp->agg_slots;

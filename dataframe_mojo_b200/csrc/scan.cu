@@ -2208,8 +2208,10 @@ __global__ void __launch_bounds__(1024) partition_offsets(const __grid_constant_
   for (uint32_t k = 0; k < per; ++k) {
     const uint32_t q = q0 + k;
     if (q < nparts) {
+      const uint32_t total = p.part_totals[q];
       p.part_start[q] = run;
-      run += p.part_totals[q];
+      p.part_range[q] = make_uint2(run, total);
+      run += total;
     }
   }
   __syncthreads();
@@ -2263,11 +2265,12 @@ __device__ __forceinline__ void place_rows(const ScanParams& p, const bool (&on)
     dst[j] = nullptr;
     if (!on[j]) continue;
     const uint32_t at = base[j] + (uint32_t)__popc(grp[j] & ((1u << lane) - 1u));
-    if (q[j] >= nparts || at >= __ldg(p.part_totals + q[j])) {
+    const uint2 range = q[j] < nparts ? __ldg(p.part_range + q[j]) : make_uint2(0u, 0u);  // {start, total}
+    if (q[j] >= nparts || at >= range.y) {
       part_check(p, CHK_RANGE);
       continue;
     }
-    dst[j] = p.part_buf + ((uint64_t)__ldg(p.part_start + q[j]) + at) * p.part_words;
+    dst[j] = p.part_buf + ((uint64_t)range.x + at) * p.part_words;
   }
 }
 
@@ -2627,9 +2630,11 @@ __global__ void __launch_bounds__(kAggThreads, 2) partition_aggregate(const __gr
     const uint32_t base_rec = s_base;
     auto copy_out = [&](unsigned char* rec, uint32_t dst) {
       if (dst < p.recs_total) {
-        unsigned long long* out = reinterpret_cast<unsigned long long*>(record_at(p, dst));
+        // Records are a multiple of 16 bytes and 16-byte aligned in the
+        // global array: 16-byte stores (the table's stride is 8 mod 16).
+        ulonglong2* out = reinterpret_cast<ulonglong2*>(record_at(p, dst));
         const unsigned long long* in = reinterpret_cast<const unsigned long long*>(rec);
-        for (size_t q = 0; q < rw; ++q) out[q] = in[q];
+        for (size_t q = 0; q + 1 < rw; q += 2) out[q / 2] = make_ulonglong2(in[q], in[q + 1]);
       }
       reset_record(rec, p.rec_stride);
     };

@@ -1148,11 +1148,16 @@ __device__ __forceinline__ void update_rows(const ScanParams& p, const ValField&
       if (nan) {
         rec_or_u32<kShared>(rec + kRecFlags, 1u << (3 * v));
       } else {
-        uint64_t bits;
-        if constexpr (std::is_same<T, float>::value) bits = __float_as_uint(val[j]);
-        else if constexpr (std::is_same<T, double>::value) bits = (uint64_t)__double_as_longlong(val[j]);
-        else bits = (uint64_t)(typename std::make_unsigned<T>::type)val[j];
-        const uint64_t e = order_encode(bits, f.dtype);
+        // order_encode of the value, by its compile-time type.
+        uint64_t e;
+        if constexpr (kFloat) {
+          const uint64_t u = xd == 0.0 ? 0ull : (uint64_t)__double_as_longlong(xd);
+          e = (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+        } else if constexpr (std::is_unsigned<T>::value) {
+          e = (uint64_t)val[j];
+        } else {
+          e = (uint64_t)(int64_t)val[j] ^ 0x8000000000000000ull;
+        }
         if (f.off_min >= 0 && ~e > lo[j]) rec_max_u64<kShared>(rec + f.off_min, ~e);
         if (f.off_max >= 0 && e > hi[j]) rec_max_u64<kShared>(rec + f.off_max, e);
         if (kFloat && xd == 0.0) rec_or_u32<kShared>(rec + kRecFlags, 1u << (3 * v + (signbit(xd) ? 2 : 1)));

@@ -1007,11 +1007,16 @@ def main() -> int:
         step_retries.append(provider.last_timings()["retries"])
     e1.record(e2e_stream)
     torch.cuda.synchronize()
-    # One more step, after the timed ones and not part of them, read by the
-    # host clock phase by phase: what an end-to-end step is made of.
-    marks = []
-    e2e_step(marks)
-    phases = {k: (b - a) * 1e3 for k, a, b in zip(("upload", "query", "download", "release"), marks, marks[1:])}
+    # Two more steps, after the timed ones and not part of them, read by the
+    # host clock phase by phase (the faster of the two): what an end-to-end
+    # step is made of.
+    phases = None
+    for _ in range(2):
+        marks = []
+        e2e_step(marks)
+        ph = {k: (b - a) * 1e3 for k, a, b in zip(("upload", "query", "download", "release"), marks, marks[1:])}
+        if phases is None or sum(ph.values()) < sum(phases.values()):
+            phases = ph
     provider.set_thread_stream(device, None)
     e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
     et = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local}")

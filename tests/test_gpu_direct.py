@@ -72,3 +72,24 @@ def test_wide_domain_stays_hashed(monkeypatch):
     assert provider.last_timings()["direct_slots"] == 0
     ref, _ = binding.run(plan)
     assert dev.equals(ref)
+
+
+@pytest.mark.parametrize("rows", [0, 1, 37])
+@pytest.mark.parametrize("regime", ["auto", "shared"])
+def test_direct_edge_cases(rows, regime, monkeypatch):
+    """Tiny inputs, all-null keys and a filter that keeps nothing."""
+    from dataframe_mojo_b200 import provider
+
+    monkeypatch.setenv("DATAFRAME_ACCEL_REGIME", regime)
+    rng = np.random.default_rng(rows + 7)
+    a = rng.integers(-3, 4, rows).astype(np.int8)
+    b = rng.integers(0, 9, rows).astype(np.uint16)
+    frame = DataFrame([Series("a", a, np.zeros(rows, bool)), Series("b", b, rng.random(rows) > 0.3),
+                       Series("v", rng.integers(-5, 5, rows).astype(np.int64)),
+                       Series("p", rng.integers(0, 10, rows).astype(np.int32))])
+    for pred in (col("p") < 7, col("p") > 100):
+        plan = frame.lazy().filter(pred).group_by(["a", "b"], maintain_order=True).agg(
+            [col("v").sum().alias("s"), col("v").count().alias("n"), col("v").first().alias("f")])
+        dev = provider.execute(plan)[0]
+        ref, _ = binding.run(plan)
+        assert dev.equals(ref), (rows, regime)

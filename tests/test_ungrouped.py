@@ -194,3 +194,26 @@ def test_gpu_register_path_and_fallback(columns):
     compare_with_oracle(plan, f"register{columns}", float_cols=floats, var_cols=vars_, scales=scales)
     provider.execute(plan)
     assert provider.last_timings()["regime"] == (3 if columns <= 2 else 1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rows", [0, 1, 1025, 4099])
+def test_gpu_register_path_edges(rows):
+    """The register path on tiny and ragged inputs (a partial last tile, a
+    partial quad), all-null values, NaN-only floats and a filter that keeps
+    nothing, against the oracle."""
+    from dataframe_mojo_b200 import provider
+
+    rng = np.random.default_rng(rows + 3)
+    f = np.full(rows, np.nan, np.float32)
+    x = rng.integers(-9, 9, rows).astype(np.int32)
+    frame = DataFrame([Series("x", x, np.zeros(rows, bool)), Series("f", f),
+                       Series("p", rng.integers(0, 10, rows).astype(np.int32))])
+    for pred in (col("p") < 6, col("p") > 50, None):
+        lf = frame.lazy() if pred is None else frame.lazy().filter(pred)
+        plan = lf.select([col("x").sum().alias("s"), col("x").count().alias("n"), col("x").min().alias("lo"),
+                          col("f").sum().alias("fs"), col("f").max().alias("fh"), col("f").var().alias("fv"),
+                          col("f").len().alias("len")])
+        dev = provider.execute(plan)[0]
+        ref, _ = binding.run(plan)
+        assert dev.equals(ref), (rows, pred, row(dev), row(ref))

@@ -108,6 +108,12 @@ class Timings(C.Structure):
     ]
 
 
+class ByteCostC(C.Structure):
+    """dfc_byte_cost."""
+
+    _fields_ = [("fixed_ns", C.c_double), ("ns_per_byte", C.c_double)]
+
+
 class DeviceColumnDesc(C.Structure):
     """dfc_device_column: a column in device memory, read in place."""
 
@@ -188,6 +194,7 @@ SIGNATURES = [
     ),
     ("dfc_result_copy_to_host", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     ("dfc_result_copy_to_device", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    ("dfc_measure_transfer", C.c_int, [C.c_int32, C.c_uint64, C.c_void_p, C.c_void_p]),
     ("dfc_result_free", None, [C.c_void_p]),
     ("dfc_result_residence", C.c_void_p, [C.c_void_p, C.c_int32]),
     ("dfc_result_validity_residence", C.c_void_p, [C.c_void_p, C.c_int32]),

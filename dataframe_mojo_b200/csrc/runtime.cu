@@ -1785,6 +1785,62 @@ DFC_API dfc_status dfc_device_info_get(int32_t ordinal, dfc_device_info* out) {
   return DFC_OK;
 }
 
+DFC_API dfc_status dfc_measure_transfer(int32_t device, uint64_t bytes, dfc_byte_cost* to_device,
+                                        dfc_byte_cost* to_host) {
+  if (!to_device || !to_host) return fail(DFC_INVALID, "null output");
+  const uint64_t small = 4096;
+  if (bytes < 2 * small) return fail(DFC_INVALID, "measure at least 8 KiB");
+  DeviceState* ds;
+  dfc_status st = device_ready(device, &ds);
+  if (st) return st;
+  DeviceGuard guard(device);
+  cudaStream_t stream = thread_stream(device);
+  void* host = nullptr;
+  void* dev = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  auto done = [&](dfc_status s) {
+    if (dev) cudaFreeAsync(dev, stream);
+    cudaStreamSynchronize(stream);
+    if (host) cudaFreeHost(host);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    return s;
+  };
+  cudaError_t e = cudaHostAlloc(&host, bytes, cudaHostAllocDefault);
+  if (e == cudaSuccess) e = pool_alloc(&dev, bytes, stream);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  if (e != cudaSuccess) return done(cuda_fail(e, "transfer buffers"));
+  memset(host, 0, bytes);
+  // The best of three timed copies (after one untimed) of n bytes.
+  auto best_ms = [&](uint64_t n, bool h2d, float& out) -> cudaError_t {
+    out = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+      cudaError_t r = cudaEventRecord(e0, stream);
+      if (r == cudaSuccess)
+        r = h2d ? cudaMemcpyAsync(dev, host, n, cudaMemcpyHostToDevice, stream)
+                : cudaMemcpyAsync(host, dev, n, cudaMemcpyDeviceToHost, stream);
+      if (r == cudaSuccess) r = cudaEventRecord(e1, stream);
+      if (r == cudaSuccess) r = cudaEventSynchronize(e1);
+      float ms = 0;
+      if (r == cudaSuccess) r = cudaEventElapsedTime(&ms, e0, e1);
+      if (r != cudaSuccess) return r;
+      if (rep > 0) out = std::min(out, ms);
+    }
+    return cudaSuccess;
+  };
+  for (int dir = 0; dir < 2; ++dir) {
+    float t_small = 0, t_large = 0;
+    e = best_ms(small, dir == 0, t_small);
+    if (e == cudaSuccess) e = best_ms(bytes, dir == 0, t_large);
+    if (e != cudaSuccess) return done(cuda_fail(e, "transfer measurement"));
+    dfc_byte_cost& c = dir == 0 ? *to_device : *to_host;
+    c.ns_per_byte = std::max(0.0, ((double)t_large - (double)t_small) * 1e6 / (double)(bytes - small));
+    c.fixed_ns = std::max(0.0, (double)t_small * 1e6 - c.ns_per_byte * (double)small);
+  }
+  return done(DFC_OK);
+}
+
 DFC_API dfc_status dfc_set_memory_limit(int32_t device, int64_t bytes) {
   if (device < 0 || device >= 64) return fail(DFC_INVALID, "device ordinal out of range");
   g_memory_limit[device].store(bytes > 0 ? bytes : 0);

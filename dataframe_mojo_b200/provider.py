@@ -24,7 +24,7 @@ import ctypes as C
 import os
 import threading
 import time
-from dataclasses import dataclass
+from dataclasses import dataclass, field
 
 import numpy as np
 
@@ -632,10 +632,31 @@ class DeviceInfo:
 
 
 @dataclass
+class ByteCost:
+    """`fixed_ns + ns_per_byte * bytes` nanoseconds; negative: not measured
+    (dataframe/devices.mojo:44-56)."""
+
+    fixed_ns: float = -1.0
+    ns_per_byte: float = -1.0
+
+    def measured(self) -> bool:
+        return self.fixed_ns >= 0 and self.ns_per_byte >= 0
+
+    def cost(self, nbytes: int) -> float:
+        return self.fixed_ns + self.ns_per_byte * nbytes
+
+
+@dataclass
 class TransferModel:
-    host_to_device_bytes_per_ns: float = -1.0
-    device_to_host_bytes_per_ns: float = -1.0
-    context_ns: float = -1.0
+    """Host <-> device copy costs measured on this machine
+    (dataframe/devices.mojo:59-80); startup_ns is not measured here."""
+
+    to_device: ByteCost = field(default_factory=ByteCost)
+    to_host: ByteCost = field(default_factory=ByteCost)
+    startup_ns: float = -1.0
+
+    def measured(self) -> bool:
+        return self.to_device.measured() and self.to_host.measured()
 
 
 @dataclass
@@ -674,22 +695,11 @@ _transfer: dict[int, TransferModel] = {}
 
 
 def calibrate_transfer(device: int, nbytes: int = 1 << 28) -> TransferModel:
-    """Measures pinned host<->device copy rates once (torch pinned buffers)."""
-    import torch
-
-    with torch.cuda.device(device):
-        h = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
-        d = torch.empty(nbytes, dtype=torch.uint8, device=f"cuda:{device}")
-        d.copy_(h, non_blocking=True)
-        torch.cuda.synchronize(device)
-        t0 = time.perf_counter_ns()
-        d.copy_(h, non_blocking=True)
-        torch.cuda.synchronize(device)
-        t1 = time.perf_counter_ns()
-        h.copy_(d, non_blocking=True)
-        torch.cuda.synchronize(device)
-        t2 = time.perf_counter_ns()
-    m = TransferModel(nbytes / max(1, t1 - t0), nbytes / max(1, t2 - t1), -1.0)
+    """Measures pinned host <-> device copies once (dfc_measure_transfer) and
+    keeps the model for transfer_model()."""
+    to_dev, to_host = N.ByteCostC(), N.ByteCostC()
+    _check(N.lib().dfc_measure_transfer(device, nbytes, C.byref(to_dev), C.byref(to_host)))
+    m = TransferModel(ByteCost(to_dev.fixed_ns, to_dev.ns_per_byte), ByteCost(to_host.fixed_ns, to_host.ns_per_byte))
     _transfer[device] = m
     return m
 

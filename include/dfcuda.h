@@ -115,6 +115,20 @@ DFC_API int32_t dfc_installed(void);
 DFC_API int32_t dfc_device_count(void);
 DFC_API dfc_status dfc_device_info_get(int32_t ordinal, dfc_device_info* out);
 
+/* A copy's cost, `fixed_ns + ns_per_byte * bytes` nanoseconds (the
+ * reference's ByteCost, dataframe/devices.mojo:44-56). */
+typedef struct dfc_byte_cost {
+  double fixed_ns;
+  double ns_per_byte;
+} dfc_byte_cost;
+
+/* Measures pinned host <-> device copies on `device` (provider
+ * transfer_model(), dataframe/devices.mojo:59-80): the best of three copies
+ * of 4 KiB and of `bytes` each way, timed by CUDA events, fitted to a fixed
+ * cost and a cost per byte.  Creates the device's context. */
+DFC_API dfc_status dfc_measure_transfer(int32_t device, uint64_t bytes, dfc_byte_cost* to_device,
+                                        dfc_byte_cost* to_host);
+
 /* ------------------------------------------------------------------------ */
 /* Device column handoff: typed values plus an Arrow LSB-first validity     */
 /* bitmap, resident in HBM across queries.                                  */

@@ -68,3 +68,18 @@ def test_run_pipeline_result_is_resident_and_feeds_a_device_query():
     assert got.equals(want)
     for c in cols.values():
         c.release()
+
+
+@pytest.mark.gpu
+def test_transfer_model_is_measured():
+    """dfc_measure_transfer: pinned copies fitted to the reference's ByteCost
+    (fixed_ns + ns_per_byte x bytes, dataframe/devices.mojo:44-80); PCIe
+    rates lie between 1 and 200 GB/s."""
+    m = provider.calibrate_transfer(0, 1 << 26)
+    assert m.measured() and provider.transfer_model(0) == m
+    for c in (m.to_device, m.to_host):
+        assert 1 / 200 <= c.ns_per_byte <= 1.0, c
+        assert 0 <= c.fixed_ns < 1e6, c
+        assert c.cost(1 << 30) > c.cost(1 << 20)
+    with pytest.raises(provider.UnsupportedError):
+        provider.calibrate_transfer(0, 1024)  # below 8 KiB: DFC_INVALID

@@ -2242,34 +2242,25 @@ __global__ void __launch_bounds__(1024) partition_offsets(const __grid_constant_
 
 // Pass A.  Dynamic shared memory: the ring of every staged column and its
 // mbarriers.  Each selected row goes to part_start[q] + a place reserved on
-// q's cursor: the lanes of a warp with the same partition reserve together
-// (__match_any_sync), the lowest of them adds their count to the cursor, and
-// the reservations of all of a lane's row slots are in flight at once.
+// q's cursor by one atomic per row; the reservations of all of a lane's row
+// slots are in flight at once.  (With thousands of partitions the lanes of a
+// warp rarely share one, and reserving per warp group with __match_any_sync
+// cost more than it saved: 1.91 against 1.69 ms on 100M rows.)
 // RS row slots per lane: kSR rows (generic path) or a quad.
 template <int RS>
 __device__ __forceinline__ void place_rows(const ScanParams& p, const bool (&on)[RS], const uint64_t (&kw)[RS],
                                            unsigned long long* (&dst)[RS]) {
-  const int lane = threadIdx.x & 31;
   const uint32_t nparts = 1u << p.part_bits;
-  uint32_t q[RS], grp[RS], base[RS];
-  int lead[RS];
+  uint32_t q[RS], base[RS];
+#pragma unroll
+  for (int j = 0; j < RS; ++j) q[j] = on[j] ? partition_of(p, kw[j]) : 0u;
+#pragma unroll
+  for (int j = 0; j < RS; ++j) base[j] = on[j] && q[j] < nparts ? atomicAdd(&p.part_cursor[q[j]], 1u) : 0u;
 #pragma unroll
   for (int j = 0; j < RS; ++j) {
-    q[j] = on[j] ? partition_of(p, kw[j]) : 0u;
-    grp[j] = __match_any_sync(0xffffffffu, on[j] ? q[j] : (0x80000000u | (uint32_t)lane));
-    lead[j] = __ffs(grp[j]) - 1;
-  }
-#pragma unroll
-  for (int j = 0; j < RS; ++j) {
-    base[j] = 0;
-    if (on[j] && lane == lead[j]) base[j] = atomicAdd(&p.part_cursor[q[j]], (uint32_t)__popc(grp[j]));
-  }
-#pragma unroll
-  for (int j = 0; j < RS; ++j) {
-    base[j] = __shfl_sync(0xffffffffu, base[j], lead[j]);
     dst[j] = nullptr;
     if (!on[j]) continue;
-    const uint32_t at = base[j] + (uint32_t)__popc(grp[j] & ((1u << lane) - 1u));
+    const uint32_t at = base[j];
     const uint2 range = q[j] < nparts ? __ldg(p.part_range + q[j]) : make_uint2(0u, 0u);  // {start, total}
     if (q[j] >= nparts || at >= range.y) {
       part_check(p, CHK_RANGE);

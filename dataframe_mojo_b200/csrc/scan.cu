@@ -2511,7 +2511,11 @@ __device__ __forceinline__ void fold_rows(const ScanParams& p, unsigned char* ta
   // Hot keys: the warp's largest group per row slot folds by butterflies.
 #pragma unroll
   for (int j = 0; j < kBR; ++j) {
-    uint32_t grp = __match_any_sync(0xffffffffu, kw[j]) & __ballot_sync(0xffffffffu, on[j]);
+    // Rows of one key found the same record: match the record's offset in
+    // the table (32 bits) rather than the 64-bit key word.
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t tag = on[j] ? (uint32_t)(recs[j] - table) : (0x80000000u | lane);
+    uint32_t grp = __match_any_sync(0xffffffffu, tag);
     if (!on[j]) grp = 0;
     int maxpop = __reduce_max_sync(0xffffffffu, (unsigned)__popc(grp));
     for (int round = 0; round < 2 && maxpop >= p.agg_collapse_min; ++round) {

@@ -316,30 +316,67 @@ __device__ uint64_t output_cell(const FinishParams& f, const OutCol& oc, const u
   return 0;
 }
 
+// A warp finishes 32 groups at a time, in rank order.  Their records lie
+// at random places of `records`, so the warp first copies the 32 records
+// whole into its slab of shared memory (16-byte loads, all issued before the
+// first store) and finishes every column from there: one round trip to HBM
+// per record instead of one per dependent field load.  A slab slot is the
+// record stride + 8 bytes, so the lanes' 8-byte field reads of one offset
+// fall on distinct banks.  Dynamic shared memory: finish_output_smem().
+//
 // Output columns with any null are noted per block in shared memory and
 // reported with one global atomicOr per block and column (a per-warp atomic
 // on the same word serialises in L2 when most warps hold a null group).
 __global__ void finish_output(const __grid_constant__ FinishParams f) {
   const ScanParams& p = f.scan;
+  extern __shared__ __align__(16) unsigned char slabs[];
   __shared__ uint32_t block_nulls[kMaxOut];
-  __shared__ __align__(16) unsigned char zero_record[kMaxRecWords * 8];
   for (int c = threadIdx.x; c < kMaxOut; c += blockDim.x) block_nulls[c] = 0;
-  for (int w = threadIdx.x; w < kMaxRecWords; w += blockDim.x) reinterpret_cast<uint64_t*>(zero_record)[w] = 0;
   __syncthreads();
   const uint32_t G = f.groups[0];
+  const uint64_t handed = records_handed_out(p);
+  const uint32_t R = (uint32_t)p.rec_stride;  // a multiple of 16
+  const uint32_t slot = R + 8;
+  const uint32_t chunks = R / 16;  // 16-byte pieces per record
+  const uint32_t pieces = 32 * chunks;
   const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const uint64_t gwarp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
+  unsigned char* slab = slabs + (size_t)(threadIdx.x >> 5) * 32 * slot;
   for (uint64_t wbase = gwarp * 32; wbase < G; wbase += warps * 32) {
     const uint64_t i = wbase + lane;
     bool active = i < G;
     const uint32_t gid = active ? f.perm[i] : 0u;
+    // The identity record (no group seen, no keys) finishes from zeros.
     const bool identity = active && gid == kIdentityRecord && p.n_keys == 0;
-    if (active && !identity && gid >= records_handed_out(p)) {
+    if (active && !identity && gid >= handed) {
       atomicOr(p.status + 2, CHK_PERM);
       active = false;
     }
-    const unsigned char* rec = identity ? zero_record : active ? record_at(p, gid) : nullptr;
+    const bool fetch = active && !identity;
+    for (uint32_t base = 0; base < pieces; base += 128) {
+      uint4 v[4];
+      uint32_t at[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const uint32_t idx = base + (uint32_t)k * 32 + (uint32_t)lane;
+        const uint32_t j = idx / chunks, c = idx - j * chunks;
+        const uint32_t g = __shfl_sync(0xffffffffu, gid, (int)(j & 31));
+        const bool want = __shfl_sync(0xffffffffu, fetch, (int)(j & 31));
+        at[k] = idx < pieces ? j * slot + c * 16 : 0xFFFFFFFFu;
+        v[k] = make_uint4(0u, 0u, 0u, 0u);
+        if (idx < pieces && want) v[k] = __ldg(reinterpret_cast<const uint4*>(record_at(p, g) + (size_t)c * 16));
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (at[k] == 0xFFFFFFFFu) continue;
+        uint2* d = reinterpret_cast<uint2*>(slab + at[k]);
+        d[0] = make_uint2(v[k].x, v[k].y);
+        d[1] = make_uint2(v[k].z, v[k].w);
+      }
+    }
+    __syncwarp();
+    const unsigned char* rec = slab + (size_t)lane * slot;
     for (int c = 0; c < f.n_out; ++c) {
       const OutCol& oc = f.out[c];
       bool ok = false;
@@ -353,6 +390,7 @@ __global__ void finish_output(const __grid_constant__ FinishParams f) {
         if (bits != want) block_nulls[c] = 1u;
       }
     }
+    __syncwarp();  // the slab is refilled next
   }
   __syncthreads();
   for (int c = threadIdx.x; c < f.n_out; c += blockDim.x)

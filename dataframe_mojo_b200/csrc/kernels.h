@@ -10,6 +10,9 @@ constexpr int kScanConsumerWarps = 8;
 constexpr int kScanConsumerThreads = kScanConsumerWarps * 32;
 constexpr int kScanThreads = kScanConsumerThreads + 32;  // + one producer warp
 constexpr int kFinishThreads = 256;
+// finish_output's dynamic shared memory: one slab slot (record stride + 8
+// bytes) per thread.
+inline size_t finish_output_smem(int rec_stride) { return (size_t)kFinishThreads * ((size_t)rec_stride + 8); }
 constexpr int kFinishChunk = 4096;  // bitmap words per prefix-scan block
 
 // The scan, one kernel per table regime: the global table only, per-CTA

@@ -266,6 +266,10 @@ dfc_status device_ready(int dev, DeviceState** out) {
     d.agg_smem_half = (prop.sharedMemPerMultiprocessor - 2 * prop.reservedSharedMemPerBlock) / 2 - fa.sharedSizeBytes;
     CK(cudaFuncSetAttribute(partition_aggregate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.agg_smem_optin),
        "cudaFuncSetAttribute");
+    // The output kernel stages each warp's records in shared memory.
+    CK(cudaFuncSetAttribute(finish_output, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)finish_output_smem(kMaxRecWords * 8)),
+       "cudaFuncSetAttribute");
     d.ready = true;
   }
   *out = &d;
@@ -1639,7 +1643,7 @@ dfc_status run_attempt(const dfc_query* q, Plan& P, DeviceState* ds, cudaStream_
   finish_word_prefix<<<(unsigned)chunks, 1024, 0, stream>>>(fp);
   finish_rank<<<std::max(1u, rec_blocks), kFinishThreads, 0, stream>>>(fp);
   const unsigned out_blocks = (unsigned)std::min<uint64_t>((out_rows + kFinishThreads - 1) / kFinishThreads, (uint64_t)ds->sms * 16);
-  finish_output<<<std::max(1u, out_blocks), kFinishThreads, 0, stream>>>(fp);
+  finish_output<<<std::max(1u, out_blocks), kFinishThreads, finish_output_smem(fp.scan.rec_stride), stream>>>(fp);
   t_timings.launches += 6;
   cudaEventRecord(ev[2], stream);
   e = cudaGetLastError();
@@ -2619,7 +2623,7 @@ DFC_API dfc_status dfc_groupby_noalloc(const dfc_query* query, int32_t device, u
     finish_rank<<<std::max(1u, rec_blocks), kFinishThreads, 0, stream>>>(fp);
     const unsigned out_blocks =
         (unsigned)std::min<uint64_t>((out_rows + kFinishThreads - 1) / kFinishThreads, (uint64_t)ds->sms * 16);
-    finish_output<<<std::max(1u, out_blocks), kFinishThreads, 0, stream>>>(fp);
+    finish_output<<<std::max(1u, out_blocks), kFinishThreads, finish_output_smem(fp.scan.rec_stride), stream>>>(fp);
     t_timings.launches += 6;
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
@@ -2843,7 +2847,7 @@ void launch_item(BatchItem& it, DeviceState* ds, unsigned char* base, Control* d
   finish_word_prefix<<<(unsigned)it.chunks, 1024, 0, stream>>>(fp);
   finish_rank<<<std::max(1u, rec_blocks), kFinishThreads, 0, stream>>>(fp);
   const unsigned out_blocks = (unsigned)std::min<uint64_t>((it.out_rows + kFinishThreads - 1) / kFinishThreads, (uint64_t)ds->sms * 16);
-  finish_output<<<std::max(1u, out_blocks), kFinishThreads, 0, stream>>>(fp);
+  finish_output<<<std::max(1u, out_blocks), kFinishThreads, finish_output_smem(fp.scan.rec_stride), stream>>>(fp);
 }
 
 }  // namespace

@@ -1305,6 +1305,16 @@ __device__ __forceinline__ void consume_rows(const ScanParams& p, const Step& s,
   }
 }
 
+// A consumer's ring position: its tile count modulo 2S, so that the slot is
+// the position modulo S and the phase is whether it is >= S, advanced by at
+// most two tiles at a time with no division by the runtime stage count.
+__device__ __forceinline__ uint32_t ring_pos(uint32_t it, uint32_t k, uint32_t S) {
+  const uint32_t x = it + k;
+  return x >= 2 * S ? x - 2 * S : x;
+}
+__device__ __forceinline__ uint32_t ring_slot(uint32_t x, uint32_t S) { return x >= S ? x - S : x; }
+__device__ __forceinline__ uint32_t ring_phase(uint32_t x, uint32_t S) { return x >= S ? 1u : 0u; }
+
 // The producer (one thread): every tile of this CTA (t = blockIdx.x, +
 // gridDim.x, ...) into the ring of S stages, as bulk copies of the first
 // n_stage staged columns (tile_tx bytes a full tile) completing on full[s];
@@ -1802,7 +1812,7 @@ __device__ __forceinline__ void scan_body(const ScanParams& p) {
         s.staged[k] = false;
         s.stage[k] = smem;
         if (tk >= p.tiles || failed) continue;
-        const uint32_t sid = (it + k) % S, ph = ((it + k) / S) & 1u;
+        const uint32_t x = ring_pos(it, (uint32_t)k, (uint32_t)S), sid = ring_slot(x, (uint32_t)S), ph = ring_phase(x, (uint32_t)S);
         if (!mbar_wait_bounded(&full[sid], ph, kWaitLimit)) {
           atomicOr(p.status, ST_TIMEOUT);
           s_abort = 1;
@@ -1828,8 +1838,8 @@ __device__ __forceinline__ void scan_body(const ScanParams& p) {
         }
         __syncwarp();
         for (int k = 0; k < nt; ++k)
-          if (lane == 0) mbar_arrive(&empty[(it + k) % S]);
-        it += nt;
+          if (lane == 0) mbar_arrive(&empty[ring_slot(ring_pos(it, (uint32_t)k, (uint32_t)S), (uint32_t)S)]);
+        it = ring_pos(it, (uint32_t)nt, (uint32_t)p.stages);
         continue;
       }
       // 1 + 2: selection words and compaction into s_idx[b].
@@ -1859,8 +1869,8 @@ __device__ __forceinline__ void scan_body(const ScanParams& p) {
         consume_rows<R>(p, s, s_idx[b], nsel, base, shift, &s_claim, p.smem_slots ? &st : nullptr);
       __syncwarp();
       for (int k = 0; k < nt; ++k)
-        if (lane == 0) mbar_arrive(&empty[(it + k) % S]);
-      it += nt;
+        if (lane == 0) mbar_arrive(&empty[ring_slot(ring_pos(it, (uint32_t)k, (uint32_t)S), (uint32_t)S)]);
+      it = ring_pos(it, (uint32_t)nt, (uint32_t)p.stages);
     }
     if (R == kScanReduce && p.smem_slots && !s_abort) reduce_flush(p, red, OwnRec{st.recs});
   }
@@ -2049,7 +2059,7 @@ __device__ __forceinline__ bool step_wait(const ScanParams& p, unsigned char* sm
     s.staged[k] = false;
     s.stage[k] = smem;
     if (tk >= p.tiles) continue;
-    const uint32_t sid = (it + k) % S, ph = ((it + k) / S) & 1u;
+    const uint32_t x = ring_pos(it, (uint32_t)k, (uint32_t)S), sid = ring_slot(x, (uint32_t)S), ph = ring_phase(x, (uint32_t)S);
     if (*s_abort || !mbar_wait_bounded(&full[sid], ph, kWaitLimit)) {
       atomicOr(p.status, ST_TIMEOUT);
       *s_abort = 1;
@@ -2085,7 +2095,7 @@ __device__ __forceinline__ void step_rows(const ScanParams& p, const Step& s, in
 __device__ __forceinline__ void step_release(const ScanParams& p, uint64_t* empty, uint32_t it, int nt) {
   __syncwarp();
   if ((threadIdx.x & 31) == 0)
-    for (int k = 0; k < nt; ++k) mbar_arrive(&empty[(it + k) % p.stages]);
+    for (int k = 0; k < nt; ++k) mbar_arrive(&empty[ring_slot(ring_pos(it, (uint32_t)k, (uint32_t)p.stages), (uint32_t)p.stages)]);
 }
 
 // Ring set-up shared by the counting pass and pass A.
@@ -2147,7 +2157,7 @@ __device__ __forceinline__ void count_body(const ScanParams& p) {
           quad_keys(p, q, kw);
         }
         step_release(p, empty, it, nt);
-        it += nt;
+        it = ring_pos(it, (uint32_t)nt, (uint32_t)p.stages);
 #pragma unroll
         for (int i = 0; i < 4; ++i)
           if ((sel >> i) & 1u) atomicAdd(&s_count[partition_of(p, kw[i])], 1u);
@@ -2158,7 +2168,7 @@ __device__ __forceinline__ void count_body(const ScanParams& p) {
         step_rows(p, s, nt, x, bits);
         key_words<kSR>(p, s, x, kw);
         step_release(p, empty, it, nt);
-        it += nt;
+        it = ring_pos(it, (uint32_t)nt, (uint32_t)p.stages);
 #pragma unroll
         for (int j = 0; j < kSR; ++j)
           if (x[j].on) atomicAdd(&s_count[partition_of(p, kw[j])], 1u);
@@ -2344,7 +2354,7 @@ __device__ __forceinline__ void place_body(const ScanParams& p) {
       }
       const uint64_t row0 = q.start + q.r0;
       step_release(p, empty, it, nt);
-      it += nt;
+      it = ring_pos(it, (uint32_t)nt, (uint32_t)p.stages);
 #pragma unroll
       for (int i = 0; i < 4; ++i)
         if (dst[i]) write_row(p, dst[i], kw[i], vflags[i], (uint32_t)(row0 + i), val0[i]);
@@ -2376,7 +2386,7 @@ __device__ __forceinline__ void place_body(const ScanParams& p) {
         }
       }
       step_release(p, empty, it, nt);
-      it += nt;
+      it = ring_pos(it, (uint32_t)nt, (uint32_t)p.stages);
 #pragma unroll
       for (int j = 0; j < kSR; ++j)
         if (dst[j]) write_row(p, dst[j], kw[j], vflags[j], (uint32_t)(s.start[x[j].tile] + x[j].r), val0[j]);

@@ -2192,59 +2192,84 @@ __global__ void __launch_bounds__(kPartThreads, 1) partition_count_quad(const __
 // The partitions' exclusive prefix (one CTA of 1024 threads), and pass B's
 // order: partitions holding more than four times the average rows (hot keys)
 // first, so none of them starts late and leaves one CTA working alone at the
-// end.
+// end.  Both walk the partitions in rows of 1024 (thread t takes partition
+// r * 1024 + t), so every load and store of a warp is one contiguous run:
+// a block scan per row with a running carry, then one shared-memory atomic
+// per warp and class for the order, the lanes ranked by their ballot.
 __global__ void __launch_bounds__(1024) partition_offsets(const __grid_constant__ ScanParams p) {
   __shared__ uint32_t s_warp[32];
-  __shared__ uint32_t s_total, s_big, s_small;
+  __shared__ uint32_t s_next_big, s_small;
   const uint32_t nparts = 1u << p.part_bits;
-  const uint32_t per = (nparts + blockDim.x - 1) / blockDim.x;
-  const uint32_t q0 = threadIdx.x * per;
-  uint32_t sum = 0;
-  for (uint32_t k = 0; k < per; ++k)
-    if (q0 + k < nparts) sum += p.part_totals[q0 + k];
+  const uint32_t B = blockDim.x;  // 1024: a multiple of 32
+  const uint32_t nw = B / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t x = sum;
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
+  const uint32_t below = (1u << lane) - 1u;
+  uint32_t carry = 0;  // rows of the partitions before this row of partitions
+  for (uint32_t r0 = 0; r0 < nparts; r0 += B) {
+    const uint32_t q = r0 + threadIdx.x;
+    const uint32_t v = q < nparts ? p.part_totals[q] : 0u;
+    uint32_t x = v;  // inclusive prefix inside the warp
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      const uint32_t w = lane < (int)nw ? s_warp[lane] : 0u;
+      uint32_t z = w;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, z, o);
+        if (lane >= o) z += y;
+      }
+      if (lane < (int)nw) s_warp[lane] = z - w;  // exclusive over the warps
+    }
+    __syncthreads();
+    const uint32_t ex = carry + s_warp[warp] + x - v;
+    if (q < nparts) {
+      p.part_start[q] = ex;
+      p.part_range[q] = make_uint2(ex, v);
+    }
+    // The next row's carry: the last thread's inclusive prefix (after every
+    // thread has read its warp's offset).
+    __syncthreads();
+    if (threadIdx.x == B - 1) s_warp[0] = ex + v;
+    __syncthreads();
+    carry = s_warp[0];
+    __syncthreads();
   }
-  if (lane == 31) s_warp[warp] = x;
-  if (threadIdx.x == 0) s_big = 0;
+  const uint32_t total = carry;
+  if (threadIdx.x == 0) {
+    *p.part_kept = total;
+    s_next_big = 0;
+  }
+  const uint64_t big_rows = 4ull * total / nparts;
+  uint32_t nbig = 0;
+  for (uint32_t q = threadIdx.x; q < nparts; q += B)
+    if (p.part_totals[q] > big_rows) ++nbig;
+  nbig = __reduce_add_sync(0xffffffffu, nbig);
+  if (lane == 0) s_warp[warp] = nbig;
   __syncthreads();
-  uint32_t before = 0;
-  for (int w = 0; w < warp; ++w) before += s_warp[w];
   if (threadIdx.x == 0) {
     uint32_t t = 0;
-    for (int w = 0; w < (int)(blockDim.x / 32); ++w) t += s_warp[w];
-    s_total = t;
-    *p.part_kept = t;
+    for (uint32_t w = 0; w < nw; ++w) t += s_warp[w];
+    s_small = t;  // the small partitions follow the big ones
   }
-  uint32_t run = before + x - sum;
-  for (uint32_t k = 0; k < per; ++k) {
-    const uint32_t q = q0 + k;
-    if (q < nparts) {
-      const uint32_t total = p.part_totals[q];
-      p.part_start[q] = run;
-      p.part_range[q] = make_uint2(run, total);
-      run += total;
+  __syncthreads();
+  for (uint32_t r0 = 0; r0 < nparts; r0 += B) {
+    const uint32_t q = r0 + threadIdx.x;
+    const bool valid = q < nparts;
+    const bool big = valid && p.part_totals[q] > big_rows;
+    const uint32_t mb = __ballot_sync(0xffffffffu, big), ms = __ballot_sync(0xffffffffu, valid && !big);
+    uint32_t bb = 0, bs = 0;
+    if (lane == 0) {
+      if (mb) bb = atomicAdd(&s_next_big, (uint32_t)__popc(mb));
+      if (ms) bs = atomicAdd(&s_small, (uint32_t)__popc(ms));
     }
-  }
-  __syncthreads();
-  const uint64_t big_rows = 4ull * s_total / nparts;
-  uint32_t nbig = 0;
-  for (uint32_t k = 0; k < per; ++k)
-    if (q0 + k < nparts && p.part_totals[q0 + k] > big_rows) ++nbig;
-  if (nbig) atomicAdd(&s_big, nbig);
-  __syncthreads();
-  if (threadIdx.x == 0) s_small = s_big;
-  __syncthreads();
-  __shared__ uint32_t s_next_big;
-  if (threadIdx.x == 0) s_next_big = 0;
-  __syncthreads();
-  for (uint32_t k = 0; k < per; ++k) {
-    const uint32_t q = q0 + k;
-    if (q >= nparts) continue;
-    const uint32_t at = p.part_totals[q] > big_rows ? atomicAdd(&s_next_big, 1u) : atomicAdd(&s_small, 1u);
+    bb = __shfl_sync(0xffffffffu, bb, 0);
+    bs = __shfl_sync(0xffffffffu, bs, 0);
+    if (!valid) continue;
+    const uint32_t at = big ? bb + (uint32_t)__popc(mb & below) : bs + (uint32_t)__popc(ms & below);
     if (at < nparts) p.part_order[at] = q;
     else part_check(p, CHK_PART);
   }
